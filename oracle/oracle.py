@@ -1,0 +1,178 @@
+"""CPU oracle for the MotionVersion::V1 path: Python face of oracle/fg_oracle.c (a plain-C restatement of
+frame-gen-ritz's proto/interp.py and the OpenCV 4.13 / numpy primitives it calls).
+
+TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it as the checker.
+The product path never imports it.
+
+Frames are numpy uint8 arrays (H, W, 4) in R,G,B,A order ("rgba"), (H, W, 4) B,G,R,A ("bgra"), or (H, W, 3) in
+interp.py's own B,G,R order ("bgr"). Outputs keep the input's layout; alpha is the nearer real frame's.
+"""
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libfg_oracle.so")
+ORDERS = {"rgba": 0, "bgra": 1, "bgr": 2}
+REASONS = {0: None, 1: "cut", 2: "untrusted"}
+
+
+@dataclass
+class Settings:
+    """The V1 fields of framegen::Settings (gpu/framegen.h:167-409) with their defaults, which are the tuned
+    constants of proto/interp.py:43-61."""
+    trustLow: float = 12.0
+    trustHigh: float = 40.0
+    globalFallback: float = 0.15
+    sceneCutSad: float = 30.0
+    hudBonus: float = 1.0
+    smoothBonus: float = 0.5
+    searchPenalty: float = 0.5
+    searchRadius: int = 2
+    searchRadiusTop: int = 6
+    subpixel: bool = True
+    flowScale: int = 2
+    pyramidMinSide: int = 48
+
+
+class _CSettings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("trustLow", "trustHigh", "globalFallback", "sceneCutSad", "hudBonus",
+                                              "smoothBonus", "searchPenalty")] + \
+               [(n, ctypes.c_int) for n in ("searchRadius", "searchRadiusTop", "subpixel", "flowScale", "pyramidMinSide")]
+
+
+def _cs(s):
+    s = s or Settings()
+    return _CSettings(*[getattr(s, n) for n, _ in _CSettings._fields_])
+
+
+def build():
+    """Compile the oracle library (gcc + OpenMP) in place."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        P = ctypes.c_void_p
+        L.fgo_layout.argtypes = [ctypes.c_int] * 4 + [P] * 4 + [ctypes.c_int]
+        L.fgo_layout.restype = ctypes.c_int
+        L.fgo_estimate.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CSettings),
+                                   P, P, P, P, P, P, P, P, ctypes.c_int]
+        L.fgo_estimate.restype = ctypes.c_int
+        L.fgo_synth.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CSettings),
+                                P, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, P, P, P, P, ctypes.c_int]
+        L.fgo_synth.restype = ctypes.c_int
+        L.fgo_mean_f32.argtypes = [P, ctypes.c_long]
+        L.fgo_mean_f32.restype = ctypes.c_float
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class Layout:
+    W: int
+    H: int
+    fw: int
+    fh: int
+    levels: list = field(default_factory=list)   # (w, h, bw, bh) per level, finest first
+
+
+def layout(W, H, flow_scale=2, min_side=48):
+    fw, fh = ctypes.c_int(), ctypes.c_int()
+    lw, lh = (ctypes.c_int * 16)(), (ctypes.c_int * 16)()
+    n = lib().fgo_layout(W, H, flow_scale, min_side, ctypes.byref(fw), ctypes.byref(fh), lw, lh, 16)
+    if n < 1:
+        raise ValueError("bad size")
+    return Layout(W, H, fw.value, fh.value, [(lw[i], lh[i], (lw[i] + 7) // 8, (lh[i] + 7) // 8) for i in range(n)])
+
+
+def _frame_args(a, order):
+    if a.dtype != np.uint8 or a.ndim != 3 or a.shape[2] != (3 if order == "bgr" else 4):
+        raise ValueError("frame must be uint8 (H, W, %d)" % (3 if order == "bgr" else 4))
+    a = np.ascontiguousarray(a)
+    return a, a.shape[1], a.shape[0], a.strides[0]
+
+
+def estimate(a, c, settings=None, order="rgba", trace=True, threads=0):
+    """interp.estimate(a, c) plus every intermediate: returns a dict with sad (the float32 mean as a Python float),
+    cut (bool), pf (fh, fw, 2) and, with trace, luma/fields/seeds/meds/sads per level."""
+    s = settings or Settings()
+    a, W, H, pitch = _frame_args(a, order)
+    c, _, _, _ = _frame_args(c, order)
+    L = layout(W, H, s.flowScale, s.pyramidMinSide)
+    nl = sum(2 * w * h for w, h, _, _ in L.levels)
+    nf = sum(4 * bw * bh for _, _, bw, bh in L.levels) + 4 * L.levels[0][2] * L.levels[0][3]
+    ns = sum(2 * bw * bh for _, _, bw, bh in L.levels)
+    luma = np.zeros(nl, np.float32) if trace else None
+    fields = np.zeros(nf, np.float32) if trace else None
+    seeds = np.zeros(ns, np.float32) if trace else None
+    meds = np.zeros(2 * len(L.levels), np.float32) if trace else None
+    nb0 = L.levels[0][2] * L.levels[0][3]
+    sads = np.zeros(nb0, np.float32)
+    pf = np.zeros((L.fh, L.fw, 2), np.float32)
+    mean, cut = ctypes.c_float(), ctypes.c_int()
+    n = lib().fgo_estimate(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), _p(luma), _p(fields),
+                           _p(seeds), _p(meds), _p(sads), _p(pf), ctypes.byref(mean), ctypes.byref(cut), threads)
+    if n != len(L.levels):
+        raise RuntimeError("fgo_estimate failed")
+    est = {"sad": float(mean.value), "cut": bool(cut.value), "pf": pf, "layout": L,
+           "sads": sads.reshape(L.levels[0][3], L.levels[0][2])}
+    if trace:
+        lum, fl, sd = [], [], []
+        o = of = os_ = 0
+        for w, h, bw, bh in L.levels:
+            lum.append((luma[o:o + w * h].reshape(h, w), luma[o + w * h:o + 2 * w * h].reshape(h, w)))
+            o += 2 * w * h
+            fl.append((fields[of:of + 2 * bw * bh].reshape(bh, bw, 2), fields[of + 2 * bw * bh:of + 4 * bw * bh].reshape(bh, bw, 2)))
+            of += 4 * bw * bh
+            sd.append(seeds[os_:os_ + 2 * bw * bh].reshape(bh, bw, 2))
+            os_ += 2 * bw * bh
+        bw0, bh0 = L.levels[0][2], L.levels[0][3]
+        est["luma"] = lum
+        est["fields"] = fl
+        est["seeds"] = sd
+        est["meds"] = meds.reshape(-1, 2)
+        est["sub"] = [fields[of:of + 2 * bw0 * bh0].reshape(bh0, bw0, 2), fields[of + 2 * bw0 * bh0:].reshape(bh0, bw0, 2)]
+        est["v"] = est["sub"][1] if s.subpixel else fl[0][1]
+    return est
+
+
+def synth(a, c, est, t, settings=None, order="rgba", trace=False, threads=0):
+    """interp.synth(a, c, est, t, why=True): returns (frame, reason) or, with trace, a dict that adds field_t,
+    e (the per-pixel mismatch before the 7x7 box) and untrusted (pixels whose trust is past 0.5)."""
+    s = settings or Settings()
+    a, W, H, pitch = _frame_args(a, order)
+    c, _, _, _ = _frame_args(c, order)
+    out = np.zeros_like(a)
+    L = est["layout"]
+    pf = np.ascontiguousarray(est["pf"], np.float32)
+    ft = np.zeros((L.fh, L.fw, 2), np.float32) if trace else None
+    e = np.zeros((H, W), np.uint8) if trace else None
+    unt, reason = ctypes.c_longlong(), ctypes.c_int()
+    r = lib().fgo_synth(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), _p(pf), int(est["cut"]),
+                        float(t), _p(out), out.strides[0], _p(ft), _p(e), ctypes.byref(unt), ctypes.byref(reason), threads)
+    if r != 0:
+        raise ValueError("fgo_synth failed (t outside (0, 1)?)")
+    if trace:
+        return {"out": out, "reason": REASONS[reason.value], "field_t": ft, "e": e, "untrusted": int(unt.value)}
+    return out, REASONS[reason.value]
+
+
+def mean_f32(a):
+    """numpy's float32 mean (pairwise) as restated in the oracle."""
+    a = np.ascontiguousarray(a, np.float32).reshape(-1)
+    return float(lib().fgo_mean_f32(_p(a), a.size))
