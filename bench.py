@@ -1,0 +1,349 @@
+#!/usr/bin/env python3
+"""Benchmark of the V1 path: 4K ms per real pair (estimate + 3 synths at t = 1/4, 1/2, 3/4), 3840x2160 Rgba8.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one real pair: recordEstimate + 3 recordSynth. `value` is device time with the inputs resident in HBM:
+each step's pair comes from a pool of distinct pairs larger than L2 (so no step reads a cached pair), and each
+pool slot's step is a CUDA graph of the library's own launches; `value` = max-over-ranks time / pairs of all ranks.
+`e2e` is the same metric through the public API with host buffers: every step copies its pair host -> device from
+pinned memory, records the estimate and 3 synths, and copies the 3 frames back.
+`roofline` is the dominant kernel (the fused synth) against the measured HBM copy bandwidth, its duration from the
+library's own per-pass CUDA events. `cpu_baseline` is the oracle (a plain-C restatement of proto/interp.py) on this
+host's cores. --impl reference times that CPU implementation itself (rank 0 only).
+Multi-GPU: every rank runs its own pairs (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(REPO, "frame-gen-ritz_b200"), os.path.join(REPO, "oracle")):
+    sys.path.insert(0, _p)
+
+METRIC = "4K ms per real pair (estimate+3 synths), CNN-seeded vs plain, PSNR within 0.1 dB"
+W4K, H4K = 3840, 2160
+TS = (0.25, 0.5, 0.75)
+FW, FH = W4K // 2, H4K // 2
+# algorithmic bytes of one fused synth launch: both frames read, the per-pixel field read, the output written
+SYNTH_BYTES = 2 * 4 * W4K * H4K + 8 * FW * FH + 4 * W4K * H4K
+PAIR_BYTES = 2 * 4 * W4K * H4K + 8 * FW * FH + 3 * SYNTH_BYTES     # (A): 431,308,800 B per pair
+CPU_CROP = (960, 540)   # the CPU sample: 1/16 of the 4K area
+
+
+def args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--pool", type=int, default=8, help="distinct 4K pairs cycled through (8 x 66 MB > L2)")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_pair():
+    import workloads
+    p, c, _ = workloads.flow_pair(W4K, H4K, seed=4 * 10 ** 6)
+    return p, c
+
+
+def cpu_sample(p, c, seconds, threads=0):
+    """The oracle on 960x540 crops of the 4K pair (estimate + 3 synths each), repeated for about `seconds`; returns
+    (ms per 4K pair, crops timed). Time scales with area: x16."""
+    import oracle
+    cw, ch = CPU_CROP
+    times = []
+    t_end = time.perf_counter() + seconds
+    k = 0
+    while True:
+        y0, x0 = (k * 540) % (H4K - ch + 1), (k * 960) % (W4K - cw + 1)
+        a, cc = np.ascontiguousarray(p[y0:y0 + ch, x0:x0 + cw]), np.ascontiguousarray(c[y0:y0 + ch, x0:x0 + cw])
+        t0 = time.perf_counter()
+        est = oracle.estimate(a, cc, trace=False, threads=threads)
+        for t in TS:
+            oracle.synth(a, cc, est, t, threads=threads)
+        times.append(time.perf_counter() - t0)
+        k += 1
+        if time.perf_counter() > t_end and k >= 2:
+            break
+    return statistics.median(times) * 1e3 * (W4K * H4K) / (cw * ch), k
+
+
+def clock_sampler(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    idx = str(local_rank)
+    if vis:
+        parts = [v.strip() for v in vis.split(",")]
+        if local_rank < len(parts):
+            idx = parts[local_rank]
+    q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", "-i", idx, f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return None
+
+
+def clock_summary(proc):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        out, _ = proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        out, _ = proc.communicate()
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.strip().splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 8:
+            continue
+        try:
+            sm.append(float(f[0]))
+            mx.append(float(f[1]))
+        except ValueError:
+            continue
+        for n, v in zip(names, f[4:8]):
+            if v.lower().startswith("active"):
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per synth launch from the committed ncu summary (profiles/synth_4k.json), if present."""
+    try:
+        with open(os.path.join(REPO, "profiles", "synth_4k.json")) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(a):
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    p, c = workload_pair()
+    cores = os.cpu_count()
+    cw, ch = CPU_CROP
+    scale = (W4K * H4K) / (cw * ch)
+    import oracle
+    step_ms = []
+    for i in range(a.warmup + a.steps):
+        y0, x0 = (i * 540) % (H4K - ch + 1), (i * 960) % (W4K - cw + 1)
+        pa, pc = np.ascontiguousarray(p[y0:y0 + ch, x0:x0 + cw]), np.ascontiguousarray(c[y0:y0 + ch, x0:x0 + cw])
+        t0 = time.perf_counter()
+        est = oracle.estimate(pa, pc, trace=False)
+        for t in TS:
+            oracle.synth(pa, pc, est, t)
+        if i >= a.warmup:
+            step_ms.append((time.perf_counter() - t0) * 1e3 * scale)
+    v = statistics.median(step_ms)
+    sample = f"{cw}x{ch} crops of the 4K pair (1/16 area), estimate + 3 synths per step, time x16; oracle, {cores} threads"
+    print(json.dumps({"metric": METRIC, "value": round(v, 3), "unit": "ms", "impl": "reference", "n_gpus": a.gpus,
+                      "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                      "config": {"workload": "V1 plain, 3840x2160 Rgba8, 4x (estimate + 3 synths), flowScale 2",
+                                 "cpu_impl": "oracle port (plain C, OpenMP) of proto/interp.py"},
+                      "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
+                      "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
+def main():
+    a = args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference(a)
+    import torch
+    import torch.distributed as dist
+    import datetime
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    import framegen as fg
+
+    p_np, c_np = workload_pair()
+    base_a = torch.from_numpy(p_np).cuda()
+    base_c = torch.from_numpy(c_np).cuda()
+    # pool of distinct pairs: the same content rolled (both frames alike, so the motion is unchanged)
+    pool = []
+    for k in range(a.pool):
+        sh = (k * 97 + rank * 13) % W4K, (k * 53 + rank * 7) % H4K
+        pool.append((torch.roll(base_a, shifts=(sh[1], sh[0]), dims=(0, 1)).contiguous(),
+                     torch.roll(base_c, shifts=(sh[1], sh[0]), dims=(0, 1)).contiguous()))
+    outs = [[torch.empty_like(base_a) for _ in TS] for _ in range(a.pool)]
+    I = fg.Interpolator()
+    assert I.init(W4K, H4K, fg.VK_R8G8B8A8_UNORM, device=local), I.init_error()
+    stream = torch.cuda.Stream()
+
+    # correctness guard: the graph path gives the eager bytes
+    with torch.cuda.stream(stream):
+        I.begin_frame()
+        assert I.record_estimate(pool[0][0], pool[0][1], stream=stream)
+        for o, t in zip(outs[0], TS):
+            assert I.record_synth(pool[0][0], pool[0][1], o, t, stream=stream)
+    torch.cuda.synchronize()
+    eager0 = [o.clone() for o in outs[0]]
+
+    graphs = []
+    for k in range(a.pool):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            I.begin_frame()
+            assert I.record_estimate(pool[k][0], pool[k][1], stream=stream)
+            for o, t in zip(outs[k], TS):
+                assert I.record_synth(pool[k][0], pool[k][1], o, t, stream=stream)
+        graphs.append(g)
+    n_levels = I.trace_layout().nLevels
+    launches_per_step = 1 + max(0, n_levels - 6) + 2 * n_levels + 2 + 2 * len(TS)
+
+    with torch.cuda.stream(stream):
+        for i in range(max(a.warmup, 3)):
+            graphs[i % a.pool].replay()
+    torch.cuda.synchronize()
+    for o, e in zip(outs[0], eager0):
+        assert torch.equal(o, e), "graph replay differs from the eager record"
+
+    # ---- timed region: K steps, device time, max over ranks
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = clock_sampler(local)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for i in range(a.steps):
+            graphs[i % a.pool].replay()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = clock_summary(clk)
+    t_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    ms_per_step = t_ms / a.steps
+    value = t_ms / (a.steps * world)
+
+    # ---- per-pass device times (the library's CUDA events on its stream; the launches queue behind a sleep so the
+    # events see back-to-back execution, not host gaps)
+    I.set_profiling(True)
+    groups = {}
+    for rep in range(5):
+        k = rep % a.pool
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(5_000_000)
+            I.begin_frame()
+            I.record_estimate(pool[k][0], pool[k][1], stream=stream)
+            for o, t in zip(outs[k], TS):
+                I.record_synth(pool[k][0], pool[k][1], o, t, stream=stream)
+        tm = I.read_timings()
+        for name, ns in tm:
+            groups.setdefault(name, []).append(ns / 1e3)
+    I.set_profiling(False)
+    synth_us = statistics.median(groups["synth"])
+    breakdown = {n: round(statistics.median(v) * (3 if n in ("synth", "fallback") else 1), 2) for n, v in groups.items()}
+
+    # ---- e2e through the public API with host buffers
+    pin_a = p_np.copy()
+    ha = torch.from_numpy(p_np).pin_memory()
+    hc = torch.from_numpy(c_np).pin_memory()
+    hout = [torch.empty(base_a.shape, dtype=torch.uint8).pin_memory() for _ in TS]
+    da, dc = torch.empty_like(base_a), torch.empty_like(base_c)
+    douts = [torch.empty_like(base_a) for _ in TS]
+
+    def e2e_step():
+        da.copy_(ha, non_blocking=True)
+        dc.copy_(hc, non_blocking=True)
+        I.begin_frame()
+        assert I.record_estimate(da, dc, stream=stream)
+        for o, h, t in zip(douts, hout, TS):
+            assert I.record_synth(da, dc, o, t, stream=stream)
+            h.copy_(o, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = e2e_ms / (a.e2e_steps * world)
+    del pin_a
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        v, n = cpu_sample(p_np, c_np, a.cpu_seconds)
+        cpu = {"value": round(v, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n} 960x540 crops of the 4K pair (1/16 area each), estimate + 3 synths, median x16; "
+                         f"oracle (plain-C restatement of proto/interp.py, OpenMP)"}
+
+    peak, peak_kind = measured_peak()
+    achieved = SYNTH_BYTES / (synth_us * 1e-6) / 1e9
+    traffic = ncu_traffic()
+    del graphs
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                "config": {"workload": "V1 plain, 3840x2160 Rgba8, 4x (estimate + synths at t=1/4, 1/2, 3/4), "
+                                       "flowScale 2, radii 6/2, subpixel on",
+                           "pairs_in_pool": a.pool, "l2": f"inputs larger than L2: {a.pool} distinct pairs "
+                                                         f"({a.pool * 2 * 4 * W4K * H4K / 1e6:.0f} MB) cycled",
+                           "parallelism": f"dp{world} (independent pairs per GPU)",
+                           "algorithmic_bytes_per_pair": PAIR_BYTES},
+                "hbm_gbs_per_pair": round(PAIR_BYTES / (value * 1e-3) / 1e9 / world, 1),
+                "roofline": {"bound": "hbm", "kernel": "k_synth", "achieved": round(achieved, 1),
+                             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                             "traffic": traffic, "algorithmic_bytes": SYNTH_BYTES, "duration_us": round(synth_us, 2)},
+                "breakdown_us": breakdown,
+                "gpu_launches": launches_per_step * a.steps,
+                "e2e": {"value": round(e2e_value, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 4 * W4K * H4K,
+                        "d2h_bytes_per_step": len(TS) * 4 * W4K * H4K},
+                "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    I.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,146 @@
+// Kernel parameter blocks and launch entry points of the V1 path (host <-> device contract inside the library).
+// Every kernel takes one of these by value; the host (framegen.cpp) fills them from the size layout and Settings.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fgk {
+
+constexpr int kBlock = 8;          // block size at every pyramid level (proto/interp.py:43 BLOCK)
+constexpr int kMaxLevels = 16;
+constexpr int kPyrInKernel = 6;    // levels 0..5 come out of the luma kernel (a 32x32 tile of level 0 -> 1x1 of level 5)
+constexpr int kMaxRadius = 12;     // Settings::searchRadius / searchRadiusTop upper bound (gpu/framegen.cpp validate)
+
+// Device-side counters and small results of one estimate / synth (one allocation, zeroed at init).
+struct DevState {
+    unsigned int untrusted[2];         // per synth parity: pixels whose trust ramp is past 0.5 (interp.py:238)
+    unsigned int sadSum256;            // finest-level sum of roundEven(block SAD * 256) (debug counters)
+    unsigned int cut;                  // scene-cut decision of the latest estimate (interp.py:190)
+    float sadMean;                     // the float32 mean block SAD the cut test compares (interp.py:164)
+    unsigned int medDone[kMaxLevels];  // last-block tickets of the median histograms
+    unsigned int subDone;              // last-block ticket of the sub-pixel pass (scene-cut mean)
+    float med[kMaxLevels][2];          // per fine level: 2 x the global median of the own-parent vectors (interp.py:142)
+    unsigned int err;                  // sticky error bits (bound checks that could only fail on a library bug)
+};
+
+enum : unsigned int { kErrHistRange = 1u, kErrPlan = 2u };
+
+struct LumaPyrParams {
+    const uint8_t* a;
+    const uint8_t* c;
+    size_t pitch;          // bytes per row of both frames
+    int W, H, fs;          // frame size, flow scale (1, 2, 4)
+    int ri, gi, bi;        // byte offsets of R, G, B in a 4-byte pixel
+    int nlev;              // levels written here (<= kPyrInKernel)
+    int lw[kPyrInKernel], lh[kPyrInKernel];
+    float* la[kPyrInKernel];
+    float* lc[kPyrInKernel];
+};
+
+struct DownParams {         // one further pyramid level (INTER_AREA 0.5)
+    const float* sa; const float* sc; int sw, sh;
+    float* da; float* dc; int dw, dh;
+};
+
+struct SearchParams {
+    const float* la; const float* lc;
+    int w, h, bw, bh;
+    int top;                   // coarsest level: the seed is zero
+    const float2* parent;      // the parent level's median-filtered field (pw x ph)
+    int pw, ph;
+    const float* med;          // 2 floats: the seed candidate "global median" (already 2x)
+    int R;
+    float lambda;              // fl32(searchPenalty): the seed stage's penalty (interp.py:143)
+    float pen[2 * kMaxRadius + 1];   // fl32(lambda * n), n = |dx| + |dy| (interp.py:121)
+    float2* out;
+    float* sadOut;             // optional: the winner's SAD (finest level when sub-pixel refinement is off)
+};
+
+struct Median3Params {
+    const float2* in; float2* out; int bw, bh;
+    // histogram of the own-parent vectors of the next finer level (fine grid fbw x fbh), 0 = none
+    int doHist, fbw, fbh, B;   // bins [-B, B] per axis
+    unsigned int* hist;        // 2 * (2B + 1) bins, zero on entry, zeroed again by the last block
+    unsigned int* done;
+    float* medOut;             // 2 floats
+    unsigned int* err;
+};
+
+struct CutPlan {               // numpy's pairwise float32 summation tree of N elements (built on the host)
+    const int2* leaves;        // (start, len) per leaf, in node-slot order 0..nLeaves-1
+    const int2* inner;         // (left slot, right slot) per inner node, deepest depth first
+    const int* depthStart;     // inner[depthStart[d] .. depthStart[d + 1]) are computed in step d
+    int nLeaves, nInner, nSteps, root;
+    float* gvals;              // nLeaves + nInner floats of global scratch, used when they exceed kPlanSmemMax
+};
+constexpr size_t kPlanSmemMax = 96 * 1024;   // node values kept in shared memory up to this size
+
+struct SubpixParams {
+    const float* la; const float* lc;
+    int w, h, bw, bh;
+    const float2* in; float2* out; float* sads;
+    float2* out0;              // optional: the vectors after the 0.5 px step
+    float pen[2][3];           // fl32(lambda * step * n), step 0.5 / 0.25, n = 0..2
+    // scene-cut mean in the last block
+    CutPlan plan;
+    float cutSad;
+    DevState* st;
+};
+
+struct CutMeanParams {         // the same scene-cut reduction as a separate pass (sub-pixel refinement off)
+    const float* sads; int n;
+    CutPlan plan;
+    float cutSad;
+    DevState* st;
+};
+
+struct PixfieldParams {
+    const float* ya; const float* yc; int w, h;
+    const float2* v; int bw, bh;   // the finest block field
+    float smooth, zero;            // bonuses (interp.py:181-182)
+    float2* pf;
+};
+
+struct SynthParams {
+    const uint8_t* a; const uint8_t* c; size_t pitch;
+    uint8_t* out; size_t outPitch;
+    int W, H, fs, fw, fh;
+    int ri, gi, bi;
+    const float2* pf;
+    int lookup;                    // t != 0.5: the field at t by 2 fixed-point steps (interp.py:194-205)
+    int mid;                       // t == 0.5: blend 0.5 * (wa + wc)
+    int nearC;                     // t > 0.5: the nearer frame is curr
+    float s, ka, kc, wA, wC;       // fl32(2t - 1), fl32(2t), fl32(2(1 - t)), fl32(1 - t), fl32(t)
+    float trust0, trustSpan;       // trustLow, fl32(trustHigh - trustLow)
+    int sZero, sOne;               // 7x7 sums S <= sZero give u = 0, S >= sOne give u = 1 (host-derived shortcuts)
+    DevState* st;
+    unsigned int* untrusted;       // this synth's counter (zero on entry)
+    uint8_t* emap;                 // optional: per-pixel mismatch before the box (debug maps), W bytes per row
+};
+
+struct FallbackParams {
+    const uint8_t* a; const uint8_t* c; size_t pitch;
+    uint8_t* out; size_t outPitch;
+    int W, H, nearC;
+    double frac;                   // globalFallback
+    const unsigned int* untrusted;
+    unsigned int* untrustedNext;   // the next synth's counter, zeroed here
+};
+
+// once per process and device: the dynamic shared-memory limits of the kernels that need more than 48 KB
+cudaError_t prepareKernels();
+size_t synthSmemBytes(int fs);
+
+// launchers (fg_kernels.cu); each returns the launch's cudaError_t
+cudaError_t launchLumaPyr(const LumaPyrParams& p, cudaStream_t s);
+cudaError_t launchDown(const DownParams& p, cudaStream_t s);
+cudaError_t launchSearch(const SearchParams& p, cudaStream_t s);
+cudaError_t launchMedian3(const Median3Params& p, cudaStream_t s);
+cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s);
+cudaError_t launchCutMean(const CutMeanParams& p, cudaStream_t s);
+cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s);
+cudaError_t launchSynth(const SynthParams& p, cudaStream_t s);
+cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s);
+
+}  // namespace fgk

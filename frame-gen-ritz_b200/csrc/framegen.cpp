@@ -1,0 +1,815 @@
+// Host side of the B200 framegen library: framegen::Interpolator (include/framegen.h) and the C ABI
+// (include/framegen_c.h). It owns the device buffers of one frame size, turns Settings into kernel parameters and
+// records the V1 passes as kernel launches on the caller's stream (fg_kernels.cu). Nothing here allocates, copies
+// to the host or synchronises while recording.
+//
+// The control flow mirrors gpu/framegen.cpp: sizeLayout :658-685, validate :1679-1700, settingsError :1702-1711,
+// setSettings / reconfigure :1723-1760, recordEstimate :2866-2940 + :3090-3154, recordSynth :3467-3532, record :3636.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fg_params.h"
+#include "framegen.h"
+#include "framegen_c.h"
+
+namespace framegen {
+
+namespace {
+
+int rintHalfEven(double v) { return (int)std::nearbyint(v); }   // == cv2 saturate_cast<int>(double)
+
+struct Level {
+    int w = 0, h = 0, bw = 0, bh = 0;
+    size_t lumaA = 0, lumaC = 0;   // float offsets into the luma buffer
+    size_t fS = 0, fM = 0;         // float2 offsets into the field buffer: search output, median3 output
+};
+
+// gpu/framegen.cpp:658-685 (interp.flow / interp.pyramid sizes). The luma and field buffers are laid out level by
+// level, finest first: luma a | c; field search | median3; then the two sub-pixel steps.
+struct SizeLayout {
+    int fw = 0, fh = 0;
+    std::vector<Level> lv;
+    size_t lumaFloats = 0, fieldF2 = 0, sub0 = 0, sub1 = 0;
+};
+
+SizeLayout sizeLayout(uint32_t W, uint32_t H, uint32_t flowScale, uint32_t minSide) {
+    SizeLayout L;
+    L.fw = rintHalfEven(W * (1.0 / flowScale));
+    L.fh = rintHalfEven(H * (1.0 / flowScale));
+    int w = L.fw, h = L.fh;
+    size_t lo = 0, fo = 0;
+    for (;;) {
+        Level l;
+        l.w = w; l.h = h;
+        l.bw = (w + 7) / 8; l.bh = (h + 7) / 8;   // pad_to_block
+        l.lumaA = lo; l.lumaC = lo + (size_t)w * h;
+        lo += 2 * (size_t)w * h;
+        l.fS = fo; l.fM = fo + (size_t)l.bw * l.bh;
+        fo += 2 * (size_t)l.bw * l.bh;
+        L.lv.push_back(l);
+        if ((uint32_t)(std::min(w, h) / 2) < minSide || L.lv.size() >= (size_t)fgk::kMaxLevels) break;
+        w = rintHalfEven(w * 0.5);
+        h = rintHalfEven(h * 0.5);
+    }
+    L.sub0 = fo;
+    fo += (size_t)L.lv[0].bw * L.lv[0].bh;
+    L.sub1 = fo;
+    fo += (size_t)L.lv[0].bw * L.lv[0].bh;
+    L.lumaFloats = lo;
+    L.fieldF2 = fo;
+    return L;
+}
+
+// gpu/framegen.cpp:430-433: the longest integer half-vector the search can reach at level j of an n-level pyramid
+int64_t reachBound(int n, int j, int R, int Rt) {
+    const int64_t a = (int64_t)1 << (n - 1 - j);
+    return Rt * a + (int64_t)R * (a - 1);
+}
+
+// numpy's pairwise summation tree over N elements (leaves of <= 128 elements, splits at n/2 rounded down to a
+// multiple of 8), with the inner nodes ordered by height so each height is one parallel step.
+struct CutPlanHost {
+    std::vector<int2> leaves, inner;
+    std::vector<int> depthStart;
+    int root = 0, nSteps = 0;
+};
+CutPlanHost buildCutPlan(int N) {
+    struct TNode { bool leaf; int idx, height; };
+    std::vector<int2> leaves;
+    std::vector<std::array<TNode, 2>> kids;
+    std::vector<int> heights;
+    std::vector<std::array<int, 3>> stack;   // explicit recursion: (start, n, state)
+    // recursive lambda (depth <= log2(N / 64) + 1)
+    struct B {
+        std::vector<int2>& leaves;
+        std::vector<std::array<TNode, 2>>& kids;
+        std::vector<int>& heights;
+        TNode go(int start, int n) {
+            if (n <= 128) {
+                leaves.push_back(make_int2(start, n));
+                return {true, (int)leaves.size() - 1, 0};
+            }
+            int n2 = n / 2;
+            n2 -= n2 % 8;
+            TNode l = go(start, n2), r = go(start + n2, n - n2);
+            kids.push_back({l, r});
+            heights.push_back(1 + std::max(l.height, r.height));
+            return {false, (int)kids.size() - 1, heights.back()};
+        }
+    } b{leaves, kids, heights};
+    TNode root = b.go(0, N);
+    CutPlanHost P;
+    P.leaves = leaves;
+    const int nL = (int)leaves.size(), nI = (int)kids.size();
+    std::vector<int> order(nI);
+    for (int i = 0; i < nI; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return heights[x] < heights[y]; });
+    std::vector<int> slot(nI);
+    for (int r = 0; r < nI; r++) slot[order[r]] = nL + r;
+    auto slotOf = [&](const TNode& t) { return t.leaf ? t.idx : slot[t.idx]; };
+    int maxH = 0;
+    for (int r = 0; r < nI; r++) {
+        const auto& k = kids[order[r]];
+        P.inner.push_back(make_int2(slotOf(k[0]), slotOf(k[1])));
+        maxH = std::max(maxH, heights[order[r]]);
+    }
+    P.nSteps = maxH;
+    P.depthStart.assign(maxH + 1, nI);
+    for (int h = maxH; h >= 1; h--)
+        for (int r = nI - 1; r >= 0; r--)
+            if (heights[order[r]] == h) P.depthStart[h - 1] = r;
+    P.depthStart[maxH] = nI;
+    for (int h = maxH - 1; h >= 0; h--) P.depthStart[h] = std::min(P.depthStart[h], P.depthStart[h + 1]);
+    P.root = slotOf(root);
+    (void)stack;
+    return P;
+}
+
+size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+const char* kErrSettings = "invalid settings: a field is out of range or not finite (see Interpolator::validate)";
+const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
+const char* kErrUi = "static-UI protection is not built into this library (Settings::uiProtection must be Off)";
+const char* kErrNoFormat = "unsupported viewFormat (see framegen::Format)";
+const char* kErrFormatNotBuilt = "the kernels of this format are not built into the library";
+const char* kErrNits = "linearWhiteNits must be in (0, 10000]";
+const char* kErrMinSize = "the frame size is below Interpolator::kMinSize (16 pixels) in width or height";
+const char* kErrMaxSize = "the frame size exceeds 2^30 pixels (32-bit indexing of the library's buffers)";
+const char* kErrDevice = "CUDA device not available";
+const char* kErrAlloc = "CUDA device memory allocation failed";
+
+struct DeviceGuard {   // makes `dev` current for the scope, restores the caller's device after
+    int old = -1;
+    bool changed = false;
+    explicit DeviceGuard(int dev) {
+        if (dev >= 0 && cudaGetDevice(&old) == cudaSuccess && old != dev) changed = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (changed) cudaSetDevice(old);
+    }
+};
+
+}  // namespace
+
+bool formatOf(uint32_t vf, Format* out) {
+    Format f;
+    switch (vf) {
+        case kVkFormatR8G8B8A8Unorm:
+        case kVkFormatB8G8R8A8Unorm: f = Format::Rgba8; break;
+        case kVkFormatA2R10G10B10UnormPack32:
+        case kVkFormatA2B10G10R10UnormPack32: f = Format::Rgb10; break;
+        case kVkFormatR16G16B16A16Sfloat: f = Format::RgbaF16; break;
+        case kVkFormatR8Unorm: f = Format::Nv12; break;
+        case kVkFormatR16Unorm: f = Format::P010; break;
+        default: return false;
+    }
+    if (out) *out = f;
+    return true;
+}
+
+struct Interpolator::Impl {
+    int device = 0;
+    Format fmt = Format::Rgba8;
+    uint32_t viewFormat = kVkFormatB8G8R8A8Unorm;
+    int ri = 2, gi = 1, bi = 0;
+    InitInfo info{};
+    Settings set{};
+    uint32_t W = 0, H = 0;
+    SizeLayout L;
+    // device memory (one allocation)
+    char* arena = nullptr;
+    size_t arenaBytes = 0;
+    float* luma = nullptr;
+    float2* field = nullptr;
+    float* sads = nullptr;
+    float2* pf = nullptr;
+    unsigned int* hist = nullptr;
+    int histB = 0;
+    fgk::DevState* st = nullptr;
+    uint8_t* emap = nullptr;
+    fgk::CutPlan plan{};
+    // trust-ramp shortcuts of the current settings
+    int sZero = 0, sOne = 0;
+    // record state
+    bool haveEst = false;
+    const void* estPrev = nullptr;
+    const void* estCurr = nullptr;
+    uint32_t estSets = 0, synthSets = 0;
+    unsigned int parity = 0, lastParity = 0;
+    bool capture = false;
+    const char* lastErr = nullptr;
+    // profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> events;
+    std::vector<const char*> evNames;
+    size_t evCount = 0;
+
+    ~Impl() { freeAll(); }
+
+    void freeAll() {
+        DeviceGuard g(device);
+        if (arena) cudaFree(arena);
+        arena = nullptr;
+        arenaBytes = 0;
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        events.clear();
+        W = H = 0;
+        haveEst = false;
+    }
+
+    void updateTrust() {
+        // u(S) = clip((float(S / 49) - trustLow) / (trustHigh - trustLow), 0, 1) for 7x7 sums S = 0 .. 49 * 255 is
+        // monotone in S: S <= sZero gives 0, S >= sOne gives 1 (the kernel computes the ramp in between exactly).
+        const float t0 = set.trustLow, span = (float)((double)set.trustHigh - (double)set.trustLow);
+        auto u = [&](int S) {
+            const float eb = (float)((double)S * (1.0 / 49.0));
+            float v = (eb - t0) / span;
+            return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+        };
+        sZero = -1;
+        for (int S = 0; S <= 49 * 255 && u(S) == 0.0f; S++) sZero = S;
+        sOne = 49 * 255 + 1;
+        for (int S = 49 * 255; S >= 0 && u(S) == 1.0f; S--) sOne = S;
+    }
+
+    // buffers of one size (createSizeDependent, gpu/framegen.cpp:994-1014)
+    const char* allocSize(uint32_t w, uint32_t h) {
+        freeAll();
+        DeviceGuard g(device);
+        L = sizeLayout(w, h, set.flowScale, set.pyramidMinSide);
+        const int n = (int)L.lv.size();
+        // the median histograms hold any parent vector the largest radii (12, 12) can reach, so a runtime change
+        // of the radii (setSettings) never needs new buffers
+        const int64_t B = n > 1 ? reachBound(n, 1, 12, 12) : 0;
+        histB = (int)B;
+        const int nb0 = L.lv[0].bw * L.lv[0].bh;
+        CutPlanHost P = buildCutPlan(nb0);
+        size_t off = 0;
+        auto take = [&](size_t bytes) { size_t o = off; off = alignUp(off + bytes, 256); return o; };
+        const size_t oLuma = take(L.lumaFloats * 4), oField = take(L.fieldF2 * 8), oSads = take((size_t)nb0 * 4);
+        const size_t oPf = take((size_t)L.fw * L.fh * 8), oHist = take((size_t)2 * (2 * histB + 1) * 4);
+        const size_t oSt = take(sizeof(fgk::DevState)), oEmap = take((size_t)((w + 3) & ~3u) * h);
+        const size_t oLeaves = take(P.leaves.size() * 8), oInner = take(std::max<size_t>(P.inner.size(), 1) * 8);
+        const size_t oDepth = take(P.depthStart.size() * 4 + 4);
+        const size_t oVals = take((P.leaves.size() + P.inner.size()) * 4);
+        if (cudaMalloc(&arena, off) != cudaSuccess) { arena = nullptr; cudaGetLastError(); return kErrAlloc; }
+        arenaBytes = off;
+        cudaMemset(arena, 0, off);
+        luma = (float*)(arena + oLuma);
+        field = (float2*)(arena + oField);
+        sads = (float*)(arena + oSads);
+        pf = (float2*)(arena + oPf);
+        hist = (unsigned int*)(arena + oHist);
+        st = (fgk::DevState*)(arena + oSt);
+        emap = (uint8_t*)(arena + oEmap);
+        cudaMemcpy(arena + oLeaves, P.leaves.data(), P.leaves.size() * 8, cudaMemcpyHostToDevice);
+        if (!P.inner.empty()) cudaMemcpy(arena + oInner, P.inner.data(), P.inner.size() * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(arena + oDepth, P.depthStart.data(), P.depthStart.size() * 4, cudaMemcpyHostToDevice);
+        if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); freeAll(); return kErrAlloc; }
+        plan.leaves = (const int2*)(arena + oLeaves);
+        plan.inner = (const int2*)(arena + oInner);
+        plan.depthStart = (const int*)(arena + oDepth);
+        plan.nLeaves = (int)P.leaves.size();
+        plan.nInner = (int)P.inner.size();
+        plan.nSteps = P.nSteps;
+        plan.root = P.root;
+        plan.gvals = (float*)(arena + oVals);
+        W = w;
+        H = h;
+        haveEst = false;
+        return nullptr;
+    }
+
+    bool frameOk(const Frame& f) const {
+        return f.data && f.pitch >= (size_t)W * 4 && f.pitch % 4 == 0 && ((uintptr_t)f.data & 3) == 0;
+    }
+
+    // --- profiling (gpu/framegen.cpp Rec::stamp)
+    void stamp(cudaStream_t s, const char* name) {
+        if (!profiling) return;
+        if (evCount >= 64) return;
+        while (events.size() <= evCount) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return; }
+            events.push_back(e);
+        }
+        cudaEventRecord(events[evCount], s);
+        if (evNames.size() <= evCount) evNames.resize(evCount + 1);
+        evNames[evCount++] = name;
+    }
+
+    bool check(cudaError_t e) {
+        if (e != cudaSuccess) { lastErr = cudaGetErrorString(e); return false; }
+        return true;
+    }
+
+    bool estimate(cudaStream_t s, const Frame& prev, const Frame& curr) {
+        const int n = (int)L.lv.size();
+        const float lam = set.searchPenalty;
+        if (profiling) { evCount = 0; stamp(s, "start"); }
+        // 1-2. luma + pyramid
+        fgk::LumaPyrParams lp{};
+        lp.a = (const uint8_t*)prev.data; lp.c = (const uint8_t*)curr.data; lp.pitch = prev.pitch;
+        lp.W = (int)W; lp.H = (int)H; lp.fs = (int)set.flowScale;
+        lp.ri = ri; lp.gi = gi; lp.bi = bi;
+        lp.nlev = std::min(n, fgk::kPyrInKernel);
+        for (int l = 0; l < lp.nlev; l++) {
+            lp.lw[l] = L.lv[l].w; lp.lh[l] = L.lv[l].h;
+            lp.la[l] = luma + L.lv[l].lumaA; lp.lc[l] = luma + L.lv[l].lumaC;
+        }
+        if (prev.pitch != curr.pitch) return false;
+        if (!check(fgk::launchLumaPyr(lp, s))) return false;
+        stamp(s, "luma");
+        for (int l = fgk::kPyrInKernel; l < n; l++) {
+            fgk::DownParams dp{luma + L.lv[l - 1].lumaA, luma + L.lv[l - 1].lumaC, L.lv[l - 1].w, L.lv[l - 1].h,
+                               luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h};
+            if (!check(fgk::launchDown(dp, s))) return false;
+        }
+        stamp(s, "pyramid");
+        // 3-5. per level, coarse -> fine
+        static const char* names[] = {"level 0 (finest)", "level 1", "level 2", "level 3", "level 4", "level 5",
+                                      "level 6", "level 7"};
+        for (int i = n - 1; i >= 0; i--) {
+            const Level& l = L.lv[i];
+            fgk::SearchParams sp{};
+            sp.la = luma + l.lumaA; sp.lc = luma + l.lumaC;
+            sp.w = l.w; sp.h = l.h; sp.bw = l.bw; sp.bh = l.bh;
+            sp.top = i == n - 1;
+            sp.R = (int)(sp.top ? set.searchRadiusTop : set.searchRadius);
+            if (!sp.top) {
+                const Level& pl = L.lv[i + 1];
+                sp.parent = field + pl.fM; sp.pw = pl.bw; sp.ph = pl.bh;
+                sp.med = st->med[i];
+            }
+            sp.lambda = lam;
+            for (int k = 0; k <= 2 * sp.R; k++) sp.pen[k] = (float)((double)lam * 1.0 * (double)k);
+            sp.out = field + l.fS;
+            sp.sadOut = (i == 0 && !set.subpixel) ? sads : nullptr;
+            if (!check(fgk::launchSearch(sp, s))) return false;
+            fgk::Median3Params mp{};
+            mp.in = field + l.fS; mp.out = field + l.fM; mp.bw = l.bw; mp.bh = l.bh;
+            mp.doHist = i > 0;
+            if (i > 0) {
+                mp.fbw = L.lv[i - 1].bw; mp.fbh = L.lv[i - 1].bh; mp.B = histB;
+                mp.hist = hist; mp.done = &st->medDone[i]; mp.medOut = st->med[i - 1];
+            }
+            mp.err = &st->err;
+            if (!check(fgk::launchMedian3(mp, s))) return false;
+            stamp(s, names[std::min(i, 7)]);
+        }
+        // 6. sub-pixel refinement + the scene-cut mean
+        const Level& l0 = L.lv[0];
+        const float2* vfin = field + l0.fM;
+        if (set.subpixel) {
+            fgk::SubpixParams sp{};
+            sp.la = luma + l0.lumaA; sp.lc = luma + l0.lumaC;
+            sp.w = l0.w; sp.h = l0.h; sp.bw = l0.bw; sp.bh = l0.bh;
+            sp.in = field + l0.fM; sp.out = field + L.sub1; sp.out0 = field + L.sub0; sp.sads = sads;
+            const float steps[2] = {0.5f, 0.25f};
+            for (int p = 0; p < 2; p++)
+                for (int k = 0; k < 3; k++) sp.pen[p][k] = (float)((double)lam * (double)steps[p] * (double)k);
+            sp.plan = plan; sp.cutSad = set.sceneCutSad; sp.st = st;
+            if (!check(fgk::launchSubpix(sp, s))) return false;
+            vfin = field + L.sub1;
+        } else {
+            fgk::CutMeanParams cp{sads, l0.bw * l0.bh, plan, set.sceneCutSad, st};
+            if (!check(fgk::launchCutMean(cp, s))) return false;
+        }
+        stamp(s, "subpixel");
+        // 8. per-pixel vector choice
+        fgk::PixfieldParams pp{luma + l0.lumaA, luma + l0.lumaC, l0.w, l0.h, vfin, l0.bw, l0.bh, set.smoothBonus,
+                               set.hudBonus, pf};
+        if (!check(fgk::launchPixfield(pp, s))) return false;
+        stamp(s, "pixel field");
+        return true;
+    }
+
+    bool synth(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t) {
+        const double td = t;
+        fgk::SynthParams sp{};
+        sp.a = (const uint8_t*)prev.data; sp.c = (const uint8_t*)curr.data; sp.pitch = prev.pitch;
+        sp.out = (uint8_t*)out.data; sp.outPitch = out.pitch;
+        sp.W = (int)W; sp.H = (int)H; sp.fs = (int)set.flowScale; sp.fw = L.fw; sp.fh = L.fh;
+        sp.ri = ri; sp.gi = gi; sp.bi = bi;
+        sp.pf = pf;
+        sp.mid = t == 0.5f;
+        sp.s = (float)(2.0 * td - 1.0);
+        sp.lookup = sp.s != 0.0f;
+        sp.nearC = t > 0.5f;
+        sp.ka = (float)(2.0 * td);
+        sp.kc = (float)(2.0 * (1.0 - td));
+        sp.wA = (float)(1.0 - td);
+        sp.wC = t;
+        sp.trust0 = set.trustLow;
+        sp.trustSpan = (float)((double)set.trustHigh - (double)set.trustLow);
+        sp.sZero = sZero; sp.sOne = sOne;
+        sp.st = st;
+        sp.untrusted = &st->untrusted[parity];
+        sp.emap = capture ? emap : nullptr;
+        if (!check(fgk::launchSynth(sp, s))) return false;
+        stamp(s, "synth");
+        fgk::FallbackParams fp{};
+        fp.a = sp.a; fp.c = sp.c; fp.pitch = sp.pitch; fp.out = sp.out; fp.outPitch = sp.outPitch;
+        fp.W = sp.W; fp.H = sp.H; fp.nearC = sp.nearC;
+        fp.frac = (double)set.globalFallback;
+        fp.untrusted = &st->untrusted[parity];
+        fp.untrustedNext = &st->untrusted[parity ^ 1u];
+        if (!check(fgk::launchFallback(fp, s))) return false;
+        stamp(s, "fallback");
+        lastParity = parity;
+        parity ^= 1u;
+        return true;
+    }
+};
+
+Interpolator::~Interpolator() { destroy(); }
+
+bool Interpolator::validate(const Settings& s) {
+    auto in = [](float v, float lo, float hi) { return std::isfinite(v) && v >= lo && v <= hi; };
+    return in(s.trustLow, 0.0f, 255.0f) && in(s.trustHigh, 0.0f, 255.0f) && s.trustHigh - s.trustLow >= 1.0f &&
+           in(s.globalFallback, 0.0f, 1.0f) && s.globalFallback > 0.0f && in(s.sceneCutSad, 0.0f, 255.0f) &&
+           s.sceneCutSad > 0.0f && in(s.hudBonus, 0.0f, 255.0f) && in(s.smoothBonus, 0.0f, 255.0f) &&
+           in(s.searchPenalty, 0.0f, 255.0f) && s.searchRadius >= 1 && s.searchRadius <= 12 && s.searchRadiusTop >= 1 &&
+           s.searchRadiusTop <= 12 && (s.flowScale == 1 || s.flowScale == 2 || s.flowScale == 4) &&
+           s.pyramidMinSide >= 16 && s.pyramidMinSide <= 256 &&
+           (uint32_t)s.uiProtection <= (uint32_t)UiProtection::CrosshairV2 &&
+           (uint32_t)s.motionVersion <= (uint32_t)MotionVersion::V3 && s.blurSamples <= kBlurMaxSamples &&
+           (uint32_t)s.blurWeights <= (uint32_t)BlurWeights::Gaussian;
+}
+
+const char* Interpolator::settingsError(const Settings& s, Format f) {
+    if (!validate(s)) return kErrSettings;
+    if (s.motionVersion != MotionVersion::V1) return kErrVersion;
+    if (s.uiProtection != UiProtection::Off) return kErrUi;
+    (void)f;
+    return nullptr;
+}
+
+const char* Interpolator::settingsError(const Settings& s) const {
+    if (const char* e = settingsError(s, m ? m->fmt : Format::Rgba8)) return e;
+    return m && m->W ? sizeError(m->W, m->H) : nullptr;
+}
+
+const char* Interpolator::sizeError(uint32_t w, uint32_t h) const {
+    if (!m) return "not initialised";
+    if (w < kMinSize || h < kMinSize) return kErrMinSize;
+    if ((uint64_t)w * h > (1ull << 30)) return kErrMaxSize;
+    return nullptr;
+}
+
+bool Interpolator::init(const InitInfo& ii) {
+    destroy();
+    err_ = nullptr;
+    Format fmt;
+    if (!validate(ii.settings)) { err_ = "missing device, or invalid settings"; return false; }
+    if (!formatOf(ii.viewFormat, &fmt)) { err_ = kErrNoFormat; return false; }
+    if (fmt != Format::Rgba8) { err_ = kErrFormatNotBuilt; return false; }
+    if (const char* e = settingsError(ii.settings, fmt)) { err_ = e; return false; }
+    if (fmt == Format::RgbaF16 && ii.transfer == Transfer::Linear && !(ii.linearWhiteNits > 0.0f && ii.linearWhiteNits <= 10000.0f)) {
+        err_ = kErrNits;
+        return false;
+    }
+    if (ii.width < kMinSize || ii.height < kMinSize) { err_ = kErrMinSize; return false; }
+    if ((uint64_t)ii.width * ii.height > (1ull << 30)) { err_ = kErrMaxSize; return false; }
+    int dev = ii.device, ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); err_ = kErrDevice; return false; }
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); err_ = kErrDevice; return false; }
+    if (dev >= ndev) { err_ = kErrDevice; return false; }
+    {
+        DeviceGuard g(dev);
+        if (fgk::prepareKernels() != cudaSuccess) { cudaGetLastError(); err_ = kErrDevice; return false; }
+    }
+    m = new Impl();
+    m->device = dev;
+    m->info = ii;
+    m->fmt = fmt;
+    m->viewFormat = ii.viewFormat;
+    m->set = ii.settings;
+    m->ri = ii.viewFormat == kVkFormatR8G8B8A8Unorm ? 0 : 2;
+    m->gi = 1;
+    m->bi = ii.viewFormat == kVkFormatR8G8B8A8Unorm ? 2 : 0;
+    m->updateTrust();
+    if (const char* e = m->allocSize(ii.width, ii.height)) {
+        err_ = e;
+        delete m;
+        m = nullptr;
+        return false;
+    }
+    return true;
+}
+
+Format Interpolator::format() const { return m ? m->fmt : Format::Rgba8; }
+
+void Interpolator::destroy() {
+    delete m;
+    m = nullptr;
+}
+
+bool Interpolator::resize(uint32_t w, uint32_t h, uint32_t viewFormat) {
+    if (!m) return false;
+    Format f;
+    if (!formatOf(viewFormat, &f) || f != m->fmt) return false;
+    if (sizeError(w, h)) return false;
+    m->viewFormat = viewFormat;
+    m->ri = viewFormat == kVkFormatR8G8B8A8Unorm ? 0 : 2;
+    m->bi = viewFormat == kVkFormatR8G8B8A8Unorm ? 2 : 0;
+    return m->allocSize(w, h) == nullptr;
+}
+
+bool Interpolator::setSettings(const Settings& s) {
+    if (!m || settingsError(s) || s.flowScale != m->set.flowScale || s.pyramidMinSide != m->set.pyramidMinSide) return false;
+    m->set = s;
+    m->updateTrust();
+    return true;
+}
+
+bool Interpolator::reconfigure(const Settings& s) {
+    if (!m || settingsError(s)) return false;
+    const Settings old = m->set;
+    const bool structural = s.flowScale != old.flowScale || s.pyramidMinSide != old.pyramidMinSide;
+    m->set = s;
+    m->updateTrust();
+    if (structural && m->W) {
+        if (m->allocSize(m->W, m->H)) { m->set = old; m->updateTrust(); m->allocSize(m->W, m->H); return false; }
+    }
+    return true;
+}
+
+Settings Interpolator::settings() const { return m ? m->set : Settings{}; }
+
+void Interpolator::beginFrame() {
+    if (m) m->estSets = m->synthSets = 0;
+}
+
+bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
+    if (!m || !m->W) return false;
+    if (!m->frameOk(prev) || !m->frameOk(curr) || prev.pitch != curr.pitch) return false;
+    if (m->estSets >= kSetRing) return false;
+    DeviceGuard g(m->device);
+    m->estSets++;
+    m->haveEst = false;
+    if (!m->estimate(stream, prev, curr)) return false;
+    m->haveEst = true;
+    m->estPrev = prev.data;
+    m->estCurr = curr.data;
+    return true;
+}
+
+bool Interpolator::recordSynth(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t) {
+    if (!m || !m->W || !(t > 0.0f && t < 1.0f)) return false;
+    if (!m->haveEst || prev.data != m->estPrev || curr.data != m->estCurr) return false;
+    if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || prev.pitch != curr.pitch) return false;
+    if (m->synthSets >= kSetRing) return false;
+    DeviceGuard g(m->device);
+    m->synthSets++;
+    if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
+    return m->synth(stream, prev, curr, out, t);
+}
+
+bool Interpolator::record(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t) {
+    if (!m || !m->W || !(t > 0.0f && t < 1.0f)) return false;
+    if (!m->frameOk(out) || m->estSets >= kSetRing || m->synthSets >= kSetRing) return false;
+    return recordEstimate(stream, prev, curr) && recordSynth(stream, prev, curr, out, t);
+}
+
+const char* Interpolator::lastCudaError() const { return m ? m->lastErr : nullptr; }
+
+bool Interpolator::setProfiling(bool on) {
+    if (!m) return false;
+    m->profiling = on;
+    m->evCount = 0;
+    return true;
+}
+
+bool Interpolator::readTimings(std::vector<const char*>& names, std::vector<uint64_t>& ticks) {
+    names.clear();
+    ticks.clear();
+    if (!m || !m->profiling || m->evCount < 2) return false;
+    DeviceGuard g(m->device);
+    if (cudaEventSynchronize(m->events[m->evCount - 1]) != cudaSuccess) { cudaGetLastError(); return false; }
+    for (size_t i = 1; i < m->evCount; i++) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, m->events[i - 1], m->events[i]) != cudaSuccess) { cudaGetLastError(); return false; }
+        names.push_back(m->evNames[i]);
+        ticks.push_back((uint64_t)std::llround((double)ms * 1e6));
+    }
+    return true;
+}
+
+bool Interpolator::recordDebugCounters(cudaStream_t stream, void* dst) {
+    if (!m || !m->W || !dst) return false;
+    DeviceGuard g(m->device);
+    return cudaMemcpyAsync(dst, &m->st->untrusted[m->lastParity], 4, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+           cudaMemcpyAsync((char*)dst + 4, &m->st->sadSum256, 4, cudaMemcpyDeviceToDevice, stream) == cudaSuccess;
+}
+
+uint32_t Interpolator::debugSadBlocks() const { return m && m->W ? (uint32_t)(m->L.lv[0].bw * m->L.lv[0].bh) : 0; }
+
+bool Interpolator::debugMapLayout(DebugMapLayout& l) const {
+    if (!m || !m->W) return false;
+    l.W = m->W; l.H = m->H; l.fw = m->L.fw; l.fh = m->L.fh;
+    l.bw = m->L.lv[0].bw; l.bh = m->L.lv[0].bh; l.fscale = m->set.flowScale; l.eStride = (m->W + 3) / 4;
+    l.blockOff = 0;
+    l.pixOff = alignUp((uint64_t)l.bw * l.bh * 8, 256);
+    l.eOff = alignUp(l.pixOff + (uint64_t)l.fw * l.fh * 8, 256);
+    l.size = l.eOff + (uint64_t)l.eStride * 4 * l.H;
+    return true;
+}
+
+bool Interpolator::recordDebugMaps(cudaStream_t stream, void* dst) {
+    DebugMapLayout l;
+    if (!debugMapLayout(l) || !dst) return false;
+    DeviceGuard g(m->device);
+    char* d = (char*)dst;
+    const float2* blk = m->field + (m->set.subpixel ? m->L.sub1 : m->L.lv[0].fM);
+    return cudaMemcpyAsync(d + l.blockOff, blk, (size_t)l.bw * l.bh * 8, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+           cudaMemcpyAsync(d + l.pixOff, m->pf, (size_t)l.fw * l.fh * 8, cudaMemcpyDeviceToDevice, stream) == cudaSuccess &&
+           cudaMemcpyAsync(d + l.eOff, m->emap, (size_t)l.eStride * 4 * l.H, cudaMemcpyDeviceToDevice, stream) == cudaSuccess;
+}
+
+bool Interpolator::setDebugCapture(bool on) {
+    if (!m) return false;
+    m->capture = on;
+    return true;
+}
+
+bool Interpolator::traceLayout(TraceLayout& l) const {
+    if (!m || !m->W) return false;
+    std::memset(&l, 0, sizeof(l));
+    const SizeLayout& L = m->L;
+    l.nLevels = (uint32_t)L.lv.size(); l.fw = L.fw; l.fh = L.fh;
+    for (size_t i = 0; i < L.lv.size(); i++) {
+        l.lw[i] = L.lv[i].w; l.lh[i] = L.lv[i].h; l.bw[i] = L.lv[i].bw; l.bh[i] = L.lv[i].bh;
+    }
+    uint64_t o = 0;
+    l.lumaOff = o; l.lumaBytes = L.lumaFloats * 4; o = alignUp(o + l.lumaBytes, 256);
+    l.fieldOff = o; l.fieldBytes = L.fieldF2 * 8; o = alignUp(o + l.fieldBytes, 256);
+    l.medOff = o; o = alignUp(o + (uint64_t)L.lv.size() * 8, 256);
+    l.sadOff = o; o = alignUp(o + (uint64_t)L.lv[0].bw * L.lv[0].bh * 4, 256);
+    l.pfOff = o; o = alignUp(o + (uint64_t)L.fw * L.fh * 8, 256);
+    l.stateOff = o; o += 16;
+    l.size = o;
+    return true;
+}
+
+bool Interpolator::recordTrace(cudaStream_t stream, void* dst) {
+    TraceLayout l;
+    if (!traceLayout(l) || !dst) return false;
+    DeviceGuard g(m->device);
+    char* d = (char*)dst;
+    const auto D2D = cudaMemcpyDeviceToDevice;
+    bool ok = cudaMemcpyAsync(d + l.lumaOff, m->luma, l.lumaBytes, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.fieldOff, m->field, l.fieldBytes, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.medOff, m->st->med, (size_t)l.nLevels * 8, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.sadOff, m->sads, (size_t)l.bw[0] * l.bh[0] * 4, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.pfOff, m->pf, (size_t)l.fw * l.fh * 8, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.stateOff, &m->st->cut, 4, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.stateOff + 4, &m->st->sadMean, 4, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.stateOff + 8, &m->st->sadSum256, 4, D2D, stream) == cudaSuccess &&
+              cudaMemcpyAsync(d + l.stateOff + 12, &m->st->err, 4, D2D, stream) == cudaSuccess;
+    return ok;
+}
+
+}  // namespace framegen
+
+// ================================================================================================== C ABI
+using namespace framegen;
+
+struct fg_interpolator {
+    Interpolator I;
+};
+
+static Settings fromC(const fg_settings* c) {
+    Settings s;
+    if (!c) return s;
+    s.trustLow = c->trustLow; s.trustHigh = c->trustHigh; s.globalFallback = c->globalFallback;
+    s.sceneCutSad = c->sceneCutSad; s.hudBonus = c->hudBonus; s.smoothBonus = c->smoothBonus;
+    s.searchPenalty = c->searchPenalty; s.searchRadius = c->searchRadius; s.searchRadiusTop = c->searchRadiusTop;
+    s.subpixel = c->subpixel != 0; s.uiProtection = (UiProtection)c->uiProtection; s.blurSamples = c->blurSamples;
+    s.blurWeights = (BlurWeights)c->blurWeights; s.motionVersion = (MotionVersion)c->motionVersion;
+    s.flowScale = c->flowScale; s.pyramidMinSide = c->pyramidMinSide;
+    return s;
+}
+static void toC(const Settings& s, fg_settings* c) {
+    c->size = sizeof(fg_settings);
+    c->trustLow = s.trustLow; c->trustHigh = s.trustHigh; c->globalFallback = s.globalFallback;
+    c->sceneCutSad = s.sceneCutSad; c->hudBonus = s.hudBonus; c->smoothBonus = s.smoothBonus;
+    c->searchPenalty = s.searchPenalty; c->searchRadius = s.searchRadius; c->searchRadiusTop = s.searchRadiusTop;
+    c->subpixel = s.subpixel; c->uiProtection = (uint32_t)s.uiProtection; c->blurSamples = s.blurSamples;
+    c->blurWeights = (uint32_t)s.blurWeights; c->motionVersion = (uint32_t)s.motionVersion;
+    c->flowScale = s.flowScale; c->pyramidMinSide = s.pyramidMinSide;
+}
+static Frame fromC(const fg_frame* f) {
+    return f ? Frame(f->data, (size_t)f->pitch, f->chroma, (size_t)f->chroma_pitch) : Frame();
+}
+
+extern "C" {
+
+uint32_t fg_abi_version(void) { return 1; }
+void fg_default_settings(fg_settings* s) {
+    if (s) toC(Settings{}, s);
+}
+void fg_default_init_info(fg_init_info* ii) {
+    if (!ii) return;
+    InitInfo d;
+    std::memset(ii, 0, sizeof(*ii));
+    ii->size = sizeof(fg_init_info);
+    ii->view_format = d.viewFormat;
+    ii->transfer = (uint32_t)d.transfer;
+    ii->linear_white_nits = d.linearWhiteNits;
+    ii->yuv_matrix = (uint32_t)d.yuvMatrix;
+    ii->yuv_full_range = d.yuvFullRange;
+    ii->device = d.device;
+    toC(d.settings, &ii->settings);
+}
+int fg_format_of(uint32_t vf, uint32_t* out) {
+    Format f;
+    if (!formatOf(vf, &f)) return 0;
+    if (out) *out = (uint32_t)f;
+    return 1;
+}
+fg_interpolator* fg_create(void) { return new fg_interpolator(); }
+void fg_destroy(fg_interpolator* fg) { delete fg; }
+int fg_init(fg_interpolator* fg, const fg_init_info* c) {
+    if (!fg || !c) return 0;
+    InitInfo ii;
+    ii.width = c->width; ii.height = c->height; ii.viewFormat = c->view_format; ii.transfer = (Transfer)c->transfer;
+    ii.linearWhiteNits = c->linear_white_nits; ii.yuvMatrix = (YuvMatrix)c->yuv_matrix;
+    ii.yuvFullRange = c->yuv_full_range != 0; ii.device = c->device; ii.settings = fromC(&c->settings);
+    return fg->I.init(ii);
+}
+const char* fg_init_error(const fg_interpolator* fg) { return fg ? fg->I.initError() : "null interpolator"; }
+uint32_t fg_format(const fg_interpolator* fg) { return fg ? (uint32_t)fg->I.format() : 0; }
+int fg_resize(fg_interpolator* fg, uint32_t w, uint32_t h, uint32_t vf) { return fg && fg->I.resize(w, h, vf); }
+int fg_validate(const fg_settings* s) { return s && Interpolator::validate(fromC(s)); }
+const char* fg_settings_error_format(const fg_settings* s, uint32_t f) {
+    return Interpolator::settingsError(fromC(s), (Format)f);
+}
+const char* fg_settings_error(const fg_interpolator* fg, const fg_settings* s) {
+    return fg ? fg->I.settingsError(fromC(s)) : Interpolator::settingsError(fromC(s), Format::Rgba8);
+}
+const char* fg_size_error(const fg_interpolator* fg, uint32_t w, uint32_t h) {
+    return fg ? fg->I.sizeError(w, h) : "not initialised";
+}
+int fg_set_settings(fg_interpolator* fg, const fg_settings* s) { return fg && s && fg->I.setSettings(fromC(s)); }
+int fg_reconfigure(fg_interpolator* fg, const fg_settings* s) { return fg && s && fg->I.reconfigure(fromC(s)); }
+void fg_get_settings(const fg_interpolator* fg, fg_settings* s) {
+    if (s) toC(fg ? fg->I.settings() : Settings{}, s);
+}
+void fg_begin_frame(fg_interpolator* fg) {
+    if (fg) fg->I.beginFrame();
+}
+int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr) {
+    return fg && prev && curr && fg->I.recordEstimate((cudaStream_t)stream, fromC(prev), fromC(curr));
+}
+int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* out,
+                    float t) {
+    return fg && prev && curr && out && fg->I.recordSynth((cudaStream_t)stream, fromC(prev), fromC(curr), fromC(out), t);
+}
+int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* out, float t) {
+    return fg && prev && curr && out && fg->I.record((cudaStream_t)stream, fromC(prev), fromC(curr), fromC(out), t);
+}
+int fg_set_profiling(fg_interpolator* fg, int on) { return fg && fg->I.setProfiling(on != 0); }
+int fg_read_timings(fg_interpolator* fg, const char** names, uint64_t* ns, uint32_t capacity, uint32_t* count) {
+    if (!fg) return 0;
+    std::vector<const char*> n;
+    std::vector<uint64_t> t;
+    if (!fg->I.readTimings(n, t)) return 0;
+    for (uint32_t i = 0; i < capacity && i < n.size(); i++) {
+        if (names) names[i] = n[i];
+        if (ns) ns[i] = t[i];
+    }
+    if (count) *count = (uint32_t)n.size();
+    return 1;
+}
+int fg_record_debug_counters(fg_interpolator* fg, void* stream, void* dst) {
+    return fg && fg->I.recordDebugCounters((cudaStream_t)stream, dst);
+}
+uint32_t fg_debug_sad_blocks(const fg_interpolator* fg) { return fg ? fg->I.debugSadBlocks() : 0; }
+int fg_get_debug_map_layout(const fg_interpolator* fg, fg_debug_map_layout* l) {
+    Interpolator::DebugMapLayout d;
+    if (!fg || !l || !fg->I.debugMapLayout(d)) return 0;
+    l->W = d.W; l->H = d.H; l->fw = d.fw; l->fh = d.fh; l->bw = d.bw; l->bh = d.bh; l->fscale = d.fscale;
+    l->eStride = d.eStride; l->blockOff = d.blockOff; l->pixOff = d.pixOff; l->eOff = d.eOff; l->size = d.size;
+    return 1;
+}
+int fg_record_debug_maps(fg_interpolator* fg, void* stream, void* dst) {
+    return fg && fg->I.recordDebugMaps((cudaStream_t)stream, dst);
+}
+int fg_set_debug_capture(fg_interpolator* fg, int on) { return fg && fg->I.setDebugCapture(on != 0); }
+int fg_get_trace_layout(const fg_interpolator* fg, fg_trace_layout* l) {
+    Interpolator::TraceLayout t;
+    if (!fg || !l || !fg->I.traceLayout(t)) return 0;
+    static_assert(sizeof(fg_trace_layout) == sizeof(Interpolator::TraceLayout), "trace layout mirrors");
+    std::memcpy(l, &t, sizeof(t));
+    return 1;
+}
+int fg_record_trace(fg_interpolator* fg, void* stream, void* dst) { return fg && fg->I.recordTrace((cudaStream_t)stream, dst); }
+const char* fg_last_error(const fg_interpolator* fg) { return fg ? fg->I.lastCudaError() : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+"""Python binding of the B200 framegen library's C ABI (include/framegen_c.h), by ctypes.
+
+It mirrors framegen::Interpolator of frame-gen-ritz's gpu/framegen.h (init, resize, setSettings, reconfigure,
+beginFrame, recordEstimate, recordSynth, record, setProfiling, readTimings, recordDebugCounters, debugMapLayout,
+recordDebugMaps) with the same argument meaning and the same bool / error-string behaviour. Frames are CUDA tensors
+(uint8, (H, W, 4), rows may be padded: pitch = stride(0)); streams are torch.cuda.Stream or raw handles.
+
+The library is the only compute path: there is no CPU fallback. Loading fails loudly if libframegen_b200.so is
+missing (build it with frame-gen-ritz_b200/build.py).
+"""
+import ctypes
+import os
+from dataclasses import dataclass, fields
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libframegen_b200.so")
+
+# framegen::Format and the VkFormat numbers of include/framegen.h
+FORMAT = {"Rgba8": 0, "Rgb10": 1, "RgbaF16": 2, "Nv12": 3, "P010": 4}
+VK_R8G8B8A8_UNORM, VK_B8G8R8A8_UNORM = 37, 44
+VK_A2R10G10B10_UNORM, VK_A2B10G10R10_UNORM = 58, 64
+VK_R16G16B16A16_SFLOAT, VK_R8_UNORM, VK_R16_UNORM = 97, 9, 70
+SET_RING, MIN_SIZE = 32, 16
+
+
+class CSettings(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_uint32)] + \
+               [(n, ctypes.c_float) for n in ("trustLow", "trustHigh", "globalFallback", "sceneCutSad", "hudBonus",
+                                              "smoothBonus", "searchPenalty")] + \
+               [(n, ctypes.c_uint32) for n in ("searchRadius", "searchRadiusTop", "subpixel", "uiProtection",
+                                               "blurSamples", "blurWeights", "motionVersion", "flowScale",
+                                               "pyramidMinSide")]
+
+
+class CFrame(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("pitch", ctypes.c_uint64), ("chroma", ctypes.c_void_p),
+                ("chroma_pitch", ctypes.c_uint64)]
+
+
+class CInitInfo(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("view_format", ctypes.c_uint32), ("transfer", ctypes.c_uint32), ("linear_white_nits", ctypes.c_float),
+                ("yuv_matrix", ctypes.c_uint32), ("yuv_full_range", ctypes.c_uint32), ("device", ctypes.c_int32),
+                ("settings", CSettings)]
+
+
+class CDebugMapLayout(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("W", "H", "fw", "fh", "bw", "bh", "fscale", "eStride")] + \
+               [(n, ctypes.c_uint64) for n in ("blockOff", "pixOff", "eOff", "size")]
+
+
+class CTraceLayout(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("nLevels", "fw", "fh")] + \
+               [(n, ctypes.c_uint32 * 16) for n in ("lw", "lh", "bw", "bh")] + \
+               [(n, ctypes.c_uint64) for n in ("lumaOff", "lumaBytes", "fieldOff", "fieldBytes", "medOff", "sadOff",
+                                               "pfOff", "stateOff", "size")]
+
+
+# every symbol include/framegen_c.h declares, with (restype, argtypes)
+_P, _U32, _I, _F, _S = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float, ctypes.c_char_p
+SIGNATURES = {
+    "fg_abi_version": (_U32, []),
+    "fg_default_settings": (None, [ctypes.POINTER(CSettings)]),
+    "fg_default_init_info": (None, [ctypes.POINTER(CInitInfo)]),
+    "fg_format_of": (_I, [_U32, ctypes.POINTER(_U32)]),
+    "fg_create": (_P, []),
+    "fg_destroy": (None, [_P]),
+    "fg_init": (_I, [_P, ctypes.POINTER(CInitInfo)]),
+    "fg_init_error": (_S, [_P]),
+    "fg_format": (_U32, [_P]),
+    "fg_resize": (_I, [_P, _U32, _U32, _U32]),
+    "fg_validate": (_I, [ctypes.POINTER(CSettings)]),
+    "fg_settings_error_format": (_S, [ctypes.POINTER(CSettings), _U32]),
+    "fg_settings_error": (_S, [_P, ctypes.POINTER(CSettings)]),
+    "fg_size_error": (_S, [_P, _U32, _U32]),
+    "fg_set_settings": (_I, [_P, ctypes.POINTER(CSettings)]),
+    "fg_reconfigure": (_I, [_P, ctypes.POINTER(CSettings)]),
+    "fg_get_settings": (None, [_P, ctypes.POINTER(CSettings)]),
+    "fg_begin_frame": (None, [_P]),
+    "fg_record_estimate": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame)]),
+    "fg_record_synth": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
+    "fg_record": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
+    "fg_set_profiling": (_I, [_P, _I]),
+    "fg_read_timings": (_I, [_P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint64), _U32,
+                             ctypes.POINTER(_U32)]),
+    "fg_record_debug_counters": (_I, [_P, _P, _P]),
+    "fg_debug_sad_blocks": (_U32, [_P]),
+    "fg_get_debug_map_layout": (_I, [_P, ctypes.POINTER(CDebugMapLayout)]),
+    "fg_record_debug_maps": (_I, [_P, _P, _P]),
+    "fg_set_debug_capture": (_I, [_P, _I]),
+    "fg_get_trace_layout": (_I, [_P, ctypes.POINTER(CTraceLayout)]),
+    "fg_record_trace": (_I, [_P, _P, _P]),
+    "fg_last_error": (_S, [_P]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libframegen_b200.so (no fallback: a missing library is an error)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with frame-gen-ritz_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+@dataclass
+class Settings:
+    """framegen::Settings (the V1 fields), defaults = the tuned constants of proto/interp.py."""
+    trustLow: float = 12.0
+    trustHigh: float = 40.0
+    globalFallback: float = 0.15
+    sceneCutSad: float = 30.0
+    hudBonus: float = 1.0
+    smoothBonus: float = 0.5
+    searchPenalty: float = 0.5
+    searchRadius: int = 2
+    searchRadiusTop: int = 6
+    subpixel: bool = True
+    uiProtection: int = 0
+    blurSamples: int = 0
+    blurWeights: int = 1
+    motionVersion: int = 0
+    flowScale: int = 2
+    pyramidMinSide: int = 48
+
+    def to_c(self):
+        c = CSettings()
+        c.size = ctypes.sizeof(CSettings)
+        for f in fields(self):
+            setattr(c, f.name, int(getattr(self, f.name)) if f.type in (int, bool) else getattr(self, f.name))
+        return c
+
+    @staticmethod
+    def from_c(c):
+        s = Settings()
+        for f in fields(s):
+            v = getattr(c, f.name)
+            setattr(s, f.name, bool(v) if f.type is bool else v)
+        return s
+
+
+def _s(b):
+    return None if b is None else b.decode()
+
+
+def frame_of(t, chroma=None):
+    """A CFrame for a CUDA tensor (H, W, C) uint8 (pitch = the row stride in bytes)."""
+    if t is None:
+        return None
+    f = CFrame()
+    f.data = t.data_ptr()
+    f.pitch = t.stride(0) * t.element_size()
+    if chroma is not None:
+        f.chroma = chroma.data_ptr()
+        f.chroma_pitch = chroma.stride(0) * chroma.element_size()
+    return f
+
+
+def _stream(s):
+    if s is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return s if isinstance(s, int) else s.cuda_stream
+
+
+def validate(settings):
+    return bool(lib().fg_validate(ctypes.byref(settings.to_c())))
+
+
+def settings_error(settings, fmt="Rgba8"):
+    return _s(lib().fg_settings_error_format(ctypes.byref(settings.to_c()), FORMAT[fmt]))
+
+
+def format_of(view_format):
+    out = ctypes.c_uint32()
+    return {v: k for k, v in FORMAT.items()}[out.value] if lib().fg_format_of(view_format, ctypes.byref(out)) else None
+
+
+class Interpolator:
+    """framegen::Interpolator through the C ABI."""
+
+    def __init__(self):
+        self._h = lib().fg_create()
+
+    def close(self):
+        if self._h:
+            lib().fg_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def init(self, width, height, view_format=VK_R8G8B8A8_UNORM, settings=None, device=-1, transfer=0,
+             linear_white_nits=80.0, yuv_matrix=1, yuv_full_range=False):
+        ii = CInitInfo()
+        lib().fg_default_init_info(ctypes.byref(ii))
+        ii.width, ii.height, ii.view_format, ii.device = width, height, view_format, device
+        ii.transfer, ii.linear_white_nits, ii.yuv_matrix, ii.yuv_full_range = transfer, linear_white_nits, yuv_matrix, int(yuv_full_range)
+        ii.settings = (settings or Settings()).to_c()
+        return bool(lib().fg_init(self._h, ctypes.byref(ii)))
+
+    def init_error(self):
+        return _s(lib().fg_init_error(self._h))
+
+    def format(self):
+        return {v: k for k, v in FORMAT.items()}[lib().fg_format(self._h)]
+
+    def resize(self, w, h, view_format=VK_R8G8B8A8_UNORM):
+        return bool(lib().fg_resize(self._h, w, h, view_format))
+
+    def settings_error(self, settings):
+        return _s(lib().fg_settings_error(self._h, ctypes.byref(settings.to_c())))
+
+    def size_error(self, w, h):
+        return _s(lib().fg_size_error(self._h, w, h))
+
+    def set_settings(self, settings):
+        return bool(lib().fg_set_settings(self._h, ctypes.byref(settings.to_c())))
+
+    def reconfigure(self, settings):
+        return bool(lib().fg_reconfigure(self._h, ctypes.byref(settings.to_c())))
+
+    def settings(self):
+        c = CSettings()
+        lib().fg_get_settings(self._h, ctypes.byref(c))
+        return Settings.from_c(c)
+
+    def begin_frame(self):
+        lib().fg_begin_frame(self._h)
+
+    def record_estimate(self, prev, curr, stream=None):
+        return bool(lib().fg_record_estimate(self._h, _stream(stream), ctypes.byref(frame_of(prev)),
+                                             ctypes.byref(frame_of(curr))))
+
+    def record_synth(self, prev, curr, out, t, stream=None):
+        return bool(lib().fg_record_synth(self._h, _stream(stream), ctypes.byref(frame_of(prev)),
+                                          ctypes.byref(frame_of(curr)), ctypes.byref(frame_of(out)), float(t)))
+
+    def record(self, prev, curr, out, t=0.5, stream=None):
+        return bool(lib().fg_record(self._h, _stream(stream), ctypes.byref(frame_of(prev)),
+                                    ctypes.byref(frame_of(curr)), ctypes.byref(frame_of(out)), float(t)))
+
+    def set_profiling(self, on):
+        return bool(lib().fg_set_profiling(self._h, int(on)))
+
+    def read_timings(self):
+        n = 64
+        names = (ctypes.c_char_p * n)()
+        ns = (ctypes.c_uint64 * n)()
+        cnt = ctypes.c_uint32()
+        if not lib().fg_read_timings(self._h, names, ns, n, ctypes.byref(cnt)):
+            return None
+        return [(names[i].decode(), int(ns[i])) for i in range(min(cnt.value, n))]
+
+    def record_debug_counters(self, dst, stream=None):
+        return bool(lib().fg_record_debug_counters(self._h, _stream(stream), dst.data_ptr()))
+
+    def debug_sad_blocks(self):
+        return int(lib().fg_debug_sad_blocks(self._h))
+
+    def debug_map_layout(self):
+        l = CDebugMapLayout()
+        return l if lib().fg_get_debug_map_layout(self._h, ctypes.byref(l)) else None
+
+    def record_debug_maps(self, dst, stream=None):
+        return bool(lib().fg_record_debug_maps(self._h, _stream(stream), dst.data_ptr()))
+
+    def set_debug_capture(self, on):
+        return bool(lib().fg_set_debug_capture(self._h, int(on)))
+
+    def trace_layout(self):
+        l = CTraceLayout()
+        return l if lib().fg_get_trace_layout(self._h, ctypes.byref(l)) else None
+
+    def record_trace(self, dst, stream=None):
+        return bool(lib().fg_record_trace(self._h, _stream(stream), dst.data_ptr()))
+
+    def last_error(self):
+        return _s(lib().fg_last_error(self._h))
+
+
+def read_trace(fg, stream=None):
+    """Copy the latest estimate's intermediates to the host: a dict in the oracle's trace layout."""
+    import numpy as np
+    import torch
+    l = fg.trace_layout()
+    buf = torch.empty(l.size, dtype=torch.uint8, device="cuda")
+    assert fg.record_trace(buf, stream)
+    torch.cuda.synchronize()
+    h = buf.cpu().numpy()
+    f32 = lambda off, n: h[off:off + 4 * n].view(np.float32)
+    n = l.nLevels
+    luma, fld, o, of = [], [], l.lumaOff, l.fieldOff
+    for i in range(n):
+        w, hh, bw, bh = l.lw[i], l.lh[i], l.bw[i], l.bh[i]
+        luma.append((f32(o, w * hh).reshape(hh, w), f32(o + 4 * w * hh, w * hh).reshape(hh, w)))
+        o += 8 * w * hh
+        fld.append((f32(of, 2 * bw * bh).reshape(bh, bw, 2), f32(of + 8 * bw * bh, 2 * bw * bh).reshape(bh, bw, 2)))
+        of += 16 * bw * bh
+    bw0, bh0 = l.bw[0], l.bh[0]
+    sub = [f32(of, 2 * bw0 * bh0).reshape(bh0, bw0, 2), f32(of + 8 * bw0 * bh0, 2 * bw0 * bh0).reshape(bh0, bw0, 2)]
+    st = h[l.stateOff:l.stateOff + 16].view(np.uint32)
+    return {"luma": luma, "fields": fld, "sub": sub, "meds": f32(l.medOff, 2 * n).reshape(n, 2),
+            "sads": f32(l.sadOff, bw0 * bh0).reshape(bh0, bw0), "pf": f32(l.pfOff, 2 * l.fw * l.fh).reshape(l.fh, l.fw, 2),
+            "cut": bool(st[0]), "sad": float(st[1:2].view(np.float32)[0]), "sadSum256": int(st[2]), "err": int(st[3])}

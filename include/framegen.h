@@ -1,0 +1,177 @@
+// framegen (B200 build): image-only frame interpolation, MotionVersion::V1, on CUDA (sm_100a).
+//
+// Drop-in for the V1 path of frame-gen-ritz's gpu/framegen.h: the same namespace, class, enums, Settings fields,
+// defaults, ranges, bool-returning conventions and error strings, with these replacements:
+//   VkCommandBuffer          -> cudaStream_t (records are kernel launches on the caller's stream; nothing is
+//                               synchronised with the host, nothing is allocated while recording, so a caller may
+//                               capture records into a CUDA graph)
+//   Frame{VkImageView, ...}  -> Frame{device pointer, row pitch in bytes} (+ the CbCr plane for the two-plane formats)
+//   InitInfo Vulkan members  -> dropped; InitInfo::device selects the CUDA device (-1: the current one)
+//   VkBuffer debug targets   -> device pointers
+//   VkFormat viewFormat      -> the same VkFormat numbers as plain uint32_t (kVkFormat* below; no Vulkan headers)
+// Out of scope here (rejected with a reason by settingsError / initError): MotionVersion V2 / Learned / V3, static-UI
+// protection modes other than Off, motion blur.
+//
+// Threading / streams: not thread-safe. All records of one Interpolator must go to ONE stream, in recording order:
+// its internal buffers are shared between records and only ordered by stream order.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+typedef struct CUstream_st* cudaStream_t;
+
+namespace framegen {
+
+// gpu/framegen.h:15-24
+enum class UiProtection : uint32_t { Off = 0, Crosshair = 1, WholeScreen = 2, CrosshairV2 = 3 };
+// gpu/framegen.h:28-59 (V1 is the only version this library runs)
+enum class MotionVersion : uint32_t { V1 = 0, V2 = 1, Learned = 2, V3 = 3 };
+// gpu/framegen.h:125-129
+enum class BlurWeights : uint32_t { Even = 0, Gaussian = 1 };
+// gpu/framegen.h:138
+enum class Format : uint32_t { Rgba8 = 0, Rgb10 = 1, RgbaF16 = 2, Nv12 = 3, P010 = 4 };
+// The VkFormat values a viewFormat may take (their numbers in the Vulkan registry).
+enum : uint32_t {
+    kVkFormatR8Unorm = 9,
+    kVkFormatR8G8B8A8Unorm = 37,
+    kVkFormatB8G8R8A8Unorm = 44,
+    kVkFormatA2R10G10B10UnormPack32 = 58,
+    kVkFormatA2B10G10R10UnormPack32 = 64,
+    kVkFormatR16Unorm = 70,
+    kVkFormatR16G16B16A16Sfloat = 97,
+};
+// gpu/framegen.h:140: the format class of a view format, false if the library does not know it.
+bool formatOf(uint32_t viewFormat, Format* out);
+// gpu/framegen.h:144-147
+enum class Transfer : uint32_t { Encoded = 0, Linear = 1 };
+// gpu/framegen.h:150
+enum class YuvMatrix : uint32_t { Bt601 = 0, Bt709 = 1, Bt2020 = 2 };
+
+// gpu/framegen.h:154-159: one image as the library takes it. Device memory; rows `pitch` bytes apart (a multiple of
+// 4 for the 4-byte formats); pixels packed as the viewFormat says. The two-plane formats add the CbCr plane.
+struct Frame {
+    void* data = nullptr;
+    size_t pitch = 0;
+    void* chroma = nullptr;
+    size_t chromaPitch = 0;
+    Frame() = default;
+    Frame(void* d, size_t p, void* c = nullptr, size_t cp = 0) : data(d), pitch(p), chroma(c), chromaPitch(cp) {}
+};
+
+// gpu/framegen.h:167-409, the fields the V1 path reads (same names, types, defaults, ranges).
+struct Settings {
+    // runtime: setSettings() at any time
+    float trustLow = 12.0f;         // [0, 255], trustHigh >= trustLow + 1
+    float trustHigh = 40.0f;
+    float globalFallback = 0.15f;   // (0, 1]
+    float sceneCutSad = 30.0f;      // (0, 255]
+    float hudBonus = 1.0f;          // [0, 255]
+    float smoothBonus = 0.5f;       // [0, 255]
+    float searchPenalty = 0.5f;     // [0, 255]
+    uint32_t searchRadius = 2;      // [1, 12]
+    uint32_t searchRadiusTop = 6;   // [1, 12]
+    bool subpixel = true;
+    UiProtection uiProtection = UiProtection::Off;   // Off only
+    uint32_t blurSamples = 0;                        // [0, 16]; recordSynthBlur is not part of this library
+    BlurWeights blurWeights = BlurWeights::Gaussian;
+    MotionVersion motionVersion = MotionVersion::V1; // V1 only
+    // structural: init() or reconfigure()
+    uint32_t flowScale = 2;         // 1, 2, 4
+    uint32_t pyramidMinSide = 48;   // [16, 256]
+};
+
+// gpu/framegen.h:411-441 without the Vulkan members.
+struct InitInfo {
+    uint32_t width = 0, height = 0;                  // >= kMinSize each
+    uint32_t viewFormat = kVkFormatB8G8R8A8Unorm;
+    Transfer transfer = Transfer::Encoded;           // RgbaF16 only
+    float linearWhiteNits = 80.0f;                   // Transfer::Linear: (0, 10000]
+    YuvMatrix yuvMatrix = YuvMatrix::Bt709;          // Nv12 / P010 only
+    bool yuvFullRange = false;
+    Settings settings{};
+    int device = -1;                                 // CUDA device ordinal, -1 = the current device at init()
+};
+
+class Interpolator {
+public:
+    Interpolator() = default;
+    ~Interpolator();
+    Interpolator(const Interpolator&) = delete;
+    Interpolator& operator=(const Interpolator&) = delete;
+
+    // gpu/framegen.h:451-461. init/resize/destroy free memory earlier records use: the caller must have retired
+    // them (stream or device synchronize) first.
+    bool init(const InitInfo&);
+    const char* initError() const { return err_; }
+    Format format() const;
+    void destroy();
+    bool resize(uint32_t w, uint32_t h, uint32_t viewFormat);
+
+    // gpu/framegen.h:464-480
+    static bool validate(const Settings&);
+    static const char* settingsError(const Settings&, Format format);
+    const char* settingsError(const Settings&) const;
+    const char* sizeError(uint32_t width, uint32_t height) const;
+    // gpu/framegen.h:500-507
+    bool setSettings(const Settings&);
+    bool reconfigure(const Settings&);
+    Settings settings() const;
+
+    // gpu/framegen.h:511: resets the per-submission record counts (kSetRing each)
+    void beginFrame();
+
+    // gpu/framegen.h:549-551: passes 1-8 once per real pair, passes 9-11 per generated time t in (0, 1), or both.
+    // false (and nothing recorded, out untouched) if not initialised, t outside (0, 1), a ring overflow since
+    // beginFrame(), a synth without an estimate since init/resize/reconfigure, or prev/curr not the estimate's frames.
+    bool recordEstimate(cudaStream_t stream, Frame prev, Frame curr);
+    bool recordSynth(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t);
+    bool record(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t = 0.5f);
+
+    // gpu/framegen.h:705-717: CUDA events after every pass group; readTimings waits for them and returns the
+    // group names and the nanoseconds of each group (the reference returns timestamp ticks; here 1 tick = 1 ns).
+    bool setProfiling(bool on);
+    bool readTimings(std::vector<const char*>& names, std::vector<uint64_t>& ticks);
+
+    // gpu/framegen.h:726-741: debug copies into device memory at dst (stream-ordered).
+    bool recordDebugCounters(cudaStream_t stream, void* dst);   // 2 uint32: [untrusted px, finest SAD sum x 256]
+    uint32_t debugSadBlocks() const;
+    struct DebugMapLayout {
+        uint32_t W, H, fw, fh, bw, bh, fscale, eStride;   // eStride in uint32 words
+        uint64_t blockOff, pixOff, eOff, size;            // byte offsets in dst and the total size
+    };
+    bool debugMapLayout(DebugMapLayout& l) const;
+    // The e part is written only by synths recorded while setDebugCapture(true) (a B200-build switch: the fused synth
+    // otherwise never stores the per-pixel mismatch).
+    bool recordDebugMaps(cudaStream_t stream, void* dst);
+    bool setDebugCapture(bool on);
+
+    // B200-build extension for stage-by-stage parity tests: every intermediate of the latest estimate.
+    struct TraceLayout {
+        uint32_t nLevels, fw, fh;
+        uint32_t lw[16], lh[16], bw[16], bh[16];
+        uint64_t lumaOff, lumaBytes;     // per level: a (lw*lh float) then c
+        uint64_t fieldOff, fieldBytes;   // per level: search then median3 (bw*bh float2 each), then sub0, sub1
+        uint64_t medOff;                 // 2 floats per level: 2 x the global median used for its seeds
+        uint64_t sadOff;                 // finest bw*bh float: the SADs of the scene-cut mean
+        uint64_t pfOff;                  // fw*fh float2
+        uint64_t stateOff;               // 4 uint32: cut, float sadMean bits, sad sum x 256, error bits
+        uint64_t size;
+    };
+    bool traceLayout(TraceLayout& l) const;
+    bool recordTrace(cudaStream_t stream, void* dst);
+
+    // The CUDA error string of the last record that failed at a launch (null if none): a B200-build diagnostic.
+    const char* lastCudaError() const;
+
+    static constexpr uint32_t kSetRing = 32;
+    static constexpr uint32_t kBlurMaxSamples = 16;
+    static constexpr uint32_t kMinSize = 16;
+    struct Impl;
+
+private:
+    Impl* m = nullptr;
+    const char* err_ = nullptr;
+};
+
+}  // namespace framegen

@@ -1,0 +1,104 @@
+/* framegen_c.h -- the C ABI of the B200 framegen library (libframegen_b200.so).
+ *
+ * Plain pointers, sizes and POD structs only: the binding surface for hosts that cannot take the C++ header
+ * (ctypes, cgo, JNI, N-API). Every entry point is a thin forward to framegen::Interpolator (include/framegen.h),
+ * whose methods each replace the like-named member of frame-gen-ritz's gpu/framegen.h (cited per function).
+ * Booleans are int (1 = true). Strings are static literals owned by the library. Streams are cudaStream_t passed as
+ * void* (NULL = the legacy default stream). Frames are device pointers with a row pitch in bytes.
+ */
+#ifndef FRAMEGEN_C_H
+#define FRAMEGEN_C_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fg_interpolator fg_interpolator;
+
+/* framegen::Settings (gpu/framegen.h:167-409, the V1 fields). `size` = sizeof(fg_settings) for ABI growth. */
+typedef struct fg_settings {
+    uint32_t size;
+    float trustLow, trustHigh, globalFallback, sceneCutSad, hudBonus, smoothBonus, searchPenalty;
+    uint32_t searchRadius, searchRadiusTop, subpixel;
+    uint32_t uiProtection, blurSamples, blurWeights, motionVersion;
+    uint32_t flowScale, pyramidMinSide;
+} fg_settings;
+
+/* framegen::Frame (gpu/framegen.h:154-159) */
+typedef struct fg_frame {
+    void* data;
+    uint64_t pitch;
+    void* chroma;
+    uint64_t chroma_pitch;
+} fg_frame;
+
+/* framegen::InitInfo (gpu/framegen.h:411-441) */
+typedef struct fg_init_info {
+    uint32_t size;
+    uint32_t width, height;
+    uint32_t view_format;      /* VkFormat number, e.g. 44 = B8G8R8A8_UNORM, 37 = R8G8B8A8_UNORM */
+    uint32_t transfer;
+    float linear_white_nits;
+    uint32_t yuv_matrix, yuv_full_range;
+    int32_t device;
+    fg_settings settings;
+} fg_init_info;
+
+/* Interpolator::DebugMapLayout (gpu/framegen.h:736-739) */
+typedef struct fg_debug_map_layout {
+    uint32_t W, H, fw, fh, bw, bh, fscale, eStride;
+    uint64_t blockOff, pixOff, eOff, size;
+} fg_debug_map_layout;
+
+/* Interpolator::TraceLayout (B200-build extension, no reference counterpart: stage parity tests) */
+typedef struct fg_trace_layout {
+    uint32_t nLevels, fw, fh;
+    uint32_t lw[16], lh[16], bw[16], bh[16];
+    uint64_t lumaOff, lumaBytes, fieldOff, fieldBytes, medOff, sadOff, pfOff, stateOff, size;
+} fg_trace_layout;
+
+uint32_t fg_abi_version(void);
+void fg_default_settings(fg_settings* s);                    /* Settings{} defaults */
+void fg_default_init_info(fg_init_info* ii);                 /* InitInfo{} defaults */
+int fg_format_of(uint32_t view_format, uint32_t* format);    /* gpu/framegen.h:140 formatOf */
+
+fg_interpolator* fg_create(void);
+void fg_destroy(fg_interpolator* fg);                        /* destroy() + free; gpu/framegen.h:456 */
+int fg_init(fg_interpolator* fg, const fg_init_info* ii);    /* gpu/framegen.h:451 */
+const char* fg_init_error(const fg_interpolator* fg);        /* gpu/framegen.h:453 */
+uint32_t fg_format(const fg_interpolator* fg);               /* gpu/framegen.h:455 */
+int fg_resize(fg_interpolator* fg, uint32_t w, uint32_t h, uint32_t view_format);   /* gpu/framegen.h:461 */
+
+int fg_validate(const fg_settings* s);                                              /* gpu/framegen.h:464 */
+const char* fg_settings_error_format(const fg_settings* s, uint32_t format);        /* gpu/framegen.h:468 */
+const char* fg_settings_error(const fg_interpolator* fg, const fg_settings* s);     /* gpu/framegen.h:472 */
+const char* fg_size_error(const fg_interpolator* fg, uint32_t w, uint32_t h);       /* gpu/framegen.h:480 */
+int fg_set_settings(fg_interpolator* fg, const fg_settings* s);                     /* gpu/framegen.h:500 */
+int fg_reconfigure(fg_interpolator* fg, const fg_settings* s);                      /* gpu/framegen.h:505 */
+void fg_get_settings(const fg_interpolator* fg, fg_settings* s);                    /* gpu/framegen.h:507 */
+
+void fg_begin_frame(fg_interpolator* fg);                                           /* gpu/framegen.h:511 */
+int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr);   /* :549 */
+int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
+                    const fg_frame* out, float t);                                                        /* :550 */
+int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
+              const fg_frame* out, float t);                                                              /* :551 */
+
+int fg_set_profiling(fg_interpolator* fg, int on);                                   /* gpu/framegen.h:705 */
+/* gpu/framegen.h:717 readTimings: up to `capacity` names and nanoseconds; *count = the number of groups */
+int fg_read_timings(fg_interpolator* fg, const char** names, uint64_t* ns, uint32_t capacity, uint32_t* count);
+
+int fg_record_debug_counters(fg_interpolator* fg, void* stream, void* dst);          /* gpu/framegen.h:726 */
+uint32_t fg_debug_sad_blocks(const fg_interpolator* fg);                             /* gpu/framegen.h:727 */
+int fg_get_debug_map_layout(const fg_interpolator* fg, fg_debug_map_layout* l);          /* gpu/framegen.h:740 */
+int fg_record_debug_maps(fg_interpolator* fg, void* stream, void* dst);              /* gpu/framegen.h:741 */
+int fg_set_debug_capture(fg_interpolator* fg, int on);      /* B200-build switch: synths store e for debug maps */
+int fg_get_trace_layout(const fg_interpolator* fg, fg_trace_layout* l);                  /* B200-build extension */
+int fg_record_trace(fg_interpolator* fg, void* stream, void* dst);                   /* B200-build extension */
+const char* fg_last_error(const fg_interpolator* fg);   /* the last CUDA error a record met (null if none) */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

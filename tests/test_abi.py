@@ -1,0 +1,99 @@
+"""The C ABI without a GPU: the library loads, exports every symbol include/framegen_c.h declares, and its host-only
+logic (defaults, validate, settingsError, formatOf, init's refusals) behaves like gpu/framegen.h / framegen.cpp."""
+import ctypes
+import math
+import os
+import re
+
+import pytest
+
+import framegen as fg
+
+HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "framegen_c.h")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    import build
+    build.build()
+
+
+def declared():
+    src = open(HDR).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(fg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_every_declared_symbol_is_exported_and_bound():
+    names = declared()
+    assert len(names) >= 30
+    L = fg.lib()
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(fg.SIGNATURES), "the Python binding covers exactly the header"
+
+
+def test_struct_sizes_match_header():
+    assert ctypes.sizeof(fg.CSettings) == 4 * 17
+    assert ctypes.sizeof(fg.CFrame) == 32
+    ii = fg.CInitInfo()
+    fg.lib().fg_default_init_info(ctypes.byref(ii))
+    assert ii.size == ctypes.sizeof(fg.CInitInfo)
+    assert ii.settings.size == ctypes.sizeof(fg.CSettings)
+
+
+def test_defaults_are_interp_constants():
+    c = fg.CSettings()
+    fg.lib().fg_default_settings(ctypes.byref(c))
+    s = fg.Settings.from_c(c)
+    assert s == fg.Settings.from_c(fg.Settings().to_c())
+    # proto/interp.py:43-61 / gpu/framegen.h:167-409
+    assert (s.trustLow, s.trustHigh, s.globalFallback, s.sceneCutSad) == (12.0, 40.0, pytest.approx(0.15), 30.0)
+    assert (s.hudBonus, s.smoothBonus, s.searchPenalty) == (1.0, 0.5, 0.5)
+    assert (s.searchRadius, s.searchRadiusTop, s.subpixel, s.flowScale, s.pyramidMinSide) == (2, 6, True, 2, 48)
+    ii = fg.CInitInfo()
+    fg.lib().fg_default_init_info(ctypes.byref(ii))
+    assert ii.view_format == fg.VK_B8G8R8A8_UNORM and ii.linear_white_nits == 80.0 and ii.device == -1
+
+
+@pytest.mark.parametrize("field,value,ok", [
+    ("trustLow", 0.0, True), ("trustLow", -0.5, False), ("trustLow", 39.5, False), ("trustHigh", 255.0, True),
+    ("trustHigh", 256.0, False), ("globalFallback", 0.0, False), ("globalFallback", 1.0, True),
+    ("sceneCutSad", 0.0, False), ("sceneCutSad", 255.0, True), ("hudBonus", math.nan, False),
+    ("smoothBonus", math.inf, False), ("searchPenalty", 255.0, True), ("searchRadius", 0, False),
+    ("searchRadius", 12, True), ("searchRadiusTop", 13, False), ("flowScale", 3, False), ("flowScale", 4, True),
+    ("flowScale", 1, True), ("pyramidMinSide", 15, False), ("pyramidMinSide", 256, True), ("blurSamples", 17, False),
+    ("uiProtection", 4, False), ("motionVersion", 4, False)])
+def test_validate_ranges(field, value, ok):
+    s = fg.Settings()
+    setattr(s, field, value)
+    assert fg.validate(s) is ok
+    err = fg.settings_error(s)
+    assert (err is None) is ok or (ok and err is not None)
+    if not ok:
+        assert err.startswith("invalid settings")
+
+
+def test_settings_error_names_unbuilt_parts():
+    s = fg.Settings(motionVersion=1)
+    assert fg.validate(s) and "V1 only" in fg.settings_error(s)
+    s = fg.Settings(uiProtection=1)
+    assert fg.validate(s) and "uiProtection must be Off" in fg.settings_error(s)
+
+
+def test_format_of():
+    assert fg.format_of(fg.VK_R8G8B8A8_UNORM) == "Rgba8" and fg.format_of(fg.VK_B8G8R8A8_UNORM) == "Rgba8"
+    assert fg.format_of(fg.VK_A2B10G10R10_UNORM) == "Rgb10" and fg.format_of(fg.VK_R16G16B16A16_SFLOAT) == "RgbaF16"
+    assert fg.format_of(fg.VK_R8_UNORM) == "Nv12" and fg.format_of(fg.VK_R16_UNORM) == "P010"
+    assert fg.format_of(12345) is None
+
+
+def test_init_refusals_without_recording():
+    I = fg.Interpolator()
+    assert not I.init(8, 8) and "kMinSize" in I.init_error()
+    assert not I.init(64, 64, view_format=12345) and "viewFormat" in I.init_error()
+    assert not I.init(64, 64, settings=fg.Settings(flowScale=3))
+    # no estimate / not initialised: every record is refused and nothing is launched
+    assert I.size_error(64, 64) == "not initialised"
+    assert I.read_timings() is None
+    I.close()
