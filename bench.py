@@ -47,6 +47,8 @@ def args():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--eager", type=int, default=0,
+                    help="profiling mode: run this many eager steps (no graphs, no timing, no JSON) and exit")
     return ap.parse_args()
 
 
@@ -200,6 +202,16 @@ def main():
     I = fg.Interpolator()
     assert I.init(W4K, H4K, fg.VK_R8G8B8A8_UNORM, device=local), I.init_error()
     stream = torch.cuda.Stream()
+    if a.eager:   # for ncu: plain records, one pair, nothing else
+        for i in range(a.eager):
+            k = i % a.pool
+            I.begin_frame()
+            assert I.record_estimate(pool[k][0], pool[k][1], stream=stream)
+            for o, t in zip(outs[k], TS):
+                assert I.record_synth(pool[k][0], pool[k][1], o, t, stream=stream)
+        torch.cuda.synchronize()
+        I.close()
+        return
 
     # correctness guard: the graph path gives the eager bytes
     with torch.cuda.stream(stream):

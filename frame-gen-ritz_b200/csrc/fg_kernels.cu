@@ -309,19 +309,23 @@ __global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
     const int nb = 2 * p.B + 1;
     const unsigned int N = (unsigned int)(p.fbw * p.fbh), ks[2] = {(N - 1) / 2, N / 2};
     const int per = (nb + 255) / 256;
+    const unsigned int lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     for (int axis = 0; axis < 2; axis++) {
         const unsigned int* h = p.hist + axis * nb;
         const int s0 = threadIdx.x * per, s1 = min(s0 + per, nb);
         unsigned int loc = 0;
         for (int i = s0; i < s1; i++) loc += __ldcg(h + i);
-        part[threadIdx.x] = loc;
-        __syncthreads();
-        if (threadIdx.x == 0) {   // exclusive prefix over 256 partial sums
-            unsigned int acc = 0;
-            for (int i = 0; i < 256; i++) { const unsigned int t = part[i]; part[i] = acc; acc += t; }
+        unsigned int inc = loc;   // inclusive scan of the 256 partial sums: within each warp, then across the 8 warps
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int n = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (unsigned int)o) inc += n;
         }
+        if (lane == 31) part[wid] = inc;
         __syncthreads();
-        unsigned int acc = part[threadIdx.x];
+        unsigned int wofs = 0;
+        for (unsigned int w = 0; w < wid; w++) wofs += part[w];
+        unsigned int acc = wofs + inc - loc;
         for (int i = s0; i < s1; i++) {
             const unsigned int hv = __ldcg(h + i);
             for (int q = 0; q < 2; q++)
@@ -399,21 +403,13 @@ __global__ void __launch_bounds__(256) k_cutmean(const CutMeanParams p) {
 
 // ============================================================================================== sub-pixel refinement
 // interp.flow :162-163: search(., 1, 0.5) then search(., 1, 0.25) around the median-filtered integer vector s, one
-// warp per finest-level block. Both frames' 13x13 windows (block +- 2 px around q -+ s) are staged in shared memory;
-// a tap at a quarter-pixel position is cv2's bilinear sample (exact here). The 72 (candidate, row) partial sums are
-// spread over the lanes. The last CTA computes the scene-cut mean of the winners' SADs.
-constexpr int kSubT = 13, kSubO = 2;
-
-__device__ __forceinline__ float tapT(const float* t, float x, float y) {
-    const float flx = floorf(x), fly = floorf(y);
-    const float fx = x - flx, fy = y - fly, gx = 1.0f - fx, gy = 1.0f - fy;
-    const float* q = t + (int)fly * kSubT + (int)flx;
-    float r = __fmul_rn(q[0], __fmul_rn(gy, gx));
-    r = __fadd_rn(r, __fmul_rn(q[1], __fmul_rn(gy, fx)));
-    r = __fadd_rn(r, __fmul_rn(q[kSubT], __fmul_rn(fy, gx)));
-    r = __fadd_rn(r, __fmul_rn(q[kSubT + 1], __fmul_rn(fy, fx)));
-    return r;
-}
+// warp per finest-level block. Both frames' 13x13 windows (block +- 2 px around q -+ s) are staged in shared memory.
+// Every pass samples each frame on a 24 x 24 lattice: per axis, the 8 pixel positions times the pass's 3 offsets
+// (base + step * {-1, 0, 1}, quarter-pixel units). The lattice is built separably (horizontal then vertical, weights
+// multiples of 1/4: every product and sum is exact, so it equals cv2's bilinear tap), after which a candidate's SAD is
+// two shared loads per pixel. The last CTA computes the scene-cut mean of the winners' SADs.
+constexpr int kSubT = 13, kSubO = 2, kSubL = 24, kSubRows = 10;   // tile, its margin, lattice side, tile rows used
+constexpr int kSubWarpFloats = 2 * kSubT * kSubT + 2 * kSubRows * kSubL + 2 * kSubL * kSubL + 72;
 
 __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
     extern __shared__ float smem[];
@@ -423,38 +419,65 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
     const int b = blockIdx.x * 4 + warp;
     const int nb = p.bw * p.bh;
     if (b < nb) {
-        float* sA = smem + warp * (2 * kSubT * kSubT + 72);
-        float* sC = sA + kSubT * kSubT;
-        float* rows = sC + kSubT * kSubT;
+        float* tA = smem + warp * kSubWarpFloats;
+        float* tC = tA + kSubT * kSubT;
+        float* hA = tC + kSubT * kSubT;      // kSubRows x kSubL: tile rows 1..10 sampled at the lattice columns
+        float* hC = hA + kSubRows * kSubL;
+        float* qA = hC + kSubRows * kSubL;   // kSubL x kSubL lattice
+        float* qC = qA + kSubL * kSubL;
+        float* rows = qC + kSubL * kSubL;
         const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
         const float2 v0 = p.in[b];
         const int sx = __float2int_rn(v0.x), sy = __float2int_rn(v0.y);
         for (int i = lane; i < kSubT * kSubT; i += 32) {
             const int x = i % kSubT, y = i / kSubT;
-            sA[i] = Lc(p.la, p.w, p.h, b0x - sx - kSubO + x, b0y - sy - kSubO + y);
-            sC[i] = Lc(p.lc, p.w, p.h, b0x + sx - kSubO + x, b0y + sy - kSubO + y);
+            tA[i] = Lc(p.la, p.w, p.h, b0x - sx - kSubO + x, b0y - sy - kSubO + y);
+            tC[i] = Lc(p.lc, p.w, p.h, b0x + sx - kSubO + x, b0y + sy - kSubO + y);
         }
         __syncwarp();
-        float ox0 = 0.0f, oy0 = 0.0f, sadBest = 0.0f;
+        int b4x = 0, b4y = 0;   // the offset chosen so far, quarter pixels
+        float sadBest = 0.0f;
         for (int pass = 0; pass < 2; pass++) {
-            const float step = pass ? 0.25f : 0.5f;
+            const int s4 = pass ? 1 : 2;
+            // horizontal stage: a at tile x + 2 - o, c at x + 2 + o, o = (b4x + s4 d) / 4, lattice column u = 3x + d + 1
+            for (int it = lane; it < kSubRows * kSubL; it += 32) {
+                const int r = it / kSubL + 1, u = it % kSubL, x = u / 3, d = u % 3 - 1;
+                const int PA = 4 * (x + kSubO) - (b4x + s4 * d), PC = 4 * (x + kSubO) + (b4x + s4 * d);
+                const float fa = (float)(PA & 3) * 0.25f, fc = (float)(PC & 3) * 0.25f;
+                const float* ra = tA + r * kSubT + (PA >> 2);
+                const float* rc = tC + r * kSubT + (PC >> 2);
+                hA[it] = __fmaf_rn(ra[1], fa, __fmul_rn(ra[0], 1.0f - fa));   // exact: dyadic, <= 16 significant bits
+                hC[it] = __fmaf_rn(rc[1], fc, __fmul_rn(rc[0], 1.0f - fc));
+            }
+            __syncwarp();
+            // vertical stage: lattice row v = 3y + d + 1
+            for (int it = lane; it < kSubL * kSubL; it += 32) {
+                const int v = it / kSubL, u = it % kSubL, y = v / 3, d = v % 3 - 1;
+                const int PA = 4 * (y + kSubO) - (b4y + s4 * d), PC = 4 * (y + kSubO) + (b4y + s4 * d);
+                const float fa = (float)(PA & 3) * 0.25f, fc = (float)(PC & 3) * 0.25f;
+                const float* ca = hA + ((PA >> 2) - 1) * kSubL + u;
+                const float* cc = hC + ((PC >> 2) - 1) * kSubL + u;
+                qA[it] = __fmaf_rn(ca[kSubL], fa, __fmul_rn(ca[0], 1.0f - fa));
+                qC[it] = __fmaf_rn(cc[kSubL], fc, __fmul_rn(cc[0], 1.0f - fc));
+            }
+            __syncwarp();
+            // (candidate, row) partial sums: candidate k = (dy + 1) * 3 + (dx + 1)
             for (int it = lane; it < 72; it += 32) {
-                const int k = it >> 3, y = it & 7;
-                const float ox = __fadd_rn(ox0, (float)(k % 3 - 1) * step), oy = __fadd_rn(oy0, (float)(k / 3 - 1) * step);
-                const float ya = (float)(y + kSubO) - oy, yc = (float)(y + kSubO) + oy;
+                const int k = it >> 3, y = it & 7, dx = k % 3, dy = k / 3;
+                const float* ra = qA + (3 * y + dy) * kSubL + dx;
+                const float* rc = qC + (3 * y + dy) * kSubL + dx;
                 float sum = 0.0f;
 #pragma unroll
-                for (int x = 0; x < 8; x++)
-                    sum += fabsf(tapT(sA, (float)(x + kSubO) - ox, ya) - tapT(sC, (float)(x + kSubO) + ox, yc));
+                for (int x = 0; x < 8; x++) sum += fabsf(ra[3 * x] - rc[3 * x]);
                 rows[it] = sum;
             }
             __syncwarp();
             float cost = FLT_MAX, sad = 0.0f;
             if (lane < 9) {
-                float s = 0.0f;
+                float sum = 0.0f;
 #pragma unroll
-                for (int y = 0; y < 8; y++) s += rows[lane * 8 + y];
-                sad = __fmul_rn(s, 1.0f / 64.0f);
+                for (int y = 0; y < 8; y++) sum += rows[lane * 8 + y];
+                sad = __fmul_rn(sum, 1.0f / 64.0f);
                 cost = __fadd_rn(sad, p.pen[pass][abs(lane % 3 - 1) + abs(lane / 3 - 1)]);
             }
             int bi = lane;
@@ -464,14 +487,15 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
                 const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
                 if (oc < cost || (oc == cost && oi < bi)) { cost = oc; bi = oi; sad = os; }
             }
-            ox0 = __fadd_rn(ox0, (float)(bi % 3 - 1) * step);
-            oy0 = __fadd_rn(oy0, (float)(bi / 3 - 1) * step);
+            b4x += s4 * (bi % 3 - 1);
+            b4y += s4 * (bi / 3 - 1);
             sadBest = sad;
-            if (pass == 0 && p.out0 && lane == 0) p.out0[b] = make_float2(__fadd_rn((float)sx, ox0), __fadd_rn((float)sy, oy0));
+            if (pass == 0 && p.out0 && lane == 0)
+                p.out0[b] = make_float2(__fadd_rn((float)sx, (float)b4x * 0.25f), __fadd_rn((float)sy, (float)b4y * 0.25f));
             __syncwarp();
         }
         if (lane == 0) {
-            p.out[b] = make_float2(__fadd_rn((float)sx, ox0), __fadd_rn((float)sy, oy0));
+            p.out[b] = make_float2(__fadd_rn((float)sx, (float)b4x * 0.25f), __fadd_rn((float)sy, (float)b4y * 0.25f));
             p.sads[b] = sadBest;
         }
     }
@@ -585,78 +609,139 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
 // interp.synth :219-246 for one time t, fused: the field at t (interp.field_at, flow res, recomputed per tile with
 // its halo), its upsampling to full resolution (cv2.resize x fs INTER_LINEAR, crop / edge pad, x fs), the two
 // bilinear 8-bit warps (cv2.remap of uint8: 5-bit fractions, integer weights, round half up), the max-channel
-// mismatch, its 7x7 replicate box, the trust ramp, the untrusted count and the blend. One CTA = 64x32 output pixels;
-// the mismatch is also computed on the 3-pixel halo the box needs. A scene cut (decided by the estimate) copies the
-// nearer frame instead; the untrusted-share decision needs every CTA's count and is taken by k_fallback.
+// mismatch, its 7x7 replicate box, the trust ramp, the untrusted count and the blend. One CTA = kSyTW x kSyTH output
+// pixels; the mismatch is also computed on the 3-pixel halo the box needs. A scene cut (decided by the estimate)
+// copies the nearer frame instead; the untrusted-share decision needs every CTA's count and is taken by k_fallback.
+//
+// Float <-> int conversions run on the FP32 pipe (magic-number additions, exact in the ranges used here) rather than
+// the conversion units; the bilinear taps run two channels per 32-bit multiply (R|B lanes, G) and the mismatch and the
+// t = 0.5 blend use byte-SIMD instructions.
 constexpr int kSyTW = 64, kSyTH = 32, kSyAp = 3, kSyEW = kSyTW + 2 * kSyAp, kSyEH = kSyTH + 2 * kSyAp;
 
-struct LinAxis {   // cv2.resize INTER_LINEAR coefficients of one output coordinate (x fs upscale)
-    int i0, i1;
-    float a0, a1;
+// round-half-even(x * 32) for |x * 32| < 2^22 (cv2's saturate_cast<int>(x * INTER_TAB_SIZE))
+__device__ __forceinline__ int rne32(float x) { return __float_as_int(__fmaf_rn(x, 32.0f, 12582912.0f)) - 0x4B400000; }
+// exact float of 0 <= i < 2^23
+__device__ __forceinline__ float i2f(int i) { return __int_as_float(0x4B000000 | i) - 8388608.0f; }
+// floor of 0 <= v < 2^23
+__device__ __forceinline__ int floorPos(float v) { return __float_as_int(__fadd_rz(v, 8388608.0f)) - 0x4B000000; }
+
+// cv2.remap INTER_LINEAR / BORDER_REPLICATE of the 2-channel float field, conversions on the FP32 pipe
+__device__ __forceinline__ float2 remapF2m(const float2* __restrict__ F, int w, int h, float x, float y) {
+    const int X = rne32(x), Y = rne32(y);
+    const int ix = X >> 5, iy = Y >> 5;
+    const float fx = i2f(X & 31) * (1.0f / 32.0f), fy = i2f(Y & 31) * (1.0f / 32.0f);
+    const float gx = 1.0f - fx, gy = 1.0f - fy;
+    const float w00 = __fmul_rn(gy, gx), w01 = __fmul_rn(gy, fx), w10 = __fmul_rn(fy, gx), w11 = __fmul_rn(fy, fx);
+    const int x0 = clampi(ix, 0, w - 1), x1 = clampi(ix + 1, 0, w - 1);
+    const size_t r0 = (size_t)clampi(iy, 0, h - 1) * w, r1 = (size_t)clampi(iy + 1, 0, h - 1) * w;
+    const float2 p00 = __ldg(F + r0 + x0), p01 = __ldg(F + r0 + x1), p10 = __ldg(F + r1 + x0), p11 = __ldg(F + r1 + x1);
+    float2 r;
+    r.x = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p00.x, w00), __fmul_rn(p01.x, w01)), __fmul_rn(p10.x, w10)), __fmul_rn(p11.x, w11));
+    r.y = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p00.y, w00), __fmul_rn(p01.y, w01)), __fmul_rn(p10.y, w10)), __fmul_rn(p11.y, w11));
+    return r;
+}
+
+// one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame: channels 0..2 of the
+// result (byte 3 = 0). Horizontal stage two channels per multiply (lanes of 16 bits hold at most 255 * 32), vertical
+// stage per channel; (v + 512) >> 10 == cv2's (32 v + 2^14) >> 15 with its 15-bit weights.
+__device__ __forceinline__ uint32_t sampleU8(const uint8_t* __restrict__ img, uint32_t pitch, int W, int H, float x, float y) {
+    const int X = rne32(x), Y = rne32(y);
+    const int ix = X >> 5, iy = Y >> 5;
+    const uint32_t fx = (uint32_t)X & 31u, fy = (uint32_t)Y & 31u;
+    uint32_t o00, o01, o10, o11;
+    if ((unsigned)ix < (unsigned)(W - 1) && (unsigned)iy < (unsigned)(H - 1)) {
+        o00 = (uint32_t)iy * pitch + (uint32_t)ix * 4u;
+        o01 = o00 + 4u;
+        o10 = o00 + pitch;
+        o11 = o10 + 4u;
+    } else {
+        const uint32_t x0 = (uint32_t)clampi(ix, 0, W - 1) * 4u, x1 = (uint32_t)clampi(ix + 1, 0, W - 1) * 4u;
+        const uint32_t r0 = (uint32_t)clampi(iy, 0, H - 1) * pitch, r1 = (uint32_t)clampi(iy + 1, 0, H - 1) * pitch;
+        o00 = r0 + x0; o01 = r0 + x1; o10 = r1 + x0; o11 = r1 + x1;
+    }
+    const uint32_t p00 = __ldg(reinterpret_cast<const uint32_t*>(img + o00));
+    const uint32_t p01 = __ldg(reinterpret_cast<const uint32_t*>(img + o01));
+    const uint32_t p10 = __ldg(reinterpret_cast<const uint32_t*>(img + o10));
+    const uint32_t p11 = __ldg(reinterpret_cast<const uint32_t*>(img + o11));
+    const uint32_t M = 0x00FF00FFu, wx0 = 32u - fx, wy0 = 32u - fy;
+    const uint32_t rb0 = (p00 & M) * wx0 + (p01 & M) * fx, rb1 = (p10 & M) * wx0 + (p11 & M) * fx;
+    const uint32_t g0 = __byte_perm(p00, 0, 0x4441) * wx0 + __byte_perm(p01, 0, 0x4441) * fx;
+    const uint32_t g1 = __byte_perm(p10, 0, 0x4441) * wx0 + __byte_perm(p11, 0, 0x4441) * fx;
+    const uint32_t c0 = ((rb0 & 0xFFFFu) * wy0 + (rb1 & 0xFFFFu) * fy + 512u) >> 10;
+    const uint32_t c2 = ((rb0 >> 16) * wy0 + (rb1 >> 16) * fy + 512u) >> 10;
+    const uint32_t c1 = (g0 * wy0 + g1 * fy + 512u) >> 10;
+    return c0 | (c1 << 8) | (c2 << 16);
+}
+
+struct SyCoef {   // one output column (or row) of the tile + halo: the upsampling taps and weights, the coordinate
+    int i0, i1;   // flow taps relative to the tile's field region
+    float a0, a1; // weights (rows: already x fs, which commutes with the rounding)
+    float pos;    // the clamped pixel coordinate as a float
+    int pi;       // ... as an int
 };
-__device__ __forceinline__ LinAxis linCoefS(int d, int n, float invfs, bool clampw) {
-    LinAxis c;
+
+__device__ __forceinline__ SyCoef syCoef(int e, int origin, int n, int un, int fn, int g0, float invfs, float fsf, bool xaxis) {
+    SyCoef c;
+    const int p = clampi(origin - kSyAp + e, 0, n - 1);
+    const int d = min(p, un - 1);   // crop [:H, :W] / edge pad of the upsampled field
     float f = __fsub_rn(__fmul_rn((float)d + 0.5f, invfs), 0.5f);   // exact for fs = 1, 2, 4
     int s = (int)floorf(f);
     f = __fsub_rn(f, (float)s);
-    if (clampw) {
+    if (xaxis) {   // cv2 resize: x weights forced to (1, 0) beyond the borders; y rows clamped, weights kept
         if (s < 0) { s = 0; f = 0.0f; }
-        if (s >= n - 1) { s = n - 1; f = 0.0f; }
+        if (s >= fn - 1) { s = fn - 1; f = 0.0f; }
     }
-    c.i0 = clampi(s, 0, n - 1);
-    c.i1 = clampi(s + 1, 0, n - 1);
-    c.a0 = 1.0f - f;
-    c.a1 = f;
+    c.i0 = clampi(s, 0, fn - 1) - g0;
+    c.i1 = clampi(s + 1, 0, fn - 1) - g0;
+    c.a0 = __fmul_rn(1.0f - f, fsf);
+    c.a1 = __fmul_rn(f, fsf);
+    c.pos = (float)p;
+    c.pi = p;
     return c;
-}
-
-// one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame, all 4 channels packed
-__device__ __forceinline__ uint32_t remapU8(const uint8_t* __restrict__ img, size_t pitch, int W, int H, float x, float y) {
-    const int X = __float2int_rn(__fmul_rn(x, 32.0f)), Y = __float2int_rn(__fmul_rn(y, 32.0f));
-    const int ix = X >> 5, iy = Y >> 5, fx = X & 31, fy = Y & 31;
-    const int x0 = clampi(ix, 0, W - 1), x1 = clampi(ix + 1, 0, W - 1);
-    const uint32_t* r0 = reinterpret_cast<const uint32_t*>(img + (size_t)clampi(iy, 0, H - 1) * pitch);
-    const uint32_t* r1 = reinterpret_cast<const uint32_t*>(img + (size_t)clampi(iy + 1, 0, H - 1) * pitch);
-    const uint32_t p00 = __ldg(r0 + x0), p01 = __ldg(r0 + x1), p10 = __ldg(r1 + x0), p11 = __ldg(r1 + x1);
-    const int w00 = (32 - fy) * (32 - fx), w01 = (32 - fy) * fx, w10 = fy * (32 - fx), w11 = fy * fx;
-    uint32_t out = 0;
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const int sh = 8 * c;
-        const int v = (int)((p00 >> sh) & 255) * w00 + (int)((p01 >> sh) & 255) * w01 + (int)((p10 >> sh) & 255) * w10 +
-                      (int)((p11 >> sh) & 255) * w11;
-        out |= (uint32_t)((v + 512) >> 10) << sh;   // == (32 v + 2^14) >> 15, cv2's 15-bit weights
-    }
-    return out;
 }
 
 __global__ void __launch_bounds__(256) k_synth(const SynthParams p) {
     extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ SyCoef colc[kSyEW], rowc[kSyEH];
+    __shared__ float TA[256], TC[256];
+    __shared__ unsigned int cnt;
+    __shared__ int gReg[4];
     const int X0 = blockIdx.x * kSyTW, Y0 = blockIdx.y * kSyTH;
     const uint8_t* nearF = p.nearC ? p.c : p.a;
+    const uint32_t pitch = (uint32_t)p.pitch;
     if (p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
         for (int i = threadIdx.x; i < kSyTW * kSyTH; i += 256) {
             const int x = X0 + (i % kSyTW), y = Y0 + (i / kSyTW);
             if (x < p.W && y < p.H)
                 reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] =
-                    __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * p.pitch) + x);
+                    __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
         }
         return;
     }
     const int fs = p.fs, uw = p.fw * fs, uh = p.fh * fs;
-    const float invfs = 1.0f / (float)fs;
-    // the flow-resolution region of the field this tile's halo touches
-    const int exLo = min(clampi(X0 - kSyAp, 0, p.W - 1), uw - 1), exHi = min(clampi(X0 + kSyTW + kSyAp - 1, 0, p.W - 1), uw - 1);
-    const int eyLo = min(clampi(Y0 - kSyAp, 0, p.H - 1), uh - 1), eyHi = min(clampi(Y0 + kSyTH + kSyAp - 1, 0, p.H - 1), uh - 1);
-    const int gx0 = linCoefS(exLo, p.fw, invfs, true).i0, gx1 = linCoefS(exHi, p.fw, invfs, true).i1;
-    const int gy0 = linCoefS(eyLo, p.fh, invfs, false).i0, gy1 = linCoefS(eyHi, p.fh, invfs, false).i1;
-    const int GW = gx1 - gx0 + 1, GH = gy1 - gy0 + 1;
-    float2* g = reinterpret_cast<float2*>(sm);                                    // GH x GW
-    uint32_t* wab = reinterpret_cast<uint32_t*>(sm + (size_t)GW * GH * 8);      // interior: wa, wc
-    uint8_t* e = reinterpret_cast<uint8_t*>(wab + 2 * kSyTW * kSyTH);           // kSyEH x kSyEW
+    const float invfs = 1.0f / (float)fs, fsf = (float)fs;
+    // 0. the field region of the tile + halo, the coefficient tables, the blend products
+    if (threadIdx.x == 0) {
+        const SyCoef lo = syCoef(0, X0, p.W, uw, p.fw, 0, invfs, 1.0f, true);
+        const SyCoef hi = syCoef(kSyEW - 1, X0, p.W, uw, p.fw, 0, invfs, 1.0f, true);
+        const SyCoef rlo = syCoef(0, Y0, p.H, uh, p.fh, 0, invfs, 1.0f, false);
+        const SyCoef rhi = syCoef(kSyEH - 1, Y0, p.H, uh, p.fh, 0, invfs, 1.0f, false);
+        gReg[0] = lo.i0; gReg[1] = hi.i1 - lo.i0 + 1; gReg[2] = rlo.i0; gReg[3] = rhi.i1 - rlo.i0 + 1;
+        cnt = 0;
+    }
+    __syncthreads();
+    const int gx0 = gReg[0], GW = gReg[1], gy0 = gReg[2], GH = gReg[3];
+    for (int i = threadIdx.x; i < kSyEW + kSyEH; i += 256) {
+        if (i < kSyEW) colc[i] = syCoef(i, X0, p.W, uw, p.fw, gx0, invfs, 1.0f, true);
+        else rowc[i - kSyEW] = syCoef(i - kSyEW, Y0, p.H, uh, p.fh, gy0, invfs, fsf, false);
+    }
+    TA[threadIdx.x] = __fmul_rn(p.wA, (float)threadIdx.x);
+    TC[threadIdx.x] = __fmul_rn(p.wC, (float)threadIdx.x);
+    float2* g = reinterpret_cast<float2*>(sm);                                     // GH x GW
+    float2* hrow = g + GW * GH;                                                    // GH x kSyEW
+    uint2* wab = reinterpret_cast<uint2*>(hrow + GH * kSyEW);                      // kSyTH x kSyTW
+    uint8_t* e = reinterpret_cast<uint8_t*>(wab + kSyTW * kSyTH);                  // kSyEH x kSyEW
     unsigned short* hsum = reinterpret_cast<unsigned short*>(e + ((kSyEH * kSyEW + 15) & ~15));   // kSyEH x kSyTW
-    __shared__ unsigned int cnt;
-    if (threadIdx.x == 0) cnt = 0;
     // 1. the field at t on the region (interp.field_at: g <- pf(q - s g), twice, from g = pf(q))
     for (int i = threadIdx.x; i < GW * GH; i += 256) {
         const int qx = gx0 + i % GW, qy = gy0 + i / GW;
@@ -665,85 +750,109 @@ __global__ void __launch_bounds__(256) k_synth(const SynthParams p) {
             const float fx = (float)qx, fy = (float)qy;
 #pragma unroll
             for (int it = 0; it < 2; it++)
-                v = remapF2(p.pf, p.fw, p.fh, __fsub_rn(fx, __fmul_rn(p.s, v.x)), __fsub_rn(fy, __fmul_rn(p.s, v.y)));
+                v = remapF2m(p.pf, p.fw, p.fh, __fsub_rn(fx, __fmul_rn(p.s, v.x)), __fsub_rn(fy, __fmul_rn(p.s, v.y)));
         }
         g[i] = v;
     }
     __syncthreads();
-    // 2. per pixel of tile + halo: half-vector, both warps, mismatch
+    // 1b. horizontal stage of the upsampling on the region's rows (cv2 resize: h = S0 a0 + S1 a1 per row)
+    for (int i = threadIdx.x; i < GH * kSyEW; i += 256) {
+        const int r = i / kSyEW, ex = i % kSyEW;
+        const SyCoef c = colc[ex];
+        const float2 s0 = g[r * GW + c.i0], s1 = g[r * GW + c.i1];
+        hrow[i] = make_float2(__fadd_rn(__fmul_rn(s0.x, c.a0), __fmul_rn(s1.x, c.a1)),
+                              __fadd_rn(__fmul_rn(s0.y, c.a0), __fmul_rn(s1.y, c.a1)));
+    }
+    __syncthreads();
+    // 2. per pixel of tile + halo: half-vector (vertical stage, x fs folded into the row weights), both warps, mismatch
     for (int i = threadIdx.x; i < kSyEW * kSyEH; i += 256) {
         const int ex = i % kSyEW, ey = i / kSyEW;
-        const int px = clampi(X0 - kSyAp + ex, 0, p.W - 1), py = clampi(Y0 - kSyAp + ey, 0, p.H - 1);
-        const LinAxis cx = linCoefS(min(px, uw - 1), p.fw, invfs, true);
-        const LinAxis cy = linCoefS(min(py, uh - 1), p.fh, invfs, false);
-        const float2 g00 = g[(cy.i0 - gy0) * GW + cx.i0 - gx0], g01 = g[(cy.i0 - gy0) * GW + cx.i1 - gx0];
-        const float2 g10 = g[(cy.i1 - gy0) * GW + cx.i0 - gx0], g11 = g[(cy.i1 - gy0) * GW + cx.i1 - gx0];
-        const float h0x = __fadd_rn(__fmul_rn(g00.x, cx.a0), __fmul_rn(g01.x, cx.a1));
-        const float h0y = __fadd_rn(__fmul_rn(g00.y, cx.a0), __fmul_rn(g01.y, cx.a1));
-        const float h1x = __fadd_rn(__fmul_rn(g10.x, cx.a0), __fmul_rn(g11.x, cx.a1));
-        const float h1y = __fadd_rn(__fmul_rn(g10.y, cx.a0), __fmul_rn(g11.y, cx.a1));
-        const float hx = __fmul_rn(__fadd_rn(__fmul_rn(h0x, cy.a0), __fmul_rn(h1x, cy.a1)), (float)fs);
-        const float hy = __fmul_rn(__fadd_rn(__fmul_rn(h0y, cy.a0), __fmul_rn(h1y, cy.a1)), (float)fs);
-        const float fpx = (float)px, fpy = (float)py;
-        float ax, ay, cxp, cyp;
+        const SyCoef cx = colc[ex], cy = rowc[ey];
+        const float2 h0 = hrow[cy.i0 * kSyEW + ex], h1 = hrow[cy.i1 * kSyEW + ex];
+        const float hx = __fadd_rn(__fmul_rn(h0.x, cy.a0), __fmul_rn(h1.x, cy.a1));
+        const float hy = __fadd_rn(__fmul_rn(h0.y, cy.a0), __fmul_rn(h1.y, cy.a1));
+        float ax, ay, bx, by;
         if (p.mid) {
-            ax = __fsub_rn(fpx, hx); ay = __fsub_rn(fpy, hy);
-            cxp = __fadd_rn(fpx, hx); cyp = __fadd_rn(fpy, hy);
+            ax = __fsub_rn(cx.pos, hx); ay = __fsub_rn(cy.pos, hy);
+            bx = __fadd_rn(cx.pos, hx); by = __fadd_rn(cy.pos, hy);
         } else {
-            ax = __fsub_rn(fpx, __fmul_rn(p.ka, hx)); ay = __fsub_rn(fpy, __fmul_rn(p.ka, hy));
-            cxp = __fadd_rn(fpx, __fmul_rn(p.kc, hx)); cyp = __fadd_rn(fpy, __fmul_rn(p.kc, hy));
+            ax = __fsub_rn(cx.pos, __fmul_rn(p.ka, hx)); ay = __fsub_rn(cy.pos, __fmul_rn(p.ka, hy));
+            bx = __fadd_rn(cx.pos, __fmul_rn(p.kc, hx)); by = __fadd_rn(cy.pos, __fmul_rn(p.kc, hy));
         }
-        const uint32_t wa = remapU8(p.a, p.pitch, p.W, p.H, ax, ay);
-        const uint32_t wc = remapU8(p.c, p.pitch, p.W, p.H, cxp, cyp);
-        const int dr = abs((int)((wa >> (8 * p.ri)) & 255) - (int)((wc >> (8 * p.ri)) & 255));
-        const int dg = abs((int)((wa >> (8 * p.gi)) & 255) - (int)((wc >> (8 * p.gi)) & 255));
-        const int db = abs((int)((wa >> (8 * p.bi)) & 255) - (int)((wc >> (8 * p.bi)) & 255));
-        e[i] = (uint8_t)max(dr, max(dg, db));
+        const uint32_t wa = sampleU8(p.a, pitch, p.W, p.H, ax, ay);
+        const uint32_t wc = sampleU8(p.c, pitch, p.W, p.H, bx, by);
+        const uint32_t d = __vabsdiffu4(wa, wc);
+        const uint32_t m = __vmaxu4(__vmaxu4(d, d >> 8), d >> 16);
+        e[i] = (uint8_t)(m & 255u);
         const int lx = ex - kSyAp, ly = ey - kSyAp;
-        if (lx >= 0 && lx < kSyTW && ly >= 0 && ly < kSyTH) {
-            wab[2 * (ly * kSyTW + lx)] = wa;
-            wab[2 * (ly * kSyTW + lx) + 1] = wc;
-        }
+        if ((unsigned)lx < (unsigned)kSyTW && (unsigned)ly < (unsigned)kSyTH) wab[ly * kSyTW + lx] = make_uint2(wa, wc);
     }
     __syncthreads();
-    // 3. horizontal 7-sums
-    for (int i = threadIdx.x; i < kSyEH * kSyTW; i += 256) {
-        const int r = i / kSyTW, c = i % kSyTW;
-        const uint8_t* q = e + r * kSyEW + c;
-        hsum[i] = (unsigned short)(q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6]);
-    }
-    __syncthreads();
-    // 4. vertical 7-sums, trust, blend
-    unsigned int myCnt = 0;
-    for (int i = threadIdx.x; i < kSyTW * kSyTH; i += 256) {
-        const int lx = i % kSyTW, ly = i / kSyTW, x = X0 + lx, y = Y0 + ly;
-        if (x >= p.W || y >= p.H) continue;
-        const unsigned short* q = hsum + ly * kSyTW + lx;
-        const int S = q[0] + q[kSyTW] + q[2 * kSyTW] + q[3 * kSyTW] + q[4 * kSyTW] + q[5 * kSyTW] + q[6 * kSyTW];
-        float u;
-        if (S <= p.sZero) u = 0.0f;
-        else if (S >= p.sOne) u = 1.0f;
-        else {
-            const float eb = (float)((double)S * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
-            u = __fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan);
-            u = fminf(fmaxf(u, 0.0f), 1.0f);
-        }
-        myCnt += u > 0.5f;
-        const uint32_t wa = wab[2 * i], wc = wab[2 * i + 1];
-        const uint32_t nq = __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * p.pitch) + x);
-        const float iu = 1.0f - u;
-        uint32_t o = nq & (0xffu << (8 * (6 - p.ri - p.gi - p.bi)));   // the near frame's alpha byte (index 6 - r - g - b)
+    // 3. horizontal 7-sums, a running window over 16 columns per item
+    for (int it = threadIdx.x; it < kSyEH * (kSyTW / 16); it += 256) {
+        const int r = it / (kSyTW / 16), c0 = (it % (kSyTW / 16)) * 16;
+        const uint8_t* q = e + r * kSyEW + c0;
+        unsigned int sum = q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6];
+        unsigned short* o = hsum + r * kSyTW + c0;
+        o[0] = (unsigned short)sum;
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const int sh = 8 * (k == 0 ? p.ri : (k == 1 ? p.gi : p.bi));
-            const float fa = (float)((wa >> sh) & 255), fc = (float)((wc >> sh) & 255), fn = (float)((nq >> sh) & 255);
-            const float mix = p.mid ? __fmul_rn(0.5f, __fadd_rn(fa, fc)) : __fadd_rn(__fmul_rn(p.wA, fa), __fmul_rn(p.wC, fc));
-            float v = __fadd_rn(__fadd_rn(__fmul_rn(mix, iu), __fmul_rn(fn, u)), 0.5f);
-            v = fminf(fmaxf(v, 0.0f), 255.0f);
-            o |= (uint32_t)(int)v << sh;
+        for (int c = 1; c < 16; c++) {
+            sum += q[c + 6] - q[c - 1];
+            o[c] = (unsigned short)sum;
         }
-        reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = o;
-        if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyEW + lx + kSyAp];
+    }
+    __syncthreads();
+    // 4. vertical 7-sums (a running window down 8 rows per thread), trust, blend, store
+    unsigned int myCnt = 0;
+    {
+        const int lx = threadIdx.x % kSyTW, ly0 = (threadIdx.x / kSyTW) * (kSyTH / 4);
+        const int x = X0 + lx;
+        const unsigned short* q = hsum + ly0 * kSyTW + lx;
+        int S = q[0] + q[kSyTW] + q[2 * kSyTW] + q[3 * kSyTW] + q[4 * kSyTW] + q[5 * kSyTW];
+        for (int k = 0; k < kSyTH / 4; k++) {
+            const int ly = ly0 + k, y = Y0 + ly;
+            S += q[(k + 6) * kSyTW];
+            const int Sk = S;
+            S -= q[k * kSyTW];
+            if (x >= p.W || y >= p.H) continue;
+            const uint2 w = wab[ly * kSyTW + lx];
+            const uint32_t nq = __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
+            uint32_t o;
+            if (Sk <= p.sZero) {   // u = 0: out = the blend rounded
+                if (p.mid) {
+                    o = __vavgu4(w.x, w.y);   // floor(0.5 (a + c) + 0.5) per byte
+                } else {
+                    o = 0;
+#pragma unroll
+                    for (int k2 = 0; k2 < 3; k2++) {
+                        const float mix = __fadd_rn(TA[(w.x >> (8 * k2)) & 255u], TC[(w.y >> (8 * k2)) & 255u]);
+                        o |= (uint32_t)floorPos(fminf(__fadd_rn(mix, 0.5f), 255.0f)) << (8 * k2);
+                    }
+                }
+            } else if (Sk >= p.sOne) {   // u = 1: the nearer frame
+                o = nq;
+                myCnt++;
+            } else {
+                const float eb = (float)((double)Sk * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
+                float u = __fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan);
+                u = fminf(fmaxf(u, 0.0f), 1.0f);
+                myCnt += u > 0.5f;
+                const float iu = 1.0f - u;
+                o = 0;
+#pragma unroll
+                for (int k2 = 0; k2 < 3; k2++) {
+                    const int sh = 8 * k2;
+                    const uint32_t ca = (w.x >> sh) & 255u, cc = (w.y >> sh) & 255u;
+                    const float fa = i2f((int)ca), fc = i2f((int)cc), fn = i2f((int)((nq >> sh) & 255u));
+                    const float mix = p.mid ? __fmul_rn(0.5f, __fadd_rn(fa, fc)) : __fadd_rn(TA[ca], TC[cc]);
+                    const float v = __fadd_rn(__fadd_rn(__fmul_rn(mix, iu), __fmul_rn(fn, u)), 0.5f);
+                    o |= (uint32_t)floorPos(fminf(fmaxf(v, 0.0f), 255.0f)) << sh;
+                }
+            }
+            o = (o & 0x00FFFFFFu) | (nq & 0xFF000000u);   // alpha (byte 3 in both pixel orders): the nearer frame's
+            reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = o;
+            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyEW + lx + kSyAp];
+        }
     }
     if (myCnt) atomicAdd(&cnt, myCnt);
     __syncthreads();
@@ -797,7 +906,7 @@ cudaError_t prepareKernels() {
     return e;
 }
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
-    const size_t tiles = (size_t)4 * (2 * kSubT * kSubT + 72) * sizeof(float);
+    const size_t tiles = (size_t)4 * kSubWarpFloats * sizeof(float);
     const size_t smem = tiles > planBytes(p.plan) ? tiles : planBytes(p.plan);
     k_subpix<<<divUp(p.bw * p.bh, 4), 128, smem, s>>>(p);
     return cudaGetLastError();
@@ -811,9 +920,10 @@ cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 size_t synthSmemBytes(int fs) {  // declared in fg_params.h
-    // worst-case field region of a tile (GW x GH float2) + interior warps + mismatch + row sums
+    // worst-case field region of a tile (GW x GH float2) + its horizontal stage + interior warps + mismatch + row sums
     const int gw = (kSyEW + fs - 1) / fs + 3, gh = (kSyEH + fs - 1) / fs + 3;
-    return (size_t)gw * gh * 8 + (size_t)2 * kSyTW * kSyTH * 4 + (size_t)((kSyEH * kSyEW + 15) & ~15) + (size_t)kSyEH * kSyTW * 2;
+    return (size_t)gw * gh * 8 + (size_t)gh * kSyEW * 8 + (size_t)kSyTW * kSyTH * 8 + (size_t)((kSyEH * kSyEW + 15) & ~15) +
+           (size_t)kSyEH * kSyTW * 2;
 }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs);
