@@ -61,6 +61,23 @@ __device__ __forceinline__ int gray8(uint32_t px, int ri, int gi, int bi) {
     return (b * 3735 + g * 19235 + r * 9798 + 16384) >> 15;
 }
 
+// Paired fp32 multiply / add (two IEEE operations per instruction). The compiler may fuse a paired multiply and add into
+// one paired FMA whatever rounding is asked for, so these are used only where every product and sum is exact (dyadic
+// operands with few significant bits): there a fused and an unfused evaluation give the same bits. Chains that round
+// (the field at t, its upsampling, the warp positions) use the scalar __fmul_rn / __fadd_rn, which are never fused.
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// round-half-even(x * 32) for |x * 32| < 2^22 (cv2's saturate_cast<int>(x * INTER_TAB_SIZE)), as the float's bits
+__device__ __forceinline__ float2 rne32bits(float2 v) {
+    return __ffma2_rn(v, make_float2(32.0f, 32.0f), make_float2(12582912.0f, 12582912.0f));
+}
+__device__ __forceinline__ int rne32(float x) { return __float_as_int(__fmaf_rn(x, 32.0f, 12582912.0f)) - 0x4B400000; }
+// exact float of 0 <= i < 2^23
+__device__ __forceinline__ float i2f(int i) { return __int_as_float(0x4B000000 | i) - 8388608.0f; }
+// floor of 0 <= v < 2^23
+__device__ __forceinline__ int floorPos(float v) { return __float_as_int(__fadd_rz(v, 8388608.0f)) - 0x4B000000; }
+
 __device__ __forceinline__ float warpSum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -76,40 +93,63 @@ __global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
     __shared__ float sl[2][1024 + 256 + 64 + 16 + 4 + 1];
     const int tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 32;
     const int fw = p.lw[0], fh = p.lh[0], fs = p.fs;
-    for (int i = threadIdx.x; i < 1024; i += 256) {
-        const int x = tx0 + (i & 31), y = ty0 + (i >> 5);
-        float va = 0.0f, vc = 0.0f;
-        if (x < fw && y < fh) {
-            int sa = 0, sc = 0, n = 0;
-            for (int j = 0; j < fs; j++) {
-                const int yy = y * fs + j;
-                if (yy >= p.H) break;
-                const uint32_t* ra = reinterpret_cast<const uint32_t*>(p.a + (size_t)yy * p.pitch);
-                const uint32_t* rc = reinterpret_cast<const uint32_t*>(p.c + (size_t)yy * p.pitch);
-                for (int k = 0; k < fs; k++) {
-                    const int xx = x * fs + k;
-                    if (xx >= p.W) break;
-                    sa += gray8(__ldg(ra + xx), p.ri, p.gi, p.bi);
-                    sc += gray8(__ldg(rc + xx), p.ri, p.gi, p.bi);
-                    n++;
-                }
-            }
-            if (fs == 1) {
-                va = (float)sa;
-                vc = (float)sc;
-            } else if (n == fs * fs) {
-                const float inv = 1.0f / (float)(fs * fs);
-                va = __fmul_rn((float)sa, inv);
-                vc = __fmul_rn((float)sc, inv);
-            } else {
-                va = __fdiv_rn((float)sa, (float)n);
-                vc = __fdiv_rn((float)sc, (float)n);
-            }
-            p.la[0][(size_t)y * fw + x] = va;
-            p.lc[0][(size_t)y * fw + x] = vc;
+    if (p.vec16 && tx0 + 32 <= fw && ty0 + 32 <= fh) {
+        // flowScale 2, 16-byte aligned rows, a full tile: thread = 4 frame pixels (one uint4) x 2 rows = 2 level-0
+        // pixels; a warp reads 2 x 256 contiguous bytes per frame and row pair
+        const int cg = threadIdx.x & 15, rp = threadIdx.x >> 4;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int ly = rp + 16 * j, y = ty0 + ly;
+            const size_t o0 = (size_t)(2 * y) * p.pitch + (size_t)(2 * tx0 + 4 * cg) * 4;
+            const uint4 a0 = __ldg(reinterpret_cast<const uint4*>(p.a + o0)), a1 = __ldg(reinterpret_cast<const uint4*>(p.a + o0 + p.pitch));
+            const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(p.c + o0)), c1 = __ldg(reinterpret_cast<const uint4*>(p.c + o0 + p.pitch));
+            const int sa0 = gray8(a0.x, p.ri, p.gi, p.bi) + gray8(a0.y, p.ri, p.gi, p.bi) + gray8(a1.x, p.ri, p.gi, p.bi) + gray8(a1.y, p.ri, p.gi, p.bi);
+            const int sa1 = gray8(a0.z, p.ri, p.gi, p.bi) + gray8(a0.w, p.ri, p.gi, p.bi) + gray8(a1.z, p.ri, p.gi, p.bi) + gray8(a1.w, p.ri, p.gi, p.bi);
+            const int sc0 = gray8(c0.x, p.ri, p.gi, p.bi) + gray8(c0.y, p.ri, p.gi, p.bi) + gray8(c1.x, p.ri, p.gi, p.bi) + gray8(c1.y, p.ri, p.gi, p.bi);
+            const int sc1 = gray8(c0.z, p.ri, p.gi, p.bi) + gray8(c0.w, p.ri, p.gi, p.bi) + gray8(c1.z, p.ri, p.gi, p.bi) + gray8(c1.w, p.ri, p.gi, p.bi);
+            // sum * 0.25 (integer sums of 4 lumas: exact)
+            const float2 va = make_float2(i2f(sa0) * 0.25f, i2f(sa1) * 0.25f), vc = make_float2(i2f(sc0) * 0.25f, i2f(sc1) * 0.25f);
+            *reinterpret_cast<float2*>(p.la[0] + (size_t)y * fw + tx0 + 2 * cg) = va;
+            *reinterpret_cast<float2*>(p.lc[0] + (size_t)y * fw + tx0 + 2 * cg) = vc;
+            sl[0][ly * 32 + 2 * cg] = va.x; sl[0][ly * 32 + 2 * cg + 1] = va.y;
+            sl[1][ly * 32 + 2 * cg] = vc.x; sl[1][ly * 32 + 2 * cg + 1] = vc.y;
         }
-        sl[0][i] = va;
-        sl[1][i] = vc;
+    } else {
+        for (int i = threadIdx.x; i < 1024; i += 256) {
+            const int x = tx0 + (i & 31), y = ty0 + (i >> 5);
+            float va = 0.0f, vc = 0.0f;
+            if (x < fw && y < fh) {
+                int sa = 0, sc = 0, n = 0;
+                for (int j = 0; j < fs; j++) {
+                    const int yy = y * fs + j;
+                    if (yy >= p.H) break;
+                    const uint32_t* ra = reinterpret_cast<const uint32_t*>(p.a + (size_t)yy * p.pitch);
+                    const uint32_t* rc = reinterpret_cast<const uint32_t*>(p.c + (size_t)yy * p.pitch);
+                    for (int k = 0; k < fs; k++) {
+                        const int xx = x * fs + k;
+                        if (xx >= p.W) break;
+                        sa += gray8(__ldg(ra + xx), p.ri, p.gi, p.bi);
+                        sc += gray8(__ldg(rc + xx), p.ri, p.gi, p.bi);
+                        n++;
+                    }
+                }
+                if (fs == 1) {
+                    va = (float)sa;
+                    vc = (float)sc;
+                } else if (n == fs * fs) {
+                    const float inv = 1.0f / (float)(fs * fs);
+                    va = __fmul_rn((float)sa, inv);
+                    vc = __fmul_rn((float)sc, inv);
+                } else {
+                    va = __fdiv_rn((float)sa, (float)n);
+                    vc = __fdiv_rn((float)sc, (float)n);
+                }
+                p.la[0][(size_t)y * fw + x] = va;
+                p.lc[0][(size_t)y * fw + x] = vc;
+            }
+            sl[0][i] = va;
+            sl[1][i] = vc;
+        }
     }
     __syncthreads();
     int off = 0, side = 32;
@@ -170,6 +210,8 @@ __global__ void __launch_bounds__(256) k_down(const DownParams p) {
 // Search: every integer offset within +-R of the seed; the (8+2R)^2 windows of a and c (bilateral: a at q - v, c at
 // q + v) are staged in shared memory; lane i scores candidates i, i+32, ...; cost = SAD + lambda |d|_1; the warp
 // keeps the lowest (cost, raster index) pair, i.e. the first minimum in interp's (dy, dx) order.
+__device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by, int lane, int& sx, int& sy);
+
 __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -179,32 +221,8 @@ __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
     float* sA = smem + warp * 2 * T * T;
     float* sC = sA + T * T;
     const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
-    int sx = 0, sy = 0;
-    if (!p.top) {
-        const int px = min(bx >> 1, p.pw - 1), py = min(by >> 1, p.ph - 1);
-        const int oy = (by & 1) ? 1 : -1, ox = (bx & 1) ? 1 : -1;
-        const int qx = b0x + (lane & 7), qy0 = b0y + (lane >> 3), qy1 = qy0 + 4;
-        float best = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            int cx = 0, cy = 0;   // own, (0, oy), (ox, 0), (ox, oy) parents x 2; zero; the global median
-            if (k < 4) {
-                const int dx = (k & 2) ? ox : 0, dy = (k & 1) ? oy : 0;
-                const float2 v = p.parent[clampi(py + dy, 0, p.ph - 1) * p.pw + clampi(px + dx, 0, p.pw - 1)];
-                cx = 2 * __float2int_rn(v.x);
-                cy = 2 * __float2int_rn(v.y);
-            } else if (k == 5) {
-                cx = __float2int_rn(p.med[0]);
-                cy = __float2int_rn(p.med[1]);
-            }
-            float s = fabsf(Lc(p.la, p.w, p.h, qx - cx, qy0 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy0 + cy));
-            s += fabsf(Lc(p.la, p.w, p.h, qx - cx, qy1 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy1 + cy));
-            s = warpSum(s);   // exact: at most 24 significant bits
-            float cost = __fmul_rn(s, 1.0f / 64.0f);
-            if (k > 0) cost = __fadd_rn(cost, p.lambda);
-            if (k == 0 || cost < best) { best = cost; sx = cx; sy = cy; }
-        }
-    }
+    int sx, sy;
+    searchSeed(p, bx, by, lane, sx, sy);
     for (int i = lane; i < T * T; i += 32) {
         const int x = i % T, y = i / T;
         sA[i] = Lc(p.la, p.w, p.h, b0x - sx - R + x, b0y - sy - R + y);
@@ -225,6 +243,131 @@ __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
         const float sad = __fmul_rn(sum, 1.0f / 64.0f);
         const float cost = __fadd_rn(sad, p.pen[abs(dx) + abs(dy)]);
         if (cost < bc) { bc = cost; bci = ci; bsad = sad; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float oc = __shfl_xor_sync(0xffffffffu, bc, o), os = __shfl_xor_sync(0xffffffffu, bsad, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bci, o);
+        if (oc < bc || (oc == bc && oi < bci)) { bc = oc; bci = oi; bsad = os; }
+    }
+    if (lane == 0) {
+        p.out[b] = make_float2((float)(sx + bci % D - R), (float)(sy + bci / D - R));
+        if (p.sadOut) p.sadOut[b] = bsad;
+    }
+}
+
+// The seed of a block (interp.seed_from :131-144 for one fine block), shared by both search kernels. A candidate equal
+// to an earlier one is skipped: its cost would equal that one's (or exceed it by lambda), so under the first-minimum
+// rule it could never be picked.
+__device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by, int lane, int& sx, int& sy) {
+    sx = 0;
+    sy = 0;
+    if (p.top) return;
+    const int b0x = bx * kBlock, b0y = by * kBlock;
+    const int px = min(bx >> 1, p.pw - 1), py = min(by >> 1, p.ph - 1);
+    const int oy = (by & 1) ? 1 : -1, ox = (bx & 1) ? 1 : -1;
+    int cxs[6], cys[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {   // own, (0, oy), (ox, 0), (ox, oy) parents x 2; zero; the global median
+        int cx = 0, cy = 0;
+        if (k < 4) {
+            const int dx = (k & 2) ? ox : 0, dy = (k & 1) ? oy : 0;
+            const float2 v = p.parent[clampi(py + dy, 0, p.ph - 1) * p.pw + clampi(px + dx, 0, p.pw - 1)];
+            cx = 2 * __float2int_rn(v.x);
+            cy = 2 * __float2int_rn(v.y);
+        } else if (k == 5) {
+            cx = __float2int_rn(p.med[0]);
+            cy = __float2int_rn(p.med[1]);
+        }
+        cxs[k] = cx;
+        cys[k] = cy;
+    }
+    const int qx = b0x + (lane & 7), qy0 = b0y + (lane >> 3), qy1 = qy0 + 4;
+    float best = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        bool dup = false;
+#pragma unroll
+        for (int j = 0; j < k; j++) dup |= cxs[j] == cxs[k] && cys[j] == cys[k];
+        if (dup) continue;   // warp-uniform
+        const int cx = cxs[k], cy = cys[k];
+        float s;
+        if (b0x - abs(cx) >= 0 && b0x + 7 + abs(cx) < p.w && b0y - abs(cy) >= 0 && b0y + 7 + abs(cy) < p.h) {
+            const float* ra = p.la + (size_t)(qy0 - cy) * p.w + (qx - cx);
+            const float* rc = p.lc + (size_t)(qy0 + cy) * p.w + (qx + cx);
+            s = fabsf(__ldg(ra) - __ldg(rc)) + fabsf(__ldg(ra + 4 * p.w) - __ldg(rc + 4 * p.w));
+        } else {
+            s = fabsf(Lc(p.la, p.w, p.h, qx - cx, qy0 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy0 + cy));
+            s += fabsf(Lc(p.la, p.w, p.h, qx - cx, qy1 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy1 + cy));
+        }
+        s = warpSum(s);   // exact: at most 24 significant bits
+        float cost = __fmul_rn(s, 1.0f / 64.0f);
+        if (k > 0) cost = __fadd_rn(cost, p.lambda);
+        if (k == 0 || cost < best) { best = cost; sx = cx; sy = cy; }
+    }
+}
+
+// interp.search at integer steps, radius R known at compile time (1..6), one warp per 8x8 block. The (8+2R)^2 windows
+// of a and c are staged in shared memory. Lane = (dy, block row y): it holds a's row y - dy and c's row y + dy in
+// registers and scores every dx from them; the 8 rows of a dy are summed by shuffles (all sums exact).
+template <int R>
+__global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
+    constexpr int T = 8 + 2 * R, D = 2 * R + 1, NI = 8 * D, ROUNDS = (NI + 31) / 32;
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * 4 + warp;
+    if (b >= p.bw * p.bh) return;
+    float* sA = smem + warp * (2 * T * T + D * D);
+    float* sC = sA + T * T;
+    float* sad = sC + T * T;   // D x D window SADs (sums over the 64 pixels)
+    const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
+    int sx, sy;
+    searchSeed(p, bx, by, lane, sx, sy);
+    const int ax0 = b0x - sx - R, ay0 = b0y - sy - R, cx0 = b0x + sx - R, cy0 = b0y + sy - R;
+    if (ax0 >= 0 && ay0 >= 0 && ax0 + T <= p.w && ay0 + T <= p.h && cx0 >= 0 && cy0 >= 0 && cx0 + T <= p.w && cy0 + T <= p.h) {
+        for (int i = lane; i < T * T; i += 32) {
+            const int x = i % T, y = i / T;
+            sA[i] = __ldg(p.la + (size_t)(ay0 + y) * p.w + ax0 + x);
+            sC[i] = __ldg(p.lc + (size_t)(cy0 + y) * p.w + cx0 + x);
+        }
+    } else {
+        for (int i = lane; i < T * T; i += 32) {
+            const int x = i % T, y = i / T;
+            sA[i] = Lc(p.la, p.w, p.h, ax0 + x, ay0 + y);
+            sC[i] = Lc(p.lc, p.w, p.h, cx0 + x, cy0 + y);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int rd = 0; rd < ROUNDS; rd++) {
+        const int it = rd * 32 + lane;
+        const bool act = it < NI;
+        const int dyi = act ? (it >> 3) : 0, y = it & 7, dy = dyi - R;
+        const float* ra = sA + (y - dy + R) * T;
+        const float* rc = sC + (y + dy + R) * T;
+        float a[T], c[T];
+#pragma unroll
+        for (int i = 0; i < T; i++) { a[i] = ra[i]; c[i] = rc[i]; }
+#pragma unroll
+        for (int dxi = 0; dxi < D; dxi++) {
+            const int dx = dxi - R;
+            float sum = 0.0f;
+#pragma unroll
+            for (int x = 0; x < 8; x++) sum += fabsf(a[x - dx + R] - c[x + dx + R]);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+            if (act && y == 0) sad[dyi * D + dxi] = sum;
+        }
+    }
+    __syncwarp();
+    float bc = FLT_MAX, bsad = 0.0f;
+    int bci = 0x7fffffff;
+    for (int ci = lane; ci < D * D; ci += 32) {
+        const int dx = ci % D - R, dy = ci / D - R;
+        const float sd = __fmul_rn(sad[ci], 1.0f / 64.0f);
+        const float cost = __fadd_rn(sd, p.pen[abs(dx) + abs(dy)]);
+        if (cost < bc) { bc = cost; bci = ci; bsad = sd; }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -409,7 +552,7 @@ __global__ void __launch_bounds__(256) k_cutmean(const CutMeanParams p) {
 // multiples of 1/4: every product and sum is exact, so it equals cv2's bilinear tap), after which a candidate's SAD is
 // two shared loads per pixel. The last CTA computes the scene-cut mean of the winners' SADs.
 constexpr int kSubT = 13, kSubO = 2, kSubL = 24, kSubRows = 10;   // tile, its margin, lattice side, tile rows used
-constexpr int kSubWarpFloats = 2 * kSubT * kSubT + 2 * kSubRows * kSubL + 2 * kSubL * kSubL + 72;
+constexpr int kSubWarpFloats = 2 * kSubT * kSubT + 2 * kSubRows * kSubL + 72;
 
 __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
     extern __shared__ float smem[];
@@ -421,11 +564,8 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
     if (b < nb) {
         float* tA = smem + warp * kSubWarpFloats;
         float* tC = tA + kSubT * kSubT;
-        float* hA = tC + kSubT * kSubT;      // kSubRows x kSubL: tile rows 1..10 sampled at the lattice columns
-        float* hC = hA + kSubRows * kSubL;
-        float* qA = hC + kSubRows * kSubL;   // kSubL x kSubL lattice
-        float* qC = qA + kSubL * kSubL;
-        float* rows = qC + kSubL * kSubL;
+        float2* H = reinterpret_cast<float2*>(tC + kSubT * kSubT);   // kSubRows x kSubL: (a, c) at tile rows 1..10
+        float* rows = reinterpret_cast<float*>(H + kSubRows * kSubL);
         const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
         const float2 v0 = p.in[b];
         const int sx = __float2int_rn(v0.x), sy = __float2int_rn(v0.y);
@@ -435,41 +575,57 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
             tC[i] = Lc(p.lc, p.w, p.h, b0x + sx - kSubO + x, b0y + sy - kSubO + y);
         }
         __syncwarp();
+        // lane constants: lattice column u = 3 x + (d + 1) (lanes 24..31 only help with the reductions)
+        const int u = lane < kSubL ? lane : kSubL - 1, ux = u / 3, ud = u % 3 - 1;
         int b4x = 0, b4y = 0;   // the offset chosen so far, quarter pixels
         float sadBest = 0.0f;
         for (int pass = 0; pass < 2; pass++) {
             const int s4 = pass ? 1 : 2;
-            // horizontal stage: a at tile x + 2 - o, c at x + 2 + o, o = (b4x + s4 d) / 4, lattice column u = 3x + d + 1
-            for (int it = lane; it < kSubRows * kSubL; it += 32) {
-                const int r = it / kSubL + 1, u = it % kSubL, x = u / 3, d = u % 3 - 1;
-                const int PA = 4 * (x + kSubO) - (b4x + s4 * d), PC = 4 * (x + kSubO) + (b4x + s4 * d);
-                const float fa = (float)(PA & 3) * 0.25f, fc = (float)(PC & 3) * 0.25f;
-                const float* ra = tA + r * kSubT + (PA >> 2);
-                const float* rc = tC + r * kSubT + (PC >> 2);
-                hA[it] = __fmaf_rn(ra[1], fa, __fmul_rn(ra[0], 1.0f - fa));   // exact: dyadic, <= 16 significant bits
-                hC[it] = __fmaf_rn(rc[1], fc, __fmul_rn(rc[0], 1.0f - fc));
-            }
-            __syncwarp();
-            // vertical stage: lattice row v = 3y + d + 1
-            for (int it = lane; it < kSubL * kSubL; it += 32) {
-                const int v = it / kSubL, u = it % kSubL, y = v / 3, d = v % 3 - 1;
-                const int PA = 4 * (y + kSubO) - (b4y + s4 * d), PC = 4 * (y + kSubO) + (b4y + s4 * d);
-                const float fa = (float)(PA & 3) * 0.25f, fc = (float)(PC & 3) * 0.25f;
-                const float* ca = hA + ((PA >> 2) - 1) * kSubL + u;
-                const float* cc = hC + ((PC >> 2) - 1) * kSubL + u;
-                qA[it] = __fmaf_rn(ca[kSubL], fa, __fmul_rn(ca[0], 1.0f - fa));
-                qC[it] = __fmaf_rn(cc[kSubL], fc, __fmul_rn(cc[0], 1.0f - fc));
-            }
-            __syncwarp();
-            // (candidate, row) partial sums: candidate k = (dy + 1) * 3 + (dx + 1)
-            for (int it = lane; it < 72; it += 32) {
-                const int k = it >> 3, y = it & 7, dx = k % 3, dy = k / 3;
-                const float* ra = qA + (3 * y + dy) * kSubL + dx;
-                const float* rc = qC + (3 * y + dy) * kSubL + dx;
-                float sum = 0.0f;
+            if (lane < kSubL) {
+                // horizontal stage of column u: a at tile column x + 2 - o, c at x + 2 + o, o = (b4x + s4 d) / 4
+                const int oA = 4 * (ux + kSubO) - (b4x + s4 * ud), oC = 4 * (ux + kSubO) + (b4x + s4 * ud);
+                const float fA = (float)(oA & 3) * 0.25f, fC = (float)(oC & 3) * 0.25f;
+                const float2 w0 = make_float2(1.0f - fA, 1.0f - fC), w1 = make_float2(fA, fC);
+                const float* ra = tA + kSubT + (oA >> 2);
+                const float* rc = tC + kSubT + (oC >> 2);
 #pragma unroll
-                for (int x = 0; x < 8; x++) sum += fabsf(ra[3 * x] - rc[3 * x]);
-                rows[it] = sum;
+                for (int r = 0; r < kSubRows; r++) {   // exact: dyadic values, <= 16 significant bits
+                    const float2 s0 = make_float2(ra[r * kSubT], rc[r * kSubT]), s1 = make_float2(ra[r * kSubT + 1], rc[r * kSubT + 1]);
+                    H[r * kSubL + u] = __ffma2_rn(s1, w1, pmul(s0, w0));
+                }
+            }
+            __syncwarp();
+            if (lane < kSubL) {
+                // vertical stage fused with the SADs: lattice row v = 3 y + (d + 1) reads the horizontal rows
+                // y + rA[d] and y + rA[d] + 1 (rA in {0, 1}); lane u = 3 x + (dx + 1) adds |a - c| of pixel (x, y)
+                // to candidate (dx, d - 1) for every y
+                int rA[3], rC[3];
+                float2 w0[3], w1[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int oA = -(b4y + s4 * (d - 1)), oC = b4y + s4 * (d - 1);
+                    const float fA = (float)(oA & 3) * 0.25f, fC = (float)(oC & 3) * 0.25f;
+                    rA[d] = 1 + (oA >> 2);
+                    rC[d] = 1 + (oC >> 2);
+                    w0[d] = make_float2(1.0f - fA, 1.0f - fC);
+                    w1[d] = make_float2(fA, fC);
+                }
+                float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+#pragma unroll
+                for (int y = 0; y < 8; y++) {
+                    const float2 r0 = H[y * kSubL + u], r1 = H[(y + 1) * kSubL + u], r2 = H[(y + 2) * kSubL + u];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        const float2 ta = rA[d] ? r1 : r0, tb = rA[d] ? r2 : r1;   // a rows
+                        const float2 tc = rC[d] ? r1 : r0, td = rC[d] ? r2 : r1;   // c rows
+                        const float2 q = __ffma2_rn(make_float2(tb.x, td.y), w1[d], pmul(make_float2(ta.x, tc.y), w0[d]));
+                        const float dd = fabsf(q.x - q.y);
+                        if (d == 0) acc0 += dd; else if (d == 1) acc1 += dd; else acc2 += dd;
+                    }
+                }
+                rows[(0 * 3 + ud + 1) * 8 + ux] = acc0;
+                rows[(1 * 3 + ud + 1) * 8 + ux] = acc1;
+                rows[(2 * 3 + ud + 1) * 8 + ux] = acc2;
             }
             __syncwarp();
             float cost = FLT_MAX, sad = 0.0f;
@@ -512,97 +668,175 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
 
 // ============================================================================================== per-pixel field
 // interp.pixel_field :167-183 at flow resolution. Candidates per pixel: the bilinear block field (cv2.resize x8,
-// INTER_LINEAR), the own block, the blocks above / below / left / right (edge-clamped), zero. Each candidate's cost
-// is the 5x5 replicate-border box of |a(q - h) - c(q + h)| where every window pixel uses its own candidate (cv2.blur
-// over the per-candidate error image). Tile 32x16 + 2 px apron; the errors are exact multiples of 2^-14, so they
-// are summed as int32 and the mean is formed in double as cv2's box filter does (sum * (1/25), then to float).
-constexpr int kPfTW = 32, kPfTH = 16, kPfAp = 2, kPfEW = kPfTW + 2 * kPfAp, kPfEH = kPfTH + 2 * kPfAp, kPfNC = 7;
+// INTER_LINEAR), the own block, the blocks above / below / left / right (edge-clamped), zero. Each candidate's cost is
+// the 5x5 replicate-border box of |a(q - h) - c(q + h)| where every window pixel uses its own candidate (cv2.blur over
+// the per-candidate error image). One CTA = a 64 x 32 region (60 x 28 outputs + a 2 px apron), one candidate at a
+// time through one error plane. A vector h enters the taps only through R = rne(32 h): cv2 samples a at 32 q - R and c
+// at 32 q + R (1/32 units; q - h is exact in float here). The taps are exact (dyadic luma, integer weights), the errors
+// are exact multiples of 2^-14 summed as int32, and the mean is formed as cv2's box filter does: (S 2^-14) * (1/25) in
+// double, then to float.
+constexpr int kPfE = 64, kPfEH = 32, kPfAp = 2, kPfTW = kPfE - 2 * kPfAp, kPfTH = kPfEH - 2 * kPfAp, kPfNC = 7;
+constexpr int kPfK = kPfEH / 4;                  // region rows per thread
+constexpr int kPfBX = kPfE / 8 + 3, kPfBY = kPfEH / 8 + 3;   // block-field region (with the +-1 neighbours)
 
-__device__ __forceinline__ float2 blockV(const float2* __restrict__ v, int bw, int bh, int bx, int by) {
-    return __ldg(v + clampi(by, 0, bh - 1) * bw + clampi(bx, 0, bw - 1));
-}
-
-// cv2.resize INTER_LINEAR coefficient along one axis for a x8 upscale; clampw: the x rule (weights (1, 0) beyond the
-// border), else the y rule (rows clamped, weights kept)
-__device__ __forceinline__ void linCoef8(int d, int n, bool clampw, int& i0, int& i1, float& a0, float& a1) {
-    float f = __fsub_rn(__fmul_rn((float)d + 0.5f, 0.125f), 0.5f);
-    int s = (int)floorf(f);
-    f = __fsub_rn(f, (float)s);
-    if (clampw) {
-        if (s < 0) { s = 0; f = 0.0f; }
-        if (s >= n - 1) { s = n - 1; f = 0.0f; }
+// one luma tap at 1/32 position (X, Y) of both frames at once: (a at (XA, YA), c at (XC, YC)); returns 1024 x the tap
+__device__ __forceinline__ float2 tapPair(const float* __restrict__ ya, const float* __restrict__ yc, int w, int h,
+                                          int XA, int YA, int XC, int YC) {
+    const int iax = XA >> 5, iay = YA >> 5, icx = XC >> 5, icy = YC >> 5;
+    float2 p00, p01, p10, p11;
+    if ((unsigned)iax < (unsigned)(w - 1) && (unsigned)iay < (unsigned)(h - 1) && (unsigned)icx < (unsigned)(w - 1) &&
+        (unsigned)icy < (unsigned)(h - 1)) {
+        const float* qa = ya + iay * w + iax;
+        const float* qc = yc + icy * w + icx;
+        p00 = make_float2(__ldg(qa), __ldg(qc));
+        p01 = make_float2(__ldg(qa + 1), __ldg(qc + 1));
+        p10 = make_float2(__ldg(qa + w), __ldg(qc + w));
+        p11 = make_float2(__ldg(qa + w + 1), __ldg(qc + w + 1));
+    } else {
+        const int ax0 = clampi(iax, 0, w - 1), ax1 = clampi(iax + 1, 0, w - 1), ay0 = clampi(iay, 0, h - 1) * w, ay1 = clampi(iay + 1, 0, h - 1) * w;
+        const int cx0 = clampi(icx, 0, w - 1), cx1 = clampi(icx + 1, 0, w - 1), cy0 = clampi(icy, 0, h - 1) * w, cy1 = clampi(icy + 1, 0, h - 1) * w;
+        p00 = make_float2(__ldg(ya + ay0 + ax0), __ldg(yc + cy0 + cx0));
+        p01 = make_float2(__ldg(ya + ay0 + ax1), __ldg(yc + cy0 + cx1));
+        p10 = make_float2(__ldg(ya + ay1 + ax0), __ldg(yc + cy1 + cx0));
+        p11 = make_float2(__ldg(ya + ay1 + ax1), __ldg(yc + cy1 + cx1));
     }
-    i0 = clampi(s, 0, n - 1);
-    i1 = clampi(s + 1, 0, n - 1);
-    a0 = 1.0f - f;
-    a1 = f;
-}
-
-__device__ __forceinline__ float2 pfCand(const PixfieldParams& p, int k, int qx, int qy) {
-    const int bx = qx >> 3, by = qy >> 3;
-    switch (k) {
-        case 0: {
-            int x0, x1, y0, y1;
-            float a0, a1, b0, b1;
-            linCoef8(qx, p.bw, true, x0, x1, a0, a1);
-            linCoef8(qy, p.bh, false, y0, y1, b0, b1);
-            const float2 v00 = blockV(p.v, p.bw, p.bh, x0, y0), v01 = blockV(p.v, p.bw, p.bh, x1, y0);
-            const float2 v10 = blockV(p.v, p.bw, p.bh, x0, y1), v11 = blockV(p.v, p.bw, p.bh, x1, y1);
-            const float h0x = __fadd_rn(__fmul_rn(v00.x, a0), __fmul_rn(v01.x, a1)), h0y = __fadd_rn(__fmul_rn(v00.y, a0), __fmul_rn(v01.y, a1));
-            const float h1x = __fadd_rn(__fmul_rn(v10.x, a0), __fmul_rn(v11.x, a1)), h1y = __fadd_rn(__fmul_rn(v10.y, a0), __fmul_rn(v11.y, a1));
-            return make_float2(__fadd_rn(__fmul_rn(h0x, b0), __fmul_rn(h1x, b1)), __fadd_rn(__fmul_rn(h0y, b0), __fmul_rn(h1y, b1)));
-        }
-        case 1: return blockV(p.v, p.bw, p.bh, bx, by);
-        case 2: return blockV(p.v, p.bw, p.bh, bx, by - 1);
-        case 3: return blockV(p.v, p.bw, p.bh, bx, by + 1);
-        case 4: return blockV(p.v, p.bw, p.bh, bx - 1, by);
-        case 5: return blockV(p.v, p.bw, p.bh, bx + 1, by);
-        default: return make_float2(0.0f, 0.0f);
-    }
+    const float2 wx1 = make_float2(i2f(XA & 31), i2f(XC & 31)), wy1 = make_float2(i2f(YA & 31), i2f(YC & 31));
+    const float2 wx0 = padd(make_float2(32.0f, 32.0f), make_float2(-wx1.x, -wx1.y));
+    const float2 wy0 = padd(make_float2(32.0f, 32.0f), make_float2(-wy1.x, -wy1.y));
+    // exact: luma (dyadic, <= 10 significant bits) x integer weights <= 32 per stage
+    const float2 h0 = __ffma2_rn(p01, wx1, pmul(p00, wx0));
+    const float2 h1 = __ffma2_rn(p11, wx1, pmul(p10, wx0));
+    return __ffma2_rn(h1, wy1, pmul(h0, wy0));
 }
 
 __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
-    __shared__ int err[kPfNC][kPfEH * kPfEW];
-    __shared__ int hs[kPfNC][kPfEH * kPfTW];
-    const int tx0 = blockIdx.x * kPfTW - kPfAp, ty0 = blockIdx.y * kPfTH - kPfAp;
-    for (int i = threadIdx.x; i < kPfEH * kPfEW; i += 256) {
-        const int qx = clampi(tx0 + i % kPfEW, 0, p.w - 1), qy = clampi(ty0 + i / kPfEW, 0, p.h - 1);
-        const float fx = (float)qx, fy = (float)qy;
-#pragma unroll
-        for (int k = 0; k < kPfNC; k++) {
-            const float2 v = pfCand(p, k, qx, qy);
-            const float e = fabsf(remapF(p.ya, p.w, p.h, __fsub_rn(fx, v.x), __fsub_rn(fy, v.y)) -
-                                  remapF(p.yc, p.w, p.h, __fadd_rn(fx, v.x), __fadd_rn(fy, v.y)));
-            err[k][i] = __float2int_rn(__fmul_rn(e, 16384.0f));
-        }
+    __shared__ int plane[kPfEH][kPfE];
+    __shared__ int hs[kPfEH][kPfE];
+    __shared__ float2 bv[kPfBY][kPfBX];
+    __shared__ int2 bR[kPfBY][kPfBX];
+    __shared__ float4 rowc[kPfEH];   // bilinear candidate, y: (row0, row1 relative to the block region, weights)
+    const int tid = threadIdx.x, ex = tid & (kPfE - 1), ey0 = tid >> 6;
+    const int X0 = blockIdx.x * kPfTW, Y0 = blockIdx.y * kPfTH;
+    // the block-field region: every block a region pixel's candidates can name
+    const int qx0 = clampi(X0 - kPfAp, 0, p.w - 1), qy0 = clampi(Y0 - kPfAp, 0, p.h - 1);
+    const int bx0 = max((qx0 >> 3) - 1, 0), by0 = max((qy0 >> 3) - 1, 0);
+    for (int i = tid; i < kPfBX * kPfBY; i += 256) {
+        const int bx = min(bx0 + i % kPfBX, p.bw - 1), by = min(by0 + i / kPfBX, p.bh - 1);
+        const float2 v = __ldg(p.v + by * p.bw + bx);
+        bv[i / kPfBX][i % kPfBX] = v;
+        const float2 r = rne32bits(v);
+        bR[i / kPfBX][i % kPfBX] = make_int2(__float_as_int(r.x) - 0x4B400000, __float_as_int(r.y) - 0x4B400000);
+    }
+    // cv2.resize x8 coefficients: x per thread column (weights (1, 0) beyond the borders), y per region row (rows
+    // clamped, weights kept)
+    const int qx = clampi(X0 - kPfAp + ex, 0, p.w - 1);
+    int cx0, cx1;
+    float ca0, ca1;
+    {
+        float f = __fsub_rn(__fmul_rn((float)qx + 0.5f, 0.125f), 0.5f);
+        int sft = (int)floorf(f);
+        f = __fsub_rn(f, (float)sft);
+        if (sft < 0) { sft = 0; f = 0.0f; }
+        if (sft >= p.bw - 1) { sft = p.bw - 1; f = 0.0f; }
+        cx0 = clampi(sft, 0, p.bw - 1) - bx0;
+        cx1 = clampi(sft + 1, 0, p.bw - 1) - bx0;
+        ca0 = 1.0f - f;
+        ca1 = f;
+    }
+    if (tid < kPfEH) {
+        const int qy = clampi(Y0 - kPfAp + tid, 0, p.h - 1);
+        float f = __fsub_rn(__fmul_rn((float)qy + 0.5f, 0.125f), 0.5f);
+        const int sft = (int)floorf(f);
+        f = __fsub_rn(f, (float)sft);
+        rowc[tid] = make_float4(__int_as_float(clampi(sft, 0, p.bh - 1) - by0), __int_as_float(clampi(sft + 1, 0, p.bh - 1) - by0),
+                                1.0f - f, f);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kPfEH * kPfTW; i += 256) {
-        const int r = i / kPfTW, c = i % kPfTW;
+    const int bxq = (qx >> 3) - bx0;   // this column's block in the region
+    const int qx32 = 32 * qx;
+    float best[kPfK];
+    int bestk[kPfK];
+    const double C = 0x1p-14 * (1.0 / 25.0);   // cv2's box scale with the 2^-14 units folded in (exact scaling)
+    for (int k = 0; k < kPfNC; k++) {
+        // 1. candidate k's error at this thread's region pixels
 #pragma unroll
-        for (int k = 0; k < kPfNC; k++) {
-            const int* e = err[k] + r * kPfEW + c;
-            hs[k][i] = e[0] + e[1] + e[2] + e[3] + e[4];
+        for (int j = 0; j < kPfK; j++) {
+            const int ey = ey0 + 4 * j;
+            const int qy = clampi(Y0 - kPfAp + ey, 0, p.h - 1);
+            int2 R;
+            if (k == 0) {
+                const float4 ry = rowc[ey];
+                const int r0 = __float_as_int(ry.x), r1 = __float_as_int(ry.y);
+                const float2 h0 = padd(pmul(bv[r0][cx0], make_float2(ca0, ca0)), pmul(bv[r0][cx1], make_float2(ca1, ca1)));
+                const float2 h1 = padd(pmul(bv[r1][cx0], make_float2(ca0, ca0)), pmul(bv[r1][cx1], make_float2(ca1, ca1)));
+                const float2 r = rne32bits(padd(pmul(h0, make_float2(ry.z, ry.z)), pmul(h1, make_float2(ry.w, ry.w))));
+                R = make_int2(__float_as_int(r.x) - 0x4B400000, __float_as_int(r.y) - 0x4B400000);
+            } else if (k == kPfNC - 1) {
+                R = make_int2(0, 0);
+            } else {
+                const int byq = (qy >> 3) - by0;
+                const int dx = k == 4 ? -1 : (k == 5 ? 1 : 0), dy = k == 2 ? -1 : (k == 3 ? 1 : 0);
+                const int bx = clampi((qx >> 3) + dx, 0, p.bw - 1) - bx0, by = clampi((qy >> 3) + dy, 0, p.bh - 1) - by0;
+                R = bR[by][bx];
+                (void)byq;
+            }
+            const int qy32 = 32 * qy;
+            const float2 t = tapPair(p.ya, p.yc, p.w, p.h, qx32 - R.x, qy32 - R.y, qx32 + R.x, qy32 + R.y);
+            plane[ey][ex] = __float_as_int(__fmaf_rn(fabsf(t.x - t.y), 16.0f, 12582912.0f)) - 0x4B400000;   // E * 2^14
+        }
+        __syncthreads();
+        // 2. horizontal 5-sums: one region row, 8 output columns per thread (a running window)
+        {
+            const int r = tid >> 3, c0 = (tid & 7) * 8;
+            const int* q = &plane[r][c0];
+            int sum = q[0] + q[1] + q[2] + q[3] + q[4];
+            hs[r][c0] = sum;
+#pragma unroll
+            for (int c = 1; c < 8; c++) {
+                if (c0 + c + 4 < kPfE) sum += q[c + 4] - q[c - 1];
+                hs[r][c0 + c] = sum;
+            }
+        }
+        __syncthreads();
+        // 3. vertical 5-sums, the cost, the running first minimum
+        const int lx = ex - kPfAp;
+        if ((unsigned)lx < (unsigned)kPfTW) {
+#pragma unroll
+            for (int j = 0; j < kPfK; j++) {
+                const int ly = ey0 + 4 * j - kPfAp;
+                if ((unsigned)ly >= (unsigned)kPfTH) continue;
+                const int S = hs[ly][lx] + hs[ly + 1][lx] + hs[ly + 2][lx] + hs[ly + 3][lx] + hs[ly + 4][lx];
+                float c = (float)(__dadd_rn(__hiloint2double(0x43300000, S), -4503599627370496.0) * C);
+                if (k == 0) c = __fsub_rn(c, p.smooth);
+                if (k == kPfNC - 1) c = __fsub_rn(c, p.zero);
+                if (k == 0 || c < best[j]) { best[j] = c; bestk[j] = k; }
+            }
         }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kPfTW * kPfTH; i += 256) {
-        const int lx = i % kPfTW, ly = i / kPfTW;
-        const int qx = blockIdx.x * kPfTW + lx, qy = blockIdx.y * kPfTH + ly;
-        if (qx >= p.w || qy >= p.h) continue;
-        float best = 0.0f;
-        int bk = 0;
+    // 4. the chosen candidate's vector
+    const int lx = ex - kPfAp, x = X0 + lx;
+    if ((unsigned)lx >= (unsigned)kPfTW || x >= p.w) return;
 #pragma unroll
-        for (int k = 0; k < kPfNC; k++) {
-            const int* h = hs[k] + ly * kPfTW + lx;
-            const int S = h[0] + h[kPfTW] + h[2 * kPfTW] + h[3 * kPfTW] + h[4 * kPfTW];
-            float c = (float)(((double)S * 0x1p-14) * (1.0 / 25.0));
-            if (k == 0) c = __fsub_rn(c, p.smooth);
-            if (k == kPfNC - 1) c = __fsub_rn(c, p.zero);
-            if (k == 0 || c < best) { best = c; bk = k; }
+    for (int j = 0; j < kPfK; j++) {
+        const int ey = ey0 + 4 * j, ly = ey - kPfAp, y = Y0 + ly;
+        if ((unsigned)ly >= (unsigned)kPfTH || y >= p.h) continue;
+        const int k = bestk[j];
+        float2 v;
+        if (k == 0) {
+            const float4 ry = rowc[ey];
+            const int r0 = __float_as_int(ry.x), r1 = __float_as_int(ry.y);
+            const float2 h0 = padd(pmul(bv[r0][cx0], make_float2(ca0, ca0)), pmul(bv[r0][cx1], make_float2(ca1, ca1)));
+            const float2 h1 = padd(pmul(bv[r1][cx0], make_float2(ca0, ca0)), pmul(bv[r1][cx1], make_float2(ca1, ca1)));
+            v = padd(pmul(h0, make_float2(ry.z, ry.z)), pmul(h1, make_float2(ry.w, ry.w)));
+        } else if (k == kPfNC - 1) {
+            v = make_float2(0.0f, 0.0f);
+        } else {
+            const int dx = k == 4 ? -1 : (k == 5 ? 1 : 0), dy = k == 2 ? -1 : (k == 3 ? 1 : 0);
+            v = bv[clampi((y >> 3) + dy, 0, p.bh - 1) - by0][clampi((x >> 3) + dx, 0, p.bw - 1) - bx0];
         }
-        p.pf[(size_t)qy * p.w + qx] = pfCand(p, bk, qx, qy);
+        p.pf[(size_t)y * p.w + x] = v;
     }
+    (void)bxq;
 }
 
 // ============================================================================================== synthesis
@@ -616,53 +850,51 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
 // Float <-> int conversions run on the FP32 pipe (magic-number additions, exact in the ranges used here) rather than
 // the conversion units; the bilinear taps run two channels per 32-bit multiply (R|B lanes, G) and the mismatch and the
 // t = 0.5 blend use byte-SIMD instructions.
-constexpr int kSyTW = 64, kSyTH = 32, kSyAp = 3, kSyEW = kSyTW + 2 * kSyAp, kSyEH = kSyTH + 2 * kSyAp;
+constexpr int kSyE = 128, kSyEH = 32, kSyAp = 3;                 // 128 x 32 mismatch region -> 122 x 26 output tile
+constexpr int kSyT = kSyE - 2 * kSyAp, kSyTH = kSyEH - 2 * kSyAp;
+constexpr int kSyThreads = 512, kSyK = kSyEH / (kSyThreads / kSyE);   // region rows per thread (512 = 128 columns x 4)
 
-// round-half-even(x * 32) for |x * 32| < 2^22 (cv2's saturate_cast<int>(x * INTER_TAB_SIZE))
-__device__ __forceinline__ int rne32(float x) { return __float_as_int(__fmaf_rn(x, 32.0f, 12582912.0f)) - 0x4B400000; }
-// exact float of 0 <= i < 2^23
-__device__ __forceinline__ float i2f(int i) { return __int_as_float(0x4B000000 | i) - 8388608.0f; }
-// floor of 0 <= v < 2^23
-__device__ __forceinline__ int floorPos(float v) { return __float_as_int(__fadd_rz(v, 8388608.0f)) - 0x4B000000; }
-
-// cv2.remap INTER_LINEAR / BORDER_REPLICATE of the 2-channel float field, conversions on the FP32 pipe
+// cv2.remap INTER_LINEAR / BORDER_REPLICATE of the 2-channel float field at (x, y): quantisation and weights paired
+// (exact), the taps' weighted sum as cv2 rounds it, ((p00 w00 + p01 w01) + p10 w10) + p11 w11 per channel
 __device__ __forceinline__ float2 remapF2m(const float2* __restrict__ F, int w, int h, float x, float y) {
-    const int X = rne32(x), Y = rne32(y);
+    const float2 bits = rne32bits(make_float2(x, y));
+    const int X = __float_as_int(bits.x) - 0x4B400000, Y = __float_as_int(bits.y) - 0x4B400000;
     const int ix = X >> 5, iy = Y >> 5;
-    const float fx = i2f(X & 31) * (1.0f / 32.0f), fy = i2f(Y & 31) * (1.0f / 32.0f);
-    const float gx = 1.0f - fx, gy = 1.0f - fy;
-    const float w00 = __fmul_rn(gy, gx), w01 = __fmul_rn(gy, fx), w10 = __fmul_rn(fy, gx), w11 = __fmul_rn(fy, fx);
+    const float2 f = pmul(make_float2(i2f(X & 31), i2f(Y & 31)), make_float2(1.0f / 32.0f, 1.0f / 32.0f));
+    const float2 g = padd(make_float2(1.0f, 1.0f), make_float2(-f.x, -f.y));
+    const float2 wA = pmul(make_float2(g.y, g.y), make_float2(g.x, f.x));   // (w00, w01)
+    const float2 wB = pmul(make_float2(f.y, f.y), make_float2(g.x, f.x));   // (w10, w11)
     const int x0 = clampi(ix, 0, w - 1), x1 = clampi(ix + 1, 0, w - 1);
     const size_t r0 = (size_t)clampi(iy, 0, h - 1) * w, r1 = (size_t)clampi(iy + 1, 0, h - 1) * w;
     const float2 p00 = __ldg(F + r0 + x0), p01 = __ldg(F + r0 + x1), p10 = __ldg(F + r1 + x0), p11 = __ldg(F + r1 + x1);
     float2 r;
-    r.x = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p00.x, w00), __fmul_rn(p01.x, w01)), __fmul_rn(p10.x, w10)), __fmul_rn(p11.x, w11));
-    r.y = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p00.y, w00), __fmul_rn(p01.y, w01)), __fmul_rn(p10.y, w10)), __fmul_rn(p11.y, w11));
+    r.x = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p00.x, wA.x), __fmul_rn(p01.x, wA.y)), __fmul_rn(p10.x, wB.x)), __fmul_rn(p11.x, wB.y));
+    r.y = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p00.y, wA.x), __fmul_rn(p01.y, wA.y)), __fmul_rn(p10.y, wB.x)), __fmul_rn(p11.y, wB.y));
     return r;
 }
 
-// one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame: channels 0..2 of the
-// result (byte 3 = 0). Horizontal stage two channels per multiply (lanes of 16 bits hold at most 255 * 32), vertical
-// stage per channel; (v + 512) >> 10 == cv2's (32 v + 2^14) >> 15 with its 15-bit weights.
-__device__ __forceinline__ uint32_t sampleU8(const uint8_t* __restrict__ img, uint32_t pitch, int W, int H, float x, float y) {
-    const int X = rne32(x), Y = rne32(y);
+// one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame at the position whose
+// rne32 bits are (bx, by): channels 0..2 of the result (byte 3 = 0). Horizontal stage two channels per multiply (16-bit
+// lanes hold at most 255 * 32), vertical stage per channel; (v + 512) >> 10 == cv2's (32 v + 2^14) >> 15.
+__device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, uint32_t pw, int W, int H, float bxf, float byf) {
+    const int X = __float_as_int(bxf) - 0x4B400000, Y = __float_as_int(byf) - 0x4B400000;
     const int ix = X >> 5, iy = Y >> 5;
     const uint32_t fx = (uint32_t)X & 31u, fy = (uint32_t)Y & 31u;
-    uint32_t o00, o01, o10, o11;
+    uint32_t p00, p01, p10, p11;
     if ((unsigned)ix < (unsigned)(W - 1) && (unsigned)iy < (unsigned)(H - 1)) {
-        o00 = (uint32_t)iy * pitch + (uint32_t)ix * 4u;
-        o01 = o00 + 4u;
-        o10 = o00 + pitch;
-        o11 = o10 + 4u;
+        const uint32_t* q = img + ((uint32_t)iy * pw + (uint32_t)ix);   // pw: row pitch in 4-byte words
+        p00 = __ldg(q);
+        p01 = __ldg(q + 1);
+        p10 = __ldg(q + pw);
+        p11 = __ldg(q + pw + 1);
     } else {
-        const uint32_t x0 = (uint32_t)clampi(ix, 0, W - 1) * 4u, x1 = (uint32_t)clampi(ix + 1, 0, W - 1) * 4u;
-        const uint32_t r0 = (uint32_t)clampi(iy, 0, H - 1) * pitch, r1 = (uint32_t)clampi(iy + 1, 0, H - 1) * pitch;
-        o00 = r0 + x0; o01 = r0 + x1; o10 = r1 + x0; o11 = r1 + x1;
+        const uint32_t x0 = (uint32_t)clampi(ix, 0, W - 1), x1 = (uint32_t)clampi(ix + 1, 0, W - 1);
+        const uint32_t r0 = (uint32_t)clampi(iy, 0, H - 1) * pw, r1 = (uint32_t)clampi(iy + 1, 0, H - 1) * pw;
+        p00 = __ldg(img + r0 + x0);
+        p01 = __ldg(img + r0 + x1);
+        p10 = __ldg(img + r1 + x0);
+        p11 = __ldg(img + r1 + x1);
     }
-    const uint32_t p00 = __ldg(reinterpret_cast<const uint32_t*>(img + o00));
-    const uint32_t p01 = __ldg(reinterpret_cast<const uint32_t*>(img + o01));
-    const uint32_t p10 = __ldg(reinterpret_cast<const uint32_t*>(img + o10));
-    const uint32_t p11 = __ldg(reinterpret_cast<const uint32_t*>(img + o11));
     const uint32_t M = 0x00FF00FFu, wx0 = 32u - fx, wy0 = 32u - fy;
     const uint32_t rb0 = (p00 & M) * wx0 + (p01 & M) * fx, rb1 = (p10 & M) * wx0 + (p11 & M) * fx;
     const uint32_t g0 = __byte_perm(p00, 0, 0x4441) * wx0 + __byte_perm(p01, 0, 0x4441) * fx;
@@ -670,17 +902,17 @@ __device__ __forceinline__ uint32_t sampleU8(const uint8_t* __restrict__ img, ui
     const uint32_t c0 = ((rb0 & 0xFFFFu) * wy0 + (rb1 & 0xFFFFu) * fy + 512u) >> 10;
     const uint32_t c2 = ((rb0 >> 16) * wy0 + (rb1 >> 16) * fy + 512u) >> 10;
     const uint32_t c1 = (g0 * wy0 + g1 * fy + 512u) >> 10;
-    return c0 | (c1 << 8) | (c2 << 16);
+    return c2 * 65536u + (c1 * 256u + c0);
 }
 
-struct SyCoef {   // one output column (or row) of the tile + halo: the upsampling taps and weights, the coordinate
-    int i0, i1;   // flow taps relative to the tile's field region
-    float a0, a1; // weights (rows: already x fs, which commutes with the rounding)
-    float pos;    // the clamped pixel coordinate as a float
-    int pi;       // ... as an int
+struct SyCoef {   // one region column (or row): upsampling taps (relative to the tile's field region) and weights
+    int i0, i1;
+    float a0, a1;   // rows: already x fs (scaling by a power of 2 commutes with the rounding)
+    float pos;      // the clamped pixel coordinate
+    int pi;
 };
 
-__device__ __forceinline__ SyCoef syCoef(int e, int origin, int n, int un, int fn, int g0, float invfs, float fsf, bool xaxis) {
+__device__ __forceinline__ SyCoef syCoef(int e, int origin, int n, int un, int fn, int g0, float invfs, float wscale, bool xaxis) {
     SyCoef c;
     const int p = clampi(origin - kSyAp + e, 0, n - 1);
     const int d = min(p, un - 1);   // crop [:H, :W] / edge pad of the upsampled field
@@ -693,25 +925,28 @@ __device__ __forceinline__ SyCoef syCoef(int e, int origin, int n, int un, int f
     }
     c.i0 = clampi(s, 0, fn - 1) - g0;
     c.i1 = clampi(s + 1, 0, fn - 1) - g0;
-    c.a0 = __fmul_rn(1.0f - f, fsf);
-    c.a1 = __fmul_rn(f, fsf);
+    c.a0 = __fmul_rn(1.0f - f, wscale);
+    c.a1 = __fmul_rn(f, wscale);
     c.pos = (float)p;
     c.pi = p;
     return c;
 }
 
-__global__ void __launch_bounds__(256) k_synth(const SynthParams p) {
+__global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
     extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ SyCoef colc[kSyEW], rowc[kSyEH];
+    __shared__ SyCoef rowc[kSyEH];
     __shared__ float TA[256], TC[256];
     __shared__ unsigned int cnt;
     __shared__ int gReg[4];
-    const int X0 = blockIdx.x * kSyTW, Y0 = blockIdx.y * kSyTH;
+    const int X0 = blockIdx.x * kSyT, Y0 = blockIdx.y * kSyTH;
+    const int tid = threadIdx.x, ex = tid & (kSyE - 1), ey0 = tid / kSyE;
     const uint8_t* nearF = p.nearC ? p.c : p.a;
-    const uint32_t pitch = (uint32_t)p.pitch;
+    const uint32_t pitch = (uint32_t)p.pitch, pw = pitch >> 2;
+    const uint32_t* fa32 = reinterpret_cast<const uint32_t*>(p.a);
+    const uint32_t* fc32 = reinterpret_cast<const uint32_t*>(p.c);
     if (p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
-        for (int i = threadIdx.x; i < kSyTW * kSyTH; i += 256) {
-            const int x = X0 + (i % kSyTW), y = Y0 + (i / kSyTW);
+        for (int i = tid; i < kSyT * kSyTH; i += kSyThreads) {
+            const int x = X0 + (i % kSyT), y = Y0 + (i / kSyT);
             if (x < p.W && y < p.H)
                 reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] =
                     __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
@@ -720,120 +955,111 @@ __global__ void __launch_bounds__(256) k_synth(const SynthParams p) {
     }
     const int fs = p.fs, uw = p.fw * fs, uh = p.fh * fs;
     const float invfs = 1.0f / (float)fs, fsf = (float)fs;
-    // 0. the field region of the tile + halo, the coefficient tables, the blend products
-    if (threadIdx.x == 0) {
+    // 0. the tile's field region, the row coefficients, the blend products; this thread's column coefficients
+    if (tid == 0) {
         const SyCoef lo = syCoef(0, X0, p.W, uw, p.fw, 0, invfs, 1.0f, true);
-        const SyCoef hi = syCoef(kSyEW - 1, X0, p.W, uw, p.fw, 0, invfs, 1.0f, true);
+        const SyCoef hi = syCoef(kSyE - 1, X0, p.W, uw, p.fw, 0, invfs, 1.0f, true);
         const SyCoef rlo = syCoef(0, Y0, p.H, uh, p.fh, 0, invfs, 1.0f, false);
         const SyCoef rhi = syCoef(kSyEH - 1, Y0, p.H, uh, p.fh, 0, invfs, 1.0f, false);
         gReg[0] = lo.i0; gReg[1] = hi.i1 - lo.i0 + 1; gReg[2] = rlo.i0; gReg[3] = rhi.i1 - rlo.i0 + 1;
         cnt = 0;
     }
+    if (tid < 256) {
+        TA[tid] = __fmul_rn(p.wA, (float)tid);
+        TC[tid] = __fmul_rn(p.wC, (float)tid);
+    }
     __syncthreads();
     const int gx0 = gReg[0], GW = gReg[1], gy0 = gReg[2], GH = gReg[3];
-    for (int i = threadIdx.x; i < kSyEW + kSyEH; i += 256) {
-        if (i < kSyEW) colc[i] = syCoef(i, X0, p.W, uw, p.fw, gx0, invfs, 1.0f, true);
-        else rowc[i - kSyEW] = syCoef(i - kSyEW, Y0, p.H, uh, p.fh, gy0, invfs, fsf, false);
-    }
-    TA[threadIdx.x] = __fmul_rn(p.wA, (float)threadIdx.x);
-    TC[threadIdx.x] = __fmul_rn(p.wC, (float)threadIdx.x);
-    float2* g = reinterpret_cast<float2*>(sm);                                     // GH x GW
-    float2* hrow = g + GW * GH;                                                    // GH x kSyEW
-    uint2* wab = reinterpret_cast<uint2*>(hrow + GH * kSyEW);                      // kSyTH x kSyTW
-    uint8_t* e = reinterpret_cast<uint8_t*>(wab + kSyTW * kSyTH);                  // kSyEH x kSyEW
-    unsigned short* hsum = reinterpret_cast<unsigned short*>(e + ((kSyEH * kSyEW + 15) & ~15));   // kSyEH x kSyTW
+    if (tid < kSyEH) rowc[tid] = syCoef(tid, Y0, p.H, uh, p.fh, gy0, invfs, fsf, false);
+    const SyCoef cx = syCoef(ex, X0, p.W, uw, p.fw, gx0, invfs, 1.0f, true);
+    float2* g = reinterpret_cast<float2*>(sm);             // GH x GW
+    float2* hrow = g + GW * GH;                            // GH x kSyE
+    uint8_t* e = reinterpret_cast<uint8_t*>(hrow + GH * kSyE);                  // kSyEH x kSyE
+    unsigned short* hsum = reinterpret_cast<unsigned short*>(e + kSyEH * kSyE);  // kSyEH x kSyE (columns < kSyT used)
     // 1. the field at t on the region (interp.field_at: g <- pf(q - s g), twice, from g = pf(q))
-    for (int i = threadIdx.x; i < GW * GH; i += 256) {
-        const int qx = gx0 + i % GW, qy = gy0 + i / GW;
-        float2 v = __ldg(p.pf + (size_t)qy * p.fw + qx);
-        if (p.lookup) {
-            const float fx = (float)qx, fy = (float)qy;
+    for (int r = ey0; r < GH; r += kSyThreads / kSyE)
+        for (int c = ex; c < GW; c += kSyE) {
+            const int qx = gx0 + c, qy = gy0 + r;
+            float2 v = __ldg(p.pf + (size_t)qy * p.fw + qx);
+            if (p.lookup) {
+                const float fx = (float)qx, fy = (float)qy;
 #pragma unroll
-            for (int it = 0; it < 2; it++)
-                v = remapF2m(p.pf, p.fw, p.fh, __fsub_rn(fx, __fmul_rn(p.s, v.x)), __fsub_rn(fy, __fmul_rn(p.s, v.y)));
+                for (int it = 0; it < 2; it++)
+                    v = remapF2m(p.pf, p.fw, p.fh, __fsub_rn(fx, __fmul_rn(p.s, v.x)), __fsub_rn(fy, __fmul_rn(p.s, v.y)));
+            }
+            g[r * GW + c] = v;
         }
-        g[i] = v;
-    }
     __syncthreads();
     // 1b. horizontal stage of the upsampling on the region's rows (cv2 resize: h = S0 a0 + S1 a1 per row)
-    for (int i = threadIdx.x; i < GH * kSyEW; i += 256) {
-        const int r = i / kSyEW, ex = i % kSyEW;
-        const SyCoef c = colc[ex];
-        const float2 s0 = g[r * GW + c.i0], s1 = g[r * GW + c.i1];
-        hrow[i] = make_float2(__fadd_rn(__fmul_rn(s0.x, c.a0), __fmul_rn(s1.x, c.a1)),
-                              __fadd_rn(__fmul_rn(s0.y, c.a0), __fmul_rn(s1.y, c.a1)));
+    for (int r = ey0; r < GH; r += kSyThreads / kSyE) {
+        const float2 s0 = g[r * GW + cx.i0], s1 = g[r * GW + cx.i1];
+        hrow[r * kSyE + ex] = make_float2(__fadd_rn(__fmul_rn(s0.x, cx.a0), __fmul_rn(s1.x, cx.a1)),
+                                          __fadd_rn(__fmul_rn(s0.y, cx.a0), __fmul_rn(s1.y, cx.a1)));
     }
     __syncthreads();
-    // 2. per pixel of tile + halo: half-vector (vertical stage, x fs folded into the row weights), both warps, mismatch
-    for (int i = threadIdx.x; i < kSyEW * kSyEH; i += 256) {
-        const int ex = i % kSyEW, ey = i / kSyEW;
-        const SyCoef cx = colc[ex], cy = rowc[ey];
-        const float2 h0 = hrow[cy.i0 * kSyEW + ex], h1 = hrow[cy.i1 * kSyEW + ex];
+    // 2. this thread's region column: half-vector (vertical stage, x fs folded in), both warps, mismatch. The warps of
+    //    output pixels stay in registers until the blend.
+    uint32_t wa[kSyK], wc[kSyK];
+    const float kA = p.mid ? 1.0f : p.ka, kC = p.mid ? 1.0f : p.kc;   // t = 0.5: the products by 1 are exact
+#pragma unroll
+    for (int k = 0; k < kSyK; k++) {
+        const int ey = ey0 + (kSyThreads / kSyE) * k;
+        const SyCoef cy = rowc[ey];
+        const float2 h0 = hrow[cy.i0 * kSyE + ex], h1 = hrow[cy.i1 * kSyE + ex];
         const float hx = __fadd_rn(__fmul_rn(h0.x, cy.a0), __fmul_rn(h1.x, cy.a1));
         const float hy = __fadd_rn(__fmul_rn(h0.y, cy.a0), __fmul_rn(h1.y, cy.a1));
-        float ax, ay, bx, by;
-        if (p.mid) {
-            ax = __fsub_rn(cx.pos, hx); ay = __fsub_rn(cy.pos, hy);
-            bx = __fadd_rn(cx.pos, hx); by = __fadd_rn(cy.pos, hy);
-        } else {
-            ax = __fsub_rn(cx.pos, __fmul_rn(p.ka, hx)); ay = __fsub_rn(cy.pos, __fmul_rn(p.ka, hy));
-            bx = __fadd_rn(cx.pos, __fmul_rn(p.kc, hx)); by = __fadd_rn(cy.pos, __fmul_rn(p.kc, hy));
-        }
-        const uint32_t wa = sampleU8(p.a, pitch, p.W, p.H, ax, ay);
-        const uint32_t wc = sampleU8(p.c, pitch, p.W, p.H, bx, by);
-        const uint32_t d = __vabsdiffu4(wa, wc);
+        // a(q - 2t h), c(q + 2(1 - t) h): float32 products, then the sums (numpy's order)
+        const float2 ba = rne32bits(make_float2(__fsub_rn(cx.pos, __fmul_rn(kA, hx)), __fsub_rn(cy.pos, __fmul_rn(kA, hy))));
+        const float2 bc = rne32bits(make_float2(__fadd_rn(cx.pos, __fmul_rn(kC, hx)), __fadd_rn(cy.pos, __fmul_rn(kC, hy))));
+        wa[k] = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y);
+        wc[k] = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y);
+        const uint32_t d = __vabsdiffu4(wa[k], wc[k]);
         const uint32_t m = __vmaxu4(__vmaxu4(d, d >> 8), d >> 16);
-        e[i] = (uint8_t)(m & 255u);
-        const int lx = ex - kSyAp, ly = ey - kSyAp;
-        if ((unsigned)lx < (unsigned)kSyTW && (unsigned)ly < (unsigned)kSyTH) wab[ly * kSyTW + lx] = make_uint2(wa, wc);
+        e[ey * kSyE + ex] = (uint8_t)(m & 255u);
     }
     __syncthreads();
-    // 3. horizontal 7-sums, a running window over 16 columns per item
-    for (int it = threadIdx.x; it < kSyEH * (kSyTW / 16); it += 256) {
-        const int r = it / (kSyTW / 16), c0 = (it % (kSyTW / 16)) * 16;
-        const uint8_t* q = e + r * kSyEW + c0;
+    // 3. horizontal 7-sums: one region row and 16 output columns per thread, a running window
+    {
+        const int r = tid >> 4, c0 = (tid & 15) * 8;
+        const uint8_t* q = e + r * kSyE + c0;
+        unsigned short* o = hsum + r * kSyE + c0;
         unsigned int sum = q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6];
-        unsigned short* o = hsum + r * kSyTW + c0;
         o[0] = (unsigned short)sum;
 #pragma unroll
-        for (int c = 1; c < 16; c++) {
-            sum += q[c + 6] - q[c - 1];
+        for (int c = 1; c < 8; c++) {
+            if (c0 + c + 6 < kSyE) sum += q[c + 6] - q[c - 1];
             o[c] = (unsigned short)sum;
         }
     }
     __syncthreads();
-    // 4. vertical 7-sums (a running window down 8 rows per thread), trust, blend, store
+    // 4. this thread's output pixels: vertical 7-sum, trust, blend, store
     unsigned int myCnt = 0;
-    {
-        const int lx = threadIdx.x % kSyTW, ly0 = (threadIdx.x / kSyTW) * (kSyTH / 4);
-        const int x = X0 + lx;
-        const unsigned short* q = hsum + ly0 * kSyTW + lx;
-        int S = q[0] + q[kSyTW] + q[2 * kSyTW] + q[3 * kSyTW] + q[4 * kSyTW] + q[5 * kSyTW];
-        for (int k = 0; k < kSyTH / 4; k++) {
-            const int ly = ly0 + k, y = Y0 + ly;
-            S += q[(k + 6) * kSyTW];
-            const int Sk = S;
-            S -= q[k * kSyTW];
-            if (x >= p.W || y >= p.H) continue;
-            const uint2 w = wab[ly * kSyTW + lx];
+    const int lx = ex - kSyAp, x = X0 + lx;
+    if ((unsigned)lx < (unsigned)kSyT && x < p.W) {
+#pragma unroll
+        for (int k = 0; k < kSyK; k++) {
+            const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = Y0 + ly;
+            if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
+            const unsigned short* q = hsum + ly * kSyE + lx;
+            const int S = q[0] + q[kSyE] + q[2 * kSyE] + q[3 * kSyE] + q[4 * kSyE] + q[5 * kSyE] + q[6 * kSyE];
             const uint32_t nq = __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
             uint32_t o;
-            if (Sk <= p.sZero) {   // u = 0: out = the blend rounded
+            if (S <= p.sZero) {   // u = 0: out = the blend rounded
                 if (p.mid) {
-                    o = __vavgu4(w.x, w.y);   // floor(0.5 (a + c) + 0.5) per byte
+                    o = __vavgu4(wa[k], wc[k]);   // floor(0.5 (a + c) + 0.5) per byte
                 } else {
                     o = 0;
 #pragma unroll
                     for (int k2 = 0; k2 < 3; k2++) {
-                        const float mix = __fadd_rn(TA[(w.x >> (8 * k2)) & 255u], TC[(w.y >> (8 * k2)) & 255u]);
+                        const float mix = __fadd_rn(TA[(wa[k] >> (8 * k2)) & 255u], TC[(wc[k] >> (8 * k2)) & 255u]);
                         o |= (uint32_t)floorPos(fminf(__fadd_rn(mix, 0.5f), 255.0f)) << (8 * k2);
                     }
                 }
-            } else if (Sk >= p.sOne) {   // u = 1: the nearer frame
+            } else if (S >= p.sOne) {   // u = 1: the nearer frame
                 o = nq;
                 myCnt++;
             } else {
-                const float eb = (float)((double)Sk * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
+                const float eb = (float)((double)S * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
                 float u = __fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan);
                 u = fminf(fmaxf(u, 0.0f), 1.0f);
                 myCnt += u > 0.5f;
@@ -842,7 +1068,7 @@ __global__ void __launch_bounds__(256) k_synth(const SynthParams p) {
 #pragma unroll
                 for (int k2 = 0; k2 < 3; k2++) {
                     const int sh = 8 * k2;
-                    const uint32_t ca = (w.x >> sh) & 255u, cc = (w.y >> sh) & 255u;
+                    const uint32_t ca = (wa[k] >> sh) & 255u, cc = (wc[k] >> sh) & 255u;
                     const float fa = i2f((int)ca), fc = i2f((int)cc), fn = i2f((int)((nq >> sh) & 255u));
                     const float mix = p.mid ? __fmul_rn(0.5f, __fadd_rn(fa, fc)) : __fadd_rn(TA[ca], TC[cc]);
                     const float v = __fadd_rn(__fadd_rn(__fmul_rn(mix, iu), __fmul_rn(fn, u)), 0.5f);
@@ -851,12 +1077,12 @@ __global__ void __launch_bounds__(256) k_synth(const SynthParams p) {
             }
             o = (o & 0x00FFFFFFu) | (nq & 0xFF000000u);   // alpha (byte 3 in both pixel orders): the nearer frame's
             reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = o;
-            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyEW + lx + kSyAp];
+            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyE + ex];
         }
     }
     if (myCnt) atomicAdd(&cnt, myCnt);
     __syncthreads();
-    if (threadIdx.x == 0 && cnt) atomicAdd(p.untrusted, cnt);
+    if (tid == 0 && cnt) atomicAdd(p.untrusted, cnt);
 }
 
 // interp.py:238-239: more than globalFallback of the pixels untrusted -> the nearer real frame over the output.
@@ -885,10 +1111,24 @@ cudaError_t launchDown(const DownParams& p, cudaStream_t s) {
     k_down<<<dim3(divUp(p.dw, 16), divUp(p.dh, 16)), 256, 0, s>>>(p);
     return cudaGetLastError();
 }
+template <int R>
+static void launchSearchR(const SearchParams& p, cudaStream_t s) {
+    constexpr int T = 8 + 2 * R, D = 2 * R + 1;
+    k_search_r<R><<<divUp(p.bw * p.bh, 4), 128, (size_t)4 * (2 * T * T + D * D) * sizeof(float), s>>>(p);
+}
 cudaError_t launchSearch(const SearchParams& p, cudaStream_t s) {
-    const int T = 8 + 2 * p.R;
-    const size_t smem = (size_t)4 * 2 * T * T * sizeof(float);
-    k_search<<<divUp(p.bw * p.bh, 4), 128, smem, s>>>(p);
+    switch (p.R) {
+        case 1: launchSearchR<1>(p, s); break;
+        case 2: launchSearchR<2>(p, s); break;
+        case 3: launchSearchR<3>(p, s); break;
+        case 4: launchSearchR<4>(p, s); break;
+        case 5: launchSearchR<5>(p, s); break;
+        case 6: launchSearchR<6>(p, s); break;
+        default: {   // radii 7..12 (settings beyond the defaults): the runtime-radius kernel
+            const int T = 8 + 2 * p.R;
+            k_search<<<divUp(p.bw * p.bh, 4), 128, (size_t)4 * 2 * T * T * sizeof(float), s>>>(p);
+        }
+    }
     return cudaGetLastError();
 }
 cudaError_t launchMedian3(const Median3Params& p, cudaStream_t s) {
@@ -920,14 +1160,13 @@ cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 size_t synthSmemBytes(int fs) {  // declared in fg_params.h
-    // worst-case field region of a tile (GW x GH float2) + its horizontal stage + interior warps + mismatch + row sums
-    const int gw = (kSyEW + fs - 1) / fs + 3, gh = (kSyEH + fs - 1) / fs + 3;
-    return (size_t)gw * gh * 8 + (size_t)gh * kSyEW * 8 + (size_t)kSyTW * kSyTH * 8 + (size_t)((kSyEH * kSyEW + 15) & ~15) +
-           (size_t)kSyEH * kSyTW * 2;
+    // worst-case field region of a tile (GW x GH float2) + its horizontal stage + mismatch + row sums
+    const int gw = (kSyE + fs - 1) / fs + 3, gh = (kSyEH + fs - 1) / fs + 3;
+    return (size_t)gw * gh * 8 + (size_t)gh * kSyE * 8 + (size_t)kSyEH * kSyE + (size_t)kSyEH * kSyE * 2;
 }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs);
-    k_synth<<<dim3(divUp(p.W, kSyTW), divUp(p.H, kSyTH)), 256, smem, s>>>(p);
+    k_synth<<<dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), kSyThreads, smem, s>>>(p);
     return cudaGetLastError();
 }
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s) {

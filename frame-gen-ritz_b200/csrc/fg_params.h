@@ -33,6 +33,7 @@ struct LumaPyrParams {
     int W, H, fs;          // frame size, flow scale (1, 2, 4)
     int ri, gi, bi;        // byte offsets of R, G, B in a 4-byte pixel
     int nlev;              // levels written here (<= kPyrInKernel)
+    int vec16;             // flowScale 2 with 16-byte aligned frames and rows: the uint4 path
     int lw[kPyrInKernel], lh[kPyrInKernel];
     float* la[kPyrInKernel];
     float* lc[kPyrInKernel];

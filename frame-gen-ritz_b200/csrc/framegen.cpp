@@ -318,6 +318,8 @@ struct Interpolator::Impl {
         lp.W = (int)W; lp.H = (int)H; lp.fs = (int)set.flowScale;
         lp.ri = ri; lp.gi = gi; lp.bi = bi;
         lp.nlev = std::min(n, fgk::kPyrInKernel);
+        lp.vec16 = set.flowScale == 2 && prev.pitch % 16 == 0 && ((uintptr_t)prev.data & 15) == 0 && ((uintptr_t)curr.data & 15) == 0 &&
+                   W % 4 == 0 && H % 2 == 0;   // complete 2x2 cells in every full tile, 8-byte aligned level-0 rows
         for (int l = 0; l < lp.nlev; l++) {
             lp.lw[l] = L.lv[l].w; lp.lh[l] = L.lv[l].h;
             lp.la[l] = luma + L.lv[l].lumaA; lp.lc[l] = luma + L.lv[l].lumaC;
