@@ -15,6 +15,15 @@
 
 namespace fgk {
 
+// Programmatic dependent launch: every kernel is launched with programmatic stream serialisation, lets the next kernel
+// of the stream be scheduled at once (its CTAs only occupy the slots this grid frees) and then waits for the previous
+// grid to complete and its memory to be visible before touching anything an earlier kernel wrote. The launch latency
+// of each small dependent pass overlaps the tail of the one before it.
+__device__ __forceinline__ void pdlEnter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 // luma texel with clamp-to-edge (== cv2 BORDER_REPLICATE and the replicate pad_to_block, interp.py:68-70)
@@ -90,6 +99,7 @@ __device__ __forceinline__ float warpSum(float v) {
 // below it, so the whole tower stays inside the tile. Mean of the valid pixels: sum * 1/n^2 when full, sum / count
 // at the frame's odd edges (cv2's INTER_AREA fast path).
 __global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
+    pdlEnter();
     __shared__ float sl[2][1024 + 256 + 64 + 16 + 4 + 1];
     const int tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 32;
     const int fw = p.lw[0], fh = p.lh[0], fs = p.fs;
@@ -187,6 +197,7 @@ __global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
 
 // a pyramid level beyond the luma kernel's tower (interp.py:76)
 __global__ void __launch_bounds__(256) k_down(const DownParams p) {
+    pdlEnter();
     const int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
     if (x >= p.dw || y >= p.dh) return;
     float sa = 0.0f, sc = 0.0f;
@@ -213,6 +224,7 @@ __global__ void __launch_bounds__(256) k_down(const DownParams p) {
 __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by, int lane, int& sx, int& sy);
 
 __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
+    pdlEnter();
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * 4 + warp;
@@ -312,6 +324,7 @@ __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by
 // registers and scores every dx from them; the 8 rows of a dy are summed by shuffles (all sums exact).
 template <int R>
 __global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
+    pdlEnter();
     constexpr int T = 8 + 2 * R, D = 2 * R + 1, NI = 8 * D, ROUNDS = (NI + 31) / 32;
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -405,6 +418,7 @@ __device__ __forceinline__ float med9(float v[9]) {
 // that take it as their own parent; the last CTA reads off the order statistics k1 = (n-1)/2, k2 = n/2 and writes
 // 2 x the median = v_k1 + v_k2, then clears the histogram for the next estimate.
 __global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
+    pdlEnter();
     const int b = blockIdx.x * 256 + threadIdx.x;
     const int n = p.bw * p.bh;
     if (b < n) {
@@ -538,6 +552,7 @@ __device__ void cutMeanBlock(const float* sads, int n, const CutPlan& plan, floa
 }
 
 __global__ void __launch_bounds__(256) k_cutmean(const CutMeanParams p) {
+    pdlEnter();
     extern __shared__ float vals[];
     __shared__ unsigned int red[256];
     const bool inSmem = (size_t)(p.plan.nLeaves + p.plan.nInner) * sizeof(float) <= kPlanSmemMax;
@@ -555,6 +570,7 @@ constexpr int kSubT = 13, kSubO = 2, kSubL = 24, kSubRows = 10;   // tile, its m
 constexpr int kSubWarpFloats = 2 * kSubT * kSubT + 2 * kSubRows * kSubL + 72;
 
 __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
+    pdlEnter();
     extern __shared__ float smem[];
     __shared__ unsigned int ticket;
     __shared__ unsigned int red[128];
@@ -710,6 +726,7 @@ __device__ __forceinline__ float2 tapPair(const float* __restrict__ ya, const fl
 }
 
 __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
+    pdlEnter();
     __shared__ int plane[kPfEH][kPfE];
     __shared__ int hs[kPfEH][kPfE];
     __shared__ float2 bv[kPfBY][kPfBX];
@@ -933,6 +950,7 @@ __device__ __forceinline__ SyCoef syCoef(int e, int origin, int n, int un, int f
 }
 
 __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
+    pdlEnter();
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ SyCoef rowc[kSyEH];
     __shared__ float TA[256], TC[256];
@@ -1048,12 +1066,15 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
                 if (p.mid) {
                     o = __vavgu4(wa[k], wc[k]);   // floor(0.5 (a + c) + 0.5) per byte
                 } else {
-                    o = 0;
-#pragma unroll
-                    for (int k2 = 0; k2 < 3; k2++) {
-                        const float mix = __fadd_rn(TA[(wa[k] >> (8 * k2)) & 255u], TC[(wc[k] >> (8 * k2)) & 255u]);
-                        o |= (uint32_t)floorPos(fminf(__fadd_rn(mix, 0.5f), 255.0f)) << (8 * k2);
-                    }
+                    // fl32(fl32((1 - t) a) + fl32(t c)) + 0.5, floored (never above 255.5 here, so no clamp is needed): the
+                    // products come from the tables, the adds are paired (adds alone cannot be fused), the floor is a
+                    // round-toward-zero add of 2^23 whose low mantissa byte is the result
+                    const uint32_t A = wa[k], C = wc[k];
+                    const float2 m01 = padd(make_float2(TA[A & 255u], TA[(A >> 8) & 255u]), make_float2(TC[C & 255u], TC[(C >> 8) & 255u]));
+                    const float m2 = __fadd_rn(TA[(A >> 16) & 255u], TC[(C >> 16) & 255u]);
+                    const float2 f01 = __ffma2_rz(padd(m01, make_float2(0.5f, 0.5f)), make_float2(1.0f, 1.0f), make_float2(8388608.0f, 8388608.0f));
+                    const float f2 = __fadd_rz(__fadd_rn(m2, 0.5f), 8388608.0f);
+                    o = __byte_perm(__byte_perm(__float_as_uint(f01.x), __float_as_uint(f01.y), 0x0040), __float_as_uint(f2), 0x0410);
                 }
             } else if (S >= p.sOne) {   // u = 1: the nearer frame
                 o = nq;
@@ -1088,6 +1109,7 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
 // interp.py:238-239: more than globalFallback of the pixels untrusted -> the nearer real frame over the output.
 // Every CTA exits at once in the normal case. Also clears the next synth's counter.
 __global__ void __launch_bounds__(256) k_fallback(const FallbackParams p) {
+    pdlEnter();
     const unsigned int cnt = *p.untrusted;
     if (blockIdx.x == 0 && threadIdx.x == 0) *p.untrustedNext = 0;
     if (!((double)cnt / ((double)p.W * (double)p.H) > p.frac)) return;
@@ -1103,37 +1125,50 @@ __global__ void __launch_bounds__(256) k_fallback(const FallbackParams p) {
 // ============================================================================================== launchers
 static inline unsigned int divUp(int a, int b) { return (unsigned int)((a + b - 1) / b); }
 
+template <typename... KArgs, typename... Args>
+static cudaError_t launchPdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+
+
 cudaError_t launchLumaPyr(const LumaPyrParams& p, cudaStream_t s) {
-    k_luma_pyr<<<dim3(divUp(p.lw[0], 32), divUp(p.lh[0], 32)), 256, 0, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_luma_pyr, dim3(divUp(p.lw[0], 32), divUp(p.lh[0], 32)), dim3(256), 0, s, p);
 }
 cudaError_t launchDown(const DownParams& p, cudaStream_t s) {
-    k_down<<<dim3(divUp(p.dw, 16), divUp(p.dh, 16)), 256, 0, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_down, dim3(divUp(p.dw, 16), divUp(p.dh, 16)), dim3(256), 0, s, p);
 }
 template <int R>
-static void launchSearchR(const SearchParams& p, cudaStream_t s) {
+static cudaError_t launchSearchR(const SearchParams& p, cudaStream_t s) {
     constexpr int T = 8 + 2 * R, D = 2 * R + 1;
-    k_search_r<R><<<divUp(p.bw * p.bh, 4), 128, (size_t)4 * (2 * T * T + D * D) * sizeof(float), s>>>(p);
+    return launchPdl(k_search_r<R>, dim3(divUp(p.bw * p.bh, 4)), dim3(128), (size_t)4 * (2 * T * T + D * D) * sizeof(float), s, p);
 }
 cudaError_t launchSearch(const SearchParams& p, cudaStream_t s) {
     switch (p.R) {
-        case 1: launchSearchR<1>(p, s); break;
-        case 2: launchSearchR<2>(p, s); break;
-        case 3: launchSearchR<3>(p, s); break;
-        case 4: launchSearchR<4>(p, s); break;
-        case 5: launchSearchR<5>(p, s); break;
-        case 6: launchSearchR<6>(p, s); break;
+        case 1: return launchSearchR<1>(p, s);
+        case 2: return launchSearchR<2>(p, s);
+        case 3: return launchSearchR<3>(p, s);
+        case 4: return launchSearchR<4>(p, s);
+        case 5: return launchSearchR<5>(p, s);
+        case 6: return launchSearchR<6>(p, s);
         default: {   // radii 7..12 (settings beyond the defaults): the runtime-radius kernel
             const int T = 8 + 2 * p.R;
-            k_search<<<divUp(p.bw * p.bh, 4), 128, (size_t)4 * 2 * T * T * sizeof(float), s>>>(p);
+            return launchPdl(k_search, dim3(divUp(p.bw * p.bh, 4)), dim3(128), (size_t)4 * 2 * T * T * sizeof(float), s, p);
         }
     }
-    return cudaGetLastError();
 }
 cudaError_t launchMedian3(const Median3Params& p, cudaStream_t s) {
-    k_median3<<<divUp(p.bw * p.bh, 256), 256, 0, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_median3, dim3(divUp(p.bw * p.bh, 256)), dim3(256), 0, s, p);
 }
 static size_t planBytes(const CutPlan& c) {
     const size_t b = (size_t)(c.nLeaves + c.nInner) * sizeof(float);
@@ -1148,16 +1183,13 @@ cudaError_t prepareKernels() {
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
     const size_t tiles = (size_t)4 * kSubWarpFloats * sizeof(float);
     const size_t smem = tiles > planBytes(p.plan) ? tiles : planBytes(p.plan);
-    k_subpix<<<divUp(p.bw * p.bh, 4), 128, smem, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_subpix, dim3(divUp(p.bw * p.bh, 4)), dim3(128), smem, s, p);
 }
 cudaError_t launchCutMean(const CutMeanParams& p, cudaStream_t s) {
-    k_cutmean<<<1, 256, planBytes(p.plan), s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_cutmean, dim3(1), dim3(256), planBytes(p.plan), s, p);
 }
 cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s) {
-    k_pixfield<<<dim3(divUp(p.w, kPfTW), divUp(p.h, kPfTH)), 256, 0, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_pixfield, dim3(divUp(p.w, kPfTW), divUp(p.h, kPfTH)), dim3(256), 0, s, p);
 }
 size_t synthSmemBytes(int fs) {  // declared in fg_params.h
     // worst-case field region of a tile (GW x GH float2) + its horizontal stage + mismatch + row sums
@@ -1166,12 +1198,10 @@ size_t synthSmemBytes(int fs) {  // declared in fg_params.h
 }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs);
-    k_synth<<<dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), kSyThreads, smem, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_synth, dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), dim3(kSyThreads), smem, s, p);
 }
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s) {
-    k_fallback<<<148 * 4, 256, 0, s>>>(p);
-    return cudaGetLastError();
+    return launchPdl(k_fallback, dim3(148 * 4), dim3(256), 0, s, p);
 }
 
 }  // namespace fgk
