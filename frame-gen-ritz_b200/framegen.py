@@ -91,6 +91,9 @@ SIGNATURES = {
     "fg_get_trace_layout": (_I, [_P, ctypes.POINTER(CTraceLayout)]),
     "fg_record_trace": (_I, [_P, _P, _P]),
     "fg_last_error": (_S, [_P]),
+    "fg_record_synth_noalloc": (_I, [_P, _U32, _U32, _U32, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame),
+                                     ctypes.POINTER(CFrame), _P, _I, _F, ctypes.POINTER(CSettings),
+                                     ctypes.POINTER(ctypes.c_char_p)]),
 }
 
 _lib = None
@@ -309,3 +312,15 @@ def read_trace(fg, stream=None):
     return {"luma": luma, "fields": fld, "sub": sub, "meds": f32(l.medOff, 2 * n).reshape(n, 2),
             "sads": f32(l.sadOff, bw0 * bh0).reshape(bh0, bw0), "pf": f32(l.pfOff, 2 * l.fw * l.fh).reshape(l.fh, l.fw, 2),
             "cut": bool(st[0]), "sad": float(st[1:2].view(np.float32)[0]), "sadSum256": int(st[2]), "err": int(st[3])}
+
+
+def record_synth_noalloc(prev, curr, out, field, cut, t, settings=None, view_format=VK_R8G8B8A8_UNORM, stream=None):
+    """fg_record_synth_noalloc: the synthesis without an Interpolator and without allocating (the per-pixel field and the
+    scene-cut decision come from the caller). Returns (ok, error message or None)."""
+    err = ctypes.c_char_p()
+    H, W = prev.shape[:2]
+    ok = lib().fg_record_synth_noalloc(_stream(stream), view_format, W, H, ctypes.byref(frame_of(prev)),
+                                       ctypes.byref(frame_of(curr)), ctypes.byref(frame_of(out)), field.data_ptr(),
+                                       int(cut), float(t), ctypes.byref((settings or Settings()).to_c()),
+                                       ctypes.byref(err))
+    return bool(ok), (err.value.decode() if err.value else None)
