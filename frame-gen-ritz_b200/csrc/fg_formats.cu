@@ -1,0 +1,487 @@
+// CUDA kernels of the V1 path for the frame formats other than 8-bit RGBA: Rgb10 (A2B10G10R10 / A2R10G10B10),
+// RgbaF16 (display-encoded, or linear light measured as PQ codes), Nv12 and P010 (two planes, 4:2:0).
+//
+// The reference defines these formats in its shaders (gpu/shaders/format.glsl:29-106, luma.comp:9-27,
+// motion_v1.glsl:86-144, resolve.comp:48-83, the constants of gpu/framegen.cpp:1508-1539); proto/interp.py has no
+// counterpart. The kernels compute exactly this arithmetic:
+//   - motion-estimate luma in quarter levels (the 10-bit code grid): Q = rint(4 clamp(y, 0, 255)) of the format's
+//     luma y; level 0 = rint(4 sum(Q) / n) / 16 over each flowScale cell; pyramid levels rounded to a multiple of
+//     2^-10. Every SAD, tap and box sum of the estimate is then exact in float32 whatever the order, so the search,
+//     median, sub-pixel and pixel-field kernels are the 8-bit RGBA path's own;
+//   - warp taps at the sample point rounded to 1/32 px (chroma: the same normalised point, 1/64 chroma texel), the
+//     bilinear tap ((p00 w00 + p01 w01) + p10 w10) + p11 w11 in float, clamped to the edge; the mismatch, blend and
+//     stores of format.glsl / resolve.comp with a fixed operation order (round-to-nearest intrinsics, no fusion);
+//   - PQ (SMPTE ST 2084) via the log2 / exp2 series below, built from IEEE float operations only.
+// Synthesis tiles are the 8-bit path's (kSyE x kSyEH mismatch region, 3-pixel halo); the warps of the output
+// pixels are taken again after the 7x7 box instead of being held in registers (up to 3 floats per channel).
+#include <cuda_fp16.h>
+
+#include "fg_device.h"
+
+namespace fgk {
+
+// ============================================================================================== float helpers
+// log2 of a positive normal float: x = 2^e m, m in [sqrt(1/2), sqrt(2)); log2 m = 2/ln2 atanh(s),
+// s = (m - 1) / (m + 1), by its odd series to s^9
+__device__ __forceinline__ float fmtLog2(float x) {
+    const uint32_t b = __float_as_uint(x);
+    int e = (int)((b >> 23) & 255u) - 127;
+    float m = __uint_as_float((b & 0x7FFFFFu) | 0x3F800000u);
+    if (m > 0x1.6a09e6p+0f) { m = __fmul_rn(m, 0.5f); e += 1; }
+    const float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+    const float z = __fmul_rn(s, s);
+    float p = 0x1.484b14p-2f;
+    p = __fadd_rn(__fmul_rn(p, z), 0x1.a61762p-2f);
+    p = __fadd_rn(__fmul_rn(p, z), 0x1.2776c6p-1f);
+    p = __fadd_rn(__fmul_rn(p, z), 0x1.ec709ep-1f);
+    p = __fadd_rn(__fmul_rn(p, z), 0x1.715476p+1f);
+    return __fadd_rn((float)e, __fmul_rn(s, p));
+}
+
+// 2^x for -126 <= x < 128 (0 below): x = n + g + 1/2, n = floor(x); 2^(g + 1/2) = sqrt2 e^(g ln2), series to g^7
+__device__ __forceinline__ float fmtExp2(float x) {
+    if (!(x >= -126.0f)) return 0.0f;
+    const float n = floorf(x);
+    const float g = __fsub_rn(__fsub_rn(x, n), 0.5f);
+    float p = 0x1.ffcbfcp-17f;
+    p = __fadd_rn(__fmul_rn(p, g), 0x1.430912p-13f);
+    p = __fadd_rn(__fmul_rn(p, g), 0x1.5d87fep-10f);
+    p = __fadd_rn(__fmul_rn(p, g), 0x1.3b2ab6p-7f);
+    p = __fadd_rn(__fmul_rn(p, g), 0x1.c6b08ep-5f);
+    p = __fadd_rn(__fmul_rn(p, g), 0x1.ebfbe0p-3f);
+    p = __fadd_rn(__fmul_rn(p, g), 0x1.62e430p-1f);
+    p = __fadd_rn(__fmul_rn(p, g), 1.0f);
+    p = __fmul_rn(p, 0x1.6a09e6p+0f);
+    return __fmul_rn(p, __uint_as_float((uint32_t)((int)n + 127) << 23));
+}
+
+__device__ __forceinline__ float clampF(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// format.glsl fgPq * 255: the level of a linear-light value as an 8-bit PQ code
+__device__ __noinline__ float fmtPq255(float v, float kWhite) {
+    const float y = clampF(__fmul_rn(v, kWhite), 0.0f, 1.0f);
+    float p = 0.0f;
+    if (y >= 0x1p-126f) p = fmtExp2(__fmul_rn(0.1593017578125f, fmtLog2(y)));
+    const float num = __fadd_rn(0.8359375f, __fmul_rn(18.8515625f, p));
+    const float den = __fadd_rn(1.0f, __fmul_rn(18.6875f, p));
+    const float r = __fdiv_rn(num, den);
+    return __fmul_rn(fmtExp2(__fmul_rn(78.84375f, fmtLog2(r))), 255.0f);
+}
+
+__device__ __forceinline__ float h2f(uint32_t h16) { return __half2float(__ushort_as_half((unsigned short)h16)); }
+
+// ============================================================================================== pixel access
+__device__ __forceinline__ uint32_t ldw(const uint8_t* base, size_t pitch, int x, int y) {
+    return __ldg(reinterpret_cast<const uint32_t*>(base + (size_t)y * pitch) + x);
+}
+__device__ __forceinline__ uint32_t ldh(const uint8_t* base, size_t pitch, int x, int y) {   // a 16-bit sample
+    return __ldg(reinterpret_cast<const unsigned short*>(base + (size_t)y * pitch) + x);
+}
+
+// a raw channel of an Rgb10 word (k: 0 R, 1 G, 2 B)
+__device__ __forceinline__ int rgb10(const FmtConst& f, uint32_t w, int k) {
+    return (int)((w >> (f.rHigh ? 20 - 10 * k : 10 * k)) & 1023u);
+}
+
+// the three raw channels of texel (x, y): Rgb10 codes, F16 values; YUV: the Y level only (r[0])
+template <int F>
+__device__ __forceinline__ void texel(const FmtConst& f, const uint8_t* base, size_t pitch, int x, int y, float r[3]) {
+    if (F == kFmtRgb10) {
+        const uint32_t w = ldw(base, pitch, x, y);
+#pragma unroll
+        for (int k = 0; k < 3; k++) r[k] = i2f(rgb10(f, w, k));
+    } else if (F == kFmtF16) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2*>(base + (size_t)y * pitch) + x);
+        r[0] = h2f(q.x & 0xFFFFu);
+        r[1] = h2f(q.x >> 16);
+        r[2] = h2f(q.y & 0xFFFFu);
+    } else if (F == kFmtNv12) {
+        r[0] = i2f(__ldg(base + (size_t)y * pitch + x));
+    } else {
+        r[0] = __fmul_rn(i2f((int)ldh(base, pitch, x, y)), 0x1p-8f);
+    }
+}
+
+// the (Cb, Cr) levels of chroma texel (x, y)
+template <int F>
+__device__ __forceinline__ float2 ctexel(const uint8_t* cbase, size_t cpitch, int x, int y) {
+    if (F == kFmtNv12) {
+        const unsigned short v = __ldg(reinterpret_cast<const unsigned short*>(cbase + (size_t)y * cpitch) + x);
+        return make_float2(i2f(v & 255), i2f(v >> 8));
+    }
+    const uint32_t v = ldw(cbase, cpitch, x, y);
+    return make_float2(__fmul_rn(i2f((int)(v & 0xFFFFu)), 0x1p-8f), __fmul_rn(i2f((int)(v >> 16)), 0x1p-8f));
+}
+
+// a raw channel -> its level (RGB formats)
+template <int F>
+__device__ __forceinline__ float levelOf(const FmtConst& f, float r) {
+    if (F == kFmtRgb10) return __fmul_rn(r, f.k10);
+    if (F == kFmtF16) return f.linear ? fmtPq255(r, f.kWhite) : __fmul_rn(r, 255.0f);
+    return r;
+}
+
+// ============================================================================================== luma
+// the motion estimate's luma of pixel (x, y) in quarter levels (luma.comp:9-27, format.glsl fgLuma)
+template <int F>
+__device__ __forceinline__ int lumaQ(const FmtConst& f, const uint8_t* base, size_t pitch, int x, int y) {
+    float r[3];
+    texel<F>(f, base, pitch, x, y, r);
+    float yl;
+    if (F == kFmtNv12 || F == kFmtP010) {
+        yl = __fmul_rn(__fsub_rn(r[0], f.black), f.ys);
+    } else {
+        const float lr = levelOf<F>(f, r[0]), lg = levelOf<F>(f, r[1]), lb = levelOf<F>(f, r[2]);
+        float d = __fmul_rn(4899.0f, lr);
+        d = __fadd_rn(d, __fmul_rn(9617.0f, lg));
+        d = __fadd_rn(d, __fmul_rn(1868.0f, lb));
+        yl = __fmul_rn(d, 1.0f / 16384.0f);
+    }
+    return __float2int_rn(__fmul_rn(clampF(yl, 0.0f, 255.0f), 4.0f));
+}
+
+// integer num / n rounded half to even (num >= 0, n > 0)
+__device__ __forceinline__ int rneDiv(int num, int n) {
+    int q = num / n;
+    const int r = num - q * n;
+    if (2 * r > n || (2 * r == n && (q & 1))) q++;
+    return q;
+}
+
+// interp.flow + pyramid for the other formats: one CTA = a 32x32 level-0 tile and its tower (as k_luma_pyr)
+template <int F>
+__global__ void __launch_bounds__(256) k_luma_fmt(const LumaPyrParams p) {
+    pdlEnter();
+    __shared__ float sl[2][kTowerFloats];
+    const int tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 32;
+    const int fw = p.lw[0], fh = p.lh[0], fs = p.fs;
+    for (int i = threadIdx.x; i < 1024; i += 256) {
+        const int x = tx0 + (i & 31), y = ty0 + (i >> 5);
+        float va = 0.0f, vc = 0.0f;
+        if (x < fw && y < fh) {
+            int sa = 0, sc = 0, n = 0;
+            for (int j = 0; j < fs; j++) {
+                const int yy = y * fs + j;
+                if (yy >= p.H) break;
+                for (int k = 0; k < fs; k++) {
+                    const int xx = x * fs + k;
+                    if (xx >= p.W) break;
+                    sa += lumaQ<F>(p.f, p.a, p.pitch, xx, yy);
+                    sc += lumaQ<F>(p.f, p.c, p.pitch, xx, yy);
+                    n++;
+                }
+            }
+            va = __fmul_rn(i2f(rneDiv(4 * sa, n)), 1.0f / 16.0f);
+            vc = __fmul_rn(i2f(rneDiv(4 * sc, n)), 1.0f / 16.0f);
+            p.la[0][(size_t)y * fw + x] = va;
+            p.lc[0][(size_t)y * fw + x] = vc;
+        }
+        sl[0][i] = va;
+        sl[1][i] = vc;
+    }
+    __syncthreads();
+    lumaTower<true>(p, sl, tx0, ty0);
+}
+
+// ============================================================================================== warps
+struct Taps {
+    int x0, x1, y0, y1;
+    float w00, w01, w10, w11;
+};
+
+// the texels and cv2's float weights of the sample point (X, Y) in 1/2^BITS texel units, clamped to w x h
+template <int BITS>
+__device__ __forceinline__ Taps mkTaps(int X, int Y, int w, int h) {
+    Taps t;
+    constexpr int mask = (1 << BITS) - 1;
+    constexpr float sc = 1.0f / (float)(1 << BITS);
+    const int ix = X >> BITS, iy = Y >> BITS;
+    const float fx = __fmul_rn(i2f(X & mask), sc), fy = __fmul_rn(i2f(Y & mask), sc);
+    const float gx = __fsub_rn(1.0f, fx), gy = __fsub_rn(1.0f, fy);
+    t.w00 = __fmul_rn(gy, gx);
+    t.w01 = __fmul_rn(gy, fx);
+    t.w10 = __fmul_rn(fy, gx);
+    t.w11 = __fmul_rn(fy, fx);
+    t.x0 = clampi(ix, 0, w - 1); t.x1 = clampi(ix + 1, 0, w - 1);
+    t.y0 = clampi(iy, 0, h - 1); t.y1 = clampi(iy + 1, 0, h - 1);
+    return t;
+}
+
+__device__ __forceinline__ float bil(const Taps& t, float p00, float p01, float p10, float p11) {
+    float r = __fmul_rn(p00, t.w00);
+    r = __fadd_rn(r, __fmul_rn(p01, t.w01));
+    r = __fadd_rn(r, __fmul_rn(p10, t.w10));
+    return __fadd_rn(r, __fmul_rn(p11, t.w11));
+}
+
+// the chroma (Cb, Cr) levels warped to the point whose 1/32-px coordinates are (X, Y)
+template <int F>
+__device__ __forceinline__ float2 warpChroma(const uint8_t* cbase, size_t cpitch, int W, int H, int X, int Y) {
+    const Taps t = mkTaps<6>(X - 16, Y - 16, (W + 1) >> 1, (H + 1) >> 1);
+    const float2 c00 = ctexel<F>(cbase, cpitch, t.x0, t.y0), c01 = ctexel<F>(cbase, cpitch, t.x1, t.y0);
+    const float2 c10 = ctexel<F>(cbase, cpitch, t.x0, t.y1), c11 = ctexel<F>(cbase, cpitch, t.x1, t.y1);
+    return make_float2(bil(t, c00.x, c01.x, c10.x, c11.x), bil(t, c00.y, c01.y, c10.y, c11.y));
+}
+
+// the warped sample at (px, py): Rgb10 RGB levels, F16 values, YUV (Y, Cb, Cr) levels
+template <int F>
+__device__ __forceinline__ void warp(const SynthParams& p, const uint8_t* base, const uint8_t* cbase, float px, float py,
+                                     float out[3]) {
+    const int X = rne32(px), Y = rne32(py);
+    const Taps t = mkTaps<5>(X, Y, p.W, p.H);
+    float r00[3], r01[3], r10[3], r11[3];
+    texel<F>(p.f, base, p.pitch, t.x0, t.y0, r00);
+    texel<F>(p.f, base, p.pitch, t.x1, t.y0, r01);
+    texel<F>(p.f, base, p.pitch, t.x0, t.y1, r10);
+    texel<F>(p.f, base, p.pitch, t.x1, t.y1, r11);
+    if (F == kFmtNv12 || F == kFmtP010) {
+        out[0] = bil(t, r00[0], r01[0], r10[0], r11[0]);
+        const float2 c = warpChroma<F>(cbase, p.cpitch, p.W, p.H, X, Y);
+        out[1] = c.x;
+        out[2] = c.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float r = bil(t, r00[k], r01[k], r10[k], r11[k]);
+            out[k] = F == kFmtRgb10 ? __fmul_rn(r, p.f.k10) : r;
+        }
+    }
+}
+
+// format.glsl FG_DIFF + FG_PACKE: the max-channel difference in levels, truncated, at most 255
+template <int F>
+__device__ __forceinline__ int mismatch(const FmtConst& f, const float wa[3], const float wc[3]) {
+    float m;
+    if (F == kFmtNv12 || F == kFmtP010) {
+        const float dy = __fsub_rn(wa[0], wc[0]), db = __fsub_rn(wa[1], wc[1]), dr = __fsub_rn(wa[2], wc[2]);
+        const float y = __fmul_rn(f.ys, dy);
+        const float r = __fadd_rn(y, __fmul_rn(f.rcr, dr));
+        const float g = __fadd_rn(__fadd_rn(y, __fmul_rn(f.gcb, db)), __fmul_rn(f.gcr, dr));
+        const float b = __fadd_rn(y, __fmul_rn(f.bcb, db));
+        m = fmaxf(fabsf(r), fmaxf(fabsf(g), fabsf(b)));
+    } else {
+        m = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float d;
+            if (F == kFmtF16 && f.linear) d = fabsf(__fsub_rn(fmtPq255(wa[k], f.kWhite), fmtPq255(wc[k], f.kWhite)));
+            else if (F == kFmtF16) d = fabsf(__fsub_rn(__fmul_rn(wa[k], 255.0f), __fmul_rn(wc[k], 255.0f)));
+            else d = fabsf(__fsub_rn(wa[k], wc[k]));
+            m = fmaxf(m, d);
+        }
+    }
+    return (int)fminf(m, 255.0f);
+}
+
+// resolve.comp: m = 0.5 (a + c) at t = 0.5, else (1 - t) a + t c; out = m (1 - u) + n u
+__device__ __forceinline__ float blendF(float a, float c, float n, float u, float iu, const SynthParams& p) {
+    const float m = p.mid ? __fmul_rn(0.5f, __fadd_rn(a, c)) : __fadd_rn(__fmul_rn(p.wA, a), __fmul_rn(p.wC, c));
+    return __fadd_rn(__fmul_rn(m, iu), __fmul_rn(n, u));
+}
+
+// the nearer frame over one output pixel (and, for YUV, the chroma texel of an even-even pixel)
+template <int F>
+__device__ __forceinline__ void copyNear(const SynthParams& p, int x, int y) {
+    const uint8_t* n = p.nearC ? p.c : p.a;
+    uint8_t* o = p.out + (size_t)y * p.outPitch;
+    if (F == kFmtRgb10) {
+        reinterpret_cast<uint32_t*>(o)[x] = ldw(n, p.pitch, x, y);
+    } else if (F == kFmtF16) {
+        reinterpret_cast<uint2*>(o)[x] = __ldg(reinterpret_cast<const uint2*>(n + (size_t)y * p.pitch) + x);
+    } else {
+        if (F == kFmtNv12) o[x] = __ldg(n + (size_t)y * p.pitch + x);
+        else reinterpret_cast<unsigned short*>(o)[x] = (unsigned short)ldh(n, p.pitch, x, y);
+        if (((x | y) & 1) == 0) {
+            const uint8_t* nc = p.nearC ? p.cc : p.ac;
+            uint8_t* oc = p.outc + (size_t)(y >> 1) * p.outCPitch;
+            if (F == kFmtNv12)
+                reinterpret_cast<unsigned short*>(oc)[x >> 1] =
+                    __ldg(reinterpret_cast<const unsigned short*>(nc + (size_t)(y >> 1) * p.cpitch) + (x >> 1));
+            else
+                reinterpret_cast<uint32_t*>(oc)[x >> 1] = ldw(nc, p.cpitch, x >> 1, y >> 1);
+        }
+    }
+}
+
+// ============================================================================================== synthesis
+// interp.synth for one t in the other formats: the 8-bit path's tile (k_synth) with each format's warp, mismatch,
+// blend and store (resolve.comp:48-83). YUV: the chroma of each 2x2 block is written with its even-even pixel, warped
+// from the block centre with that pixel's half-vector and blended with that pixel's trust.
+template <int F>
+__global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
+    pdlEnter();
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ SyCoef rowc[kSyEH];
+    __shared__ unsigned int cnt;
+    __shared__ int gReg[4];
+    const int X0 = blockIdx.x * kSyT, Y0 = blockIdx.y * kSyTH;
+    const int tid = threadIdx.x, ex = tid & (kSyE - 1), ey0 = tid / kSyE;
+    if (p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
+        for (int i = tid; i < kSyT * kSyTH; i += kSyThreads) {
+            const int x = X0 + (i % kSyT), y = Y0 + (i / kSyT);
+            if (x < p.W && y < p.H) copyNear<F>(p, x, y);
+        }
+        return;
+    }
+    if (tid == 0) cnt = 0;
+    float2* hrow;
+    uint8_t* e;
+    unsigned short* hsum;
+    const SyCoef cx = syFieldStage(p, X0, Y0, tid, ex, ey0, rowc, gReg, sm, hrow, e, hsum);
+    const float kA = p.mid ? 1.0f : p.ka, kC = p.mid ? 1.0f : p.kc;
+    // 2. the mismatch over the region
+    for (int k = 0; k < kSyK; k++) {
+        const int ey = ey0 + (kSyThreads / kSyE) * k;
+        const SyCoef cy = rowc[ey];
+        const float2 h = syHalfVec(cy, hrow, ex);
+        float wa[3], wc[3];
+        warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
+        warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
+        e[ey * kSyE + ex] = (uint8_t)mismatch<F>(p.f, wa, wc);
+    }
+    __syncthreads();
+    // 3. horizontal 7-sums (as k_synth)
+    {
+        const int r = tid >> 4, c0 = (tid & 15) * 8;
+        const uint8_t* q = e + r * kSyE + c0;
+        unsigned short* o = hsum + r * kSyE + c0;
+        unsigned int sum = q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6];
+        o[0] = (unsigned short)sum;
+#pragma unroll
+        for (int c = 1; c < 8; c++) {
+            if (c0 + c + 6 < kSyE) sum += q[c + 6] - q[c - 1];
+            o[c] = (unsigned short)sum;
+        }
+    }
+    __syncthreads();
+    // 4. output pixels: vertical 7-sum, trust, the warps again, blend, store
+    unsigned int myCnt = 0;
+    const int lx = ex - kSyAp, x = X0 + lx;
+    if ((unsigned)lx < (unsigned)kSyT && x < p.W) {
+        const uint8_t* nearF = p.nearC ? p.c : p.a;
+        for (int k = 0; k < kSyK; k++) {
+            const int ey = ey0 + (kSyThreads / kSyE) * k, ly = ey - kSyAp, y = Y0 + ly;
+            if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
+            const unsigned short* q = hsum + ly * kSyE + lx;
+            const int S = q[0] + q[kSyE] + q[2 * kSyE] + q[3 * kSyE] + q[4 * kSyE] + q[5 * kSyE] + q[6 * kSyE];
+            const float eb = (float)((double)S * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
+            const float u = clampF(__fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan), 0.0f, 1.0f);
+            myCnt += u > 0.5f;
+            const float iu = __fsub_rn(1.0f, u);
+            const SyCoef cy = rowc[ey];
+            const float2 h = syHalfVec(cy, hrow, ex);
+            float wa[3], wc[3];
+            warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
+            warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
+            uint8_t* orow = p.out + (size_t)y * p.outPitch;
+            if (F == kFmtRgb10) {
+                const uint32_t nw = ldw(nearF, p.pitch, x, y);
+                uint32_t ow = nw & 0xC0000000u;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float nl = __fmul_rn(i2f(rgb10(p.f, nw, c)), p.f.k10);
+                    const float v = clampF(blendF(wa[c], wc[c], nl, u, iu, p), 0.0f, 255.0f);
+                    const int code = clampi((int)floorf(__fadd_rn(__fmul_rn(v, p.f.k10i), 0.5f)), 0, 1023);
+                    ow |= (uint32_t)code << (p.f.rHigh ? 20 - 10 * c : 10 * c);
+                }
+                reinterpret_cast<uint32_t*>(orow)[x] = ow;
+            } else if (F == kFmtF16) {
+                const uint2 nq = __ldg(reinterpret_cast<const uint2*>(nearF + (size_t)y * p.pitch) + x);
+                const float n0 = h2f(nq.x & 0xFFFFu), n1 = h2f(nq.x >> 16), n2 = h2f(nq.y & 0xFFFFu);
+                const uint32_t o0 = __half_as_ushort(__float2half_rn(blendF(wa[0], wc[0], n0, u, iu, p)));
+                const uint32_t o1 = __half_as_ushort(__float2half_rn(blendF(wa[1], wc[1], n1, u, iu, p)));
+                const uint32_t o2 = __half_as_ushort(__float2half_rn(blendF(wa[2], wc[2], n2, u, iu, p)));
+                reinterpret_cast<uint2*>(orow)[x] = make_uint2(o0 | (o1 << 16), o2 | (nq.y & 0xFFFF0000u));
+            } else {
+                constexpr float ql = F == kFmtP010 ? 4.0f : 1.0f;   // 1 / YU_QL
+                constexpr int codes = F == kFmtP010 ? 1023 : 255;
+                float ny[3];
+                texel<F>(p.f, nearF, p.pitch, x, y, ny);
+                const float v = blendF(wa[0], wc[0], ny[0], u, iu, p);
+                const int code = clampi((int)floorf(__fadd_rn(__fmul_rn(v, ql), 0.5f)), 0, codes);
+                if (F == kFmtP010) reinterpret_cast<unsigned short*>(orow)[x] = (unsigned short)(code << 6);
+                else orow[x] = (uint8_t)code;
+                if (((x | y) & 1) == 0) {   // the chroma of this 2x2 block, warped from its centre
+                    const float bx = __fadd_rn(cx.pos, 0.5f), by = __fadd_rn(cy.pos, 0.5f);
+                    const float2 ca = warpChroma<F>(p.ac, p.cpitch, p.W, p.H, rne32(__fsub_rn(bx, __fmul_rn(kA, h.x))),
+                                                    rne32(__fsub_rn(by, __fmul_rn(kA, h.y))));
+                    const float2 cc = warpChroma<F>(p.cc, p.cpitch, p.W, p.H, rne32(__fadd_rn(bx, __fmul_rn(kC, h.x))),
+                                                    rne32(__fadd_rn(by, __fmul_rn(kC, h.y))));
+                    const float2 nc = ctexel<F>(p.nearC ? p.cc : p.ac, p.cpitch, x >> 1, y >> 1);
+                    const int cb = clampi((int)floorf(__fadd_rn(__fmul_rn(blendF(ca.x, cc.x, nc.x, u, iu, p), ql), 0.5f)), 0, codes);
+                    const int cr = clampi((int)floorf(__fadd_rn(__fmul_rn(blendF(ca.y, cc.y, nc.y, u, iu, p), ql), 0.5f)), 0, codes);
+                    uint8_t* oc = p.outc + (size_t)(y >> 1) * p.outCPitch;
+                    if (F == kFmtP010) reinterpret_cast<uint32_t*>(oc)[x >> 1] = ((uint32_t)cb << 6) | ((uint32_t)cr << 22);
+                    else reinterpret_cast<unsigned short*>(oc)[x >> 1] = (unsigned short)(cb | (cr << 8));
+                }
+            }
+            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[ey * kSyE + ex];
+        }
+    }
+    if (myCnt) atomicAdd(&cnt, myCnt);
+    __syncthreads();
+    if (tid == 0 && cnt) atomicAdd(p.untrusted, cnt);
+}
+
+// interp.py:238-239 for the other formats: more than globalFallback of the pixels untrusted -> the nearer real frame
+// (both planes of YUV) over the output. Every CTA exits at once in the normal case; clears the next synth's counter.
+__global__ void __launch_bounds__(256) k_fallback_fmt(const FallbackParams p) {
+    pdlEnter();
+    const unsigned int cnt = *p.untrusted;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *p.untrustedNext = 0;
+    if (!((double)cnt / ((double)p.W * (double)p.H) > p.frac)) return;
+    const uint8_t* n = p.nearC ? p.c : p.a;
+    const size_t stride = (size_t)gridDim.x * 256;
+    const size_t n0 = p.rowBytes * (size_t)p.H;
+    for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < n0; i += stride) {
+        const size_t y = i / p.rowBytes, b = i % p.rowBytes;
+        p.out[y * p.outPitch + b] = __ldg(n + y * p.pitch + b);
+    }
+    if (p.outc) {
+        const uint8_t* nc = p.nearC ? p.cc : p.ac;
+        const size_t n1 = p.cbytes * (size_t)p.ch;
+        for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < n1; i += stride) {
+            const size_t y = i / p.cbytes, b = i % p.cbytes;
+            p.outc[y * p.outCPitch + b] = __ldg(nc + y * p.cpitch + b);
+        }
+    }
+}
+
+// ============================================================================================== launchers
+cudaError_t prepareFormatKernels() {
+    const int smem = (int)synthSmemBytes(1);
+    cudaError_t e = cudaFuncSetAttribute(k_synth_fmt<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
+
+cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s) {
+    const dim3 grid(divUp(p.lw[0], 32), divUp(p.lh[0], 32));
+    switch (p.f.format) {
+        case kFmtRgb10: return launchPdl(k_luma_fmt<kFmtRgb10>, grid, dim3(256), 0, s, p);
+        case kFmtF16: return launchPdl(k_luma_fmt<kFmtF16>, grid, dim3(256), 0, s, p);
+        case kFmtNv12: return launchPdl(k_luma_fmt<kFmtNv12>, grid, dim3(256), 0, s, p);
+        case kFmtP010: return launchPdl(k_luma_fmt<kFmtP010>, grid, dim3(256), 0, s, p);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
+    const dim3 grid(divUp(p.W, kSyT), divUp(p.H, kSyTH));
+    const size_t smem = synthSmemBytes(p.fs);
+    switch (p.f.format) {
+        case kFmtRgb10: return launchPdl(k_synth_fmt<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
+        case kFmtF16: return launchPdl(k_synth_fmt<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);
+        case kFmtNv12: return launchPdl(k_synth_fmt<kFmtNv12>, grid, dim3(kSyThreads), smem, s, p);
+        case kFmtP010: return launchPdl(k_synth_fmt<kFmtP010>, grid, dim3(kSyThreads), smem, s, p);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s) {
+    return launchPdl(k_fallback_fmt, dim3(148 * 4), dim3(256), 0, s, p);
+}
+
+}  // namespace fgk

@@ -26,6 +26,17 @@ struct DevState {
 
 enum : unsigned int { kErrHistRange = 1u, kErrPlan = 2u };
 
+// Frame formats other than 8-bit RGBA (framegen::Format) and their constants, computed on the host from InitInfo
+enum : int { kFmtRgba8 = 0, kFmtRgb10 = 1, kFmtF16 = 2, kFmtNv12 = 3, kFmtP010 = 4 };
+struct FmtConst {
+    int format;                    // kFmt*
+    int rHigh;                     // Rgb10: R in bits 20..29 (A2R10G10B10) rather than 0..9 (A2B10G10R10)
+    int linear;                    // RgbaF16: Transfer::Linear, the mismatch in PQ codes
+    float kWhite;                  // RgbaF16 linear: fl32(linearWhiteNits / 10000)
+    float k10, k10i;               // Rgb10: fl32(255 / 1023), fl32(1023 / 255)
+    float black, ys, rcr, bcb, gcb, gcr;   // YUV: luma black level, luma gain, Cr/Cb -> R'G'B' (gpu/framegen.cpp:1518-1533)
+};
+
 struct LumaPyrParams {
     const uint8_t* a;
     const uint8_t* c;
@@ -37,11 +48,13 @@ struct LumaPyrParams {
     int lw[kPyrInKernel], lh[kPyrInKernel];
     float* la[kPyrInKernel];
     float* lc[kPyrInKernel];
+    FmtConst f;            // the luma kernel of the other formats (k_luma_fmt)
 };
 
 struct DownParams {         // one further pyramid level (INTER_AREA 0.5)
     const float* sa; const float* sc; int sw, sh;
     float* da; float* dc; int dw, dh;
+    int round10;               // the other formats: round each mean to a multiple of 2^-10
 };
 
 struct SearchParams {
@@ -118,6 +131,10 @@ struct SynthParams {
     DevState* st;
     unsigned int* untrusted;       // this synth's counter (zero on entry)
     uint8_t* emap;                 // optional: per-pixel mismatch before the box (debug maps), W bytes per row
+    // the other formats (k_synth_fmt): constants and the CbCr planes of YUV frames (chroma pitch shared by a and c)
+    FmtConst f;
+    const uint8_t* ac; const uint8_t* cc; size_t cpitch;
+    uint8_t* outc; size_t outCPitch;
 };
 
 struct FallbackParams {
@@ -127,6 +144,11 @@ struct FallbackParams {
     double frac;                   // globalFallback
     const unsigned int* untrusted;
     unsigned int* untrustedNext;   // the next synth's counter, zeroed here
+    // the other formats (k_fallback_fmt): bytes per row of plane 0, and the CbCr planes (rows of cbytes bytes, ch rows)
+    size_t rowBytes, cbytes;
+    int ch;
+    const uint8_t* ac; const uint8_t* cc; size_t cpitch;
+    uint8_t* outc; size_t outCPitch;
 };
 
 // once per process and device: the dynamic shared-memory limits of the kernels that need more than 48 KB
@@ -143,5 +165,10 @@ cudaError_t launchCutMean(const CutMeanParams& p, cudaStream_t s);
 cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s);
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s);
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s);
+// the other formats (fg_formats.cu)
+cudaError_t prepareFormatKernels();
+cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s);
+cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s);
+cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s);
 
 }  // namespace fgk

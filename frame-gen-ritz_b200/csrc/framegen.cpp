@@ -136,12 +136,39 @@ const char* kErrSettings = "invalid settings: a field is out of range or not fin
 const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
 const char* kErrUi = "static-UI protection is not built into this library (Settings::uiProtection must be Off)";
 const char* kErrNoFormat = "unsupported viewFormat (see framegen::Format)";
-const char* kErrFormatNotBuilt = "the kernels of this format are not built into the library";
+const char* kErrYuvMatrix = "yuvMatrix must be Bt601, Bt709 or Bt2020";
 const char* kErrNits = "linearWhiteNits must be in (0, 10000]";
 const char* kErrMinSize = "the frame size is below Interpolator::kMinSize (16 pixels) in width or height";
 const char* kErrMaxSize = "the frame size exceeds 2^30 pixels (32-bit indexing of the library's buffers)";
 const char* kErrDevice = "CUDA device not available";
 const char* kErrAlloc = "CUDA device memory allocation failed";
+
+// the per-format constants of the kernels (gpu/framegen.cpp:1508-1539 for YUV; fg_formats.cu for their use)
+fgk::FmtConst makeFmtConst(Format fmt, uint32_t viewFormat, const InitInfo& ii) {
+    fgk::FmtConst c{};
+    c.format = (int)fmt;
+    c.rHigh = viewFormat == kVkFormatA2R10G10B10UnormPack32;
+    c.linear = ii.transfer == Transfer::Linear;
+    c.kWhite = ii.linearWhiteNits / 10000.0f;
+    c.k10 = (float)(255.0 / 1023.0);
+    c.k10i = (float)(1023.0 / 255.0);
+    double kr = 0.2126, kb = 0.0722;   // BT.709
+    if (ii.yuvMatrix == YuvMatrix::Bt601) { kr = 0.299; kb = 0.114; }
+    if (ii.yuvMatrix == YuvMatrix::Bt2020) { kr = 0.2627; kb = 0.0593; }
+    const double kg = 1.0 - kr - kb;
+    const double sY = ii.yuvFullRange ? 1.0 : 255.0 / 219.0, sC = ii.yuvFullRange ? 1.0 : 255.0 / 224.0;
+    c.black = ii.yuvFullRange ? 0.0f : 16.0f;
+    c.ys = (float)sY;
+    c.rcr = (float)(sC * 2.0 * (1.0 - kr));
+    c.bcb = (float)(sC * 2.0 * (1.0 - kb));
+    c.gcb = (float)(-sC * 2.0 * (1.0 - kb) * kb / kg);
+    c.gcr = (float)(-sC * 2.0 * (1.0 - kr) * kr / kg);
+    return c;
+}
+
+// bytes per pixel of plane 0 and per texel of the CbCr plane (0: none)
+int planeBytes(Format f) { return f == Format::RgbaF16 ? 8 : (f == Format::Nv12 ? 1 : (f == Format::P010 ? 2 : 4)); }
+int chromaBytes(Format f) { return f == Format::Nv12 ? 2 : (f == Format::P010 ? 4 : 0); }
 
 struct DeviceGuard {   // makes `dev` current for the scope, restores the caller's device after
     int old = -1;
@@ -177,6 +204,7 @@ struct Interpolator::Impl {
     Format fmt = Format::Rgba8;
     uint32_t viewFormat = kVkFormatB8G8R8A8Unorm;
     int ri = 2, gi = 1, bi = 0;
+    fgk::FmtConst fc{};
     InitInfo info{};
     Settings set{};
     uint32_t W = 0, H = 0;
@@ -285,8 +313,17 @@ struct Interpolator::Impl {
         return nullptr;
     }
 
+    // a frame the kernels can address: plane 0 (and the CbCr plane of YUV) aligned to its sample size, rows wide enough
     bool frameOk(const Frame& f) const {
-        return f.data && f.pitch >= (size_t)W * 4 && f.pitch % 4 == 0 && ((uintptr_t)f.data & 3) == 0;
+        const size_t bpp = (size_t)planeBytes(fmt), cb = (size_t)chromaBytes(fmt);
+        const size_t al = fmt == Format::Nv12 ? 1 : bpp;
+        if (!f.data || f.pitch < (size_t)W * bpp || f.pitch % al || ((uintptr_t)f.data % al)) return false;
+        if (!cb) return true;
+        return f.chroma && f.chromaPitch >= (size_t)((W + 1) / 2) * cb && f.chromaPitch % cb == 0 &&
+               (uintptr_t)f.chroma % cb == 0;
+    }
+    bool samePitch(const Frame& a, const Frame& b) const {
+        return a.pitch == b.pitch && (!chromaBytes(fmt) || a.chromaPitch == b.chromaPitch);
     }
 
     // --- profiling (gpu/framegen.cpp Rec::stamp)
@@ -318,18 +355,19 @@ struct Interpolator::Impl {
         lp.W = (int)W; lp.H = (int)H; lp.fs = (int)set.flowScale;
         lp.ri = ri; lp.gi = gi; lp.bi = bi;
         lp.nlev = std::min(n, fgk::kPyrInKernel);
-        lp.vec16 = set.flowScale == 2 && prev.pitch % 16 == 0 && ((uintptr_t)prev.data & 15) == 0 && ((uintptr_t)curr.data & 15) == 0 &&
+        lp.f = fc;
+        lp.vec16 = fmt == Format::Rgba8 && set.flowScale == 2 && prev.pitch % 16 == 0 && ((uintptr_t)prev.data & 15) == 0 && ((uintptr_t)curr.data & 15) == 0 &&
                    W % 4 == 0 && H % 2 == 0;   // complete 2x2 cells in every full tile, 8-byte aligned level-0 rows
         for (int l = 0; l < lp.nlev; l++) {
             lp.lw[l] = L.lv[l].w; lp.lh[l] = L.lv[l].h;
             lp.la[l] = luma + L.lv[l].lumaA; lp.lc[l] = luma + L.lv[l].lumaC;
         }
         if (prev.pitch != curr.pitch) return false;
-        if (!check(fgk::launchLumaPyr(lp, s))) return false;
+        if (!check(fmt == Format::Rgba8 ? fgk::launchLumaPyr(lp, s) : fgk::launchLumaFmt(lp, s))) return false;
         stamp(s, "luma");
         for (int l = fgk::kPyrInKernel; l < n; l++) {
             fgk::DownParams dp{luma + L.lv[l - 1].lumaA, luma + L.lv[l - 1].lumaC, L.lv[l - 1].w, L.lv[l - 1].h,
-                               luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h};
+                               luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h, fmt != Format::Rgba8};
             if (!check(fgk::launchDown(dp, s))) return false;
         }
         stamp(s, "pyramid");
@@ -413,7 +451,10 @@ struct Interpolator::Impl {
         sp.st = st;
         sp.untrusted = &st->untrusted[parity];
         sp.emap = capture ? emap : nullptr;
-        if (!check(fgk::launchSynth(sp, s))) return false;
+        sp.f = fc;
+        sp.ac = (const uint8_t*)prev.chroma; sp.cc = (const uint8_t*)curr.chroma; sp.cpitch = prev.chromaPitch;
+        sp.outc = (uint8_t*)out.chroma; sp.outCPitch = out.chromaPitch;
+        if (!check(fmt == Format::Rgba8 ? fgk::launchSynth(sp, s) : fgk::launchSynthFmt(sp, s))) return false;
         stamp(s, "synth");
         fgk::FallbackParams fp{};
         fp.a = sp.a; fp.c = sp.c; fp.pitch = sp.pitch; fp.out = sp.out; fp.outPitch = sp.outPitch;
@@ -421,7 +462,13 @@ struct Interpolator::Impl {
         fp.frac = (double)set.globalFallback;
         fp.untrusted = &st->untrusted[parity];
         fp.untrustedNext = &st->untrusted[parity ^ 1u];
-        if (!check(fgk::launchFallback(fp, s))) return false;
+        fp.rowBytes = (size_t)W * planeBytes(fmt);
+        if (chromaBytes(fmt)) {
+            fp.cbytes = (size_t)((W + 1) / 2) * chromaBytes(fmt);
+            fp.ch = (int)(H + 1) / 2;
+            fp.ac = sp.ac; fp.cc = sp.cc; fp.cpitch = sp.cpitch; fp.outc = sp.outc; fp.outCPitch = sp.outCPitch;
+        }
+        if (!check(fmt == Format::Rgba8 ? fgk::launchFallback(fp, s) : fgk::launchFallbackFmt(fp, s))) return false;
         stamp(s, "fallback");
         lastParity = parity;
         parity ^= 1u;
@@ -470,10 +517,13 @@ bool Interpolator::init(const InitInfo& ii) {
     Format fmt;
     if (!validate(ii.settings)) { err_ = "missing device, or invalid settings"; return false; }
     if (!formatOf(ii.viewFormat, &fmt)) { err_ = kErrNoFormat; return false; }
-    if (fmt != Format::Rgba8) { err_ = kErrFormatNotBuilt; return false; }
     if (const char* e = settingsError(ii.settings, fmt)) { err_ = e; return false; }
     if (fmt == Format::RgbaF16 && ii.transfer == Transfer::Linear && !(ii.linearWhiteNits > 0.0f && ii.linearWhiteNits <= 10000.0f)) {
         err_ = kErrNits;
+        return false;
+    }
+    if ((fmt == Format::Nv12 || fmt == Format::P010) && (uint32_t)ii.yuvMatrix > (uint32_t)YuvMatrix::Bt2020) {
+        err_ = kErrYuvMatrix;
         return false;
     }
     if (ii.width < kMinSize || ii.height < kMinSize) { err_ = kErrMinSize; return false; }
@@ -484,7 +534,11 @@ bool Interpolator::init(const InitInfo& ii) {
     if (dev >= ndev) { err_ = kErrDevice; return false; }
     {
         DeviceGuard g(dev);
-        if (fgk::prepareKernels() != cudaSuccess) { cudaGetLastError(); err_ = kErrDevice; return false; }
+        if (fgk::prepareKernels() != cudaSuccess || fgk::prepareFormatKernels() != cudaSuccess) {
+            cudaGetLastError();
+            err_ = kErrDevice;
+            return false;
+        }
     }
     m = new Impl();
     m->device = dev;
@@ -495,6 +549,7 @@ bool Interpolator::init(const InitInfo& ii) {
     m->ri = ii.viewFormat == kVkFormatR8G8B8A8Unorm ? 0 : 2;
     m->gi = 1;
     m->bi = ii.viewFormat == kVkFormatR8G8B8A8Unorm ? 2 : 0;
+    m->fc = makeFmtConst(fmt, ii.viewFormat, ii);
     m->updateTrust();
     if (const char* e = m->allocSize(ii.width, ii.height)) {
         err_ = e;
@@ -520,6 +575,7 @@ bool Interpolator::resize(uint32_t w, uint32_t h, uint32_t viewFormat) {
     m->viewFormat = viewFormat;
     m->ri = viewFormat == kVkFormatR8G8B8A8Unorm ? 0 : 2;
     m->bi = viewFormat == kVkFormatR8G8B8A8Unorm ? 2 : 0;
+    m->fc = makeFmtConst(m->fmt, viewFormat, m->info);
     return m->allocSize(w, h) == nullptr;
 }
 
@@ -550,7 +606,7 @@ void Interpolator::beginFrame() {
 
 bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
     if (!m || !m->W) return false;
-    if (!m->frameOk(prev) || !m->frameOk(curr) || prev.pitch != curr.pitch) return false;
+    if (!m->frameOk(prev) || !m->frameOk(curr) || !m->samePitch(prev, curr)) return false;
     if (m->estSets >= kSetRing) return false;
     DeviceGuard g(m->device);
     m->estSets++;
@@ -565,7 +621,7 @@ bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
 bool Interpolator::recordSynth(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t) {
     if (!m || !m->W || !(t > 0.0f && t < 1.0f)) return false;
     if (!m->haveEst || prev.data != m->estPrev || curr.data != m->estCurr) return false;
-    if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || prev.pitch != curr.pitch) return false;
+    if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || !m->samePitch(prev, curr)) return false;
     if (m->synthSets >= kSetRing) return false;
     DeviceGuard g(m->device);
     m->synthSets++;

@@ -154,9 +154,12 @@ def _s(b):
 
 
 def frame_of(t, chroma=None):
-    """A CFrame for a CUDA tensor (H, W, C) uint8 (pitch = the row stride in bytes)."""
+    """A CFrame for a CUDA tensor (pitch = the row stride in bytes): (H, W, 4) uint8 for Rgba8, (H, W) int32 words
+    for Rgb10, (H, W, 4) float16 for RgbaF16; Nv12 / P010 frames are (Y plane, CbCr plane) tuples or pass chroma."""
     if t is None:
         return None
+    if isinstance(t, tuple):
+        t, chroma = t
     f = CFrame()
     f.data = t.data_ptr()
     f.pitch = t.stride(0) * t.element_size()

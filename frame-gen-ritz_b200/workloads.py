@@ -137,3 +137,58 @@ def contrast_pair(W=160, H=96, seed=0, kind="cut"):
     else:
         c = np.clip(_shift(a, 3, -2) * 0.6 + 0.2 + rng.normal(0, 0.12, a.shape), 0, 1)
     return _to_rgba(a), _to_rgba(c)
+
+
+# ---------------------------------------------------------------------------------------------- other frame formats
+# Conversions of the 8-bit RGBA pairs above into the library's other formats (framegen::Format), deterministic per
+# pixel value so a pair keeps its motion: Rgb10 words, RgbaF16 (linear light log-uniform in 1e-3..10, or display
+# encoded), Nv12 / P010 planes (BT.601 / 709 / 2020, limited or full range, 4:2:0 chroma from 2x2 means).
+_KR_KB = {"bt601": (0.299, 0.114), "bt709": (0.2126, 0.0722), "bt2020": (0.2627, 0.0593)}
+
+
+def to_rgb10(rgba, r_high=False):
+    """(H, W) uint32 A2B10G10R10 words (A2R10G10B10 with r_high): code = 4 v + (v >> 6), alpha 3."""
+    v = rgba[..., :3].astype(np.uint32)
+    c = 4 * v + (v >> 6)
+    r, g, b = c[..., 0], c[..., 1], c[..., 2]
+    lo, hi = (b, r) if r_high else (r, b)
+    return (np.uint32(3) << 30) | (hi << 20) | (g << 10) | lo
+
+
+def to_f16(rgba, linear=True):
+    """(H, W, 4) float16: linear light 10^(-3 + 4 v / 255) (log-uniform in 1e-3..10), or encoded v / 255; alpha 1."""
+    v = rgba[..., :3].astype(np.float64) / 255.0
+    rgb = 10.0 ** (-3.0 + 4.0 * v) if linear else v
+    out = np.empty(rgba.shape[:2] + (4,), np.float16)
+    out[..., :3] = rgb.astype(np.float16)
+    out[..., 3] = 1.0
+    return out
+
+
+def to_yuv(rgba, bits=8, matrix="bt709", full_range=False):
+    """(Y, CbCr) planes: Nv12 (bits 8: uint8) or P010 (bits 10: uint16 words, the code in the high 10 bits).
+    Y' = kr R' + kg G' + kb B', Cb = (B' - Y') / (2 (1 - kb)), Cr = (R' - Y') / (2 (1 - kr)); chroma = the mean of
+    each 2x2 block (edge pixels repeated for odd sizes)."""
+    kr, kb = _KR_KB[matrix]
+    kg = 1.0 - kr - kb
+    e = rgba[..., :3].astype(np.float64) / 255.0
+    y = kr * e[..., 0] + kg * e[..., 1] + kb * e[..., 2]
+    cb = (e[..., 2] - y) / (2.0 * (1.0 - kb))
+    cr = (e[..., 0] - y) / (2.0 * (1.0 - kr))
+    H, W = y.shape
+    ph, pw = H + (H & 1), W + (W & 1)
+    cbp = np.pad(cb, ((0, ph - H), (0, pw - W)), mode="edge")
+    crp = np.pad(cr, ((0, ph - H), (0, pw - W)), mode="edge")
+    cbm = cbp.reshape(ph // 2, 2, pw // 2, 2).mean(axis=(1, 3))
+    crm = crp.reshape(ph // 2, 2, pw // 2, 2).mean(axis=(1, 3))
+    q = 1 << (bits - 8)
+    top = (1 << bits) - 1
+    if full_range:
+        yc, cbc, crc = y * top, 128 * q + cbm * top, 128 * q + crm * top
+    else:
+        yc, cbc, crc = 16 * q + 219 * q * y, 128 * q + 224 * q * cbm, 128 * q + 224 * q * crm
+    Y = np.clip(np.rint(yc), 0, top).astype(np.uint32)
+    C = np.stack([np.clip(np.rint(cbc), 0, top), np.clip(np.rint(crc), 0, top)], axis=2).astype(np.uint32)
+    if bits == 8:
+        return Y.astype(np.uint8), C.astype(np.uint8)
+    return (Y << 6).astype(np.uint16), (C << 6).astype(np.uint16)

@@ -33,13 +33,7 @@
 #include <omp.h>
 #endif
 
-#define BLOCK 8
-#define MAXLV 16
-
-typedef struct fgo_settings {
-    float trustLow, trustHigh, globalFallback, sceneCutSad, hudBonus, smoothBonus, searchPenalty;
-    int searchRadius, searchRadiusTop, subpixel, flowScale, pyramidMinSide;
-} fgo_settings;
+#include "fg_oracle_internal.h"
 
 /* pixel layout of an 8-bit frame: 0 = R,G,B,A; 1 = B,G,R,A; 2 = B,G,R (interp.py's own, 3 bytes per pixel) */
 typedef struct img8 {
@@ -100,8 +94,9 @@ static void luma_area(const img8* m, int fs, float* out, int fw, int fh) {
         }
 }
 
-/* interp.pyramid :76: INTER_AREA 0.5 of a float level */
-static void area_half(const float* src, int sw, int sh, float* dst, int dw, int dh) {
+/* interp.pyramid :76: INTER_AREA 0.5 of a float level (round10: then rounded half-even to a multiple of 2^-10, the
+ * grid the restatement of the other frame formats keeps its coarse levels on) */
+void fgo_i_area_half(const float* src, int sw, int sh, float* dst, int dw, int dh, int round10) {
     #pragma omp parallel for schedule(static)
     for (int y = 0; y < dh; y++)
         for (int x = 0; x < dw; x++) {
@@ -112,14 +107,16 @@ static void area_half(const float* src, int sw, int sh, float* dst, int dw, int 
                     int yy = 2 * y + j, xx = 2 * x + i;
                     if (yy < sh && xx < sw) { s += src[(size_t)yy * sw + xx]; n++; }
                 }
-            dst[(size_t)y * dw + x] = n == 4 ? s * 0.25f : s / (float)n;
+            float v = n == 4 ? s * 0.25f : s / (float)n;
+            if (round10) v = nearbyintf(v * 1024.0f) * (1.0f / 1024.0f);
+            dst[(size_t)y * dw + x] = v;
         }
 }
 
 /* ---------------------------------------------------------------------------------------------- cv2 remap */
 
 /* one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a float plane (stride `cs` floats between pixels) */
-static inline float remap_f(const float* img, int w, int h, int cs, float x, float y) {
+float fgo_i_remap_f(const float* img, int w, int h, int cs, float x, float y) {
     int X = (int)nearbyintf(x * 32.0f), Y = (int)nearbyintf(y * 32.0f);
     int ix = X >> 5, iy = Y >> 5;
     float fx = (float)(X & 31) * (1.0f / 32.0f), fy = (float)(Y & 31) * (1.0f / 32.0f);
@@ -174,7 +171,7 @@ static lincoef lin_coeffs(int n_dst, int n_src, int clampw) {
 static void lin_free(lincoef c) { free(c.i0); free(c.i1); free(c.a0); free(c.a1); }
 
 /* cv2.resize(src (sh x sw x 2 float), (dw, dh), INTER_LINEAR) */
-static void resize_lin2(const float* src, int sw, int sh, float* dst, int dw, int dh) {
+void fgo_i_resize_lin2(const float* src, int sw, int sh, float* dst, int dw, int dh) {
     lincoef cx = lin_coeffs(dw, sw, 1), cy = lin_coeffs(dh, sh, 0);
     float* rows = malloc(sizeof(float) * (size_t)sh * dw * 2);
     #pragma omp parallel for schedule(static)
@@ -232,8 +229,8 @@ static float block_sad1(const float* la, const float* lc, int w, int h, int bx, 
     for (int y = 0; y < BLOCK; y++)
         for (int x = 0; x < BLOCK; x++) {
             float gx = (float)(bx * BLOCK + x), gy = (float)(by * BLOCK + y);
-            float a = remap_f(la, w, h, 1, gx - vx, gy - vy);
-            float c = remap_f(lc, w, h, 1, gx + vx, gy + vy);
+            float a = fgo_i_remap_f(la, w, h, 1, gx - vx, gy - vy);
+            float c = fgo_i_remap_f(lc, w, h, 1, gx + vx, gy + vy);
             sum += (double)absf(a - c);
         }
     return (float)sum / 64.0f;
@@ -338,7 +335,7 @@ static void seed_from(const float* v, int pw, int ph, const float* la, const flo
 /* ---------------------------------------------------------------------------------------------- pixel field */
 
 /* cv2.blur(err, (k, k), BORDER_REPLICATE) of a float plane: the window sum in double times 1/(k*k), to float */
-static void box_blur(const float* src, int w, int h, int k, float* dst) {
+void fgo_i_box_blur(const float* src, int w, int h, int k, float* dst) {
     int r = k / 2;
     double* hs = malloc(sizeof(double) * (size_t)w * h);
     #pragma omp parallel for schedule(static)
@@ -364,7 +361,7 @@ static void pixel_field(const float* v, int bw, int bh, const float* ya, const f
                         float smooth, float zero, float* pf) {
     size_t np_ = (size_t)w * h;
     float* bil = malloc(sizeof(float) * (size_t)bw * BLOCK * bh * BLOCK * 2);
-    resize_lin2(v, bw, bh, bil, bw * BLOCK, bh * BLOCK);
+    fgo_i_resize_lin2(v, bw, bh, bil, bw * BLOCK, bh * BLOCK);
     float* cand = malloc(sizeof(float) * np_ * 2 * 7);
     float* err = malloc(sizeof(float) * np_);
     float* cost = malloc(sizeof(float) * np_ * 7);
@@ -392,11 +389,11 @@ static void pixel_field(const float* v, int bw, int bh, const float* ya, const f
             for (int x = 0; x < w; x++) {
                 size_t q = (size_t)y * w + x;
                 float hx = cand[q * 14 + 2 * k], hy = cand[q * 14 + 2 * k + 1];
-                float a = remap_f(ya, w, h, 1, (float)x - hx, (float)y - hy);
-                float c = remap_f(yc, w, h, 1, (float)x + hx, (float)y + hy);
+                float a = fgo_i_remap_f(ya, w, h, 1, (float)x - hx, (float)y - hy);
+                float c = fgo_i_remap_f(yc, w, h, 1, (float)x + hx, (float)y + hy);
                 err[q] = absf(a - c);
             }
-        box_blur(err, w, h, 5, cost + np_ * k);
+        fgo_i_box_blur(err, w, h, 5, cost + np_ * k);
     }
     #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < np_; q++) {
@@ -437,16 +434,23 @@ int fgo_estimate(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, 
     if (n < 1) return -1;
     img8 A = mkimg(a8, W, H, pitch, order), C = mkimg(c8, W, H, pitch, order);
     float* L[MAXLV][2];
-    int bw[MAXLV], bh[MAXLV];
-    size_t lofs = 0, fofs = 0, sofs = 0;
-    for (int l = 0; l < n; l++) {
-        bw[l] = (lw[l] + 7) / 8; bh[l] = (lh[l] + 7) / 8;
+    for (int l = 0; l < n; l++)
         for (int k = 0; k < 2; k++) L[l][k] = malloc(sizeof(float) * (size_t)lw[l] * lh[l]);
-    }
     luma_area(&A, s->flowScale, L[0][0], fw, fh);
     luma_area(&C, s->flowScale, L[0][1], fw, fh);
     for (int l = 1; l < n; l++)
-        for (int k = 0; k < 2; k++) area_half(L[l - 1][k], lw[l - 1], lh[l - 1], L[l][k], lw[l], lh[l]);
+        for (int k = 0; k < 2; k++) fgo_i_area_half(L[l - 1][k], lw[l - 1], lh[l - 1], L[l][k], lw[l], lh[l], 0);
+    int r = fgo_i_estimate_levels(L, n, lw, lh, s, luma, fields, seeds, meds, sads, pf, sad_mean, cut);
+    for (int l = 0; l < n; l++) { free(L[l][0]); free(L[l][1]); }
+    return r;
+}
+
+int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, const fgo_settings* s, float* luma,
+                          float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean, int* cut) {
+    if (n < 1 || n > MAXLV) return -1;
+    int bw[MAXLV] = {0}, bh[MAXLV] = {0};
+    size_t lofs = 0, fofs = 0, sofs = 0;
+    for (int l = 0; l < n; l++) { bw[l] = (lw[l] + 7) / 8; bh[l] = (lh[l] + 7) / 8; }
     if (luma)
         for (int l = 0; l < n; l++)
             for (int k = 0; k < 2; k++) {
@@ -497,16 +501,15 @@ int fgo_estimate(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, 
     if (sads) memcpy(sads, sadbuf, sizeof(float) * nb0);
     *sad_mean = mean;
     *cut = (double)mean > (double)s->sceneCutSad;
-    pixel_field(v, bw[0], bh[0], L[0][0], L[0][1], fw, fh, s->smoothBonus, s->hudBonus, pf);
+    pixel_field(v, bw[0], bh[0], L[0][0], L[0][1], lw[0], lh[0], s->smoothBonus, s->hudBonus, pf);
     free(v); free(sadbuf);
-    for (int l = 0; l < n; l++) { free(L[l][0]); free(L[l][1]); }
     return n;
 }
 
 /* ---------------------------------------------------------------------------------------------- synth */
 
 /* interp.field_at: the midpoint-grid field looked up at time t (2 fixed-point bilinear steps) */
-static void field_at(const float* pf, int w, int h, float sf, float* out) {
+void fgo_i_field_at(const float* pf, int w, int h, float sf, float* out) {
     float* g = malloc(sizeof(float) * (size_t)w * h * 2);
     memcpy(g, pf, sizeof(float) * (size_t)w * h * 2);
     for (int it = 0; it < 2; it++) {
@@ -515,8 +518,8 @@ static void field_at(const float* pf, int w, int h, float sf, float* out) {
             for (int x = 0; x < w; x++) {
                 size_t q = (size_t)y * w + x;
                 float px = (float)x - sf * g[2 * q], py = (float)y - sf * g[2 * q + 1];
-                out[2 * q] = remap_f(pf, w, h, 2, px, py);
-                out[2 * q + 1] = remap_f(pf + 1, w, h, 2, px, py);
+                out[2 * q] = fgo_i_remap_f(pf, w, h, 2, px, py);
+                out[2 * q + 1] = fgo_i_remap_f(pf + 1, w, h, 2, px, py);
             }
         memcpy(g, out, sizeof(float) * (size_t)w * h * 2);
     }
@@ -550,11 +553,11 @@ int fgo_synth(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int
     float sf = (float)(2.0 * td - 1.0);
     float* g = malloc(sizeof(float) * (size_t)fw * fh * 2);
     if (sf == 0.0f) memcpy(g, pf, sizeof(float) * (size_t)fw * fh * 2);
-    else field_at(pf, fw, fh, sf, g);
+    else fgo_i_field_at(pf, fw, fh, sf, g);
     if (field_t) memcpy(field_t, g, sizeof(float) * (size_t)fw * fh * 2);
     int uw = fw * fs, uh = fh * fs;
     float* hv = malloc(sizeof(float) * (size_t)uw * uh * 2);
-    resize_lin2(g, fw, fh, hv, uw, uh);
+    fgo_i_resize_lin2(g, fw, fh, hv, uw, uh);
     free(g);
     float ka = (float)(2.0 * td), kc = (float)(2.0 * (1.0 - td));
     float wA = (float)(1.0 - td), wC = t;
@@ -588,7 +591,7 @@ int fgo_synth(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int
     free(hv);
     if (emap) memcpy(emap, e, (size_t)W * H);
     float* eb = malloc(sizeof(float) * (size_t)W * H);
-    box_blur(ef, W, H, 7, eb);
+    fgo_i_box_blur(ef, W, H, 7, eb);
     float t0 = s->trustLow, span = (float)((double)s->trustHigh - (double)s->trustLow);
     long long cnt = 0;
     #pragma omp parallel for schedule(static) reduction(+ : cnt)

@@ -176,3 +176,166 @@ def mean_f32(a):
     """numpy's float32 mean (pairwise) as restated in the oracle."""
     a = np.ascontiguousarray(a, np.float32).reshape(-1)
     return float(lib().fgo_mean_f32(_p(a), a.size))
+
+
+# ---------------------------------------------------------------------------------------------- other frame formats
+# Restated from the reference's shader math (fg_oracle_fmt.c): Rgb10, RgbaF16, Nv12, P010. Frames:
+#   rgb10: uint32 (H, W) pixel words;  f16: float16 (H, W, 4);  nv12: (Y uint8 (H, W), CbCr uint8 (ch, cw, 2));
+#   p010: (Y uint16 (H, W), CbCr uint16 (ch, cw, 2)), ch, cw = ceil(H / 2), ceil(W / 2).
+FORMATS = {"rgb10": 1, "f16": 2, "nv12": 3, "p010": 4}
+MATRICES = {"bt601": 0, "bt709": 1, "bt2020": 2}
+
+
+@dataclass
+class FormatSpec:
+    """A frame format and what InitInfo says about it (gpu/framegen.h:411-441)."""
+    format: str
+    r_high: bool = False        # rgb10: A2R10G10B10 (R in bits 20..29) rather than A2B10G10R10
+    linear: bool = False        # f16: Transfer::Linear (mismatch measured as PQ codes)
+    white: float = 80.0         # f16 linear: nits of 1.0
+    matrix: str = "bt709"       # yuv
+    full_range: bool = False    # yuv
+
+
+class _CFmt(ctypes.Structure):
+    _fields_ = [("format", ctypes.c_int), ("rHigh", ctypes.c_int), ("linear", ctypes.c_int)] + \
+               [(n, ctypes.c_float) for n in ("kWhite", "k10", "k10i", "black", "ys", "rcr", "bcb", "gcb", "gcr")]
+
+
+class _CFrame(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_void_p), ("pitch", ctypes.c_long), ("c", ctypes.c_void_p), ("cpitch", ctypes.c_long)]
+
+
+def _fmt_lib():
+    L = lib()
+    if not hasattr(L, "_fmt_ready"):
+        P = ctypes.c_void_p
+        L.fgo_fmt_init.argtypes = [ctypes.POINTER(_CFmt), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                   ctypes.c_int, ctypes.c_int]
+        L.fgo_estimate_fmt.argtypes = [ctypes.POINTER(_CFrame), ctypes.POINTER(_CFrame), ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(_CFmt), ctypes.POINTER(_CSettings)] + [P] * 8 + [ctypes.c_int]
+        L.fgo_estimate_fmt.restype = ctypes.c_int
+        L.fgo_synth_fmt.argtypes = [ctypes.POINTER(_CFrame), ctypes.POINTER(_CFrame), ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(_CFmt), ctypes.POINTER(_CSettings), P, ctypes.c_int, ctypes.c_float,
+                                    ctypes.POINTER(_CFrame), P, P, P, P, ctypes.c_int]
+        L.fgo_synth_fmt.restype = ctypes.c_int
+        for n in ("fgo_log2", "fgo_exp2"):
+            getattr(L, n).argtypes = [ctypes.c_float]
+            getattr(L, n).restype = ctypes.c_float
+        L.fgo_pq255.argtypes = [ctypes.c_float, ctypes.c_float]
+        L.fgo_pq255.restype = ctypes.c_float
+        L.fgo_f2h.argtypes = [ctypes.c_float]
+        L.fgo_f2h.restype = ctypes.c_uint16
+        L.fgo_h2f.argtypes = [ctypes.c_uint16]
+        L.fgo_h2f.restype = ctypes.c_float
+        L._fmt_ready = True
+    return L
+
+
+def fmt_struct(spec):
+    f = _CFmt()
+    _fmt_lib().fgo_fmt_init(ctypes.byref(f), FORMATS[spec.format], int(spec.r_high), int(spec.linear),
+                            float(spec.white), MATRICES[spec.matrix], int(spec.full_range))
+    return f
+
+
+def frame_size(frame, spec):
+    y = frame[0] if spec.format in ("nv12", "p010") else frame
+    return y.shape[1], y.shape[0]
+
+
+def _cframe(frame, spec):
+    if spec.format in ("nv12", "p010"):
+        y, uv = frame
+        return _CFrame(y.ctypes.data, y.strides[0], uv.ctypes.data, uv.strides[0])
+    return _CFrame(frame.ctypes.data, frame.strides[0], None, 0)
+
+
+def empty_like_frame(frame, spec):
+    if spec.format in ("nv12", "p010"):
+        return (np.zeros_like(frame[0]), np.zeros_like(frame[1]))
+    return np.zeros_like(frame)
+
+
+def estimate_fmt(a, c, spec, settings=None, trace=True, threads=0):
+    """estimate() for the other formats (same dict)."""
+    s = settings or Settings()
+    W, H = frame_size(a, spec)
+    L = layout(W, H, s.flowScale, s.pyramidMinSide)
+    nl = sum(2 * w * h for w, h, _, _ in L.levels)
+    nf = sum(4 * bw * bh for _, _, bw, bh in L.levels) + 4 * L.levels[0][2] * L.levels[0][3]
+    ns = sum(2 * bw * bh for _, _, bw, bh in L.levels)
+    luma = np.zeros(nl, np.float32) if trace else None
+    fields = np.zeros(nf, np.float32) if trace else None
+    seeds = np.zeros(ns, np.float32) if trace else None
+    meds = np.zeros(2 * len(L.levels), np.float32) if trace else None
+    nb0 = L.levels[0][2] * L.levels[0][3]
+    sads = np.zeros(nb0, np.float32)
+    pf = np.zeros((L.fh, L.fw, 2), np.float32)
+    mean, cut = ctypes.c_float(), ctypes.c_int()
+    fa, fc = _cframe(a, spec), _cframe(c, spec)
+    n = _fmt_lib().fgo_estimate_fmt(ctypes.byref(fa), ctypes.byref(fc), W, H, ctypes.byref(fmt_struct(spec)),
+                                    ctypes.byref(_cs(s)), _p(luma), _p(fields), _p(seeds), _p(meds), _p(sads), _p(pf),
+                                    ctypes.byref(mean), ctypes.byref(cut), threads)
+    if n != len(L.levels):
+        raise RuntimeError("fgo_estimate_fmt failed")
+    est = {"sad": float(mean.value), "cut": bool(cut.value), "pf": pf, "layout": L,
+           "sads": sads.reshape(L.levels[0][3], L.levels[0][2])}
+    if trace:
+        lum, fl = [], []
+        o = of = 0
+        for w, h, bw, bh in L.levels:
+            lum.append((luma[o:o + w * h].reshape(h, w), luma[o + w * h:o + 2 * w * h].reshape(h, w)))
+            o += 2 * w * h
+            fl.append((fields[of:of + 2 * bw * bh].reshape(bh, bw, 2), fields[of + 2 * bw * bh:of + 4 * bw * bh].reshape(bh, bw, 2)))
+            of += 4 * bw * bh
+        bw0, bh0 = L.levels[0][2], L.levels[0][3]
+        est["luma"] = lum
+        est["fields"] = fl
+        est["meds"] = meds.reshape(-1, 2)
+        est["sub"] = [fields[of:of + 2 * bw0 * bh0].reshape(bh0, bw0, 2), fields[of + 2 * bw0 * bh0:].reshape(bh0, bw0, 2)]
+    return est
+
+
+def synth_fmt(a, c, est, t, spec, settings=None, trace=False, threads=0):
+    """synth() for the other formats: returns (frame, reason) or, with trace, a dict with out, reason, field_t, e,
+    untrusted. The frame has the input's layout (a tuple of planes for YUV)."""
+    s = settings or Settings()
+    W, H = frame_size(a, spec)
+    out = empty_like_frame(a, spec)
+    L = est["layout"]
+    pf = np.ascontiguousarray(est["pf"], np.float32)
+    ft = np.zeros((L.fh, L.fw, 2), np.float32) if trace else None
+    e = np.zeros((H, W), np.uint8) if trace else None
+    unt, reason = ctypes.c_longlong(), ctypes.c_int()
+    fa, fc, fo = _cframe(a, spec), _cframe(c, spec), _cframe(out, spec)
+    r = _fmt_lib().fgo_synth_fmt(ctypes.byref(fa), ctypes.byref(fc), W, H, ctypes.byref(fmt_struct(spec)),
+                                 ctypes.byref(_cs(s)), _p(pf), int(est["cut"]), float(t), ctypes.byref(fo), _p(ft), _p(e),
+                                 ctypes.byref(unt), ctypes.byref(reason), threads)
+    if r != 0:
+        raise ValueError("fgo_synth_fmt failed (t outside (0, 1)?)")
+    if trace:
+        return {"out": out, "reason": REASONS[reason.value], "field_t": ft, "e": e, "untrusted": int(unt.value)}
+    return out, REASONS[reason.value]
+
+
+def pq255(v, white=80.0):
+    """the oracle's PQ level of a linear value (format.glsl fgPq * 255)"""
+    L = _fmt_lib()
+    return float(L.fgo_pq255(float(v), float(np.float32(white) / np.float32(10000.0))))
+
+
+def f2h(v):
+    return int(_fmt_lib().fgo_f2h(float(v)))
+
+
+def h2f(h):
+    return float(_fmt_lib().fgo_h2f(int(h)))
+
+
+def log2(v):
+    return float(_fmt_lib().fgo_log2(float(v)))
+
+
+def exp2(v):
+    return float(_fmt_lib().fgo_exp2(float(v)))
