@@ -1,0 +1,292 @@
+// The seed proposer: a 6-layer 3x3 convolutional net that reads the 2-channel luma (prev, curr) of one pyramid level
+// and proposes, per 8x8 block of that level, two candidate half-vectors and a confidence for the integer block
+// search. No counterpart in the reference's V1 path (its learned estimator, MotionVersion::Learned, is a different
+// net that replaces the search); here the plain integer search keeps the decision, the net only adds candidates.
+//
+//   layer  in -> out  stride  activation     output grid (level w x h)
+//   1      2  -> 32   2       ReLU           ceil(w/2) x ceil(h/2)
+//   2      32 -> 32   2       ReLU           ceil(w/4) x ceil(h/4)
+//   3      32 -> 32   2       ReLU           ceil(w/8) x ceil(h/8)   (= the level's block grid)
+//   4, 5   32 -> 32   1       ReLU
+//   6      32 -> 8    1       none           (c1x, c1y, c2x, c2y, confidence logit, 3 unused) per block
+// 3x3 kernels, zero padding 1. Activations NHWC bfloat16; weights bfloat16 [cout][tap][cin] (tap = 3 ky + kx);
+// biases and every accumulation float32.
+//
+// Forward: implicit GEMM on the tensor cores (mma.sync m16n8k16, bf16 x bf16 -> f32): M = output pixels, N = cout,
+// K = 9 cin (layer 1: 18, zero-padded to 32); a CTA = 4 warps x 16 output pixels, the layer's weights staged once in
+// shared memory. The GEMMs are small (a 4K frame's level 1: 1.2 GFLOP in all), so warp-level MMA with
+// register-gathered A fragments is enough; no TMEM / TMA staging.
+// Training (backward, Adam): CUDA-core kernels, bf16 operands and float32 accumulation and gradients.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "fg_device.h"
+#include "fg_seednet.h"
+
+namespace fgk {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ uint32_t ldBf2(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// level luma (float, levels) -> the net's input: (v - 128) / 64 in bfloat16, channels (prev, curr)
+__global__ void __launch_bounds__(256) k_sn_pack(const float* __restrict__ la, const float* __restrict__ lc, int n,
+                                                bf16* __restrict__ x) {
+    pdlEnter();
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const float a = __fmul_rn(__fsub_rn(la[i], 128.0f), 1.0f / 64.0f), c = __fmul_rn(__fsub_rn(lc[i], 128.0f), 1.0f / 64.0f);
+    reinterpret_cast<__nv_bfloat162*>(x)[i] = __floats2bfloat162_rn(a, c);
+}
+
+// one 3x3 convolution layer, forward. in: [B][H][W][CIN] bf16; out: [B][Ho][Wo][COUT] bf16 (ReLU) or float (last layer)
+template <int CIN, int COUT, int STRIDE, bool LAST>
+__global__ void __launch_bounds__(128) k_sn_conv(const SnConvArgs a) {
+    pdlEnter();
+    constexpr int K = 9 * CIN, KP = (K + 15) / 16 * 16, NT = COUT / 8;
+    __shared__ __align__(16) bf16 ws[COUT * KP];
+    __shared__ float bs[COUT];
+    const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
+    for (int i = threadIdx.x; i < COUT * KP; i += 128) {
+        const int n = i / KP, k = i % KP;
+        ws[i] = k < K ? w[n * K + k] : __float2bfloat16(0.0f);
+    }
+    if (threadIdx.x < COUT) bs[threadIdx.x] = a.b[threadIdx.x];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int npix = a.B * a.Ho * a.Wo;
+    const int p0 = (blockIdx.x * 4 + warp) * 16;
+    if (p0 >= npix) return;
+    // the two output pixels of this thread's A rows
+    int base[2], oy[2], ox[2];
+    bool val[2];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int p = p0 + gid + 8 * r;
+        val[r] = p < npix;
+        const int pp = val[r] ? p : 0;
+        const int b = pp / (a.Ho * a.Wo), rem = pp % (a.Ho * a.Wo);
+        oy[r] = (rem / a.Wo) * STRIDE - 1;
+        ox[r] = (rem % a.Wo) * STRIDE - 1;
+        base[r] = b * a.H * a.W;
+    }
+    const bf16* __restrict__ x = reinterpret_cast<const bf16*>(a.x);
+    float acc[NT][4];
+#pragma unroll
+    for (int t = 0; t < NT; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0f;
+#pragma unroll 2
+    for (int kc = 0; kc < KP / 16; kc++) {
+        uint32_t af[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {   // register q: row gid (+8 for q odd), k columns +8 for q >= 2
+            const int r = q & 1, k = kc * 16 + tig * 2 + ((q >> 1) << 3);
+            uint32_t v = 0;
+            if (k < K && val[r]) {
+                const int tap = k / CIN, ci = k % CIN;
+                const int iy = oy[r] + tap / 3, ix = ox[r] + tap % 3;
+                if ((unsigned)iy < (unsigned)a.H && (unsigned)ix < (unsigned)a.W)
+                    v = ldBf2(x + (size_t)(base[r] + iy * a.W + ix) * CIN + ci);
+            }
+            af[q] = v;
+        }
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            const bf16* wb = ws + (t * 8 + gid) * KP + kc * 16 + tig * 2;
+            mma16816(acc[t], af, ldBf2(wb), ldBf2(wb + 8));
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        const int n = t * 8 + tig * 2;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int p = p0 + gid + 8 * r;
+            if (p >= npix) continue;
+            float v0 = acc[t][2 * r] + bs[n], v1 = acc[t][2 * r + 1] + bs[n + 1];
+            if (LAST) {
+                *reinterpret_cast<float2*>(a.yf + (size_t)p * COUT + n) = make_float2(v0, v1);
+            } else {
+                v0 = fmaxf(v0, 0.0f);
+                v1 = fmaxf(v1, 0.0f);
+                reinterpret_cast<__nv_bfloat162*>(a.y)[((size_t)p * COUT + n) >> 1] = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------- training kernels
+// dX of one layer, masked by the previous layer's ReLU: dpre_in[q][ci] = [x[q][ci] > 0] * sum_{tap, co} w[co][tap][ci]
+// dpre_out[p][co] over the output pixels p with STRIDE p + tap - 1 = q. One thread per (q, ci).
+template <int CIN, int COUT, int STRIDE>
+__global__ void __launch_bounds__(256) k_sn_dx(const SnBackArgs a) {
+    __shared__ float wsh[COUT * 9 * CIN];
+    const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
+    for (int i = threadIdx.x; i < COUT * 9 * CIN; i += 256) wsh[i] = __bfloat162float(w[i]);
+    __syncthreads();
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    const int n = a.B * a.H * a.W * CIN;
+    if (i >= n) return;
+    const int ci = i % CIN, q = i / CIN;
+    const int b = q / (a.H * a.W), rem = q % (a.H * a.W), qy = rem / a.W, qx = rem % a.W;
+    const bf16* __restrict__ x = reinterpret_cast<const bf16*>(a.x);
+    if (!(__bfloat162float(x[i]) > 0.0f)) { a.dx[i] = 0.0f; return; }
+    float s = 0.0f;
+#pragma unroll
+    for (int tap = 0; tap < 9; tap++) {
+        const int ty = qy + 1 - tap / 3, tx = qx + 1 - tap % 3;   // STRIDE * p = t
+        if (ty < 0 || tx < 0 || ty % STRIDE || tx % STRIDE) continue;
+        const int py = ty / STRIDE, px = tx / STRIDE;
+        if (py >= a.Ho || px >= a.Wo) continue;
+        const float* g = a.dy + ((size_t)(b * a.Ho + py) * a.Wo + px) * COUT;
+#pragma unroll 8
+        for (int co = 0; co < COUT; co++) s += g[co] * wsh[(co * 9 + tap) * CIN + ci];
+    }
+    a.dx[i] = s;
+}
+
+// dW[co][tap][ci] += sum_p x[STRIDE p + tap - 1][ci] dpre[p][co] and db[co] += sum_p dpre[p][co], over a slice of the
+// output pixels per CTA (grid.y slices); one CTA row per (co, tap), threads = (pixel lane, ci)
+template <int CIN, int COUT, int STRIDE>
+__global__ void __launch_bounds__(256) k_sn_dw(const SnBackArgs a) {
+    constexpr int LANES = 256 / CIN;
+    __shared__ float red[256];
+    __shared__ float redb[256];
+    const int co = blockIdx.x / 9, tap = blockIdx.x % 9;
+    const int ci = threadIdx.x % CIN, lane = threadIdx.x / CIN;
+    const int npix = a.B * a.Ho * a.Wo;
+    const int per = (npix + gridDim.y - 1) / gridDim.y;
+    const int p0 = blockIdx.y * per, p1 = min(npix, p0 + per);
+    const bf16* __restrict__ x = reinterpret_cast<const bf16*>(a.x);
+    float s = 0.0f, sb = 0.0f;
+    for (int p = p0 + lane; p < p1; p += LANES) {
+        const float g = a.dy[(size_t)p * COUT + co];
+        if (g == 0.0f) continue;
+        if (tap == 0 && ci == 0) sb += g;
+        const int b = p / (a.Ho * a.Wo), rem = p % (a.Ho * a.Wo);
+        const int iy = (rem / a.Wo) * STRIDE - 1 + tap / 3, ix = (rem % a.Wo) * STRIDE - 1 + tap % 3;
+        if ((unsigned)iy >= (unsigned)a.H || (unsigned)ix >= (unsigned)a.W) continue;
+        s += g * __bfloat162float(x[((size_t)(b * a.H + iy) * a.W + ix) * CIN + ci]);
+    }
+    red[threadIdx.x] = s;
+    redb[threadIdx.x] = sb;
+    __syncthreads();
+    for (int h = 128; h >= CIN; h >>= 1) {
+        if (threadIdx.x < h) {
+            red[threadIdx.x] += red[threadIdx.x + h];
+            redb[threadIdx.x] += redb[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < CIN) atomicAdd(a.dw + (co * 9 + tap) * CIN + threadIdx.x, red[threadIdx.x]);
+    if (threadIdx.x == 0 && tap == 0) atomicAdd(a.db + co, redb[0]);
+}
+
+// the loss of one batch and its gradient at the last layer's output (per block: huber(c1 - truth) +
+// huber(c2 - search) + BCE(confidence, |c1 - truth|_inf < 1), each block weighted by its target's weight; scale =
+// 1 / blocks: the batch mean)
+__global__ void __launch_bounds__(256) k_sn_loss(const float* __restrict__ out, const float* __restrict__ tgt, int n,
+                                                float* __restrict__ dout, float* __restrict__ loss, float scale) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    float l = 0.0f;
+    if (i < n) {
+        const float* o = out + (size_t)i * kSnOut;
+        const float* t = tgt + (size_t)i * kSnTargets;   // truth (2), search (2), weight, unused
+        float* d = dout + (size_t)i * kSnOut;
+        const float wgt = t[4];
+        float err = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float e = o[k] - t[k];
+            const float ae = fabsf(e);
+            l += wgt * (ae < 1.0f ? 0.5f * e * e : ae - 0.5f);
+            d[k] = scale * wgt * (ae < 1.0f ? e : copysignf(1.0f, e));
+            if (k < 2) err = fmaxf(err, ae);
+        }
+        const float y = err < 1.0f ? 1.0f : 0.0f, z = o[4];
+        const float sg = 1.0f / (1.0f + expf(-z));
+        l += wgt * (fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z))));
+        d[4] = scale * wgt * (sg - y);
+        d[5] = d[6] = d[7] = 0.0f;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l * scale);
+}
+
+// Adam on the float32 master parameters; refreshes their bfloat16 copy (the forward's weights) and zeroes the gradient
+__global__ void __launch_bounds__(256) k_sn_adam(const SnAdamArgs a) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= a.n) return;
+    const float g = a.grad[i];
+    const float m = a.b1 * a.m[i] + (1.0f - a.b1) * g;
+    const float v = a.b2 * a.v[i] + (1.0f - a.b2) * g * g;
+    a.m[i] = m;
+    a.v[i] = v;
+    const float p = a.p[i] - a.lr * (m * a.c1) / (sqrtf(v * a.c2) + a.eps);
+    a.p[i] = p;
+    a.grad[i] = 0.0f;
+    reinterpret_cast<bf16*>(a.wb)[i] = __float2bfloat16(p);
+}
+
+// ---------------------------------------------------------------------------------------------- launchers
+cudaError_t launchSnPack(const float* la, const float* lc, int n, void* x, cudaStream_t s) {
+    return launchPdl(k_sn_pack, dim3(divUp(n, 256)), dim3(256), 0, s, la, lc, n, reinterpret_cast<bf16*>(x));
+}
+
+cudaError_t launchSnConv(int layer, const SnConvArgs& a, cudaStream_t s) {
+    const dim3 grid(divUp(a.B * a.Ho * a.Wo, 64));
+    switch (layer) {
+        case 0: return launchPdl(k_sn_conv<2, 32, 2, false>, grid, dim3(128), 0, s, a);
+        case 1:
+        case 2: return launchPdl(k_sn_conv<32, 32, 2, false>, grid, dim3(128), 0, s, a);
+        case 3:
+        case 4: return launchPdl(k_sn_conv<32, 32, 1, false>, grid, dim3(128), 0, s, a);
+        case 5: return launchPdl(k_sn_conv<32, kSnOut, 1, true>, grid, dim3(128), 0, s, a);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchSnBackward(int layer, const SnBackArgs& a, bool needDx, cudaStream_t s) {
+    const int npix = a.B * a.Ho * a.Wo;
+    const unsigned slices = (unsigned)std::max(1, std::min(64, npix / 2048));
+    const unsigned nx = divUp(a.B * a.H * a.W * 32, 256);
+    switch (layer) {
+        case 0: k_sn_dw<2, 32, 2><<<dim3(32 * 9, slices), 256, 0, s>>>(a); break;
+        case 1:
+        case 2:
+            k_sn_dw<32, 32, 2><<<dim3(32 * 9, slices), 256, 0, s>>>(a);
+            if (needDx) k_sn_dx<32, 32, 2><<<nx, 256, 0, s>>>(a);
+            break;
+        case 3:
+        case 4:
+            k_sn_dw<32, 32, 1><<<dim3(32 * 9, slices), 256, 0, s>>>(a);
+            if (needDx) k_sn_dx<32, 32, 1><<<nx, 256, 0, s>>>(a);
+            break;
+        case 5:
+            k_sn_dw<32, kSnOut, 1><<<dim3(kSnOut * 9, slices), 256, 0, s>>>(a);
+            if (needDx) k_sn_dx<32, kSnOut, 1><<<nx, 256, 0, s>>>(a);
+            break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchSnLoss(const float* out, const float* tgt, int n, float* dout, float* loss, float scale, cudaStream_t s) {
+    k_sn_loss<<<divUp(n, 256), 256, 0, s>>>(out, tgt, n, dout, loss, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t launchSnAdam(const SnAdamArgs& a, cudaStream_t s) {
+    k_sn_adam<<<divUp(a.n, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace fgk

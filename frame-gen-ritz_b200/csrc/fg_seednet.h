@@ -1,0 +1,52 @@
+// fg_seednet.h -- the seed proposer's parameter layout and kernel arguments (fg_seednet.cu), shared with the host
+// code (fg_seednet_host.cpp, framegen.cpp).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace fgk {
+
+constexpr int kSnLayers = 6;
+constexpr int kSnOut = 8;                   // per block: c1x, c1y, c2x, c2y, confidence logit, 3 unused
+constexpr int kSnTargets = 6;               // per block: truth (2), search vector (2), weight, unused
+constexpr int kSnCin[kSnLayers] = {2, 32, 32, 32, 32, 32};
+constexpr int kSnCout[kSnLayers] = {32, 32, 32, 32, 32, kSnOut};
+constexpr int kSnStride[kSnLayers] = {2, 2, 2, 1, 1, 1};
+
+// the flat parameter array: per layer, weights [cout][9][cin] then biases [cout]
+constexpr int snWeightOff(int l) { return l == 0 ? 0 : snWeightOff(l - 1) + kSnCout[l - 1] * (9 * kSnCin[l - 1] + 1); }
+constexpr int snBiasOff(int l) { return snWeightOff(l) + kSnCout[l] * 9 * kSnCin[l]; }
+constexpr int kSnParams = snWeightOff(kSnLayers);   // 39,912
+
+struct SnConvArgs {
+    const void* x;     // layer input, NHWC bf16 [B][H][W][cin]
+    const void* w;     // bf16 [cout][9][cin]
+    const float* b;    // float [cout]
+    void* y;           // layer output, NHWC bf16 (ReLU layers)
+    float* yf;         // last layer: float [B][Ho][Wo][8]
+    int B, H, W, Ho, Wo;
+};
+
+struct SnBackArgs {
+    const void* x;     // layer input (bf16), the previous layer's ReLU output (its mask for dx)
+    const void* w;     // bf16 weights of this layer
+    const float* dy;   // gradient at this layer's pre-activation, float [B][Ho][Wo][cout]
+    float* dx;         // gradient at the previous layer's pre-activation, float [B][H][W][cin]
+    float* dw;         // += dL/dW, float [cout][9][cin]
+    float* db;         // += dL/db, float [cout]
+    int B, H, W, Ho, Wo;
+};
+
+struct SnAdamArgs {
+    float* p; float* m; float* v; float* grad;   // float32 master parameters, moments, gradients (zeroed here)
+    void* wb;                                    // bf16 copy of p (the forward's weights)
+    int n;
+    float lr, b1, b2, eps, c1, c2;               // c1 = 1 / (1 - b1^t), c2 = 1 / (1 - b2^t)
+};
+
+cudaError_t launchSnPack(const float* la, const float* lc, int n, void* x, cudaStream_t s);
+cudaError_t launchSnConv(int layer, const SnConvArgs& a, cudaStream_t s);
+cudaError_t launchSnBackward(int layer, const SnBackArgs& a, bool needDx, cudaStream_t s);
+cudaError_t launchSnLoss(const float* out, const float* tgt, int n, float* dout, float* loss, float scale, cudaStream_t s);
+cudaError_t launchSnAdam(const SnAdamArgs& a, cudaStream_t s);
+
+}  // namespace fgk

@@ -12,6 +12,8 @@ import ctypes
 import os
 from dataclasses import dataclass, fields
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libframegen_b200.so")
 
@@ -94,6 +96,18 @@ SIGNATURES = {
     "fg_record_synth_noalloc": (_I, [_P, _U32, _U32, _U32, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame),
                                      ctypes.POINTER(CFrame), _P, _I, _F, ctypes.POINTER(CSettings),
                                      ctypes.POINTER(ctypes.c_char_p)]),
+    "fg_seednet_param_count": (_U32, []),
+    "fg_seednet_create": (_P, [_I, _I, _I, _I]),
+    "fg_seednet_destroy": (None, [_P]),
+    "fg_seednet_error": (_S, [_P]),
+    "fg_seednet_set_params": (_I, [_P, _P]),
+    "fg_seednet_get_params": (_I, [_P, _P]),
+    "fg_seednet_get_grads": (_I, [_P, _P]),
+    "fg_seednet_pack": (_I, [_P, _P, _P, _I, _P]),
+    "fg_seednet_forward": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "fg_seednet_backward": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
+    "fg_seednet_zero_grads": (_I, [_P, _P]),
+    "fg_seednet_adam": (_I, [_P, _P, _F]),
 }
 
 _lib = None
@@ -293,7 +307,6 @@ class Interpolator:
 
 def read_trace(fg, stream=None):
     """Copy the latest estimate's intermediates to the host: a dict in the oracle's trace layout."""
-    import numpy as np
     import torch
     l = fg.trace_layout()
     buf = torch.empty(l.size, dtype=torch.uint8, device="cuda")
@@ -327,3 +340,70 @@ def record_synth_noalloc(prev, curr, out, field, cut, t, settings=None, view_for
                                        int(cut), float(t), ctypes.byref((settings or Settings()).to_c()),
                                        ctypes.byref(err))
     return bool(ok), (err.value.decode() if err.value else None)
+
+
+class SeedNet:
+    """The seed proposer (fg_seednet_*): parameters, forward pass and training step on the GPU. Inputs are CUDA
+    tensors: x (B, h, w, 2) bfloat16 from pack(), targets (B, ceil(h/8), ceil(w/8), 6) float32."""
+
+    N_OUT, N_TGT = 8, 6
+
+    def __init__(self, max_batch, max_h, max_w, device=-1):
+        self._h = lib().fg_seednet_create(device, max_batch, max_h, max_w)
+        if not self._h:
+            raise RuntimeError("fg_seednet_create failed")
+        self.n_params = int(lib().fg_seednet_param_count())
+
+    def close(self):
+        if self._h and _lib is not None:
+            _lib.fg_seednet_destroy(self._h)
+        self._h = None
+
+    __del__ = close
+
+    def _ok(self, r):
+        if not r:
+            raise RuntimeError(f"seed net call failed: {_s(lib().fg_seednet_error(self._h))}")
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == self.n_params
+        self._ok(lib().fg_seednet_set_params(self._h, p.ctypes.data))
+
+    def params(self):
+        p = np.zeros(self.n_params, np.float32)
+        self._ok(lib().fg_seednet_get_params(self._h, p.ctypes.data))
+        return p
+
+    def grads(self):
+        g = np.zeros(self.n_params, np.float32)
+        self._ok(lib().fg_seednet_get_grads(self._h, g.ctypes.data))
+        return g
+
+    @staticmethod
+    def pack(luma_prev, luma_curr, stream=None):
+        """(..., h, w) float32 CUDA luma pair -> (..., h, w, 2) bfloat16 net input"""
+        import torch
+        x = torch.empty(tuple(luma_prev.shape) + (2,), dtype=torch.bfloat16, device=luma_prev.device)
+        assert lib().fg_seednet_pack(_stream(stream), luma_prev.data_ptr(), luma_curr.data_ptr(), luma_prev.numel(),
+                                     x.data_ptr())
+        return x
+
+    def forward(self, x, out=None, stream=None):
+        import torch
+        B, h, w = x.shape[:3]
+        if out is None:
+            out = torch.empty((B, (h + 7) // 8, (w + 7) // 8, self.N_OUT), dtype=torch.float32, device=x.device)
+        self._ok(lib().fg_seednet_forward(self._h, _stream(stream), x.data_ptr(), B, h, w, out.data_ptr()))
+        return out
+
+    def backward(self, x, targets, loss=None, stream=None):
+        B, h, w = x.shape[:3]
+        self._ok(lib().fg_seednet_backward(self._h, _stream(stream), x.data_ptr(), B, h, w, targets.data_ptr(),
+                                           None if loss is None else loss.data_ptr()))
+
+    def zero_grads(self, stream=None):
+        self._ok(lib().fg_seednet_zero_grads(self._h, _stream(stream)))
+
+    def adam(self, lr, stream=None):
+        self._ok(lib().fg_seednet_adam(self._h, _stream(stream), float(lr)))

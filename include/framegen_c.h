@@ -98,6 +98,29 @@ int fg_get_trace_layout(const fg_interpolator* fg, fg_trace_layout* l);         
 int fg_record_trace(fg_interpolator* fg, void* stream, void* dst);                   /* B200-build extension */
 const char* fg_last_error(const fg_interpolator* fg);   /* the last CUDA error a record met (null if none) */
 
+/* The seed proposer -- no counterpart in the reference's V1 path (B200-build extension). A 6-layer 3x3 conv net
+ * (csrc/fg_seednet.cu) reading one pyramid level's luma (prev, curr) and proposing, per 8x8 block of that level, two
+ * candidate half-vectors and a confidence logit for the integer block search. Inputs are NHWC bfloat16 [B][h][w][2]
+ * made by fg_seednet_pack; outputs float [B][ceil(h/8)][ceil(w/8)][8] (c1x, c1y, c2x, c2y, logit, 3 unused);
+ * training targets float [B][ceil(h/8)][ceil(w/8)][6] (truth x, y, search x, y, weight, unused). Parameters: a flat
+ * float array of fg_seednet_param_count() values, per layer weights [cout][3*ky+kx][cin] then biases [cout].
+ * All device pointers; calls go to the net's device, stream-ordered; returns 1 on success, 0 otherwise. */
+typedef struct fg_seednet fg_seednet;
+uint32_t fg_seednet_param_count(void);
+fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w);   /* workspace for inputs up to this */
+void fg_seednet_destroy(fg_seednet* net);
+const char* fg_seednet_error(const fg_seednet* net);
+int fg_seednet_set_params(fg_seednet* net, const float* host_params);   /* also resets Adam's state */
+int fg_seednet_get_params(fg_seednet* net, float* host_params);
+int fg_seednet_get_grads(fg_seednet* net, float* host_grads);         /* the gradient accumulated since the last step */
+int fg_seednet_pack(void* stream, const float* luma_prev, const float* luma_curr, int n, void* x);
+int fg_seednet_forward(fg_seednet* net, void* stream, const void* x, int batch, int h, int w, float* out);
+/* forward + loss + backward: adds dLoss/dParams to the gradient; *loss (device float, optional) = the batch's loss */
+int fg_seednet_backward(fg_seednet* net, void* stream, const void* x, int batch, int h, int w, const float* targets,
+                        float* loss);
+int fg_seednet_zero_grads(fg_seednet* net, void* stream);
+int fg_seednet_adam(fg_seednet* net, void* stream, float lr);          /* one Adam step (0.9, 0.999, 1e-8); zeroes grads */
+
 /* fg_record_synth_noalloc -- no counterpart in the reference. The synthesis of one generated frame (what
  * fg_record_synth records after an estimate) for hosts that cannot allocate device memory when they generate frames:
  * a compositor or overlay running inside another program's frame callback under that program's memory budget, a
