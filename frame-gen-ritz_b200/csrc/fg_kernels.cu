@@ -168,23 +168,36 @@ __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by
     sy = 0;
     if (p.top) return;
     const int b0x = bx * kBlock, b0y = by * kBlock;
-    const int px = min(bx >> 1, p.pw - 1), py = min(by >> 1, p.ph - 1);
-    const int oy = (by & 1) ? 1 : -1, ox = (bx & 1) ? 1 : -1;
     int cxs[6], cys[6];
+    bool pen0 = false;   // the first candidate pays lambda too
+    if (p.cnn) {
+        // seed-net level: its two candidates (rounded half-even, clamped to +-256), then zero; the first is free of
+        // the penalty only when the net is confident (logit >= 0). Slots 3..5 repeat zero and are skipped as such.
+        const float* o = p.cnn + (size_t)(by * p.bw + bx) * kSeedNetOut;
 #pragma unroll
-    for (int k = 0; k < 6; k++) {   // own, (0, oy), (ox, 0), (ox, oy) parents x 2; zero; the global median
-        int cx = 0, cy = 0;
-        if (k < 4) {
-            const int dx = (k & 2) ? ox : 0, dy = (k & 1) ? oy : 0;
-            const float2 v = p.parent[clampi(py + dy, 0, p.ph - 1) * p.pw + clampi(px + dx, 0, p.pw - 1)];
-            cx = 2 * __float2int_rn(v.x);
-            cy = 2 * __float2int_rn(v.y);
-        } else if (k == 5) {
-            cx = __float2int_rn(p.med[0]);
-            cy = __float2int_rn(p.med[1]);
+        for (int k = 0; k < 6; k++) {
+            cxs[k] = k < 2 ? __float2int_rn(fminf(fmaxf(o[2 * k], -256.0f), 256.0f)) : 0;
+            cys[k] = k < 2 ? __float2int_rn(fminf(fmaxf(o[2 * k + 1], -256.0f), 256.0f)) : 0;
         }
-        cxs[k] = cx;
-        cys[k] = cy;
+        pen0 = !(o[4] >= 0.0f);
+    } else {
+        const int px = min(bx >> 1, p.pw - 1), py = min(by >> 1, p.ph - 1);
+        const int oy = (by & 1) ? 1 : -1, ox = (bx & 1) ? 1 : -1;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {   // own, (0, oy), (ox, 0), (ox, oy) parents x 2; zero; the global median
+            int cx = 0, cy = 0;
+            if (k < 4) {
+                const int dx = (k & 2) ? ox : 0, dy = (k & 1) ? oy : 0;
+                const float2 v = p.parent[clampi(py + dy, 0, p.ph - 1) * p.pw + clampi(px + dx, 0, p.pw - 1)];
+                cx = 2 * __float2int_rn(v.x);
+                cy = 2 * __float2int_rn(v.y);
+            } else if (k == 5) {
+                cx = __float2int_rn(p.med[0]);
+                cy = __float2int_rn(p.med[1]);
+            }
+            cxs[k] = cx;
+            cys[k] = cy;
+        }
     }
     const int qx = b0x + (lane & 7), qy0 = b0y + (lane >> 3), qy1 = qy0 + 4;
     float best = 0.0f;
@@ -206,7 +219,7 @@ __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by
         }
         s = warpSum(s);   // exact: at most 24 significant bits
         float cost = __fmul_rn(s, 1.0f / 64.0f);
-        if (k > 0) cost = __fadd_rn(cost, p.lambda);
+        if (k > 0 || pen0) cost = __fadd_rn(cost, p.lambda);
         if (k == 0 || cost < best) { best = cost; sx = cx; sy = cy; }
     }
 }

@@ -10,6 +10,7 @@ namespace fgk {
 constexpr int kBlock = 8;          // block size at every pyramid level (proto/interp.py:43 BLOCK)
 constexpr int kMaxLevels = 16;
 constexpr int kPyrInKernel = 6;    // levels 0..5 come out of the luma kernel (a 32x32 tile of level 0 -> 1x1 of level 5)
+constexpr int kSeedNetOut = 8;    // seed net outputs per block: c1x, c1y, c2x, c2y, confidence logit, 3 unused
 constexpr int kMaxRadius = 12;     // Settings::searchRadius / searchRadiusTop upper bound (gpu/framegen.cpp validate)
 
 // Device-side counters and small results of one estimate / synth (one allocation, zeroed at init).
@@ -69,6 +70,7 @@ struct SearchParams {
     float pen[2 * kMaxRadius + 1];   // fl32(lambda * n), n = |dx| + |dy| (interp.py:121)
     float2* out;
     float* sadOut;             // optional: the winner's SAD (finest level when sub-pixel refinement is off)
+    const float* cnn;          // optional: the seed net's output at this level (kSeedNetOut floats per block)
 };
 
 struct Median3Params {

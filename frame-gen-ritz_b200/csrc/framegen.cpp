@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "fg_params.h"
+#include "fg_seednet.h"
 #include "framegen.h"
 #include "framegen_c.h"
 
@@ -231,6 +232,12 @@ struct Interpolator::Impl {
     unsigned int parity = 0, lastParity = 0;
     bool capture = false;
     const char* lastErr = nullptr;
+    // the seed net (setSeedNet): its parameters, the requested level, the level of this size, its buffers
+    std::vector<float> snParams;
+    int snLevelReq = -1, snK = -1;
+    fg_seednet* snet = nullptr;
+    void* snX = nullptr;       // packed input of level snK (bf16 x 2)
+    float* snOut = nullptr;    // its output, bw x bh x kSeedNetOut floats
     // profiling
     bool profiling = false;
     std::vector<cudaEvent_t> events;
@@ -239,8 +246,37 @@ struct Interpolator::Impl {
 
     ~Impl() { freeAll(); }
 
+    void freeSeedNet() {
+        if (snet) fg_seednet_destroy(snet);
+        if (snX) cudaFree(snX);
+        if (snOut) cudaFree(snOut);
+        snet = nullptr;
+        snX = nullptr;
+        snOut = nullptr;
+        snK = -1;
+    }
+
+    // the seed net's buffers for the current size (after allocSize; outside any capture)
+    const char* setupSeedNet() {
+        DeviceGuard g(device);
+        freeSeedNet();
+        if (snLevelReq < 0 || !W) return nullptr;
+        snK = std::min(snLevelReq, (int)L.lv.size() - 1);
+        const Level& lk = L.lv[snK];
+        snet = fg_seednet_create(device, 1, lk.h, lk.w);
+        if (!snet || !fg_seednet_set_params(snet, snParams.data()) ||
+            cudaMalloc(&snX, (size_t)lk.w * lk.h * 4) != cudaSuccess ||
+            cudaMalloc((void**)&snOut, (size_t)lk.bw * lk.bh * fgk::kSeedNetOut * 4) != cudaSuccess) {
+            cudaGetLastError();
+            freeSeedNet();
+            return kErrAlloc;
+        }
+        return nullptr;
+    }
+
     void freeAll() {
         DeviceGuard g(device);
+        freeSeedNet();
         if (arena) cudaFree(arena);
         arena = nullptr;
         arenaBytes = 0;
@@ -273,7 +309,12 @@ struct Interpolator::Impl {
         const int n = (int)L.lv.size();
         // the median histograms hold any parent vector the largest radii (12, 12) can reach, so a runtime change
         // of the radii (setSettings) never needs new buffers
-        const int64_t B = n > 1 ? reachBound(n, 1, 12, 12) : 0;
+        int64_t B = n > 1 ? reachBound(n, 1, 12, 12) : 0;
+        if (snLevelReq >= 1 && n > 1) {   // seed-net candidates (clamped to +-256) can start anywhere at its level
+            const int k = std::min(snLevelReq, n - 1);
+            const int64_t a = (int64_t)1 << (k - 1);
+            B = std::max<int64_t>(B, (256 + 12) * a + 12 * (a - 1));
+        }
         histB = (int)B;
         const int nb0 = L.lv[0].bw * L.lv[0].bh;
         CutPlanHost P = buildCutPlan(nb0);
@@ -310,7 +351,7 @@ struct Interpolator::Impl {
         W = w;
         H = h;
         haveEst = false;
-        return nullptr;
+        return setupSeedNet();
     }
 
     // a frame the kernels can address: plane 0 (and the CbCr plane of YUV) aligned to its sample size, rows wide enough
@@ -354,7 +395,8 @@ struct Interpolator::Impl {
         lp.a = (const uint8_t*)prev.data; lp.c = (const uint8_t*)curr.data; lp.pitch = prev.pitch;
         lp.W = (int)W; lp.H = (int)H; lp.fs = (int)set.flowScale;
         lp.ri = ri; lp.gi = gi; lp.bi = bi;
-        lp.nlev = std::min(n, fgk::kPyrInKernel);
+        const int top = snK >= 0 ? snK : n - 1;   // the coarsest level searched
+        lp.nlev = std::min(top + 1, fgk::kPyrInKernel);
         lp.f = fc;
         lp.vec16 = fmt == Format::Rgba8 && set.flowScale == 2 && prev.pitch % 16 == 0 && ((uintptr_t)prev.data & 15) == 0 && ((uintptr_t)curr.data & 15) == 0 &&
                    W % 4 == 0 && H % 2 == 0;   // complete 2x2 cells in every full tile, 8-byte aligned level-0 rows
@@ -365,23 +407,30 @@ struct Interpolator::Impl {
         if (prev.pitch != curr.pitch) return false;
         if (!check(fmt == Format::Rgba8 ? fgk::launchLumaPyr(lp, s) : fgk::launchLumaFmt(lp, s))) return false;
         stamp(s, "luma");
-        for (int l = fgk::kPyrInKernel; l < n; l++) {
+        for (int l = fgk::kPyrInKernel; l <= top; l++) {
             fgk::DownParams dp{luma + L.lv[l - 1].lumaA, luma + L.lv[l - 1].lumaC, L.lv[l - 1].w, L.lv[l - 1].h,
                                luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h, fmt != Format::Rgba8};
             if (!check(fgk::launchDown(dp, s))) return false;
         }
         stamp(s, "pyramid");
+        if (snK >= 0) {   // the seed net on level snK
+            const Level& lk = L.lv[snK];
+            if (!check(fgk::launchSnPack(luma + lk.lumaA, luma + lk.lumaC, lk.w * lk.h, snX, s))) return false;
+            if (!fg_seednet_forward(snet, s, snX, 1, lk.h, lk.w, snOut)) { lastErr = fg_seednet_error(snet); return false; }
+            stamp(s, "seed net");
+        }
         // 3-5. per level, coarse -> fine
         static const char* names[] = {"level 0 (finest)", "level 1", "level 2", "level 3", "level 4", "level 5",
                                       "level 6", "level 7"};
-        for (int i = n - 1; i >= 0; i--) {
+        for (int i = top; i >= 0; i--) {
             const Level& l = L.lv[i];
             fgk::SearchParams sp{};
             sp.la = luma + l.lumaA; sp.lc = luma + l.lumaC;
             sp.w = l.w; sp.h = l.h; sp.bw = l.bw; sp.bh = l.bh;
-            sp.top = i == n - 1;
+            sp.top = i == n - 1 && snK < 0;
+            sp.cnn = i == snK ? snOut : nullptr;
             sp.R = (int)(sp.top ? set.searchRadiusTop : set.searchRadius);
-            if (!sp.top) {
+            if (!sp.top && !sp.cnn) {
                 const Level& pl = L.lv[i + 1];
                 sp.parent = field + pl.fM; sp.pw = pl.bw; sp.ph = pl.bh;
                 sp.med = st->med[i];
@@ -637,6 +686,21 @@ bool Interpolator::record(cudaStream_t stream, Frame prev, Frame curr, Frame out
 
 const char* Interpolator::lastCudaError() const { return m ? m->lastErr : nullptr; }
 
+bool Interpolator::setSeedNet(const float* params, uint32_t level) {
+    if (!m) return false;
+    if (params) {
+        m->snParams.assign(params, params + fgk::kSnParams);
+        m->snLevelReq = (int)std::min<uint32_t>(level, fgk::kMaxLevels - 1);
+    } else {
+        m->snParams.clear();
+        m->snLevelReq = -1;
+    }
+    if (!m->W) return true;
+    return m->allocSize(m->W, m->H) == nullptr;   // the histogram bound and the net's buffers depend on the level
+}
+
+uint32_t Interpolator::seedNetLevel() const { return m && m->snK >= 0 ? (uint32_t)m->snK : UINT32_MAX; }
+
 bool Interpolator::setProfiling(bool on) {
     if (!m) return false;
     m->profiling = on;
@@ -710,7 +774,10 @@ bool Interpolator::traceLayout(TraceLayout& l) const {
     l.medOff = o; o = alignUp(o + (uint64_t)L.lv.size() * 8, 256);
     l.sadOff = o; o = alignUp(o + (uint64_t)L.lv[0].bw * L.lv[0].bh * 4, 256);
     l.pfOff = o; o = alignUp(o + (uint64_t)L.fw * L.fh * 8, 256);
-    l.stateOff = o; o += 16;
+    l.stateOff = o; o = alignUp(o + 16, 256);
+    l.seedLevel = m->snK >= 0 ? (uint32_t)m->snK : UINT32_MAX;
+    l.seedOff = o;
+    if (m->snK >= 0) o += (uint64_t)L.lv[m->snK].bw * L.lv[m->snK].bh * fgk::kSeedNetOut * 4;
     l.size = o;
     return true;
 }
@@ -730,6 +797,9 @@ bool Interpolator::recordTrace(cudaStream_t stream, void* dst) {
               cudaMemcpyAsync(d + l.stateOff + 4, &m->st->sadMean, 4, D2D, stream) == cudaSuccess &&
               cudaMemcpyAsync(d + l.stateOff + 8, &m->st->sadSum256, 4, D2D, stream) == cudaSuccess &&
               cudaMemcpyAsync(d + l.stateOff + 12, &m->st->err, 4, D2D, stream) == cudaSuccess;
+    if (ok && m->snK >= 0)
+        ok = cudaMemcpyAsync(d + l.seedOff, m->snOut, (size_t)l.bw[m->snK] * l.bh[m->snK] * fgk::kSeedNetOut * 4, D2D,
+                             stream) == cudaSuccess;
     return ok;
 }
 
@@ -868,6 +938,10 @@ int fg_get_trace_layout(const fg_interpolator* fg, fg_trace_layout* l) {
     return 1;
 }
 int fg_record_trace(fg_interpolator* fg, void* stream, void* dst) { return fg && fg->I.recordTrace((cudaStream_t)stream, dst); }
+int fg_set_seed_net(fg_interpolator* fg, const float* host_params, uint32_t level) {
+    return fg && fg->I.setSeedNet(host_params, level);
+}
+uint32_t fg_seed_net_level(const fg_interpolator* fg) { return fg ? fg->I.seedNetLevel() : UINT32_MAX; }
 const char* fg_last_error(const fg_interpolator* fg) { return fg ? fg->I.lastCudaError() : nullptr; }
 
 }  // extern "C"

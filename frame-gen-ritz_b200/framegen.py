@@ -55,7 +55,8 @@ class CTraceLayout(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("nLevels", "fw", "fh")] + \
                [(n, ctypes.c_uint32 * 16) for n in ("lw", "lh", "bw", "bh")] + \
                [(n, ctypes.c_uint64) for n in ("lumaOff", "lumaBytes", "fieldOff", "fieldBytes", "medOff", "sadOff",
-                                               "pfOff", "stateOff", "size")]
+                                               "pfOff", "stateOff", "size")] + \
+               [("seedLevel", ctypes.c_uint32), ("seedOff", ctypes.c_uint64)]
 
 
 # every symbol include/framegen_c.h declares, with (restype, argtypes)
@@ -96,6 +97,8 @@ SIGNATURES = {
     "fg_record_synth_noalloc": (_I, [_P, _U32, _U32, _U32, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame),
                                      ctypes.POINTER(CFrame), _P, _I, _F, ctypes.POINTER(CSettings),
                                      ctypes.POINTER(ctypes.c_char_p)]),
+    "fg_set_seed_net": (_I, [_P, _P, _U32]),
+    "fg_seed_net_level": (_U32, [_P]),
     "fg_seednet_param_count": (_U32, []),
     "fg_seednet_create": (_P, [_I, _I, _I, _I]),
     "fg_seednet_destroy": (None, [_P]),
@@ -304,6 +307,17 @@ class Interpolator:
     def last_error(self):
         return _s(lib().fg_last_error(self._h))
 
+    def set_seed_net(self, params, level=1):
+        """Interpolator::setSeedNet: CNN-seeded estimates from `level` with these flat float32 parameters (None: off)"""
+        if params is None:
+            return bool(lib().fg_set_seed_net(self._h, None, 0))
+        p = np.ascontiguousarray(params, np.float32)
+        return bool(lib().fg_set_seed_net(self._h, p.ctypes.data, int(level)))
+
+    def seed_net_level(self):
+        v = int(lib().fg_seed_net_level(self._h))
+        return None if v == 0xFFFFFFFF else v
+
 
 def read_trace(fg, stream=None):
     """Copy the latest estimate's intermediates to the host: a dict in the oracle's trace layout."""
@@ -325,7 +339,11 @@ def read_trace(fg, stream=None):
     bw0, bh0 = l.bw[0], l.bh[0]
     sub = [f32(of, 2 * bw0 * bh0).reshape(bh0, bw0, 2), f32(of + 8 * bw0 * bh0, 2 * bw0 * bh0).reshape(bh0, bw0, 2)]
     st = h[l.stateOff:l.stateOff + 16].view(np.uint32)
-    return {"luma": luma, "fields": fld, "sub": sub, "meds": f32(l.medOff, 2 * n).reshape(n, 2),
+    seed = None
+    if l.seedLevel != 0xFFFFFFFF:
+        k = l.seedLevel
+        seed = f32(l.seedOff, 8 * l.bw[k] * l.bh[k]).reshape(l.bh[k], l.bw[k], 8)
+    return {"seed_level": None if seed is None else int(l.seedLevel), "seed": seed,"luma": luma, "fields": fld, "sub": sub, "meds": f32(l.medOff, 2 * n).reshape(n, 2),
             "sads": f32(l.sadOff, bw0 * bh0).reshape(bh0, bw0), "pf": f32(l.pfOff, 2 * l.fw * l.fh).reshape(l.fh, l.fw, 2),
             "cut": bool(st[0]), "sad": float(st[1:2].view(np.float32)[0]), "sadSum256": int(st[2]), "err": int(st[3])}
 

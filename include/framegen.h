@@ -157,9 +157,20 @@ public:
         uint64_t pfOff;                  // fw*fh float2
         uint64_t stateOff;               // 4 uint32: cut, float sadMean bits, sad sum x 256, error bits
         uint64_t size;
+        uint32_t seedLevel;              // the level the seed net read (UINT32_MAX: plain estimate)
+        uint64_t seedOff;                // that level's bw*bh x 8 floats of net output (seedLevel != UINT32_MAX)
     };
     bool traceLayout(TraceLayout& l) const;
     bool recordTrace(cudaStream_t stream, void* dst);
+
+    // B200-build extension (no reference counterpart): CNN-seeded estimates. params = the seed net's flat parameters
+    // (fg_seednet_param_count() floats in host memory; see framegen_c.h), or null to switch the net off; level = the
+    // pyramid level it reads (0 = finest; clamped to the coarsest level of the size). With the net on, recordEstimate
+    // skips the levels above that level, seeds its integer search with the net's two candidates and zero (the first
+    // free of the penalty when the net is confident) and runs the levels below as usual. Allocates (like resize):
+    // call it outside stream capture, with earlier work retired.
+    bool setSeedNet(const float* params, uint32_t level);
+    uint32_t seedNetLevel() const;   // the level the next estimate seeds from, UINT32_MAX when the net is off
 
     // The CUDA error string of the last record that failed at a launch (null if none): a B200-build diagnostic.
     const char* lastCudaError() const;

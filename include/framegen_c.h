@@ -56,6 +56,8 @@ typedef struct fg_trace_layout {
     uint32_t nLevels, fw, fh;
     uint32_t lw[16], lh[16], bw[16], bh[16];
     uint64_t lumaOff, lumaBytes, fieldOff, fieldBytes, medOff, sadOff, pfOff, stateOff, size;
+    uint32_t seedLevel;
+    uint64_t seedOff;
 } fg_trace_layout;
 
 uint32_t fg_abi_version(void);
@@ -106,6 +108,9 @@ const char* fg_last_error(const fg_interpolator* fg);   /* the last CUDA error a
  * float array of fg_seednet_param_count() values, per layer weights [cout][3*ky+kx][cin] then biases [cout].
  * All device pointers; calls go to the net's device, stream-ordered; returns 1 on success, 0 otherwise. */
 typedef struct fg_seednet fg_seednet;
+/* Interpolator::setSeedNet / seedNetLevel (include/framegen.h): CNN-seeded estimates from level `level` (null = off) */
+int fg_set_seed_net(fg_interpolator* fg, const float* host_params, uint32_t level);
+uint32_t fg_seed_net_level(const fg_interpolator* fg);
 uint32_t fg_seednet_param_count(void);
 fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w);   /* workspace for inputs up to this */
 void fg_seednet_destroy(fg_seednet* net);

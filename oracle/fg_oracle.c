@@ -332,6 +332,31 @@ static void seed_from(const float* v, int pw, int ph, const float* la, const flo
     free(own); free(tmp);
 }
 
+/* The seeds of the level the seed net reads (no counterpart in interp.py): per block the net's two candidates
+ * (rounded half-even after clamping to +-256) and zero, scored like seed_from's candidates (block SAD + lambda), the
+ * first free of lambda when the net's confidence logit is >= 0; the first minimum wins. cnn: bw*bh x 8 floats. */
+static void seed_cnn(const float* cnn, const float* la, const float* lc, int w, int h, int bw, int bh, float lambda,
+                     float* seed) {
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int b = 0; b < bw * bh; b++) {
+        const float* o = cnn + (size_t)b * 8;
+        float cx[3], cy[3];
+        for (int k = 0; k < 2; k++) {
+            cx[k] = nearbyintf(fminf(fmaxf(o[2 * k], -256.0f), 256.0f));
+            cy[k] = nearbyintf(fminf(fmaxf(o[2 * k + 1], -256.0f), 256.0f));
+        }
+        cx[2] = 0.0f; cy[2] = 0.0f;
+        const int free0 = o[4] >= 0.0f;
+        float best = 0.0f, sx = 0.0f, sy = 0.0f;
+        for (int k = 0; k < 3; k++) {
+            float sd = block_sad1(la, lc, w, h, b % bw, b / bw, cx[k], cy[k]);
+            float cost = (k == 0 && free0) ? sd + 0.0f : sd + lambda;
+            if (k == 0 || cost < best) { best = cost; sx = cx[k]; sy = cy[k]; }
+        }
+        seed[2 * b] = sx; seed[2 * b + 1] = sy;
+    }
+}
+
 /* ---------------------------------------------------------------------------------------------- pixel field */
 
 /* cv2.blur(err, (k, k), BORDER_REPLICATE) of a float plane: the window sum in double times 1/(k*k), to float */
@@ -421,9 +446,22 @@ static void pixel_field(const float* v, int bw, int bh, const float* ya, const f
  *   meds   : per level l, 2 x the global median (the seed candidate), 0 at the coarsest
  *   sads   : the finest level's per-block SAD the cut test averages
  * Returns the number of levels, or -1. pf is written even for a cut (interp skips it: its pf is None). */
+int fgo_estimate_cnn(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                     int cnnLevel, const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads,
+                     float* pf, float* sad_mean, int* cut, int nthreads);
+
 int fgo_estimate(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
                  float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean, int* cut,
                  int nthreads) {
+    return fgo_estimate_cnn(a8, c8, W, H, pitch, order, s, -1, NULL, luma, fields, seeds, meds, sads, pf, sad_mean, cut,
+                            nthreads);
+}
+
+/* fgo_estimate with the seed net's output at level cnnLevel (cnn: that level's bw*bh x 8 floats, NULL = plain): the
+ * levels above it are skipped and its search is seeded by seed_cnn */
+int fgo_estimate_cnn(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                     int cnnLevel, const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads,
+                     float* pf, float* sad_mean, int* cut, int nthreads) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #else
@@ -440,13 +478,14 @@ int fgo_estimate(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, 
     luma_area(&C, s->flowScale, L[0][1], fw, fh);
     for (int l = 1; l < n; l++)
         for (int k = 0; k < 2; k++) fgo_i_area_half(L[l - 1][k], lw[l - 1], lh[l - 1], L[l][k], lw[l], lh[l], 0);
-    int r = fgo_i_estimate_levels(L, n, lw, lh, s, luma, fields, seeds, meds, sads, pf, sad_mean, cut);
+    int r = fgo_i_estimate_levels(L, n, lw, lh, s, cnnLevel, cnn, luma, fields, seeds, meds, sads, pf, sad_mean, cut);
     for (int l = 0; l < n; l++) { free(L[l][0]); free(L[l][1]); }
     return r;
 }
 
-int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, const fgo_settings* s, float* luma,
-                          float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean, int* cut) {
+int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, const fgo_settings* s, int cnnLevel,
+                          const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf,
+                          float* sad_mean, int* cut) {
     if (n < 1 || n > MAXLV) return -1;
     int bw[MAXLV] = {0}, bh[MAXLV] = {0};
     size_t lofs = 0, fofs = 0, sofs = 0;
@@ -463,7 +502,8 @@ int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, co
     float* v = NULL;
     int pw = 0, ph = 0;
     float* sadbuf = malloc(sizeof(float) * (size_t)bw[0] * bh[0]);
-    for (int l = n - 1; l >= 0; l--) {
+    const int top = cnn ? (cnnLevel < n - 1 ? cnnLevel : n - 1) : n - 1;
+    for (int l = top; l >= 0; l--) {
         int nb = bw[l] * bh[l];
         float* seed = calloc((size_t)2 * nb, sizeof(float));
         float med[2] = {0.0f, 0.0f};
@@ -471,7 +511,8 @@ int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, co
         float* vm = malloc(sizeof(float) * 2 * nb);
         float* sd = malloc(sizeof(float) * nb);
         int radius = s->searchRadius;
-        if (v == NULL) radius = s->searchRadiusTop;
+        if (cnn && l == top) seed_cnn(cnn, L[l][0], L[l][1], lw[l], lh[l], bw[l], bh[l], s->searchPenalty, seed);
+        else if (v == NULL) radius = s->searchRadiusTop;
         else seed_from(v, pw, ph, L[l][0], L[l][1], lw[l], lh[l], bw[l], bh[l], s->searchPenalty, seed, med);
         search(L[l][0], L[l][1], lw[l], lh[l], bw[l], bh[l], seed, radius, 1.0f, s->searchPenalty, vs, sd);
         median3(vs, bw[l], bh[l], vm);

@@ -286,7 +286,7 @@ int fgo_estimate_fmt(const fgo_frame* A, const fgo_frame* C, int W, int H, const
     }
     for (int l = 1; l < n; l++)
         for (int k = 0; k < 2; k++) fgo_i_area_half(L[l - 1][k], lw[l - 1], lh[l - 1], L[l][k], lw[l], lh[l], 1);
-    const int r = fgo_i_estimate_levels(L, n, lw, lh, s, luma, fields, seeds, meds, sads, pf, sad_mean, cut);
+    const int r = fgo_i_estimate_levels(L, n, lw, lh, s, -1, NULL, luma, fields, seeds, meds, sads, pf, sad_mean, cut);
     for (int l = 0; l < n; l++) { free(L[l][0]); free(L[l][1]); }
     return r;
 }

@@ -27,7 +27,9 @@ void fgo_i_box_blur(const float* src, int w, int h, int k, float* dst);
 /* interp.field_at: the field looked up at time t (sf = 2t - 1) */
 void fgo_i_field_at(const float* pf, int w, int h, float sf, float* out);
 /* interp.estimate from a built pyramid L[l][0] (a), L[l][1] (c), l < n: the search, median3, sub-pixel steps, the
- * cut test and the pixel field, with the outputs fgo_estimate documents. */
-int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, const fgo_settings* s, float* luma,
-                          float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean, int* cut);
+ * cut test and the pixel field, with the outputs fgo_estimate documents; with cnn (the seed net's output at
+ * cnnLevel) the search starts at that level, seeded by the net's candidates. */
+int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, const fgo_settings* s, int cnnLevel,
+                          const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf,
+                          float* sad_mean, int* cut);
 #endif

@@ -69,6 +69,9 @@ def lib():
         L.fgo_estimate.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CSettings),
                                    P, P, P, P, P, P, P, P, ctypes.c_int]
         L.fgo_estimate.restype = ctypes.c_int
+        L.fgo_estimate_cnn.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(_CSettings), ctypes.c_int, P, P, P, P, P, P, P, P, P, ctypes.c_int]
+        L.fgo_estimate_cnn.restype = ctypes.c_int
         L.fgo_synth.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CSettings),
                                 P, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, P, P, P, P, ctypes.c_int]
         L.fgo_synth.restype = ctypes.c_int
@@ -107,9 +110,10 @@ def _frame_args(a, order):
     return a, a.shape[1], a.shape[0], a.strides[0]
 
 
-def estimate(a, c, settings=None, order="rgba", trace=True, threads=0):
+def estimate(a, c, settings=None, order="rgba", trace=True, threads=0, seed_net=None):
     """interp.estimate(a, c) plus every intermediate: returns a dict with sad (the float32 mean as a Python float),
-    cut (bool), pf (fh, fw, 2) and, with trace, luma/fields/seeds/meds/sads per level."""
+    cut (bool), pf (fh, fw, 2) and, with trace, luma/fields/seeds/meds/sads per level. seed_net = (level, output):
+    the CNN-seeded estimate from the seed net's output (bh, bw, 8) at that level (no counterpart in interp.py)."""
     s = settings or Settings()
     a, W, H, pitch = _frame_args(a, order)
     c, _, _, _ = _frame_args(c, order)
@@ -125,8 +129,10 @@ def estimate(a, c, settings=None, order="rgba", trace=True, threads=0):
     sads = np.zeros(nb0, np.float32)
     pf = np.zeros((L.fh, L.fw, 2), np.float32)
     mean, cut = ctypes.c_float(), ctypes.c_int()
-    n = lib().fgo_estimate(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), _p(luma), _p(fields),
-                           _p(seeds), _p(meds), _p(sads), _p(pf), ctypes.byref(mean), ctypes.byref(cut), threads)
+    lvl, cnn = (-1, None) if seed_net is None else (int(seed_net[0]), np.ascontiguousarray(seed_net[1], np.float32))
+    n = lib().fgo_estimate_cnn(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), lvl, _p(cnn), _p(luma),
+                               _p(fields), _p(seeds), _p(meds), _p(sads), _p(pf), ctypes.byref(mean), ctypes.byref(cut),
+                               threads)
     if n != len(L.levels):
         raise RuntimeError("fgo_estimate failed")
     est = {"sad": float(mean.value), "cut": bool(cut.value), "pf": pf, "layout": L,
