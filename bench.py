@@ -49,6 +49,11 @@ def args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--eager", type=int, default=0,
                     help="profiling mode: run this many eager steps (no graphs, no timing, no JSON) and exit")
+    ap.add_argument("--seed-net", default=os.path.join(REPO, "frame-gen-ritz_b200", "seednet_l1.bin"),
+                    help="seed-net weights of the CNN-seeded arm (reported beside the plain path)")
+    ap.add_argument("--seed-level", type=int, default=1)
+    ap.add_argument("--no-seed-net", action="store_true")
+    ap.add_argument("--psnr-pairs", type=int, default=8, help="held-out 4K pairs of the CNN-vs-plain PSNR check")
     return ap.parse_args()
 
 
@@ -173,6 +178,72 @@ def run_reference(a):
           flush=True)
 
 
+def seed_net_arm(a, fg, pool, outs, stream, world, plain):
+    """The CNN-seeded arm (Interpolator::setSeedNet at --seed-level, the trained weights): its graph-replayed ms per
+    pair on the same pool as the plain path, and its PSNR against the plain path's on --psnr-pairs held-out 4K pairs
+    of the config-1 generator (ground truth at t = 1/4, 1/2, 3/4)."""
+    import torch
+    import torch.distributed as dist
+    import workloads_gpu
+    params = np.fromfile(a.seed_net, np.float32)
+    I = fg.Interpolator()
+    assert I.init(W4K, H4K, fg.VK_R8G8B8A8_UNORM, device=torch.cuda.current_device()), I.init_error()
+    assert I.set_seed_net(params, a.seed_level), "setSeedNet failed"
+    graphs = []
+    for k in range(a.pool):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            I.begin_frame()
+            assert I.record_estimate(pool[k][0], pool[k][1], stream=stream)
+            for o, t in zip(outs[k], TS):
+                assert I.record_synth(pool[k][0], pool[k][1], o, t, stream=stream)
+        graphs.append(g)
+    with torch.cuda.stream(stream):
+        for i in range(max(a.warmup, 3)):
+            graphs[i % a.pool].replay()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for i in range(a.steps):
+            graphs[i % a.pool].replay()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    t_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    del graphs
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(424242)
+    o = torch.empty((H4K, W4K, 4), dtype=torch.uint8, device="cuda")
+    ps = {"plain": [], "cnn": []}
+
+    def psnr(x, y):
+        mse = float(((x[..., :3].float() - y[..., :3].float()) ** 2).mean())
+        return 99.0 if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse)
+
+    for i in range(a.psnr_pairs):
+        d = workloads_gpu.flow_batch(1, W4K, H4K, gen, ts=TS)
+        p, c = d["prev"][0], d["curr"][0]
+        for name, J in (("plain", plain), ("cnn", I)):
+            J.begin_frame()
+            assert J.record_estimate(p, c)
+            for t in TS:
+                assert J.record_synth(p, c, o, t)
+                ps[name].append(psnr(o, d["truth"][t][0]))
+    torch.cuda.synchronize()
+    I.close()
+    dp = float(np.mean(ps["cnn"]) - np.mean(ps["plain"]))
+    return {"level": a.seed_level, "ms_per_pair": round(t_ms / (a.steps * world), 4),
+            "psnr_db": round(float(np.mean(ps["cnn"])), 3), "plain_psnr_db": round(float(np.mean(ps["plain"])), 3),
+            "psnr_delta_db": round(dp, 4), "within_0_1_db": abs(dp) <= 0.1, "psnr_frames": len(ps["cnn"]),
+            "data": "held-out config-1 pairs (workloads_gpu, seed 424242), 4K, ground truth at t = 1/4, 1/2, 3/4"}
+
+
 def main():
     a = args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -232,6 +303,7 @@ def main():
                 assert I.record_synth(pool[k][0], pool[k][1], o, t, stream=stream)
         graphs.append(g)
     n_levels = I.trace_layout().nLevels
+    # luma (+ deeper downsamples), search + median3 per level, subpixel, pixel field, synth + fallback per t
     launches_per_step = 1 + max(0, n_levels - 6) + 2 * n_levels + 2 + 2 * len(TS)
 
     with torch.cuda.stream(stream):
@@ -321,6 +393,10 @@ def main():
     e2e_value = e2e_ms / (a.e2e_steps * world)
     del pin_a
 
+    seed = None
+    if not a.no_seed_net and os.path.exists(a.seed_net):
+        seed = seed_net_arm(a, fg, pool, outs, stream, world, I)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         v, n = cpu_sample(p_np, c_np, a.cpu_seconds)
@@ -350,7 +426,7 @@ def main():
                 "gpu_launches": launches_per_step * a.steps,
                 "e2e": {"value": round(e2e_value, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 4 * W4K * H4K,
                         "d2h_bytes_per_step": len(TS) * 4 * W4K * H4K},
-                "cpu_baseline": cpu, "clocks": clocks}
+                "cpu_baseline": cpu, "clocks": clocks, "seed_net": seed}
         print(json.dumps(line), flush=True)
     I.close()
     if world > 1:

@@ -31,7 +31,7 @@ using bf16 = __nv_bfloat16;
 __device__ __forceinline__ uint32_t ldBf2(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
 __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
+    asm(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
         "{%0,%1,%2,%3};\n"
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
@@ -48,29 +48,43 @@ __global__ void __launch_bounds__(256) k_sn_pack(const float* __restrict__ la, c
     reinterpret_cast<__nv_bfloat162*>(x)[i] = __floats2bfloat162_rn(a, c);
 }
 
-// one 3x3 convolution layer, forward. in: [B][H][W][CIN] bf16; out: [B][Ho][Wo][COUT] bf16 (ReLU) or float (last layer)
-template <int CIN, int COUT, int STRIDE, bool LAST>
-__global__ void __launch_bounds__(128) k_sn_conv(const SnConvArgs a) {
-    pdlEnter();
-    constexpr int K = 9 * CIN, KP = (K + 15) / 16 * 16, NT = COUT / 8;
-    __shared__ __align__(16) bf16 ws[COUT * KP];
-    __shared__ float bs[COUT];
-    const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
-    for (int i = threadIdx.x; i < COUT * KP; i += 128) {
-        const int n = i / KP, k = i % KP;
-        ws[i] = k < K ? w[n * K + k] : __float2bfloat16(0.0f);
+// One 3x3 convolution layer, forward, in tiles of 64 output pixels (4 warps x 16). in: [B][H][W][CIN] bf16 (layer 1
+// with a.la set: the two float luma planes, normalised on the fly exactly as k_sn_pack does); out: [B][Ho][Wo][COUT]
+// bf16 (ReLU) or float (last layer).
+template <int CIN>
+struct SnShape {
+    static constexpr int K = 9 * CIN, KP = (K + 15) / 16 * 16, NKC = KP / 16;
+};
+
+// the layer's weights (bf16 [cout][9 cin], k zero-padded to a multiple of 16) and biases into shared memory
+template <int CIN, int COUT>
+__device__ __forceinline__ void snStage(const SnConvArgs& a, bf16* ws, float* bs) {
+    constexpr int K = SnShape<CIN>::K, KP = SnShape<CIN>::KP;
+    if (K == KP) {   // [cout][9 cin] is already the staged layout: a straight 16-byte copy
+        const uint4* src = reinterpret_cast<const uint4*>(a.w);
+        uint4* dst = reinterpret_cast<uint4*>(ws);
+        for (int i = threadIdx.x; i < COUT * K / 8; i += blockDim.x) dst[i] = src[i];
+    } else {
+        const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
+        for (int i = threadIdx.x; i < COUT * KP; i += blockDim.x) {
+            const int n = i / KP, k = i % KP;
+            ws[i] = k < K ? w[n * K + k] : __float2bfloat16(0.0f);
+        }
     }
     if (threadIdx.x < COUT) bs[threadIdx.x] = a.b[threadIdx.x];
-    __syncthreads();
+}
+
+// this thread's A fragments of every k chunk of tile `tile`, gathered up front (independent loads in flight together)
+template <int CIN, int STRIDE>
+__device__ __forceinline__ void snGather(const SnConvArgs& a, int tile, uint32_t (*af)[4]) {
+    constexpr int K = SnShape<CIN>::K, NKC = SnShape<CIN>::NKC;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
     const int npix = a.B * a.Ho * a.Wo;
-    const int p0 = (blockIdx.x * 4 + warp) * 16;
-    if (p0 >= npix) return;
-    // the two output pixels of this thread's A rows
+    const int p0 = (tile * 4 + warp) * 16;
     int base[2], oy[2], ox[2];
     bool val[2];
 #pragma unroll
-    for (int r = 0; r < 2; r++) {
+    for (int r = 0; r < 2; r++) {   // the two output pixels of this thread's A rows
         const int p = p0 + gid + 8 * r;
         val[r] = p < npix;
         const int pp = val[r] ? p : 0;
@@ -80,30 +94,53 @@ __global__ void __launch_bounds__(128) k_sn_conv(const SnConvArgs a) {
         base[r] = b * a.H * a.W;
     }
     const bf16* __restrict__ x = reinterpret_cast<const bf16*>(a.x);
+#pragma unroll
+    for (int kc = 0; kc < NKC; kc++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {   // register q: row gid (+8 for q odd), k columns +8 for q >= 2
+            const int r = q & 1;
+            // CIN = 32: a 16-wide k chunk lies in one tap; CIN = 2: pairs (tap, ci 0..1)
+            const int k = kc * 16 + tig * 2 + ((q >> 1) << 3);
+            const int tap = CIN == 32 ? (kc >> 1) : k / CIN;
+            const int ci = CIN == 32 ? ((kc & 1) << 4) + tig * 2 + ((q >> 1) << 3) : 0;
+            uint32_t v = 0;
+            if ((CIN == 32 || k < K) && val[r]) {
+                const int iy = oy[r] + tap / 3, ix = ox[r] + tap % 3;
+                if ((unsigned)iy < (unsigned)a.H && (unsigned)ix < (unsigned)a.W) {
+                    const size_t pix = (size_t)(base[r] + iy * a.W + ix);
+                    if (CIN == 2 && a.la) {
+                        const float la = __fmul_rn(__fsub_rn(__ldg(a.la + pix), 128.0f), 1.0f / 64.0f);
+                        const float lc = __fmul_rn(__fsub_rn(__ldg(a.lc + pix), 128.0f), 1.0f / 64.0f);
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(la, lc);
+                        v = *reinterpret_cast<const uint32_t*>(&h);
+                    } else {
+                        v = ldBf2(x + pix * CIN + ci);
+                    }
+                }
+            }
+            af[kc][q] = v;
+        }
+}
+
+// the MMAs of one tile and its store (bias, ReLU or the float output)
+template <int CIN, int COUT, bool LAST>
+__device__ __forceinline__ void snMmaStore(const SnConvArgs& a, int tile, const uint32_t (*af)[4], const bf16* ws,
+                                           const float* bs) {
+    constexpr int KP = SnShape<CIN>::KP, NKC = SnShape<CIN>::NKC, NT = COUT / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int npix = a.B * a.Ho * a.Wo;
+    const int p0 = (tile * 4 + warp) * 16;
+    if (p0 >= npix) return;
     float acc[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0f;
-#pragma unroll 2
-    for (int kc = 0; kc < KP / 16; kc++) {
-        uint32_t af[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {   // register q: row gid (+8 for q odd), k columns +8 for q >= 2
-            const int r = q & 1, k = kc * 16 + tig * 2 + ((q >> 1) << 3);
-            uint32_t v = 0;
-            if (k < K && val[r]) {
-                const int tap = k / CIN, ci = k % CIN;
-                const int iy = oy[r] + tap / 3, ix = ox[r] + tap % 3;
-                if ((unsigned)iy < (unsigned)a.H && (unsigned)ix < (unsigned)a.W)
-                    v = ldBf2(x + (size_t)(base[r] + iy * a.W + ix) * CIN + ci);
-            }
-            af[q] = v;
-        }
+    for (int kc = 0; kc < NKC; kc++)
 #pragma unroll
         for (int t = 0; t < NT; t++) {
             const bf16* wb = ws + (t * 8 + gid) * KP + kc * 16 + tig * 2;
-            mma16816(acc[t], af, ldBf2(wb), ldBf2(wb + 8));
+            mma16816(acc[t], af[kc], ldBf2(wb), ldBf2(wb + 8));
         }
-    }
 #pragma unroll
     for (int t = 0; t < NT; t++) {
         const int n = t * 8 + tig * 2;
@@ -121,6 +158,19 @@ __global__ void __launch_bounds__(128) k_sn_conv(const SnConvArgs a) {
             }
         }
     }
+}
+
+// one layer, one launch: a CTA per tile
+template <int CIN, int COUT, int STRIDE, bool LAST>
+__global__ void __launch_bounds__(128) k_sn_conv(const SnConvArgs a) {
+    pdlEnter();
+    __shared__ __align__(16) bf16 ws[COUT * SnShape<CIN>::KP];
+    __shared__ float bs[COUT];
+    uint32_t af[SnShape<CIN>::NKC][4];
+    snGather<CIN, STRIDE>(a, blockIdx.x, af);
+    snStage<CIN, COUT>(a, ws, bs);
+    __syncthreads();
+    snMmaStore<CIN, COUT, LAST>(a, blockIdx.x, af, ws, bs);
 }
 
 // ---------------------------------------------------------------------------------------------- training kernels

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+struct fg_seednet;   // the C ABI's handle (framegen_c.h)
+
 namespace fgk {
 
 constexpr int kSnLayers = 6;
@@ -24,6 +26,8 @@ struct SnConvArgs {
     void* y;           // layer output, NHWC bf16 (ReLU layers)
     float* yf;         // last layer: float [B][Ho][Wo][8]
     int B, H, W, Ho, Wo;
+    const float* la;   // layer 1 only, optional: read the float luma planes (prev, curr) instead of x
+    const float* lc;
 };
 
 struct SnBackArgs {
@@ -45,6 +49,10 @@ struct SnAdamArgs {
 
 cudaError_t launchSnPack(const float* la, const float* lc, int n, void* x, cudaStream_t s);
 cudaError_t launchSnConv(int layer, const SnConvArgs& a, cudaStream_t s);
+// the forward of a net (fg_seednet_host.cpp) for the Interpolator: one image of h x w from its float luma planes;
+// *why = the failure's message
+bool seedNetForwardLuma(::fg_seednet* n, cudaStream_t s, const float* la, const float* lc, int h, int w, float* out,
+                        const char** why);
 cudaError_t launchSnBackward(int layer, const SnBackArgs& a, bool needDx, cudaStream_t s);
 cudaError_t launchSnLoss(const float* out, const float* tgt, int n, float* dout, float* loss, float scale, cudaStream_t s);
 cudaError_t launchSnAdam(const SnAdamArgs& a, cudaStream_t s);

@@ -80,20 +80,32 @@ struct fg_seednet {
     }
     bool fits(int B, int H, int W) const { return B >= 1 && H >= 1 && W >= 1 && B <= maxB && H <= maxH && W <= maxW; }
 
-    bool forward(cudaStream_t s, const void* x, int B, int H, int W, float* dst) {
+    // the arguments of every layer. x: the packed input, or null with la / lc: the float luma planes read by the
+    // first layer directly
+    void layerArgs(SnConvArgs* args, const void* x, int B, int H, int W, float* dst, const float* la, const float* lc) {
         const SnDims d(H, W);
         const void* in = x;
         for (int l = 0; l < kSnLayers; l++) {
-            SnConvArgs a{};
+            SnConvArgs& a = args[l];
+            a = SnConvArgs{};
             a.x = in;
+            if (l == 0) { a.la = la; a.lc = lc; }
             a.w = wb + snWeightOff(l);
             a.b = p + snBiasOff(l);
             a.y = l < kSnLayers - 1 ? act[l] : nullptr;
             a.yf = l == kSnLayers - 1 ? dst : nullptr;
             a.B = B; a.H = d.h[l]; a.W = d.w[l]; a.Ho = d.h[l + 1]; a.Wo = d.w[l + 1];
-            if (!ok(launchSnConv(l, a, s), "forward", l)) return false;
             if (l < kSnLayers - 1) in = act[l];
         }
+    }
+
+    // one launch per layer (PDL-chained)
+    bool forward(cudaStream_t s, const void* x, int B, int H, int W, float* dst, const float* la = nullptr,
+                 const float* lc = nullptr) {
+        SnConvArgs args[kSnLayers];
+        layerArgs(args, x, B, H, W, dst, la, lc);
+        for (int l = 0; l < kSnLayers; l++)
+            if (!ok(launchSnConv(l, args[l], s), "forward", l)) return false;
         return true;
     }
 
@@ -119,6 +131,17 @@ struct fg_seednet {
         return true;
     }
 };
+
+namespace fgk {
+bool seedNetForwardLuma(::fg_seednet* n, cudaStream_t s, const float* la, const float* lc, int h, int w, float* out,
+                        const char** why) {
+    if (!n || !n->fits(1, h, w)) { *why = "seed net workspace too small"; return false; }
+    DevScope g(n->device);
+    if (n->forward(s, nullptr, 1, h, w, out, la, lc)) return true;
+    *why = n->err;
+    return false;
+}
+}  // namespace fgk
 
 extern "C" {
 
@@ -212,6 +235,13 @@ int fg_seednet_forward(fg_seednet* n, void* stream, const void* x, int batch, in
     if (!n || !x || !out || !n->fits(batch, h, w)) return 0;
     DevScope g(n->device);
     return n->forward((cudaStream_t)stream, x, batch, h, w, out);
+}
+
+int fg_seednet_forward_luma(fg_seednet* n, void* stream, const float* luma_prev, const float* luma_curr, int batch, int h,
+                           int w, float* out) {
+    if (!n || !luma_prev || !luma_curr || !out || !n->fits(batch, h, w)) return 0;
+    DevScope g(n->device);
+    return n->forward((cudaStream_t)stream, nullptr, batch, h, w, out, luma_prev, luma_curr);
 }
 
 int fg_seednet_backward(fg_seednet* n, void* stream, const void* x, int batch, int h, int w, const float* targets,

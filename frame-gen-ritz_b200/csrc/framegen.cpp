@@ -236,7 +236,6 @@ struct Interpolator::Impl {
     std::vector<float> snParams;
     int snLevelReq = -1, snK = -1;
     fg_seednet* snet = nullptr;
-    void* snX = nullptr;       // packed input of level snK (bf16 x 2)
     float* snOut = nullptr;    // its output, bw x bh x kSeedNetOut floats
     // profiling
     bool profiling = false;
@@ -248,10 +247,8 @@ struct Interpolator::Impl {
 
     void freeSeedNet() {
         if (snet) fg_seednet_destroy(snet);
-        if (snX) cudaFree(snX);
         if (snOut) cudaFree(snOut);
         snet = nullptr;
-        snX = nullptr;
         snOut = nullptr;
         snK = -1;
     }
@@ -265,7 +262,6 @@ struct Interpolator::Impl {
         const Level& lk = L.lv[snK];
         snet = fg_seednet_create(device, 1, lk.h, lk.w);
         if (!snet || !fg_seednet_set_params(snet, snParams.data()) ||
-            cudaMalloc(&snX, (size_t)lk.w * lk.h * 4) != cudaSuccess ||
             cudaMalloc((void**)&snOut, (size_t)lk.bw * lk.bh * fgk::kSeedNetOut * 4) != cudaSuccess) {
             cudaGetLastError();
             freeSeedNet();
@@ -415,8 +411,8 @@ struct Interpolator::Impl {
         stamp(s, "pyramid");
         if (snK >= 0) {   // the seed net on level snK
             const Level& lk = L.lv[snK];
-            if (!check(fgk::launchSnPack(luma + lk.lumaA, luma + lk.lumaC, lk.w * lk.h, snX, s))) return false;
-            if (!fg_seednet_forward(snet, s, snX, 1, lk.h, lk.w, snOut)) { lastErr = fg_seednet_error(snet); return false; }
+            if (!fgk::seedNetForwardLuma(snet, s, luma + lk.lumaA, luma + lk.lumaC, lk.h, lk.w, snOut, &lastErr))
+                return false;
             stamp(s, "seed net");
         }
         // 3-5. per level, coarse -> fine

@@ -108,6 +108,7 @@ SIGNATURES = {
     "fg_seednet_get_grads": (_I, [_P, _P]),
     "fg_seednet_pack": (_I, [_P, _P, _P, _I, _P]),
     "fg_seednet_forward": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "fg_seednet_forward_luma": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
     "fg_seednet_backward": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
     "fg_seednet_zero_grads": (_I, [_P, _P]),
     "fg_seednet_adam": (_I, [_P, _P, _F]),
@@ -413,6 +414,16 @@ class SeedNet:
         if out is None:
             out = torch.empty((B, (h + 7) // 8, (w + 7) // 8, self.N_OUT), dtype=torch.float32, device=x.device)
         self._ok(lib().fg_seednet_forward(self._h, _stream(stream), x.data_ptr(), B, h, w, out.data_ptr()))
+        return out
+
+    def forward_luma(self, luma_prev, luma_curr, out=None, stream=None):
+        """the forward pass straight from (B, h, w) float32 luma planes (the first layer packs them)"""
+        import torch
+        B, h, w = luma_prev.shape
+        if out is None:
+            out = torch.empty((B, (h + 7) // 8, (w + 7) // 8, self.N_OUT), dtype=torch.float32, device=luma_prev.device)
+        self._ok(lib().fg_seednet_forward_luma(self._h, _stream(stream), luma_prev.data_ptr(), luma_curr.data_ptr(), B,
+                                               h, w, out.data_ptr()))
         return out
 
     def backward(self, x, targets, loss=None, stream=None):

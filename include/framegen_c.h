@@ -120,6 +120,9 @@ int fg_seednet_get_params(fg_seednet* net, float* host_params);
 int fg_seednet_get_grads(fg_seednet* net, float* host_grads);         /* the gradient accumulated since the last step */
 int fg_seednet_pack(void* stream, const float* luma_prev, const float* luma_curr, int n, void* x);
 int fg_seednet_forward(fg_seednet* net, void* stream, const void* x, int batch, int h, int w, float* out);
+/* the same from the float luma planes [B][h][w] of prev and curr (the first layer packs them as it reads) */
+int fg_seednet_forward_luma(fg_seednet* net, void* stream, const float* luma_prev, const float* luma_curr, int batch, int h,
+                           int w, float* out);
 /* forward + loss + backward: adds dLoss/dParams to the gradient; *loss (device float, optional) = the batch's loss */
 int fg_seednet_backward(fg_seednet* net, void* stream, const void* x, int batch, int h, int w, const float* targets,
                         float* loss);

@@ -140,3 +140,17 @@ def test_training_lowers_the_loss():
             hist.append(float(loss))
     assert hist[-1] < 0.5 * hist[0], hist
     net.close()
+
+
+def test_forward_from_luma_equals_packed_forward():
+    """fg_seednet_forward_luma (the first layer packing the float luma planes as it reads them) gives the bits of
+    fg_seednet_pack + fg_seednet_forward"""
+    la, lc = level1_lumas(2, seed=40)
+    net = fg.SeedNet(2, 64, 64)
+    net.set_params(params(6))
+    dla, dlc = torch.from_numpy(la).cuda(), torch.from_numpy(lc).cuda()
+    a = net.forward(fg.SeedNet.pack(dla, dlc))
+    b = net.forward_luma(dla, dlc)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    net.close()
