@@ -135,6 +135,7 @@ __device__ __forceinline__ void lumaTower(const LumaPyrParams& p, float (*sl)[kT
 constexpr int kSyE = 128, kSyEH = 32, kSyAp = 3;                 // 128 x 32 mismatch region -> 122 x 26 output tile
 constexpr int kSyT = kSyE - 2 * kSyAp, kSyTH = kSyEH - 2 * kSyAp;
 constexpr int kSyThreads = 512, kSyK = kSyEH / (kSyThreads / kSyE);   // region rows per thread (512 = 128 columns x 4)
+constexpr size_t kSyWarpBytes = (size_t)2 * kSyTH * kSyE * 4;   // k_synth: both warps of the output rows, after the row sums
 
 // cv2.remap INTER_LINEAR / BORDER_REPLICATE of the 2-channel float field at (x, y): quantisation and weights paired
 // (exact), the taps' weighted sum as cv2 rounds it, ((p00 w00 + p01 w01) + p10 w10) + p11 w11 per channel

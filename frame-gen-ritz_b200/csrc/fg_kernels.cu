@@ -780,21 +780,12 @@ __device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, u
     const int X = __float_as_int(bxf) - 0x4B400000, Y = __float_as_int(byf) - 0x4B400000;
     const int ix = X >> 5, iy = Y >> 5;
     const uint32_t fx = (uint32_t)X & 31u, fy = (uint32_t)Y & 31u;
-    uint32_t p00, p01, p10, p11;
-    if ((unsigned)ix < (unsigned)(W - 1) && (unsigned)iy < (unsigned)(H - 1)) {
-        const uint32_t* q = img + ((uint32_t)iy * pw + (uint32_t)ix);   // pw: row pitch in 4-byte words
-        p00 = __ldg(q);
-        p01 = __ldg(q + 1);
-        p10 = __ldg(q + pw);
-        p11 = __ldg(q + pw + 1);
-    } else {
-        const uint32_t x0 = (uint32_t)clampi(ix, 0, W - 1), x1 = (uint32_t)clampi(ix + 1, 0, W - 1);
-        const uint32_t r0 = (uint32_t)clampi(iy, 0, H - 1) * pw, r1 = (uint32_t)clampi(iy + 1, 0, H - 1) * pw;
-        p00 = __ldg(img + r0 + x0);
-        p01 = __ldg(img + r0 + x1);
-        p10 = __ldg(img + r1 + x0);
-        p11 = __ldg(img + r1 + x1);
-    }
+    // taps clamped one by one, without a branch, so the loads of the samples a thread takes can all be in flight
+    // together (pw: row pitch in 4-byte words)
+    const uint32_t x0 = (uint32_t)clampi(ix, 0, W - 1), x1 = (uint32_t)clampi(ix + 1, 0, W - 1);
+    const uint32_t r0 = (uint32_t)clampi(iy, 0, H - 1) * pw, r1 = (uint32_t)clampi(iy + 1, 0, H - 1) * pw;
+    const uint32_t p00 = __ldg(img + r0 + x0), p01 = __ldg(img + r0 + x1);
+    const uint32_t p10 = __ldg(img + r1 + x0), p11 = __ldg(img + r1 + x1);
     const uint32_t M = 0x00FF00FFu, wx0 = 32u - fx, wy0 = 32u - fy;
     const uint32_t rb0 = (p00 & M) * wx0 + (p01 & M) * fx, rb1 = (p10 & M) * wx0 + (p11 & M) * fx;
     const uint32_t g0 = __byte_perm(p00, 0, 0x4441) * wx0 + __byte_perm(p01, 0, 0x4441) * fx;
@@ -836,9 +827,10 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
     uint8_t* e;
     unsigned short* hsum;
     const SyCoef cx = syFieldStage(p, X0, Y0, tid, ex, ey0, rowc, gReg, sm, hrow, e, hsum);
-    // 2. this thread's region column: half-vector (vertical stage, x fs folded in), both warps, mismatch. The warps of
-    //    output pixels stay in registers until the blend.
-    uint32_t wa[kSyK], wc[kSyK];
+    // 2. this thread's region column: half-vector (vertical stage, x fs folded in), both warps, mismatch. The warps
+    //    wait in shared memory for the blend (in registers they would leave too few for the sample loads in flight).
+    uint32_t* sWA = reinterpret_cast<uint32_t*>(hsum + kSyEH * kSyE);   // the output rows: kSyTH x kSyE
+    uint32_t* sWC = sWA + kSyTH * kSyE;
     const float kA = p.mid ? 1.0f : p.ka, kC = p.mid ? 1.0f : p.kc;   // t = 0.5: the products by 1 are exact
 #pragma unroll
     for (int k = 0; k < kSyK; k++) {
@@ -850,9 +842,12 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
         // a(q - 2t h), c(q + 2(1 - t) h): float32 products, then the sums (numpy's order)
         const float2 ba = rne32bits(make_float2(__fsub_rn(cx.pos, __fmul_rn(kA, hx)), __fsub_rn(cy.pos, __fmul_rn(kA, hy))));
         const float2 bc = rne32bits(make_float2(__fadd_rn(cx.pos, __fmul_rn(kC, hx)), __fadd_rn(cy.pos, __fmul_rn(kC, hy))));
-        wa[k] = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y);
-        wc[k] = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y);
-        const uint32_t d = __vabsdiffu4(wa[k], wc[k]);
+        const uint32_t A = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y), C = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y);
+        if ((unsigned)(ey - kSyAp) < (unsigned)kSyTH) {   // warp-uniform
+            sWA[(ey - kSyAp) * kSyE + ex] = A;
+            sWC[(ey - kSyAp) * kSyE + ex] = C;
+        }
+        const uint32_t d = __vabsdiffu4(A, C);
         const uint32_t m = __vmaxu4(__vmaxu4(d, d >> 8), d >> 16);
         e[ey * kSyE + ex] = (uint8_t)(m & 255u);
     }
@@ -882,15 +877,16 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
             const unsigned short* q = hsum + ly * kSyE + lx;
             const int S = q[0] + q[kSyE] + q[2 * kSyE] + q[3 * kSyE] + q[4 * kSyE] + q[5 * kSyE] + q[6 * kSyE];
             const uint32_t nq = __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
+            const uint32_t wak = sWA[ly * kSyE + ex], wck = sWC[ly * kSyE + ex];
             uint32_t o;
             if (S <= p.sZero) {   // u = 0: out = the blend rounded
                 if (p.mid) {
-                    o = __vavgu4(wa[k], wc[k]);   // floor(0.5 (a + c) + 0.5) per byte
+                    o = __vavgu4(wak, wck);   // floor(0.5 (a + c) + 0.5) per byte
                 } else {
                     // fl32(fl32((1 - t) a) + fl32(t c)) + 0.5, floored (never above 255.5 here, so no clamp is needed): the
                     // products come from the tables, the adds are paired (adds alone cannot be fused), the floor is a
                     // round-toward-zero add of 2^23 whose low mantissa byte is the result
-                    const uint32_t A = wa[k], C = wc[k];
+                    const uint32_t A = wak, C = wck;
                     const float2 m01 = padd(make_float2(TA[A & 255u], TA[(A >> 8) & 255u]), make_float2(TC[C & 255u], TC[(C >> 8) & 255u]));
                     const float m2 = __fadd_rn(TA[(A >> 16) & 255u], TC[(C >> 16) & 255u]);
                     const float2 f01 = __ffma2_rz(padd(m01, make_float2(0.5f, 0.5f)), make_float2(1.0f, 1.0f), make_float2(8388608.0f, 8388608.0f));
@@ -910,7 +906,7 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
 #pragma unroll
                 for (int k2 = 0; k2 < 3; k2++) {
                     const int sh = 8 * k2;
-                    const uint32_t ca = (wa[k] >> sh) & 255u, cc = (wc[k] >> sh) & 255u;
+                    const uint32_t ca = (wak >> sh) & 255u, cc = (wck >> sh) & 255u;
                     const float fa = i2f((int)ca), fc = i2f((int)cc), fn = i2f((int)((nq >> sh) & 255u));
                     const float mix = p.mid ? __fmul_rn(0.5f, __fadd_rn(fa, fc)) : __fadd_rn(TA[ca], TC[cc]);
                     const float v = __fadd_rn(__fadd_rn(__fmul_rn(mix, iu), __fmul_rn(fn, u)), 0.5f);
@@ -979,7 +975,8 @@ static size_t planBytes(const CutPlan& c) {
 cudaError_t prepareKernels() {
     cudaError_t e = cudaFuncSetAttribute(k_subpix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cutmean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)synthSmemBytes(1));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(synthSmemBytes(1) + kSyWarpBytes));
     return e;
 }
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
@@ -999,7 +996,7 @@ size_t synthSmemBytes(int fs) {  // declared in fg_params.h
     return (size_t)gw * gh * 8 + (size_t)gh * kSyE * 8 + (size_t)kSyEH * kSyE + (size_t)kSyEH * kSyE * 2;
 }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
-    const size_t smem = synthSmemBytes(p.fs);
+    const size_t smem = synthSmemBytes(p.fs) + kSyWarpBytes;
     return launchPdl(k_synth, dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), dim3(kSyThreads), smem, s, p);
 }
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s) {
