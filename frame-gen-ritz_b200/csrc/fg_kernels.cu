@@ -470,15 +470,96 @@ __global__ void __launch_bounds__(256) k_cutmean(const CutMeanParams p) {
 // Every pass samples each frame on a 24 x 24 lattice: per axis, the 8 pixel positions times the pass's 3 offsets
 // (base + step * {-1, 0, 1}, quarter-pixel units). The lattice is built separably (horizontal then vertical, weights
 // multiples of 1/4: every product and sum is exact, so it equals cv2's bilinear tap), after which a candidate's SAD is
-// two shared loads per pixel. The last CTA computes the scene-cut mean of the winners' SADs.
+// two shared loads per pixel. The scene-cut mean of the winners' SADs (numpy's pairwise sum) is spread over the grid:
+// the warp that writes the last SAD of a leaf of the summation tree sums that leaf, and the warp that completes the
+// last leaf adds the inner nodes.
 constexpr int kSubT = 13, kSubO = 2, kSubL = 24, kSubRows = 10;   // tile, its margin, lattice side, tile rows used
 constexpr int kSubWarpFloats = 2 * kSubT * kSubT + 2 * kSubRows * kSubL + 72;
+
+// One leaf of the pairwise tree by one warp, in numpy's order: lanes 0..7 are its 8 accumulators (independent loads),
+// combined as ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), then the tail; leaves under 8 elements by lane 0
+// alone. Also returns (in every lane) the leaf's sum of roundEven(sad * 256), the debug counter's share.
+__device__ __forceinline__ float warpLeafSum(const float* a, int n, int lane, unsigned int& s256) {
+    unsigned int s = 0;
+    for (int i = lane; i < n; i += 32) s += (unsigned int)__float2int_rn(__fmul_rn(__ldcg(a + i), 256.0f));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    s256 = s;
+    float res = 0.0f;
+    if (n < 8) {
+        if (lane == 0)
+            for (int i = 0; i < n; i++) res = __fadd_rn(res, __ldcg(a + i));
+        return __shfl_sync(0xffffffffu, res, 0);
+    }
+    const int body = n - (n % 8);
+    float r = 0.0f;
+    if (lane < 8) {
+        r = __ldcg(a + lane);
+        for (int i = 8 + lane; i < body; i += 8) r = __fadd_rn(r, __ldcg(a + i));
+    }
+    const float r1 = __shfl_down_sync(0xffffffffu, r, 1);   // lane 2k: r[2k] + r[2k+1]
+    const float p2 = __fadd_rn(r, r1);
+    const float p2b = __shfl_down_sync(0xffffffffu, p2, 2);  // lane 4k: (r0 + r1) + (r2 + r3)
+    const float p4 = __fadd_rn(p2, p2b);
+    const float p4b = __shfl_down_sync(0xffffffffu, p4, 4);
+    if (lane == 0) {
+        res = __fadd_rn(p4, p4b);
+        for (int i = body; i < n; i++) res = __fadd_rn(res, __ldcg(a + i));
+    }
+    return __shfl_sync(0xffffffffu, res, 0);
+}
+
+// the scene-cut mean's share of the warp that wrote the SAD of block b (warp-uniform call)
+__device__ __forceinline__ void cutMeanShare(const SubpixParams& p, int b, int nb, int lane) {
+    const CutPlan& pl = p.plan;
+    const int leaf = pl.leafOf[b];
+    unsigned int old = 0;
+    if (lane == 0) {
+        __threadfence();   // this warp's SAD before its arrival
+        old = atomicAdd(pl.leafCnt + leaf, 1u);
+    }
+    old = __shfl_sync(0xffffffffu, old, 0);
+    const int2 lf = pl.leaves[leaf];
+    if (old != (unsigned int)lf.y - 1u) return;
+    __threadfence();
+    unsigned int s256;
+    const float v = warpLeafSum(p.sads + lf.x, lf.y, lane, s256);
+    unsigned int done = 0;
+    if (lane == 0) {
+        pl.gvals[leaf] = v;
+        pl.leafS256[leaf] = s256;
+        pl.leafCnt[leaf] = 0;
+        __threadfence();
+        done = atomicAdd(&p.st->subDone, 1u);
+    }
+    done = __shfl_sync(0xffffffffu, done, 0);
+    if (done != (unsigned int)pl.nLeaves - 1u) return;
+    // the last leaf: the inner nodes, one height per step, then the mean and the debug counter
+    __threadfence();
+    for (int d = 0; d < pl.nSteps; d++) {
+        for (int j = pl.depthStart[d] + lane; j < pl.depthStart[d + 1]; j += 32) {
+            const int2 c = pl.inner[j];
+            pl.gvals[pl.nLeaves + j] = __fadd_rn(__ldcg(pl.gvals + c.x), __ldcg(pl.gvals + c.y));
+        }
+        __threadfence_block();
+        __syncwarp();
+    }
+    unsigned int tot = 0;
+    for (int i = lane; i < pl.nLeaves; i += 32) tot += __ldcg(pl.leafS256 + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0) {
+        const float mean = __fdiv_rn(__ldcg(pl.gvals + pl.root), (float)nb);
+        p.st->sadMean = mean;
+        p.st->cut = mean > p.cutSad ? 1u : 0u;
+        p.st->sadSum256 = tot;
+        p.st->subDone = 0;
+    }
+}
 
 __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
     pdlEnter();
     extern __shared__ float smem[];
-    __shared__ unsigned int ticket;
-    __shared__ unsigned int red[128];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * 4 + warp;
     const int nb = p.bw * p.bh;
@@ -575,16 +656,8 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
             p.out[b] = make_float2(__fadd_rn((float)sx, (float)b4x * 0.25f), __fadd_rn((float)sy, (float)b4y * 0.25f));
             p.sads[b] = sadBest;
         }
+        cutMeanShare(p, b, nb, lane);
     }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) ticket = atomicAdd(&p.st->subDone, 1u);
-    __syncthreads();
-    if (ticket != gridDim.x - 1) return;
-    __threadfence();
-    const bool inSmem = (size_t)(p.plan.nLeaves + p.plan.nInner) * sizeof(float) <= kPlanSmemMax;
-    cutMeanBlock(p.sads, nb, p.plan, p.cutSad, p.st, inSmem ? smem : p.plan.gvals, red);
-    if (threadIdx.x == 0) p.st->subDone = 0;
 }
 
 // ============================================================================================== per-pixel field
@@ -980,8 +1053,7 @@ cudaError_t prepareKernels() {
     return e;
 }
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
-    const size_t tiles = (size_t)4 * kSubWarpFloats * sizeof(float);
-    const size_t smem = tiles > planBytes(p.plan) ? tiles : planBytes(p.plan);
+    const size_t smem = (size_t)4 * kSubWarpFloats * sizeof(float);
     return launchPdl(k_subpix, dim3(divUp(p.bw * p.bh, 4)), dim3(128), smem, s, p);
 }
 cudaError_t launchCutMean(const CutMeanParams& p, cudaStream_t s) {

@@ -20,7 +20,7 @@ struct DevState {
     unsigned int cut;                  // scene-cut decision of the latest estimate (interp.py:190)
     float sadMean;                     // the float32 mean block SAD the cut test compares (interp.py:164)
     unsigned int medDone[kMaxLevels];  // last-block tickets of the median histograms
-    unsigned int subDone;              // last-block ticket of the sub-pixel pass (scene-cut mean)
+    unsigned int subDone;              // leaves of the scene-cut sum completed in the sub-pixel pass
     float med[kMaxLevels][2];          // per fine level: 2 x the global median of the own-parent vectors (interp.py:142)
     unsigned int err;                  // sticky error bits (bound checks that could only fail on a library bug)
 };
@@ -88,7 +88,10 @@ struct CutPlan {               // numpy's pairwise float32 summation tree of N e
     const int2* inner;         // (left slot, right slot) per inner node, deepest depth first
     const int* depthStart;     // inner[depthStart[d] .. depthStart[d + 1]) are computed in step d
     int nLeaves, nInner, nSteps, root;
-    float* gvals;              // nLeaves + nInner floats of global scratch, used when they exceed kPlanSmemMax
+    float* gvals;              // nLeaves + nInner floats of global scratch (k_cutmean: when they exceed kPlanSmemMax)
+    const int* leafOf;         // k_subpix: the leaf of every element
+    unsigned int* leafCnt;     // k_subpix: arrivals per leaf (zero between launches)
+    unsigned int* leafS256;    // k_subpix: per leaf, the sum of roundEven(sad * 256)
 };
 constexpr size_t kPlanSmemMax = 96 * 1024;   // node values kept in shared memory up to this size
 

@@ -322,6 +322,7 @@ struct Interpolator::Impl {
         const size_t oLeaves = take(P.leaves.size() * 8), oInner = take(std::max<size_t>(P.inner.size(), 1) * 8);
         const size_t oDepth = take(P.depthStart.size() * 4 + 4);
         const size_t oVals = take((P.leaves.size() + P.inner.size()) * 4);
+        const size_t oLeafOf = take((size_t)nb0 * 4), oLeafCnt = take(P.leaves.size() * 4), oLeafS = take(P.leaves.size() * 4);
         if (cudaMalloc(&arena, off) != cudaSuccess) { arena = nullptr; cudaGetLastError(); return kErrAlloc; }
         arenaBytes = off;
         cudaMemset(arena, 0, off);
@@ -335,6 +336,12 @@ struct Interpolator::Impl {
         cudaMemcpy(arena + oLeaves, P.leaves.data(), P.leaves.size() * 8, cudaMemcpyHostToDevice);
         if (!P.inner.empty()) cudaMemcpy(arena + oInner, P.inner.data(), P.inner.size() * 8, cudaMemcpyHostToDevice);
         cudaMemcpy(arena + oDepth, P.depthStart.data(), P.depthStart.size() * 4, cudaMemcpyHostToDevice);
+        {
+            std::vector<int> leafOf((size_t)nb0);
+            for (size_t i = 0; i < P.leaves.size(); i++)
+                for (int k = 0; k < P.leaves[i].y; k++) leafOf[(size_t)P.leaves[i].x + k] = (int)i;
+            cudaMemcpy(arena + oLeafOf, leafOf.data(), (size_t)nb0 * 4, cudaMemcpyHostToDevice);
+        }
         if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); freeAll(); return kErrAlloc; }
         plan.leaves = (const int2*)(arena + oLeaves);
         plan.inner = (const int2*)(arena + oInner);
@@ -344,6 +351,9 @@ struct Interpolator::Impl {
         plan.nSteps = P.nSteps;
         plan.root = P.root;
         plan.gvals = (float*)(arena + oVals);
+        plan.leafOf = (const int*)(arena + oLeafOf);
+        plan.leafCnt = (unsigned int*)(arena + oLeafCnt);
+        plan.leafS256 = (unsigned int*)(arena + oLeafS);
         W = w;
         H = h;
         haveEst = false;
