@@ -847,9 +847,10 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
 // t = 0.5 blend use byte-SIMD instructions.
 
 // one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame at the position whose
-// rne32 bits are (bx, by): channels 0..2 of the result (byte 3 = 0). Horizontal stage two channels per multiply (16-bit
+// rne32 bits are (bx, by): channels 0..2 of the result (byte 3 = 0; also unpacked in ch). Horizontal stage two channels per multiply (16-bit
 // lanes hold at most 255 * 32), vertical stage per channel; (v + 512) >> 10 == cv2's (32 v + 2^14) >> 15.
-__device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, uint32_t pw, int W, int H, float bxf, float byf) {
+__device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, uint32_t pw, int W, int H, float bxf, float byf,
+                                             int ch[3]) {
     const int X = __float_as_int(bxf) - 0x4B400000, Y = __float_as_int(byf) - 0x4B400000;
     const int ix = X >> 5, iy = Y >> 5;
     const uint32_t fx = (uint32_t)X & 31u, fy = (uint32_t)Y & 31u;
@@ -866,6 +867,9 @@ __device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, u
     const uint32_t c0 = ((rb0 & 0xFFFFu) * wy0 + (rb1 & 0xFFFFu) * fy + 512u) >> 10;
     const uint32_t c2 = ((rb0 >> 16) * wy0 + (rb1 >> 16) * fy + 512u) >> 10;
     const uint32_t c1 = (g0 * wy0 + g1 * fy + 512u) >> 10;
+    ch[0] = (int)c0;
+    ch[1] = (int)c1;
+    ch[2] = (int)c2;
     return c2 * 65536u + (c1 * 256u + c0);
 }
 
@@ -915,14 +919,14 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
         // a(q - 2t h), c(q + 2(1 - t) h): float32 products, then the sums (numpy's order)
         const float2 ba = rne32bits(make_float2(__fsub_rn(cx.pos, __fmul_rn(kA, hx)), __fsub_rn(cy.pos, __fmul_rn(kA, hy))));
         const float2 bc = rne32bits(make_float2(__fadd_rn(cx.pos, __fmul_rn(kC, hx)), __fadd_rn(cy.pos, __fmul_rn(kC, hy))));
-        const uint32_t A = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y), C = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y);
+        int ca[3], cc[3];
+        const uint32_t A = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y, ca), C = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y, cc);
         if ((unsigned)(ey - kSyAp) < (unsigned)kSyTH) {   // warp-uniform
             sWA[(ey - kSyAp) * kSyE + ex] = A;
             sWC[(ey - kSyAp) * kSyE + ex] = C;
         }
-        const uint32_t d = __vabsdiffu4(A, C);
-        const uint32_t m = __vmaxu4(__vmaxu4(d, d >> 8), d >> 16);
-        e[ey * kSyE + ex] = (uint8_t)(m & 255u);
+        const int m = max(max(abs(ca[0] - cc[0]), abs(ca[1] - cc[1])), abs(ca[2] - cc[2]));
+        e[ey * kSyE + ex] = (uint8_t)m;
     }
     __syncthreads();
     // 3. horizontal 7-sums: one region row and 16 output columns per thread, a running window
