@@ -958,7 +958,8 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
             uint32_t o;
             if (S <= p.sZero) {   // u = 0: out = the blend rounded
                 if (p.mid) {
-                    o = __vavgu4(wak, wck);   // floor(0.5 (a + c) + 0.5) per byte
+                    // floor(0.5 (a + c) + 0.5) per byte: (a | c) - ((a ^ c) >> 1), no borrow between bytes
+                    o = (wak | wck) - (((wak ^ wck) >> 1) & 0x7F7F7F7Fu);
                 } else {
                     // fl32(fl32((1 - t) a) + fl32(t c)) + 0.5, floored (never above 255.5 here, so no clamp is needed): the
                     // products come from the tables, the adds are paired (adds alone cannot be fused), the floor is a
