@@ -873,14 +873,14 @@ __device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, u
     return c2 * 65536u + (c1 * 256u + c0);
 }
 
-__global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
-    pdlEnter();
+// one output tile (bx, by) of one synthesis; all threads of the CTA take part (the cut path returns at once)
+__device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ SyCoef rowc[kSyEH];
     __shared__ float TA[256], TC[256];
     __shared__ unsigned int cnt;
     __shared__ int gReg[4];
-    const int X0 = blockIdx.x * kSyT, Y0 = blockIdx.y * kSyTH;
+    const int X0 = bx * kSyT, Y0 = by * kSyTH;
     const int tid = threadIdx.x, ex = tid & (kSyE - 1), ey0 = tid / kSyE;
     const uint8_t* nearF = p.nearC ? p.c : p.a;
     const uint32_t pitch = (uint32_t)p.pitch, pw = pitch >> 2;
@@ -1001,6 +1001,56 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
     if (tid == 0 && cnt) atomicAdd(p.untrusted, cnt);
 }
 
+__global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
+    pdlEnter();
+    synthTile(p, blockIdx.x, blockIdx.y);
+}
+
+// Many syntheses (of several frame pairs and times) in one persistent launch: every CTA takes the next tile of the
+// work list (items in the host's order, each item's tiles in raster order) from an atomic counter until the list is
+// exhausted; an item's parameters are staged in shared memory per tile. Mixed sizes balance across the SMs.
+__global__ void __launch_bounds__(kSyThreads, 3) k_synth_batch(const SynthBatchArgs b) {
+    pdlEnter();
+    __shared__ int work, item;
+    __shared__ __align__(16) SynthParams sp;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            work = (int)atomicAdd(b.counter, 1u);
+            int lo = 0, hi = b.nItems - 1;   // the item whose tile range holds `work`
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (b.tileStart[mid] <= work) lo = mid; else hi = mid - 1;
+            }
+            item = lo;
+        }
+        __syncthreads();
+        const int w = work, it = item;
+        if (w >= b.total) break;
+        static_assert(sizeof(SynthParams) % 4 == 0, "SynthParams copies as words");
+        for (int i = threadIdx.x; i < (int)(sizeof(SynthParams) / 4); i += kSyThreads)
+            reinterpret_cast<uint32_t*>(&sp)[i] = __ldg(reinterpret_cast<const uint32_t*>(b.items + it) + i);
+        __syncthreads();
+        const int t = w - b.tileStart[it], tx = b.tilesX[it];
+        synthTile(sp, t % tx, t / tx);
+        __syncthreads();   // the tile's shared memory is free again
+    }
+}
+
+// the untrusted-share decision of many syntheses (grid.y = item), the batched k_fallback (the item counters are
+// zeroed by the host before the batch's synth launch)
+__global__ void __launch_bounds__(256) k_fallback_batch(const FallbackParams* __restrict__ items) {
+    const FallbackParams& p = items[blockIdx.y];
+    const unsigned int cnt = *p.untrusted;
+    if (!((double)cnt / ((double)p.W * (double)p.H) > p.frac)) return;
+    const uint8_t* nearF = p.nearC ? p.c : p.a;
+    const size_t n = (size_t)p.W * p.H;
+    for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (size_t)gridDim.x * 256) {
+        const int x = (int)(i % p.W), y = (int)(i / p.W);
+        reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] =
+            __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * p.pitch) + x);
+    }
+}
+
 // interp.py:238-239: more than globalFallback of the pixels untrusted -> the nearer real frame over the output.
 // Every CTA exits at once in the normal case. Also clears the next synth's counter.
 __global__ void __launch_bounds__(256) k_fallback(const FallbackParams p) {
@@ -1055,6 +1105,9 @@ cudaError_t prepareKernels() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cutmean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(synthSmemBytes(1) + kSyWarpBytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(synthSmemBytes(1) + kSyWarpBytes));
     return e;
 }
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
@@ -1072,9 +1125,26 @@ size_t synthSmemBytes(int fs) {  // declared in fg_params.h
     const int gw = (kSyE + fs - 1) / fs + 3, gh = (kSyEH + fs - 1) / fs + 3;
     return (size_t)gw * gh * 8 + (size_t)gh * kSyE * 8 + (size_t)kSyEH * kSyE + (size_t)kSyEH * kSyE * 2;
 }
+size_t synthKernelSmem(int fs) { return synthSmemBytes(fs) + kSyWarpBytes; }
+int synthTilesX(int W) { return (int)divUp(W, kSyT); }
+int synthTilesY(int H) { return (int)divUp(H, kSyTH); }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs) + kSyWarpBytes;
     return launchPdl(k_synth, dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), dim3(kSyThreads), smem, s, p);
+}
+cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s) {
+    return launchPdl(k_synth_batch, dim3(grid), dim3(kSyThreads), smem, s, b);
+}
+int synthBatchCtasPerSm(size_t smem) {   // resident k_synth_batch CTAs per SM with this dynamic shared memory
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_synth_batch, kSyThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ;
+}
+cudaError_t launchFallbackBatch(const FallbackParams* items, int nItems, cudaStream_t s) {
+    return launchPdl(k_fallback_batch, dim3(148, nItems), dim3(256), 0, s, items);
 }
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s) {
     return launchPdl(k_fallback, dim3(148 * 4), dim3(256), 0, s, p);

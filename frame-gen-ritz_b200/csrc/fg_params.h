@@ -142,6 +142,14 @@ struct SynthParams {
     uint8_t* outc; size_t outCPitch;
 };
 
+struct SynthBatchArgs {             // k_synth_batch: a work list of syntheses
+    const SynthParams* items;      // per item (device array)
+    const int* tileStart;          // nItems + 1: the first tile of each item in the list, then the total
+    const int* tilesX;             // per item: output tiles across
+    int nItems, total;
+    unsigned int* counter;         // the next tile to take (zero before the launch)
+};
+
 struct FallbackParams {
     const uint8_t* a; const uint8_t* c; size_t pitch;
     uint8_t* out; size_t outPitch;
@@ -170,6 +178,13 @@ cudaError_t launchCutMean(const CutMeanParams& p, cudaStream_t s);
 cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s);
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s);
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s);
+// batches (framegen.cpp Batch): many syntheses in one persistent launch, their fallbacks in one launch
+cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s);
+int synthBatchCtasPerSm(size_t smem);
+cudaError_t launchFallbackBatch(const FallbackParams* items, int nItems, cudaStream_t s);
+size_t synthKernelSmem(int fs);   // k_synth's / k_synth_batch's dynamic shared memory at this flow scale
+int synthTilesX(int W);           // output tiles of a synthesis across / down
+int synthTilesY(int H);
 // the other formats (fg_formats.cu)
 cudaError_t prepareFormatKernels();
 cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s);

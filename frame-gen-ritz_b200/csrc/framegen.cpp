@@ -11,6 +11,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "fg_params.h"
@@ -484,7 +485,8 @@ struct Interpolator::Impl {
         return true;
     }
 
-    bool synth(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t) {
+    // the parameters of one synthesis (interp.synth's t constants, this size's buffers); untrusted: its counter
+    fgk::SynthParams synthParams(const Frame& prev, const Frame& curr, const Frame& out, float t, unsigned int* untrusted) const {
         const double td = t;
         fgk::SynthParams sp{};
         sp.a = (const uint8_t*)prev.data; sp.c = (const uint8_t*)curr.data; sp.pitch = prev.pitch;
@@ -504,25 +506,36 @@ struct Interpolator::Impl {
         sp.trustSpan = (float)((double)set.trustHigh - (double)set.trustLow);
         sp.sZero = sZero; sp.sOne = sOne;
         sp.st = st;
-        sp.untrusted = &st->untrusted[parity];
+        sp.untrusted = untrusted;
         sp.emap = capture ? emap : nullptr;
         sp.f = fc;
         sp.ac = (const uint8_t*)prev.chroma; sp.cc = (const uint8_t*)curr.chroma; sp.cpitch = prev.chromaPitch;
         sp.outc = (uint8_t*)out.chroma; sp.outCPitch = out.chromaPitch;
-        if (!check(fmt == Format::Rgba8 ? fgk::launchSynth(sp, s) : fgk::launchSynthFmt(sp, s))) return false;
-        stamp(s, "synth");
+        return sp;
+    }
+
+    // the parameters of its whole-frame fallback (interp.py:238-239); next: the counter to clear (may be null)
+    fgk::FallbackParams fallbackParams(const fgk::SynthParams& sp, unsigned int* next) const {
         fgk::FallbackParams fp{};
         fp.a = sp.a; fp.c = sp.c; fp.pitch = sp.pitch; fp.out = sp.out; fp.outPitch = sp.outPitch;
         fp.W = sp.W; fp.H = sp.H; fp.nearC = sp.nearC;
         fp.frac = (double)set.globalFallback;
-        fp.untrusted = &st->untrusted[parity];
-        fp.untrustedNext = &st->untrusted[parity ^ 1u];
+        fp.untrusted = sp.untrusted;
+        fp.untrustedNext = next;
         fp.rowBytes = (size_t)W * planeBytes(fmt);
         if (chromaBytes(fmt)) {
             fp.cbytes = (size_t)((W + 1) / 2) * chromaBytes(fmt);
             fp.ch = (int)(H + 1) / 2;
             fp.ac = sp.ac; fp.cc = sp.cc; fp.cpitch = sp.cpitch; fp.outc = sp.outc; fp.outCPitch = sp.outCPitch;
         }
+        return fp;
+    }
+
+    bool synth(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t) {
+        const fgk::SynthParams sp = synthParams(prev, curr, out, t, &st->untrusted[parity]);
+        if (!check(fmt == Format::Rgba8 ? fgk::launchSynth(sp, s) : fgk::launchSynthFmt(sp, s))) return false;
+        stamp(s, "synth");
+        const fgk::FallbackParams fp = fallbackParams(sp, &st->untrusted[parity ^ 1u]);
         if (!check(fmt == Format::Rgba8 ? fgk::launchFallback(fp, s) : fgk::launchFallbackFmt(fp, s))) return false;
         stamp(s, "fallback");
         lastParity = parity;
@@ -809,6 +822,201 @@ bool Interpolator::recordTrace(cudaStream_t stream, void* dst) {
     return ok;
 }
 
+
+// ================================================================================================== batches
+struct Batch::Impl {
+    static constexpr int kRing = 8;   // pinned upload buffers: at most this many records in flight
+    std::vector<std::unique_ptr<Interpolator>> slots;
+    std::vector<uint32_t> mult;
+    Shape shape;
+    const char* err = nullptr;
+    int device = -1, sms = 0;
+    int maxItems = 0;
+    // the work list on the device, one blob: items, fallbacks, tile starts, tiles across; then the counters
+    char* dev = nullptr;
+    unsigned int* counters = nullptr;   // maxItems per-item untrusted counters + the work counter
+    size_t oFall = 0, oStart = 0, oTx = 0, blobBytes = 0;
+    char* host = nullptr;               // kRing x blobBytes, pinned
+    int ring = 0;
+
+    ~Impl() { release(); }
+    void release() {
+        DeviceGuard g(device);
+        if (dev) cudaFree(dev);
+        if (host) cudaFreeHost(host);
+        dev = nullptr;
+        host = nullptr;
+        counters = nullptr;
+    }
+    bool grow() {   // the work-list buffers for the current slots (called by add, outside any capture)
+        DeviceGuard g(device);
+        release();
+        maxItems = 0;
+        for (uint32_t v : mult) maxItems += (int)v - 1;
+        const size_t n = (size_t)std::max(maxItems, 1);
+        oFall = alignUp(n * sizeof(fgk::SynthParams), 256);
+        oStart = alignUp(oFall + n * sizeof(fgk::FallbackParams), 256);
+        oTx = alignUp(oStart + (n + 1) * 4, 256);
+        blobBytes = alignUp(oTx + n * 4, 256);
+        if (cudaMalloc(&dev, blobBytes + (n + 1) * 4) != cudaSuccess ||
+            cudaMallocHost(&host, blobBytes * kRing) != cudaSuccess) {
+            cudaGetLastError();
+            release();
+            return false;
+        }
+        counters = (unsigned int*)(dev + blobBytes);
+        return true;
+    }
+};
+
+Batch::Batch() : m(new Impl()) {}
+Batch::~Batch() { delete m; }
+const char* Batch::error() const { return m->err; }
+uint32_t Batch::slots() const { return (uint32_t)m->slots.size(); }
+uint32_t Batch::synthsOf(uint32_t i) const { return i < m->mult.size() ? m->mult[i] - 1 : 0; }
+Interpolator* Batch::slot(uint32_t i) { return i < m->slots.size() ? m->slots[i].get() : nullptr; }
+Batch::Shape Batch::shape() const { return m->shape; }
+bool Batch::setShape(const Shape& s) {
+    if (s.ctasPerSm > 4 || s.order > 1) return false;
+    m->shape = s;
+    return true;
+}
+
+int Batch::add(const InitInfo& ii, uint32_t multiplier) {
+    m->err = nullptr;
+    if (multiplier < 2 || multiplier > 8) { m->err = "the multiplier must be 2 .. 8"; return -1; }
+    int dev = ii.device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); m->err = kErrDevice; return -1; }
+    if (m->device >= 0 && dev != m->device) { m->err = "every slot of a batch must be on the batch's device"; return -1; }
+    std::unique_ptr<Interpolator> I(new Interpolator());
+    InitInfo j = ii;
+    j.device = dev;
+    if (!I->init(j)) { m->err = I->initError(); return -1; }
+    m->device = dev;
+    if (!m->sms && cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        m->err = kErrDevice;
+        return -1;
+    }
+    m->slots.push_back(std::move(I));
+    m->mult.push_back(multiplier);
+    if (!m->grow()) {
+        m->slots.pop_back();
+        m->mult.pop_back();
+        m->grow();
+        m->err = kErrAlloc;
+        return -1;
+    }
+    return (int)m->slots.size() - 1;
+}
+
+bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const Frame* outs) {
+    m->err = nullptr;
+    const int ns = (int)m->slots.size();
+    if (!ns || !prev || !curr || !outs || !m->dev) { m->err = "empty batch or missing frames"; return false; }
+    DeviceGuard g(m->device);
+    std::vector<int> first(ns);   // each slot's first output frame in outs
+    for (int i = 0, o = 0; i < ns; i++) { first[i] = o; o += (int)m->mult[i] - 1; }
+    // 1. every slot's estimate
+    for (int i = 0; i < ns; i++) {
+        Interpolator& I = *m->slots[i];
+        I.beginFrame();
+        if (!I.recordEstimate(s, prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
+    }
+    // 2. the work list of the 8-bit RGBA syntheses
+    struct Item { int slot, k, tiles; };
+    std::vector<Item> items;
+    const bool batched = m->shape.ctasPerSm > 0;
+    for (int i = 0; i < ns && batched; i++) {
+        const Interpolator::Impl* im = m->slots[i]->m;
+        if (im->fmt != Format::Rgba8) continue;
+        const int tiles = fgk::synthTilesX((int)im->W) * fgk::synthTilesY((int)im->H);
+        for (uint32_t k = 1; k < m->mult[i]; k++) items.push_back({i, (int)k, tiles});
+    }
+    if (m->shape.order == 1)
+        std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.tiles > y.tiles; });
+    const int n = (int)items.size();
+    if (n) {
+        char* blob = m->host + (size_t)m->ring * m->blobBytes;
+        m->ring = (m->ring + 1) % Impl::kRing;
+        fgk::SynthParams* sp = (fgk::SynthParams*)blob;
+        fgk::FallbackParams* fp = (fgk::FallbackParams*)(blob + m->oFall);
+        int* start = (int*)(blob + m->oStart);
+        int* tx = (int*)(blob + m->oTx);
+        size_t smem = 0;
+        int total = 0;
+        for (int j = 0; j < n; j++) {
+            const Item& it = items[j];
+            const Interpolator::Impl* im = m->slots[it.slot]->m;
+            const Frame& out = outs[first[it.slot] + it.k - 1];
+            if (!im->frameOk(out)) { m->err = "an output frame does not fit its slot"; return false; }
+            const float t = (float)it.k / (float)m->mult[it.slot];
+            sp[j] = im->synthParams(prev[it.slot], curr[it.slot], out, t, m->counters + j);
+            sp[j].emap = nullptr;
+            fp[j] = im->fallbackParams(sp[j], nullptr);
+            start[j] = total;
+            tx[j] = fgk::synthTilesX((int)im->W);
+            total += it.tiles;
+            smem = std::max(smem, fgk::synthKernelSmem((int)im->set.flowScale));
+        }
+        start[n] = total;
+        fgk::SynthBatchArgs a{};
+        a.items = (const fgk::SynthParams*)m->dev;
+        a.tileStart = (const int*)(m->dev + m->oStart);
+        a.tilesX = (const int*)(m->dev + m->oTx);
+        a.nItems = n;
+        a.total = total;
+        a.counter = m->counters + n;
+        const int occ = fgk::synthBatchCtasPerSm(smem);
+        const int grid = m->sms * std::max(1, std::min((int)m->shape.ctasPerSm, occ));
+        if (cudaMemcpyAsync(m->dev, blob, m->blobBytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemsetAsync(m->counters, 0, (size_t)(n + 1) * 4, s) != cudaSuccess ||
+            fgk::launchSynthBatch(a, std::min(grid, total), smem, s) != cudaSuccess ||
+            fgk::launchFallbackBatch((const fgk::FallbackParams*)(m->dev + m->oFall), n, s) != cudaSuccess) {
+            m->err = cudaGetErrorString(cudaGetLastError());
+            return false;
+        }
+    }
+    // 3. the other syntheses, one by one
+    for (int i = 0; i < ns; i++) {
+        Interpolator& I = *m->slots[i];
+        if (batched && I.m->fmt == Format::Rgba8) continue;
+        for (uint32_t k = 1; k < m->mult[i]; k++)
+            if (!I.recordSynth(s, prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
+                m->err = "a slot's synthesis was refused (frames?)";
+                return false;
+            }
+    }
+    return true;
+}
+
+int Batch::tune(cudaStream_t s, const Frame* prev, const Frame* curr, const Frame* outs, uint32_t reps) {
+    static const Shape cand[] = {{0, 0}, {2, 0}, {2, 1}, {3, 0}, {3, 1}};
+    DeviceGuard g(m->device);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { cudaGetLastError(); return -1; }
+    int best = -1;
+    float bestMs = 0.0f;
+    for (int c = 0; c < (int)(sizeof(cand) / sizeof(cand[0])); c++) {
+        m->shape = cand[c];
+        bool ok = record(s, prev, curr, outs) && cudaStreamSynchronize(s) == cudaSuccess;   // warm
+        ok = ok && cudaEventRecord(e0, s) == cudaSuccess;
+        for (uint32_t r = 0; ok && r < std::max(reps, 1u); r++) {
+            ok = record(s, prev, curr, outs);
+            if ((r + 1) % (Impl::kRing / 2) == 0) ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+        }
+        float ms = 0.0f;
+        ok = ok && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+             cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+        if (!ok) { cudaGetLastError(); continue; }
+        if (best < 0 || ms < bestMs) { best = c; bestMs = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best >= 0) m->shape = cand[best];
+    return best;
+}
+
 }  // namespace framegen
 
 // ================================================================================================== C ABI
@@ -816,6 +1024,9 @@ using namespace framegen;
 
 struct fg_interpolator {
     Interpolator I;
+};
+struct fg_batch {
+    Batch B;
 };
 
 static Settings fromC(const fg_settings* c) {
@@ -948,6 +1159,64 @@ int fg_set_seed_net(fg_interpolator* fg, const float* host_params, uint32_t leve
     return fg && fg->I.setSeedNet(host_params, level);
 }
 uint32_t fg_seed_net_level(const fg_interpolator* fg) { return fg ? fg->I.seedNetLevel() : UINT32_MAX; }
+
+static InitInfo fromC(const fg_init_info* c) {
+    InitInfo ii;
+    ii.width = c->width; ii.height = c->height; ii.viewFormat = c->view_format; ii.transfer = (Transfer)c->transfer;
+    ii.linearWhiteNits = c->linear_white_nits; ii.yuvMatrix = (YuvMatrix)c->yuv_matrix;
+    ii.yuvFullRange = c->yuv_full_range != 0; ii.device = c->device; ii.settings = fromC(&c->settings);
+    return ii;
+}
+fg_batch* fg_batch_create(void) { return new fg_batch(); }
+void fg_batch_destroy(fg_batch* b) { delete b; }
+int fg_batch_add(fg_batch* b, const fg_init_info* ii, uint32_t multiplier) {
+    return b && ii ? b->B.add(fromC(ii), multiplier) : -1;
+}
+const char* fg_batch_error(const fg_batch* b) { return b ? b->B.error() : "null batch"; }
+uint32_t fg_batch_slots(const fg_batch* b) { return b ? b->B.slots() : 0; }
+static std::vector<Frame> framesOf(const fg_frame* f, size_t n) {
+    std::vector<Frame> v(n);
+    for (size_t i = 0; i < n; i++) v[i] = fromC(f + i);
+    return v;
+}
+static size_t batchOuts(fg_batch* b) {
+    size_t n = 0;
+    for (uint32_t i = 0; i < b->B.slots(); i++) n += b->B.synthsOf(i);
+    return n;
+}
+int fg_batch_record(fg_batch* b, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* outs) {
+    if (!b || !prev || !curr || !outs) return 0;
+    const size_t ns = b->B.slots();
+    const std::vector<Frame> p = framesOf(prev, ns), c = framesOf(curr, ns), o = framesOf(outs, batchOuts(b));
+    return b->B.record((cudaStream_t)stream, p.data(), c.data(), o.data());
+}
+int fg_batch_tune(fg_batch* b, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* outs,
+                  uint32_t reps) {
+    if (!b || !prev || !curr || !outs) return -1;
+    const size_t ns = b->B.slots();
+    const std::vector<Frame> p = framesOf(prev, ns), c = framesOf(curr, ns), o = framesOf(outs, batchOuts(b));
+    return b->B.tune((cudaStream_t)stream, p.data(), c.data(), o.data(), reps);
+}
+void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order) {
+    if (!b) return;
+    const Batch::Shape s = b->B.shape();
+    if (ctas_per_sm) *ctas_per_sm = s.ctasPerSm;
+    if (order) *order = s.order;
+}
+int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order) {
+    Batch::Shape s;
+    s.ctasPerSm = ctas_per_sm;
+    s.order = order;
+    return b && b->B.setShape(s);
+}
+int fg_batch_trace(fg_batch* b, uint32_t slot, void* stream, void* dst) {
+    Interpolator* I = b ? b->B.slot(slot) : nullptr;
+    return I && I->recordTrace((cudaStream_t)stream, dst);
+}
+int fg_batch_trace_layout(fg_batch* b, uint32_t slot, fg_trace_layout* l) {
+    Interpolator* I = b ? b->B.slot(slot) : nullptr;
+    return I && l && I->traceLayout(*reinterpret_cast<Interpolator::TraceLayout*>(l));
+}
 const char* fg_last_error(const fg_interpolator* fg) { return fg ? fg->I.lastCudaError() : nullptr; }
 
 }  // extern "C"

@@ -97,6 +97,17 @@ SIGNATURES = {
     "fg_record_synth_noalloc": (_I, [_P, _U32, _U32, _U32, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame),
                                      ctypes.POINTER(CFrame), _P, _I, _F, ctypes.POINTER(CSettings),
                                      ctypes.POINTER(ctypes.c_char_p)]),
+    "fg_batch_create": (_P, []),
+    "fg_batch_destroy": (None, [_P]),
+    "fg_batch_add": (_I, [_P, ctypes.POINTER(CInitInfo), _U32]),
+    "fg_batch_error": (_S, [_P]),
+    "fg_batch_slots": (_U32, [_P]),
+    "fg_batch_record": (_I, [_P, _P, _P, _P, _P]),
+    "fg_batch_tune": (_I, [_P, _P, _P, _P, _P, _U32]),
+    "fg_batch_get_shape": (None, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "fg_batch_set_shape": (_I, [_P, _U32, _U32]),
+    "fg_batch_trace_layout": (_I, [_P, _U32, ctypes.POINTER(CTraceLayout)]),
+    "fg_batch_trace": (_I, [_P, _U32, _P, _P]),
     "fg_set_seed_net": (_I, [_P, _P, _U32]),
     "fg_seed_net_level": (_U32, [_P]),
     "fg_seednet_param_count": (_U32, []),
@@ -436,3 +447,62 @@ class SeedNet:
 
     def adam(self, lr, stream=None):
         self._ok(lib().fg_seednet_adam(self._h, _stream(stream), float(lr)))
+
+
+class Batch:
+    """framegen::Batch through the C ABI: many frame pairs (slots) of any sizes and formats recorded together; the
+    8-bit RGBA syntheses of all slots run in one persistent launch. Frames as for Interpolator (tuples for YUV)."""
+
+    def __init__(self):
+        self._h = lib().fg_batch_create()
+        self.mult = []
+
+    def close(self):
+        if self._h and _lib is not None:
+            _lib.fg_batch_destroy(self._h)
+        self._h = None
+
+    __del__ = close
+
+    def add(self, width, height, view_format=VK_R8G8B8A8_UNORM, multiplier=2, settings=None, device=-1, transfer=0,
+            linear_white_nits=80.0, yuv_matrix=1, yuv_full_range=False):
+        ii = CInitInfo()
+        lib().fg_default_init_info(ctypes.byref(ii))
+        ii.width, ii.height, ii.view_format, ii.device = width, height, view_format, device
+        ii.transfer, ii.linear_white_nits, ii.yuv_matrix, ii.yuv_full_range = transfer, linear_white_nits, yuv_matrix, int(yuv_full_range)
+        ii.settings = (settings or Settings()).to_c()
+        i = lib().fg_batch_add(self._h, ctypes.byref(ii), int(multiplier))
+        if i >= 0:
+            self.mult.append(int(multiplier))
+        return i
+
+    def error(self):
+        return _s(lib().fg_batch_error(self._h))
+
+    @staticmethod
+    def times(multiplier):
+        import numpy as np
+        return [float(np.float32(k) / np.float32(multiplier)) for k in range(1, multiplier)]
+
+    def _frames(self, prev, curr, outs):
+        p = (CFrame * len(prev))(*[frame_of(f) for f in prev])
+        c = (CFrame * len(curr))(*[frame_of(f) for f in curr])
+        o = (CFrame * len(outs))(*[frame_of(f) for f in outs])
+        return p, c, o
+
+    def record(self, prev, curr, outs, stream=None):
+        """prev, curr: one frame per slot; outs: every slot's multiplier - 1 output frames, slots in order"""
+        p, c, o = self._frames(prev, curr, outs)
+        return bool(lib().fg_batch_record(self._h, _stream(stream), p, c, o))
+
+    def tune(self, prev, curr, outs, reps=3, stream=None):
+        p, c, o = self._frames(prev, curr, outs)
+        return int(lib().fg_batch_tune(self._h, _stream(stream), p, c, o, int(reps)))
+
+    def shape(self):
+        a, b = ctypes.c_uint32(), ctypes.c_uint32()
+        lib().fg_batch_get_shape(self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def set_shape(self, ctas_per_sm, order):
+        return bool(lib().fg_batch_set_shape(self._h, int(ctas_per_sm), int(order)))

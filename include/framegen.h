@@ -181,8 +181,43 @@ public:
     struct Impl;
 
 private:
+    friend class Batch;
     Impl* m = nullptr;
     const char* err_ = nullptr;
+};
+
+// B200-build extension (no counterpart in the reference): many frame pairs of any sizes and formats recorded
+// together, one Interpolator per pair ("slot"). record() records every slot's estimate as recordEstimate does; the
+// syntheses of all 8-bit RGBA slots and times then run in ONE persistent launch whose CTAs take output tiles from a
+// shared work counter (mixed sizes balance across the SMs) and their whole-frame fallbacks in one more launch; slots
+// of the other formats record their syntheses one by one. A slot of multiplier m gets the generated frames at
+// t = k/m, k = 1 .. m-1 (outs: each slot's m - 1 output frames, slots in order). Records allocate nothing and can be
+// captured in a CUDA graph; their small parameter upload goes through a ring of 8 pinned buffers, so at most 8 records
+// may be in flight. tune() times the candidate launch shapes on the device (synchronising the stream) and keeps the
+// fastest. Not thread-safe, like Interpolator.
+class Batch {
+public:
+    struct Shape {
+        uint32_t ctasPerSm = 3;   // CTAs per SM of the persistent synthesis launch; 0: one launch per synthesis
+        uint32_t order = 1;       // work order: 0 the slots as added, 1 the largest syntheses first
+    };
+    Batch();
+    ~Batch();
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+    int add(const InitInfo& ii, uint32_t multiplier);   // the slot's index, or -1 (see error())
+    const char* error() const;
+    uint32_t slots() const;
+    uint32_t synthsOf(uint32_t slot) const;             // the slot's multiplier - 1
+    Interpolator* slot(uint32_t i);
+    bool record(cudaStream_t stream, const Frame* prev, const Frame* curr, const Frame* outs);
+    int tune(cudaStream_t stream, const Frame* prev, const Frame* curr, const Frame* outs, uint32_t reps = 3);
+    Shape shape() const;
+    bool setShape(const Shape& s);
+    struct Impl;
+
+private:
+    Impl* m = nullptr;
 };
 
 }  // namespace framegen

@@ -100,6 +100,26 @@ int fg_get_trace_layout(const fg_interpolator* fg, fg_trace_layout* l);         
 int fg_record_trace(fg_interpolator* fg, void* stream, void* dst);                   /* B200-build extension */
 const char* fg_last_error(const fg_interpolator* fg);   /* the last CUDA error a record met (null if none) */
 
+/* Batches -- no counterpart in the reference (B200-build extension; framegen::Batch in include/framegen.h): many
+ * frame pairs of any sizes and formats recorded together, one interpolator per slot; the 8-bit RGBA syntheses of all
+ * slots run in one persistent launch. fg_batch_add: the slot's init info and multiplier m (t = k/m, k = 1 .. m-1);
+ * returns its index or -1. fg_batch_record: prev[i], curr[i] per slot and outs = every slot's m - 1 output frames,
+ * slots in order. fg_batch_tune: times the launch shapes on these frames (synchronises the stream), keeps the
+ * fastest, returns its index (-1 on failure). */
+typedef struct fg_batch fg_batch;
+fg_batch* fg_batch_create(void);
+void fg_batch_destroy(fg_batch* b);
+int fg_batch_add(fg_batch* b, const fg_init_info* ii, uint32_t multiplier);
+const char* fg_batch_error(const fg_batch* b);
+uint32_t fg_batch_slots(const fg_batch* b);
+int fg_batch_record(fg_batch* b, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* outs);
+int fg_batch_tune(fg_batch* b, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* outs,
+                  uint32_t reps);
+void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order);
+int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order);
+int fg_batch_trace_layout(fg_batch* b, uint32_t slot, fg_trace_layout* l);   /* a slot's Interpolator::traceLayout */
+int fg_batch_trace(fg_batch* b, uint32_t slot, void* stream, void* dst);     /* a slot's Interpolator::recordTrace */
+
 /* The seed proposer -- no counterpart in the reference's V1 path (B200-build extension). A 6-layer 3x3 conv net
  * (csrc/fg_seednet.cu) reading one pyramid level's luma (prev, curr) and proposing, per 8x8 block of that level, two
  * candidate half-vectors and a confidence logit for the integer block search. Inputs are NHWC bfloat16 [B][h][w][2]

@@ -1,0 +1,163 @@
+"""framegen::Batch (fg_batch_*): many frame pairs of mixed sizes, formats and multipliers recorded together, the
+8-bit RGBA syntheses of all slots in one persistent launch. Every slot's outputs must equal, byte for byte, those of a
+standalone Interpolator on the same pair (whose parity with the oracle the other test files establish), for every
+launch shape the autotuner chooses from, after tune(), and through a CUDA graph.
+"""
+import numpy as np
+import pytest
+import torch
+
+import framegen as fg
+import oracle
+import workloads
+
+pytestmark = pytest.mark.gpu
+
+VK = {"rgba8": fg.VK_R8G8B8A8_UNORM, "rgb10": fg.VK_A2B10G10R10_UNORM, "nv12": fg.VK_R8_UNORM,
+      "p010": fg.VK_R16_UNORM}
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    import build
+    build.build()
+
+
+def convert(fmt, rgba):
+    if fmt == "rgba8":
+        return rgba
+    if fmt == "rgb10":
+        return workloads.to_rgb10(rgba)
+    return workloads.to_yuv(rgba, 8 if fmt == "nv12" else 10, "bt709")
+
+
+def dev(frame):
+    def plane(a):
+        if a.dtype == np.uint32:
+            a = a.view(np.int32)
+        elif a.dtype == np.uint16:
+            a = a.view(np.int16)
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return tuple(plane(a) for a in frame) if isinstance(frame, tuple) else plane(frame)
+
+
+def like(d):
+    return tuple(torch.zeros_like(x) for x in d) if isinstance(d, tuple) else torch.zeros_like(d)
+
+
+def host(d):
+    return tuple(x.cpu().numpy() for x in d) if isinstance(d, tuple) else d.cpu().numpy()
+
+
+def same(a, b):
+    if isinstance(a, tuple):
+        return all(np.array_equal(x, y) for x, y in zip(a, b))
+    return np.array_equal(a, b)
+
+
+def c3_slots(scale=4, n=64):
+    """config 3's structure at 1/scale resolution: sizes 1280x720 / 1920x1080 / 2560x1440 / 3840x2160 in ratio
+    8:4:2:1 (34 / 17 / 9 / 4 of 64), formats cycling Rgba8 / Rgb10 / Nv12 / P010, multipliers cycling 2 / 3 / 4"""
+    sizes = [(1280, 720)] * 34 + [(1920, 1080)] * 17 + [(2560, 1440)] * 9 + [(3840, 2160)] * 4
+    fmts = ["rgba8", "rgb10", "nv12", "p010"]
+    out = []
+    for i, (w, h) in enumerate(sizes[:n]):
+        out.append((w // scale, h // scale, fmts[i % 4], 2 + i % 3))
+    return out
+
+
+def build_case(slots, seed=0):
+    B = fg.Batch()
+    prev, curr, outs, ref = [], [], [], []
+    for i, (w, h, fmt, m) in enumerate(slots):
+        assert B.add(w, h, VK[fmt], multiplier=m) == i, B.error()
+        p, c, _ = workloads.flow_pair(w, h, seed=seed + i)
+        prev.append(dev(convert(fmt, p)))
+        curr.append(dev(convert(fmt, c)))
+        for _ in range(m - 1):
+            outs.append(like(prev[-1]))
+    # the standalone references
+    for i, (w, h, fmt, m) in enumerate(slots):
+        I = fg.Interpolator()
+        assert I.init(w, h, VK[fmt]), I.init_error()
+        I.begin_frame()
+        assert I.record_estimate(prev[i], curr[i])
+        for t in fg.Batch.times(m):
+            o = like(prev[i])
+            assert I.record_synth(prev[i], curr[i], o, t)
+            ref.append(o)
+        torch.cuda.synchronize()
+        I.close()
+    return B, prev, curr, outs, [host(r) for r in ref]
+
+
+@pytest.fixture(scope="module")
+def case():
+    return build_case(c3_slots(scale=8, n=24))
+
+
+@pytest.mark.parametrize("shape", [(0, 0), (2, 0), (2, 1), (3, 0), (3, 1)])
+def test_batch_matches_standalone(case, shape):
+    B, prev, curr, outs, ref = case
+    assert B.set_shape(*shape)
+    for o in outs:   # poison the outputs
+        for x in (o if isinstance(o, tuple) else (o,)):
+            x.fill_(7)
+    for _ in range(2):   # twice: the counters and the work list start from scratch each record
+        assert B.record(prev, curr, outs), B.error()
+        torch.cuda.synchronize()
+        bad = [j for j, (o, r) in enumerate(zip(outs, ref)) if not same(host(o), r)]
+        assert not bad, f"shape {shape}: outputs {bad} differ"
+
+
+def test_tune_then_record(case):
+    B, prev, curr, outs, ref = case
+    best = B.tune(prev, curr, outs, reps=2)
+    assert 0 <= best < 5
+    assert B.record(prev, curr, outs)
+    torch.cuda.synchronize()
+    assert all(same(host(o), r) for o, r in zip(outs, ref))
+
+
+def test_batch_graph_capture(case):
+    B, prev, curr, outs, ref = case
+    assert B.set_shape(3, 1)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        assert B.record(prev, curr, outs, stream=s)   # warm (parameter upload ring, lazy module loads)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            assert B.record(prev, curr, outs, stream=s)
+    for o in outs:
+        for x in (o if isinstance(o, tuple) else (o,)):
+            x.fill_(3)
+    g.replay()
+    torch.cuda.synchronize()
+    assert all(same(host(o), r) for o, r in zip(outs, ref))
+    del g
+
+
+def test_rgba8_slot_against_the_oracle():
+    """one batched 8-bit RGBA slot straight against the oracle (interp.py's restatement)"""
+    p, c, _ = workloads.flow_pair(320, 180, seed=99)
+    B = fg.Batch()
+    assert B.add(320, 180, fg.VK_R8G8B8A8_UNORM, multiplier=4) == 0
+    outs = [torch.zeros((180, 320, 4), dtype=torch.uint8, device="cuda") for _ in range(3)]
+    assert B.record([dev(p)], [dev(c)], outs)
+    torch.cuda.synchronize()
+    est = oracle.estimate(p, c)
+    for o, t in zip(outs, fg.Batch.times(4)):
+        ref, _ = oracle.synth(p, c, est, t)
+        assert np.array_equal(o.cpu().numpy(), ref), t
+
+
+def test_batch_refusals():
+    B = fg.Batch()
+    assert B.add(64, 48, fg.VK_R8G8B8A8_UNORM, multiplier=1) == -1 and "multiplier" in B.error()
+    assert B.add(8, 8, fg.VK_R8G8B8A8_UNORM, multiplier=2) == -1
+    assert B.add(64, 48, fg.VK_R8G8B8A8_UNORM, multiplier=2) == 0
+    x = torch.zeros((48, 64, 4), dtype=torch.uint8, device="cuda")
+    narrow = torch.zeros((48, 60, 4), dtype=torch.uint8, device="cuda")   # a pitch below the slot's 64 pixels
+    assert not B.record([x], [x], [narrow])
+    assert B.record([x], [x], [torch.zeros_like(x)])
