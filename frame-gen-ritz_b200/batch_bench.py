@@ -1,0 +1,100 @@
+"""Time the batched path on the config-3 workload: 64 frame pairs in one batch, sizes 1280x720 / 1920x1080 /
+2560x1440 / 3840x2160 in ratio 8:4:2:1 (34 / 17 / 9 / 4), formats cycling Rgba8 / Rgb10 / Nv12 / P010, multipliers
+cycling 2 / 3 / 4, content from the config-1 generator (workloads_gpu, per-pair seeds).
+
+    python frame-gen-ritz_b200/batch_bench.py [--reps 20]
+
+Each launch shape is timed as a CUDA graph of one whole-batch record (device time, CUDA events, median of --reps
+replays); tune() then picks its shape. Prints one JSON line.
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import framegen as fg  # noqa: E402
+import workloads  # noqa: E402
+import workloads_gpu  # noqa: E402
+
+VK = {"rgba8": fg.VK_R8G8B8A8_UNORM, "rgb10": fg.VK_A2B10G10R10_UNORM, "nv12": fg.VK_R8_UNORM,
+      "p010": fg.VK_R16_UNORM}
+SHAPES = [(0, 0, 1), (3, 1, 1), (0, 0, 4), (3, 1, 4), (0, 0, 8), (2, 1, 8), (3, 0, 8), (3, 1, 8)]
+
+
+def slots():
+    sizes = [(1280, 720)] * 34 + [(1920, 1080)] * 17 + [(2560, 1440)] * 9 + [(3840, 2160)] * 4
+    fmts = ["rgba8", "rgb10", "nv12", "p010"]
+    return [(w, h, fmts[i % 4], 2 + i % 3) for i, (w, h) in enumerate(sizes)]
+
+
+def to_dev(fmt, rgba):
+    if fmt == "rgba8":
+        return rgba
+    a = rgba.cpu().numpy()
+    if fmt == "rgb10":
+        return torch.from_numpy(workloads.to_rgb10(a).view(np.int32)).cuda()
+    y, c = workloads.to_yuv(a, 8 if fmt == "nv12" else 10, "bt709")
+    if fmt == "p010":
+        y, c = y.view(np.int16), c.view(np.int16)
+    return torch.from_numpy(y).cuda(), torch.from_numpy(c).cuda()
+
+
+def like(d):
+    return tuple(torch.zeros_like(x) for x in d) if isinstance(d, tuple) else torch.zeros_like(d)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    torch.cuda.set_device(0)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3 * 10 ** 6)
+    B = fg.Batch()
+    prev, curr, outs = [], [], []
+    px = 0
+    for i, (w, h, fmt, m) in enumerate(slots()):
+        assert B.add(w, h, VK[fmt], multiplier=m) == i, B.error()
+        d = workloads_gpu.flow_batch(1, w, h, gen)
+        prev.append(to_dev(fmt, d["prev"][0]))
+        curr.append(to_dev(fmt, d["curr"][0]))
+        outs += [like(prev[-1]) for _ in range(m - 1)]
+        px += w * h * (m - 1)
+    s = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {}
+    for shape in SHAPES:
+        B.set_shape(*shape)
+        with torch.cuda.stream(s):
+            assert B.record(prev, curr, outs, stream=s), B.error()
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                assert B.record(prev, curr, outs, stream=s)
+            g.replay()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(a.reps):
+                e0.record(s)
+                g.replay()
+                e1.record(s)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        res["%d_%d_%d" % shape] = round(float(np.median(ts)), 3)
+        del g
+    with torch.cuda.stream(s):
+        best = B.tune(prev, curr, outs, reps=3, stream=s)
+    print(json.dumps({"workload": "config 3: 64 pairs, 34x720p / 17x1080p / 9x1440p / 4x2160p, Rgba8 / Rgb10 / Nv12 / "
+                                  "P010, 2x / 3x / 4x", "generated_frames": len(outs), "generated_megapixels": round(px / 1e6, 1),
+                      "ms_per_batch": res, "shape_keys": "ctasPerSm_order_streams (ctasPerSm 0: one launch per synthesis)",
+                      "tuned_shape": "%d_%d_%d" % SHAPES[best] if best >= 0 else None}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -838,8 +838,30 @@ struct Batch::Impl {
     size_t oFall = 0, oStart = 0, oTx = 0, blobBytes = 0;
     char* host = nullptr;               // kRing x blobBytes, pinned
     int ring = 0;
+    // the fork / join pool of the slots' estimates
+    static constexpr int kMaxStreams = 8;
+    cudaStream_t pool[kMaxStreams] = {};
+    cudaEvent_t fork = nullptr, join[kMaxStreams] = {};
 
-    ~Impl() { release(); }
+    ~Impl() {
+        release();
+        DeviceGuard g(device);
+        for (int i = 0; i < kMaxStreams; i++) {
+            if (pool[i]) cudaStreamDestroy(pool[i]);
+            if (join[i]) cudaEventDestroy(join[i]);
+        }
+        if (fork) cudaEventDestroy(fork);
+    }
+    bool makePool() {
+        if (fork) return true;
+        DeviceGuard g(device);
+        bool ok = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess;
+        for (int i = 0; ok && i < kMaxStreams; i++)
+            ok = cudaStreamCreateWithFlags(&pool[i], cudaStreamNonBlocking) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+        return ok;
+    }
     void release() {
         DeviceGuard g(device);
         if (dev) cudaFree(dev);
@@ -877,7 +899,7 @@ uint32_t Batch::synthsOf(uint32_t i) const { return i < m->mult.size() ? m->mult
 Interpolator* Batch::slot(uint32_t i) { return i < m->slots.size() ? m->slots[i].get() : nullptr; }
 Batch::Shape Batch::shape() const { return m->shape; }
 bool Batch::setShape(const Shape& s) {
-    if (s.ctasPerSm > 4 || s.order > 1) return false;
+    if (s.ctasPerSm > 4 || s.order > 1 || s.streams < 1 || s.streams > (uint32_t)Impl::kMaxStreams) return false;
     m->shape = s;
     return true;
 }
@@ -900,7 +922,7 @@ int Batch::add(const InitInfo& ii, uint32_t multiplier) {
     }
     m->slots.push_back(std::move(I));
     m->mult.push_back(multiplier);
-    if (!m->grow()) {
+    if (!m->makePool() || !m->grow()) {
         m->slots.pop_back();
         m->mult.pop_back();
         m->grow();
@@ -917,16 +939,39 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
     DeviceGuard g(m->device);
     std::vector<int> first(ns);   // each slot's first output frame in outs
     for (int i = 0, o = 0; i < ns; i++) { first[i] = o; o += (int)m->mult[i] - 1; }
-    // 1. every slot's estimate
+    const bool batched = m->shape.ctasPerSm > 0;
+    // 1. every slot's estimate (and, for the slots outside the persistent launch, its syntheses), forked over the
+    //    pool: slot i on stream i % streams, joined back into s before the persistent launch
+    const int nst = (int)std::min<uint32_t>(m->shape.streams, (uint32_t)Impl::kMaxStreams);
+    auto streamOf = [&](int i) { return nst > 1 ? m->pool[i % nst] : s; };
+    if (nst > 1) {
+        if (cudaEventRecord(m->fork, s) != cudaSuccess) { m->err = cudaGetErrorString(cudaGetLastError()); return false; }
+        for (int k = 0; k < nst; k++)
+            if (cudaStreamWaitEvent(m->pool[k], m->fork, 0) != cudaSuccess) {
+                m->err = cudaGetErrorString(cudaGetLastError());
+                return false;
+            }
+    }
     for (int i = 0; i < ns; i++) {
         Interpolator& I = *m->slots[i];
         I.beginFrame();
-        if (!I.recordEstimate(s, prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
+        if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
+        if (batched && I.m->fmt == Format::Rgba8) continue;
+        for (uint32_t k = 1; k < m->mult[i]; k++)
+            if (!I.recordSynth(streamOf(i), prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
+                m->err = "a slot's synthesis was refused (frames?)";
+                return false;
+            }
     }
+    if (nst > 1)
+        for (int k = 0; k < nst; k++)
+            if (cudaEventRecord(m->join[k], m->pool[k]) != cudaSuccess || cudaStreamWaitEvent(s, m->join[k], 0) != cudaSuccess) {
+                m->err = cudaGetErrorString(cudaGetLastError());
+                return false;
+            }
     // 2. the work list of the 8-bit RGBA syntheses
     struct Item { int slot, k, tiles; };
     std::vector<Item> items;
-    const bool batched = m->shape.ctasPerSm > 0;
     for (int i = 0; i < ns && batched; i++) {
         const Interpolator::Impl* im = m->slots[i]->m;
         if (im->fmt != Format::Rgba8) continue;
@@ -977,21 +1022,11 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
             return false;
         }
     }
-    // 3. the other syntheses, one by one
-    for (int i = 0; i < ns; i++) {
-        Interpolator& I = *m->slots[i];
-        if (batched && I.m->fmt == Format::Rgba8) continue;
-        for (uint32_t k = 1; k < m->mult[i]; k++)
-            if (!I.recordSynth(s, prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
-                m->err = "a slot's synthesis was refused (frames?)";
-                return false;
-            }
-    }
     return true;
 }
 
 int Batch::tune(cudaStream_t s, const Frame* prev, const Frame* curr, const Frame* outs, uint32_t reps) {
-    static const Shape cand[] = {{0, 0}, {2, 0}, {2, 1}, {3, 0}, {3, 1}};
+    static const Shape cand[] = {{0, 0, 1}, {3, 1, 1}, {0, 0, 4}, {3, 1, 4}, {0, 0, 8}, {2, 1, 8}, {3, 0, 8}, {3, 1, 8}};
     DeviceGuard g(m->device);
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { cudaGetLastError(); return -1; }
@@ -1197,16 +1232,18 @@ int fg_batch_tune(fg_batch* b, void* stream, const fg_frame* prev, const fg_fram
     const std::vector<Frame> p = framesOf(prev, ns), c = framesOf(curr, ns), o = framesOf(outs, batchOuts(b));
     return b->B.tune((cudaStream_t)stream, p.data(), c.data(), o.data(), reps);
 }
-void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order) {
+void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order, uint32_t* streams) {
     if (!b) return;
     const Batch::Shape s = b->B.shape();
     if (ctas_per_sm) *ctas_per_sm = s.ctasPerSm;
     if (order) *order = s.order;
+    if (streams) *streams = s.streams;
 }
-int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order) {
+int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order, uint32_t streams) {
     Batch::Shape s;
     s.ctasPerSm = ctas_per_sm;
     s.order = order;
+    s.streams = streams;
     return b && b->B.setShape(s);
 }
 int fg_batch_trace(fg_batch* b, uint32_t slot, void* stream, void* dst) {

@@ -190,7 +190,8 @@ private:
 // together, one Interpolator per pair ("slot"). record() records every slot's estimate as recordEstimate does; the
 // syntheses of all 8-bit RGBA slots and times then run in ONE persistent launch whose CTAs take output tiles from a
 // shared work counter (mixed sizes balance across the SMs) and their whole-frame fallbacks in one more launch; slots
-// of the other formats record their syntheses one by one. A slot of multiplier m gets the generated frames at
+// of the other formats record their syntheses one by one. The slots' estimate chains (small, launch-latency bound
+// passes) are forked onto a pool of streams (events join them back), so independent slots overlap on the GPU. A slot of multiplier m gets the generated frames at
 // t = k/m, k = 1 .. m-1 (outs: each slot's m - 1 output frames, slots in order). Records allocate nothing and can be
 // captured in a CUDA graph; their small parameter upload goes through a ring of 8 pinned buffers, so at most 8 records
 // may be in flight. tune() times the candidate launch shapes on the device (synchronising the stream) and keeps the
@@ -200,6 +201,7 @@ public:
     struct Shape {
         uint32_t ctasPerSm = 3;   // CTAs per SM of the persistent synthesis launch; 0: one launch per synthesis
         uint32_t order = 1;       // work order: 0 the slots as added, 1 the largest syntheses first
+        uint32_t streams = 8;     // the slots' estimates run on this many forked streams (1 = the caller's only)
     };
     Batch();
     ~Batch();

@@ -115,8 +115,8 @@ uint32_t fg_batch_slots(const fg_batch* b);
 int fg_batch_record(fg_batch* b, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* outs);
 int fg_batch_tune(fg_batch* b, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* outs,
                   uint32_t reps);
-void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order);
-int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order);
+void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order, uint32_t* streams);
+int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order, uint32_t streams);
 int fg_batch_trace_layout(fg_batch* b, uint32_t slot, fg_trace_layout* l);   /* a slot's Interpolator::traceLayout */
 int fg_batch_trace(fg_batch* b, uint32_t slot, void* stream, void* dst);     /* a slot's Interpolator::recordTrace */
 
