@@ -147,7 +147,6 @@ def ncu_traffic():
 
 
 def run_reference(a):
-    import torch.distributed as dist
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -184,6 +183,7 @@ def seed_net_arm(a, fg, pool, outs, stream, world, plain):
     of the config-1 generator (ground truth at t = 1/4, 1/2, 3/4)."""
     import torch
     import torch.distributed as dist
+    import replicas
     import workloads_gpu
     params = np.fromfile(a.seed_net, np.float32)
     I = fg.Interpolator()
@@ -211,11 +211,7 @@ def seed_net_arm(a, fg, pool, outs, stream, world, plain):
             graphs[i % a.pool].replay()
         ev1.record(stream)
     torch.cuda.synchronize()
-    t_ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
     del graphs
     gen = torch.Generator(device="cuda")
     gen.manual_seed(424242)
@@ -259,6 +255,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
                                 device_id=torch.device("cuda", local))
     import framegen as fg
+    import replicas
 
     p_np, c_np = workload_pair()
     base_a = torch.from_numpy(p_np).cuda()
@@ -329,11 +326,7 @@ def main():
     if world > 1:
         dist.barrier()
     clocks = clock_summary(clk)
-    t_ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
     ms_per_step = t_ms / a.steps
     value = t_ms / (a.steps * world)
 
@@ -403,11 +396,7 @@ def main():
         e2e_step()
     ev1.record(s_out)
     torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
     e2e_value = e2e_ms / (a.e2e_steps * world)
     if rank == 0:   # the downloaded frames are the pair's (pool pair 0 is the unshifted pair on rank 0)
         last = (step_no[0] - 1) % 2

@@ -3,9 +3,12 @@
 cycling 2 / 3 / 4, content from the config-1 generator (workloads_gpu, per-pair seeds).
 
     python frame-gen-ritz_b200/batch_bench.py [--reps 20]
+    torchrun --nproc-per-node N --master-addr 127.0.0.1 frame-gen-ritz_b200/batch_bench.py
 
 Each launch shape is timed as a CUDA graph of one whole-batch record (device time, CUDA events, median of --reps
-replays); tune() then picks its shape. Prints one JSON line.
+replays); tune() then picks its shape. Prints one JSON line. Under torchrun the 64 pairs are partitioned over the ranks
+by cost (replicas.shard_by_cost: the pixels each pair moves), each rank records its share as one batch on its GPU,
+and a shape's time is the slowest rank's (no collective on the data path).
 """
 import argparse
 import json
@@ -19,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 import framegen as fg  # noqa: E402
+import replicas  # noqa: E402
 import workloads  # noqa: E402
 import workloads_gpu  # noqa: E402
 
@@ -53,14 +57,24 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reps", type=int, default=20)
     a = ap.parse_args()
-    torch.cuda.set_device(0)
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(3 * 10 ** 6)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    rank, n = replicas.world()
+    all_slots = slots()
+    mine = replicas.shard_by_cost([replicas.pair_cost(w, h, m) for w, h, _, m in all_slots], n)[rank]
     B = fg.Batch()
     prev, curr, outs = [], [], []
     px = 0
-    for i, (w, h, fmt, m) in enumerate(slots()):
-        assert B.add(w, h, VK[fmt], multiplier=m) == i, B.error()
+    for j, i in enumerate(mine):
+        w, h, fmt, m = all_slots[i]
+        assert B.add(w, h, VK[fmt], multiplier=m) == j, B.error()
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(3 * 10 ** 6 + i)   # the pair's content does not depend on the partition
         d = workloads_gpu.flow_batch(1, w, h, gen)
         prev.append(to_dev(fmt, d["prev"][0]))
         curr.append(to_dev(fmt, d["curr"][0]))
@@ -86,14 +100,23 @@ def main():
                 e1.record(s)
                 torch.cuda.synchronize()
                 ts.append(e0.elapsed_time(e1))
-        res["%d_%d_%d" % shape] = round(float(np.median(ts)), 3)
+        res["%d_%d_%d" % shape] = round(replicas.max_over_ranks(float(np.median(ts)), device="cuda"), 3)
         del g
     with torch.cuda.stream(s):
         best = B.tune(prev, curr, outs, reps=3, stream=s)
-    print(json.dumps({"workload": "config 3: 64 pairs, 34x720p / 17x1080p / 9x1440p / 4x2160p, Rgba8 / Rgb10 / Nv12 / "
-                                  "P010, 2x / 3x / 4x", "generated_frames": len(outs), "generated_megapixels": round(px / 1e6, 1),
-                      "ms_per_batch": res, "shape_keys": "ctasPerSm_order_streams (ctasPerSm 0: one launch per synthesis)",
-                      "tuned_shape": "%d_%d_%d" % SHAPES[best] if best >= 0 else None}), flush=True)
+    frames = len(outs)
+    if n > 1:   # totals over the ranks
+        import torch.distributed as dist
+        t = torch.tensor([len(outs), px], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        frames, px = int(t[0]), int(t[1])
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"workload": "config 3: 64 pairs, 34x720p / 17x1080p / 9x1440p / 4x2160p, Rgba8 / Rgb10 / "
+                                      "Nv12 / P010, 2x / 3x / 4x", "ranks": n, "generated_frames": frames,
+                          "generated_megapixels": round(px / 1e6, 1), "ms_per_batch": res,
+                          "shape_keys": "ctasPerSm_order_streams (ctasPerSm 0: one launch per synthesis)",
+                          "tuned_shape_rank0": "%d_%d_%d" % SHAPES[best] if best >= 0 else None}), flush=True)
 
 
 if __name__ == "__main__":

@@ -271,11 +271,12 @@ __global__ void __launch_bounds__(256) k_sn_loss(const float* __restrict__ out, 
     if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l * scale);
 }
 
-// Adam on the float32 master parameters; refreshes their bfloat16 copy (the forward's weights) and zeroes the gradient
+// Adam on the float32 master parameters; refreshes their bfloat16 copy (the forward's weights) and zeroes the gradient.
+// The gradient is scaled by gscale as it is read (data-parallel training: the ranks' sum times 1 / ranks).
 __global__ void __launch_bounds__(256) k_sn_adam(const SnAdamArgs a) {
     const int i = blockIdx.x * 256 + threadIdx.x;
     if (i >= a.n) return;
-    const float g = a.grad[i];
+    const float g = a.grad[i] * a.gscale;
     const float m = a.b1 * a.m[i] + (1.0f - a.b1) * g;
     const float v = a.b2 * a.v[i] + (1.0f - a.b2) * g * g;
     a.m[i] = m;

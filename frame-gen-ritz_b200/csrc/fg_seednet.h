@@ -45,6 +45,7 @@ struct SnAdamArgs {
     void* wb;                                    // bf16 copy of p (the forward's weights)
     int n;
     float lr, b1, b2, eps, c1, c2;               // c1 = 1 / (1 - b1^t), c2 = 1 / (1 - b2^t)
+    float gscale;                                // the gradient is read as grad * gscale (1 / ranks after a sum)
 };
 
 cudaError_t launchSnPack(const float* la, const float* lc, int n, void* x, cudaStream_t s);

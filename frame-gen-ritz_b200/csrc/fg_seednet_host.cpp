@@ -259,13 +259,17 @@ int fg_seednet_zero_grads(fg_seednet* n, void* stream) {
     return n->ok(cudaMemsetAsync(n->grad, 0, (size_t)kSnParams * 4, (cudaStream_t)stream));
 }
 
-int fg_seednet_adam(fg_seednet* n, void* stream, float lr) {
+float* fg_seednet_grad_buffer(fg_seednet* n) { return n ? n->grad : nullptr; }
+
+int fg_seednet_adam(fg_seednet* n, void* stream, float lr) { return fg_seednet_adam_scaled(n, stream, lr, 1.0f); }
+
+int fg_seednet_adam_scaled(fg_seednet* n, void* stream, float lr, float grad_scale) {
     if (!n) return 0;
     DevScope g(n->device);
     n->step++;
     SnAdamArgs a{};
     a.p = n->p; a.m = n->m; a.v = n->v; a.grad = n->grad; a.wb = n->wb; a.n = kSnParams;
-    a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f;
+    a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f; a.gscale = grad_scale;
     a.c1 = (float)(1.0 / (1.0 - std::pow(0.9, n->step)));
     a.c2 = (float)(1.0 / (1.0 - std::pow(0.999, n->step)));
     return n->ok(launchSnAdam(a, (cudaStream_t)stream));

@@ -123,6 +123,8 @@ SIGNATURES = {
     "fg_seednet_backward": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
     "fg_seednet_zero_grads": (_I, [_P, _P]),
     "fg_seednet_adam": (_I, [_P, _P, _F]),
+    "fg_seednet_adam_scaled": (_I, [_P, _P, _F, _F]),
+    "fg_seednet_grad_buffer": (_P, [_P]),
 }
 
 _lib = None
@@ -445,8 +447,25 @@ class SeedNet:
     def zero_grads(self, stream=None):
         self._ok(lib().fg_seednet_zero_grads(self._h, _stream(stream)))
 
-    def adam(self, lr, stream=None):
-        self._ok(lib().fg_seednet_adam(self._h, _stream(stream), float(lr)))
+    def adam(self, lr, grad_scale=1.0, stream=None):
+        """one Adam step on the gradient times grad_scale (1 / ranks after a data-parallel all-reduce sum)"""
+        if grad_scale == 1.0:
+            self._ok(lib().fg_seednet_adam(self._h, _stream(stream), float(lr)))
+        else:
+            self._ok(lib().fg_seednet_adam_scaled(self._h, _stream(stream), float(lr), float(grad_scale)))
+
+    def grad_buffer(self):
+        """the float32 gradient accumulator as a CUDA tensor view (no copy; valid while the net lives), for an
+        in-place all-reduce between backward() and adam()"""
+        import torch
+        ptr = lib().fg_seednet_grad_buffer(self._h)
+        if not ptr:
+            raise RuntimeError("fg_seednet_grad_buffer failed")
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (self.n_params,), "typestr": "<f4", "data": (ptr, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_View(), device=torch.device("cuda", torch.cuda.current_device()))
 
 
 class Batch:

@@ -1,6 +1,12 @@
 """Train the seed proposer (csrc/fg_seednet.cu) on the GPU with the library's own kernels.
 
     python frame-gen-ritz_b200/seednet_train.py [--steps 3125] [--batch 64] [--lr 1e-3] [--out seednet_l1.bin]
+    torchrun --nproc-per-node N --master-addr 127.0.0.1 frame-gen-ritz_b200/seednet_train.py --batch 64 ...
+
+Data-parallel under torchrun (one process per GPU, NCCL): every rank draws its own crops (--batch per rank, a global
+batch of N x --batch), the ranks' gradients are summed by one all-reduce of the 39,912 float32 values per step,
+in place in the net's gradient buffer, and the Adam step reads them times 1 / N (the mean gradient of the global
+batch); the ranks start from the same parameters and so stay identical. Rank 0 logs and writes the parameters.
 
 Data: 256x256 crops from the config-1 flow generator (workloads_gpu.flow_batch: smooth motion up to 24 px, 5 % scene
 cuts, 5 % fresh content), 3125 steps x 64 crops = 200k crops, each crop new. Input: the crop pair's level-1 luma
@@ -26,6 +32,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 import framegen as fg  # noqa: E402
+import replicas  # noqa: E402
 import workloads_gpu  # noqa: E402
 
 CROP = 256
@@ -93,11 +100,19 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "seednet_l1.bin"))
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
-    torch.cuda.set_device(0)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    sync = replicas.GradSync()
     gen = torch.Generator(device="cuda")
-    gen.manual_seed(a.seed)
-    net = fg.SeedNet(a.batch, CROP // 4, CROP // 4)
+    gen.manual_seed(sync.rank_seed(a.seed))
+    net = fg.SeedNet(a.batch, CROP // 4, CROP // 4, device=local)
     net.set_params(init_params(a.seed))
+    grad = net.grad_buffer()
     lab = Labeller(a.batch)
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
     hist, t0 = [], time.time()
@@ -106,18 +121,29 @@ def main():
         la, lc, v1 = lab(d["prev"], d["curr"])
         x = fg.SeedNet.pack(la.contiguous(), lc.contiguous())
         net.backward(x, targets(d["v"], d["kind"], v1), loss)
-        net.adam(a.lr)
+        sync(grad)
+        net.adam(a.lr, grad_scale=sync.scale())
         if step % 100 == 0 or step == a.steps - 1:
             torch.cuda.synchronize()
             hist.append((step, float(loss)))
-            print(f"step {step} loss {float(loss):.4f} ({time.time() - t0:.1f} s)", flush=True)
+            if sync.rank == 0:
+                print(f"step {step} loss {float(loss):.4f} ({time.time() - t0:.1f} s)", flush=True)
     p = net.params()
-    p.tofile(a.out)
-    if a.log:
-        with open(a.log, "w") as f:
-            json.dump({"steps": a.steps, "batch": a.batch, "lr": a.lr, "crops": a.steps * a.batch,
-                       "seconds": round(time.time() - t0, 1), "loss": hist}, f)
-    print("wrote", a.out)
+    if sync.n > 1:   # the ranks took identical steps: their parameters agree bit for bit
+        import torch.distributed as dist
+        lo, hi = torch.from_numpy(p).cuda(), torch.from_numpy(p).cuda()
+        dist.all_reduce(lo, op=dist.ReduceOp.MIN)
+        dist.all_reduce(hi, op=dist.ReduceOp.MAX)
+        assert torch.equal(lo, hi), "ranks' parameters diverged"
+        dist.destroy_process_group()
+    if sync.rank == 0:
+        p.tofile(a.out)
+        if a.log:
+            with open(a.log, "w") as f:
+                json.dump({"steps": a.steps, "batch": a.batch * sync.n, "ranks": sync.n, "lr": a.lr,
+                           "crops": a.steps * a.batch * sync.n, "seconds": round(time.time() - t0, 1),
+                           "loss": hist}, f)
+        print("wrote", a.out)
 
 
 if __name__ == "__main__":

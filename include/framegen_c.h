@@ -148,6 +148,11 @@ int fg_seednet_backward(fg_seednet* net, void* stream, const void* x, int batch,
                         float* loss);
 int fg_seednet_zero_grads(fg_seednet* net, void* stream);
 int fg_seednet_adam(fg_seednet* net, void* stream, float lr);          /* one Adam step (0.9, 0.999, 1e-8); zeroes grads */
+/* Data-parallel training: the float32 gradient accumulator on the net's device (fg_seednet_param_count() values, valid
+ * until destroy), for an in-place all-reduce (sum) between backward and the step; the step then reads it scaled by
+ * grad_scale (1 / ranks), which gives every rank the update of the whole global batch. */
+float* fg_seednet_grad_buffer(fg_seednet* net);
+int fg_seednet_adam_scaled(fg_seednet* net, void* stream, float lr, float grad_scale);
 
 /* fg_record_synth_noalloc -- no counterpart in the reference. The synthesis of one generated frame (what
  * fg_record_synth records after an estimate) for hosts that cannot allocate device memory when they generate frames:

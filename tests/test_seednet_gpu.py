@@ -121,6 +121,32 @@ def test_adam_step():
     net.close()
 
 
+def test_grad_buffer_and_scaled_step():
+    """the data-parallel hooks: grad_buffer() is the accumulator itself (a write through it is what the step reads),
+    and adam(grad_scale=s) on a summed gradient equals adam() on the gradient times s, bit for bit when s is a power
+    of two (two ranks: sum / 2 is the mean)"""
+    la, lc = level1_lumas(2, seed=21)
+    p = params(8)
+    tgt = targets(2, 8, 8, 9)
+    x = fg.SeedNet.pack(torch.from_numpy(la).cuda(), torch.from_numpy(lc).cuda())
+    a, b = fg.SeedNet(2, 64, 64), fg.SeedNet(2, 64, 64)
+    for net in (a, b):
+        net.set_params(p)
+        net.backward(x, torch.from_numpy(tgt).cuda())
+    torch.cuda.synchronize()
+    ga, gb = a.grad_buffer(), b.grad_buffer()
+    assert ga.dtype == torch.float32 and ga.numel() == ref.N_PARAMS
+    assert np.array_equal(ga.cpu().numpy(), a.grads())
+    ga.mul_(2.0)                        # what an all-reduce sum of two equal ranks leaves
+    a.adam(1e-3, grad_scale=0.5)
+    b.adam(1e-3)
+    torch.cuda.synchronize()
+    assert np.array_equal(a.params(), b.params())
+    assert not ga.any() and not gb.any(), "the step zeroes the buffer"
+    a.close()
+    b.close()
+
+
 def test_training_lowers_the_loss():
     """200 Adam steps on one fixed batch: the loss falls well below its start (the kernels train the net)"""
     la, lc = level1_lumas(8, seed=30)
