@@ -54,6 +54,7 @@ def args():
     ap.add_argument("--seed-level", type=int, default=1)
     ap.add_argument("--no-seed-net", action="store_true")
     ap.add_argument("--psnr-pairs", type=int, default=8, help="held-out 4K pairs of the CNN-vs-plain PSNR check")
+    ap.add_argument("--blur-samples", type=int, default=4, help="sub-frames of the motion-blur line (0: no line)")
     return ap.parse_args()
 
 
@@ -240,6 +241,55 @@ def seed_net_arm(a, fg, pool, outs, stream, world, plain):
             "data": "held-out config-1 pairs (workloads_gpu, seed 424242), 4K, ground truth at t = 1/4, 1/2, 3/4"}
 
 
+def blur_arm(a, fg, pool, stream, world):
+    """recordSynthBlur at 4K: one Gaussian-weighted output over [0.25, 0.75] from --blur-samples sub-frames, against
+    the same sub-frames as separate recordSynth outputs (the unfused way, before any blend of them). Both timed as CUDA
+    graphs behind the pair's estimate, cycling the pool; their cost = that graph minus the estimate-only graph."""
+    import torch
+    import replicas
+    n = a.blur_samples
+    fs = fg.Settings()
+    fs.blurSamples, fs.blurWeights = n, 1
+    I = fg.Interpolator()
+    assert I.init(W4K, H4K, fg.VK_R8G8B8A8_UNORM, settings=fs, device=torch.cuda.current_device()), I.init_error()
+    times, _ = fg.blur_plan(n, 1, 0.25, 0.75)
+    o = torch.empty_like(pool[0][0])
+
+    def graph(k, what):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            I.begin_frame()
+            assert I.record_estimate(pool[k][0], pool[k][1], stream=stream)
+            if what == "blur":
+                assert I.record_synth_blur(pool[k][0], pool[k][1], o, 0.25, 0.75, stream=stream)
+            elif what == "synths":
+                for t in times.tolist():
+                    assert I.record_synth(pool[k][0], pool[k][1], o, t, stream=stream)
+        return g
+
+    res = {}
+    for what in ("estimate", "blur", "synths"):
+        gs = [graph(k, what) for k in range(a.pool)]
+        with torch.cuda.stream(stream):
+            for i in range(max(a.warmup, 3)):
+                gs[i % a.pool].replay()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for i in range(a.steps):
+                gs[i % a.pool].replay()
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        res[what] = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda") / a.steps
+        del gs
+    I.close()
+    return {"samples": n, "weights": "gaussian", "window": [0.25, 0.75],
+            "blur_ms": round(res["blur"] - res["estimate"], 4),
+            "separate_synths_ms": round(res["synths"] - res["estimate"], 4),
+            "method": "graph replay over the pool, minus the estimate-only graph; 3840x2160 Rgba8"}
+
+
 def main():
     a = args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -402,6 +452,7 @@ def main():
         last = (step_no[0] - 1) % 2
         assert all(torch.equal(h, e.cpu()) for h, e in zip(hout[last], eager0)), "e2e output differs"
 
+    blur = blur_arm(a, fg, pool, stream, world) if a.blur_samples >= 2 else None
     seed = None
     if not a.no_seed_net and os.path.exists(a.seed_net):
         seed = seed_net_arm(a, fg, pool, outs, stream, world, I)
@@ -435,7 +486,7 @@ def main():
                 "gpu_launches": launches_per_step * a.steps,
                 "e2e": {"value": round(e2e_value, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 4 * W4K * H4K,
                         "d2h_bytes_per_step": len(TS) * 4 * W4K * H4K},
-                "cpu_baseline": cpu, "clocks": clocks, "seed_net": seed}
+                "cpu_baseline": cpu, "clocks": clocks, "seed_net": seed, "motion_blur": blur}
         print(json.dumps(line), flush=True)
     I.close()
     if world > 1:

@@ -873,8 +873,13 @@ __device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, u
     return c2 * 65536u + (c1 * 256u + c0);
 }
 
-// one output tile (bx, by) of one synthesis; all threads of the CTA take part (the cut path returns at once)
-__device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) {
+// one output tile (bx, by) of one synthesis; all threads of the CTA take part. Each output pixel goes to
+// sink(k, x, y, ly, o): k = this thread's region-row slot, (x, y) the pixel, ly its tile row, o the packed result
+// (alpha = the nearer frame's). The untrusted count is added to *p.untrusted unless that is null. kCut: under a scene
+// cut the tile is a copy of the nearer frame to p.out (and the core returns at once); without kCut the caller has
+// taken the cut into account.
+template <bool kCut, class Sink>
+__device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int by, Sink&& sink) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ SyCoef rowc[kSyEH];
     __shared__ float TA[256], TC[256];
@@ -886,7 +891,7 @@ __device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) 
     const uint32_t pitch = (uint32_t)p.pitch, pw = pitch >> 2;
     const uint32_t* fa32 = reinterpret_cast<const uint32_t*>(p.a);
     const uint32_t* fc32 = reinterpret_cast<const uint32_t*>(p.c);
-    if (p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
+    if (kCut && p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
         for (int i = tid; i < kSyT * kSyTH; i += kSyThreads) {
             const int x = X0 + (i % kSyT), y = Y0 + (i / kSyT);
             if (x < p.W && y < p.H)
@@ -992,18 +997,112 @@ __device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) 
                 }
             }
             o = (o & 0x00FFFFFFu) | (nq & 0xFF000000u);   // alpha (byte 3 in both pixel orders): the nearer frame's
-            reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = o;
+            sink(k, x, y, ly, o);
             if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyE + ex];
         }
     }
     if (myCnt) atomicAdd(&cnt, myCnt);
     __syncthreads();
-    if (tid == 0 && cnt) atomicAdd(p.untrusted, cnt);
+    if (tid == 0 && cnt && p.untrusted) atomicAdd(p.untrusted, cnt);
+}
+
+// one output tile of one synthesis, stored to p.out
+__device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) {
+    synthTileCore<true>(p, bx, by, [&](int, int x, int y, int, uint32_t o) {
+        reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = o;
+    });
 }
 
 __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
     pdlEnter();
     synthTile(p, blockIdx.x, blockIdx.y);
+}
+
+// Motion blur (gpu/framegen.h:553-573, gpu/shaders/blur_resolve.comp): out = round(sum_k w_k frame_k), frame_k the
+// 8-bit frame recordSynth(t_k) gives (the nearer real frame under a scene cut or a whole-frame flick; prev / curr at
+// t_k <= 0 / >= 1). One CTA per output tile runs the synthesis of every sample on the tile and accumulates it in
+// registers (no sub-frame is written): per pixel and colour channel acc = sum q_k v_k, the weights q_k integers
+// summing to 2^16; out = (acc + 2^15) >> 16. Alpha is the nearer frame's in every sub-frame, so it is the weighted
+// mean of prev's and curr's alpha. A flick (more than globalFallback of a sample's pixels untrusted) is known only
+// when every tile has counted: the main pass (fix = 0) assumes none and counts per sample; the fix-up pass (fix = 1)
+// exits at once unless some synthesized sample flicked, and then redoes every tile with those samples replaced.
+__global__ void __launch_bounds__(kSyThreads, 2) k_synth_blur(const BlurParams bp) {
+    pdlEnter();
+    __shared__ __align__(16) SynthParams sp;
+    __shared__ unsigned int sRepl, sRedo;   // samples replaced by a real frame; whether this pass has work
+    __shared__ uint32_t sWp, sWc, sWap;     // weights of the replaced samples taking prev / curr; alpha weight of prev
+    const int tid = threadIdx.x, ex = tid & (kSyE - 1), ey0 = tid / kSyE;
+    const SynthParams& b = bp.base;
+    if (tid == 0) {
+        const bool cut = b.st->cut != 0;
+        unsigned int repl = 0, flick = 0;
+        uint32_t wp = 0, wc = 0, wap = 0;
+        for (int k = 0; k < bp.n; k++) {
+            const BlurSample& m = bp.smp[k];
+            const bool nearC = m.mode == 2 || (m.mode == 0 && m.nearC);
+            bool r = m.mode != 0 || cut;
+            if (!r && bp.fix && (double)bp.cnt[k] / ((double)b.W * (double)b.H) > bp.frac) {
+                r = true;
+                flick |= 1u << k;
+            }
+            if (r) {
+                repl |= 1u << k;
+                if (nearC) wc += m.q; else wp += m.q;
+            }
+            if (!nearC) wap += m.q;
+        }
+        sRepl = repl;
+        sRedo = !bp.fix || flick != 0;
+        sWp = wp; sWc = wc; sWap = wap;
+    }
+    __syncthreads();
+    if (!sRedo) return;
+    const unsigned int repl = sRepl;
+    uint32_t acc[kSyK][3];
+#pragma unroll
+    for (int k = 0; k < kSyK; k++) acc[k][0] = acc[k][1] = acc[k][2] = 0u;
+    for (int j = 0; j < bp.n; j++) {
+        if ((repl >> j) & 1u) continue;   // uniform over the CTA
+        static_assert(sizeof(SynthParams) % 4 == 0, "SynthParams copies as words");
+        for (int i = tid; i < (int)(sizeof(SynthParams) / 4); i += kSyThreads)
+            reinterpret_cast<uint32_t*>(&sp)[i] = reinterpret_cast<const uint32_t*>(&b)[i];
+        __syncthreads();
+        if (tid == 0) {
+            const BlurSample& m = bp.smp[j];
+            sp.lookup = m.lookup; sp.mid = m.mid; sp.nearC = m.nearC;
+            sp.s = m.s; sp.ka = m.ka; sp.kc = m.kc; sp.wA = m.wA; sp.wC = m.wC;
+            sp.untrusted = bp.fix ? nullptr : bp.cnt + j;
+            sp.emap = nullptr;
+        }
+        __syncthreads();
+        const uint32_t q = bp.smp[j].q;
+        synthTileCore<false>(sp, blockIdx.x, blockIdx.y, [&](int k, int, int, int, uint32_t o) {
+            acc[k][0] += q * (o & 255u);
+            acc[k][1] += q * ((o >> 8) & 255u);
+            acc[k][2] += q * ((o >> 16) & 255u);
+        });
+        __syncthreads();   // the tile's shared memory and sp are free again
+    }
+    // the output: the synthesized samples' sums plus the replaced samples' real pixels, rounded once
+    const uint32_t wp = sWp, wc = sWc, wap = sWap, wac = 65536u - wap;
+    const uint32_t pitch = (uint32_t)b.pitch;
+    const int lx = ex - kSyAp, x = blockIdx.x * kSyT + lx;
+    if ((unsigned)lx >= (unsigned)kSyT || x >= b.W) return;
+#pragma unroll
+    for (int k = 0; k < kSyK; k++) {
+        const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = blockIdx.y * kSyTH + ly;
+        if ((unsigned)ly >= (unsigned)kSyTH || y >= b.H) continue;
+        const uint32_t pa = __ldg(reinterpret_cast<const uint32_t*>(b.a + (size_t)y * pitch) + x);
+        const uint32_t pc = __ldg(reinterpret_cast<const uint32_t*>(b.c + (size_t)y * pitch) + x);
+        uint32_t o = 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const uint32_t v = acc[k][c] + wp * ((pa >> (8 * c)) & 255u) + wc * ((pc >> (8 * c)) & 255u) + 32768u;
+            o |= (v >> 16) << (8 * c);
+        }
+        o |= ((wap * (pa >> 24) + wac * (pc >> 24) + 32768u) >> 16) << 24;
+        reinterpret_cast<uint32_t*>(b.out + (size_t)y * b.outPitch)[x] = o;
+    }
 }
 
 // Many syntheses (of several frame pairs and times) in one persistent launch: every CTA takes the next tile of the
@@ -1108,6 +1207,9 @@ cudaError_t prepareKernels() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_synth_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(synthSmemBytes(1) + kSyWarpBytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_blur, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(synthSmemBytes(1) + kSyWarpBytes));
     return e;
 }
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
@@ -1131,6 +1233,16 @@ int synthTilesY(int H) { return (int)divUp(H, kSyTH); }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs) + kSyWarpBytes;
     return launchPdl(k_synth, dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), dim3(kSyThreads), smem, s, p);
+}
+cudaError_t launchSynthBlur(const BlurParams& bp, cudaStream_t s) {
+    const size_t smem = synthSmemBytes(bp.base.fs) + kSyWarpBytes;
+    const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
+    BlurParams p = bp;
+    p.fix = 0;
+    cudaError_t e = launchPdl(k_synth_blur, grid, dim3(kSyThreads), smem, s, p);
+    p.fix = 1;
+    if (e == cudaSuccess) e = launchPdl(k_synth_blur, grid, dim3(kSyThreads), smem, s, p);
+    return e;
 }
 cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s) {
     return launchPdl(k_synth_batch, dim3(grid), dim3(kSyThreads), smem, s, b);

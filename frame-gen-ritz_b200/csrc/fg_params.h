@@ -150,6 +150,25 @@ struct SynthBatchArgs {             // k_synth_batch: a work list of syntheses
     unsigned int* counter;         // the next tile to take (zero before the launch)
 };
 
+// Motion blur (recordSynthBlur, gpu/framegen.h:553-573): one output = the weighted average of n sub-frames, each
+// exactly the 8-bit frame recordSynth(t_k) gives; the weights are integers summing to 2^16 (out = (sum q_k v_k +
+// 2^15) >> 16 per byte).
+constexpr int kBlurMax = 16;
+struct BlurSample {
+    int mode;                      // 0: a synthesis at t_k; 1: the real frame prev (t_k <= 0); 2: curr (t_k >= 1)
+    int lookup, mid, nearC;        // recordSynth(t_k)'s SynthParams fields
+    float s, ka, kc, wA, wC;
+    uint32_t q;                    // weight, units of 2^-16
+};
+struct BlurParams {
+    SynthParams base;              // the t-independent fields (untrusted and emap unused)
+    BlurSample smp[kBlurMax];
+    int n;
+    int fix;                       // 0: main pass, counts each synthesis' untrusted pixels into cnt[k]; 1: the fix-up
+    double frac;                   // globalFallback (interp.py:238): a sample past it is its nearer real frame
+    unsigned int* cnt;             // kBlurMax counters, zero before the main pass
+};
+
 struct FallbackParams {
     const uint8_t* a; const uint8_t* c; size_t pitch;
     uint8_t* out; size_t outPitch;
@@ -180,6 +199,8 @@ cudaError_t launchSynth(const SynthParams& p, cudaStream_t s);
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s);
 // batches (framegen.cpp Batch): many syntheses in one persistent launch, their fallbacks in one launch
 cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s);
+// the main pass (bp.fix = 0) then the fix-up (bp.fix = 1) of a motion blur, 8-bit RGBA frames
+cudaError_t launchSynthBlur(const BlurParams& bp, cudaStream_t s);
 int synthBatchCtasPerSm(size_t smem);
 cudaError_t launchFallbackBatch(const FallbackParams* items, int nItems, cudaStream_t s);
 size_t synthKernelSmem(int fs);   // k_synth's / k_synth_batch's dynamic shared memory at this flow scale

@@ -221,6 +221,7 @@ struct Interpolator::Impl {
     unsigned int* hist = nullptr;
     int histB = 0;
     fgk::DevState* st = nullptr;
+    unsigned int* blurCnt = nullptr;   // recordSynthBlur: per sample, its untrusted pixels (kBlurMax)
     uint8_t* emap = nullptr;
     fgk::CutPlan plan{};
     // trust-ramp shortcuts of the current settings
@@ -320,6 +321,7 @@ struct Interpolator::Impl {
         const size_t oLuma = take(L.lumaFloats * 4), oField = take(L.fieldF2 * 8), oSads = take((size_t)nb0 * 4);
         const size_t oPf = take((size_t)L.fw * L.fh * 8), oHist = take((size_t)2 * (2 * histB + 1) * 4);
         const size_t oSt = take(sizeof(fgk::DevState)), oEmap = take((size_t)((w + 3) & ~3u) * h);
+        const size_t oBlur = take((size_t)fgk::kBlurMax * 4);
         const size_t oLeaves = take(P.leaves.size() * 8), oInner = take(std::max<size_t>(P.inner.size(), 1) * 8);
         const size_t oDepth = take(P.depthStart.size() * 4 + 4);
         const size_t oVals = take((P.leaves.size() + P.inner.size()) * 4);
@@ -333,6 +335,7 @@ struct Interpolator::Impl {
         pf = (float2*)(arena + oPf);
         hist = (unsigned int*)(arena + oHist);
         st = (fgk::DevState*)(arena + oSt);
+        blurCnt = (unsigned int*)(arena + oBlur);
         emap = (uint8_t*)(arena + oEmap);
         cudaMemcpy(arena + oLeaves, P.leaves.data(), P.leaves.size() * 8, cudaMemcpyHostToDevice);
         if (!P.inner.empty()) cudaMemcpy(arena + oInner, P.inner.data(), P.inner.size() * 8, cudaMemcpyHostToDevice);
@@ -531,6 +534,36 @@ struct Interpolator::Impl {
         return fp;
     }
 
+    // recordSynthBlur (gpu/framegen.cpp:3534-3630): every sample's synthesis parameters as recordSynth(t_k) builds
+    // them, the per-sample counters zeroed, then the blur's main and fix-up passes
+    bool blur(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t0, float t1) {
+        float tk[Interpolator::kBlurMaxSamples];
+        uint32_t q[Interpolator::kBlurMaxSamples];
+        const int n = (int)Interpolator::blurPlan(set.blurSamples, set.blurWeights, t0, t1, tk, q);
+        if (n < 1) return false;
+        fgk::BlurParams bp{};
+        bp.base = synthParams(prev, curr, out, 0.5f, nullptr);
+        bp.base.emap = nullptr;
+        for (int k = 0; k < n; k++) {
+            fgk::BlurSample& m = bp.smp[k];
+            m.q = q[k];
+            if (tk[k] <= 0.0f || tk[k] >= 1.0f) {
+                m.mode = tk[k] <= 0.0f ? 1 : 2;
+                continue;
+            }
+            const fgk::SynthParams sp = synthParams(prev, curr, out, tk[k], nullptr);
+            m.lookup = sp.lookup; m.mid = sp.mid; m.nearC = sp.nearC;
+            m.s = sp.s; m.ka = sp.ka; m.kc = sp.kc; m.wA = sp.wA; m.wC = sp.wC;
+        }
+        bp.n = n;
+        bp.frac = (double)set.globalFallback;
+        bp.cnt = blurCnt;
+        if (!check(cudaMemsetAsync(blurCnt, 0, (size_t)fgk::kBlurMax * 4, s))) return false;
+        if (!check(fgk::launchSynthBlur(bp, s))) return false;
+        stamp(s, "blur");
+        return true;
+    }
+
     bool synth(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t) {
         const fgk::SynthParams sp = synthParams(prev, curr, out, t, &st->untrusted[parity]);
         if (!check(fmt == Format::Rgba8 ? fgk::launchSynth(sp, s) : fgk::launchSynthFmt(sp, s))) return false;
@@ -695,6 +728,52 @@ bool Interpolator::recordSynth(cudaStream_t stream, Frame prev, Frame curr, Fram
     m->synthSets++;
     if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
     return m->synth(stream, prev, curr, out, t);
+}
+
+uint32_t Interpolator::blurPlan(uint32_t samples, BlurWeights weights, float t0, float t1, float* times, uint32_t* q) {
+    if (!(t0 >= 0.0f && t1 <= 1.0f && t0 <= t1) || !times || !q) return 0;   // (also false for NaN)
+    const bool on = samples >= 2 && t0 < t1;
+    const int n = on ? (int)std::min(samples, kBlurMaxSamples) : 1;
+    double w[kBlurMaxSamples], frac[kBlurMaxSamples], sum = 0.0;
+    for (int k = 0; k < n; k++) {
+        // the midpoints of n equal slices of [t0, t1] (gpu/framegen.cpp:3552-3557); one instant t1 without blur
+        const double t = on ? t0 + ((double)t1 - (double)t0) * (k + 0.5) / n : (double)t1;
+        times[k] = std::min(std::max((float)t, t0), t1);
+        const double x = (2.0 * k + 1.0 - n) / n;   // the slice centre; the window ends are x = -+1
+        w[k] = weights == BlurWeights::Gaussian ? std::exp(-2.0 * x * x) : 1.0;
+        sum += w[k];
+    }
+    // the normalised weights in units of 2^-16: floors, then the remaining units to the largest remainders (ties to
+    // the lower sample), so that they sum to exactly 2^16
+    int64_t tot = 0;
+    for (int k = 0; k < n; k++) {
+        const double r = w[k] / sum * 65536.0;
+        q[k] = (uint32_t)std::floor(r);
+        frac[k] = r - (double)q[k];
+        tot += q[k];
+    }
+    while (tot != 65536) {
+        int best = 0;
+        for (int k = 1; k < n; k++)
+            if (tot < 65536 ? frac[k] > frac[best] : frac[k] < frac[best]) best = k;
+        if (tot < 65536) { q[best]++; frac[best] -= 1.0; tot++; }
+        else { q[best]--; frac[best] += 1.0; tot--; }
+    }
+    return (uint32_t)n;
+}
+
+bool Interpolator::recordSynthBlur(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t0, float t1) {
+    if (!m || !m->W || !(t0 >= 0.0f && t1 <= 1.0f && t0 <= t1)) return false;   // (also false for NaN)
+    const bool blur = m->set.blurSamples >= 2 && t0 < t1;
+    if (!blur && t1 > 0.0f && t1 < 1.0f) return recordSynth(stream, prev, curr, out, t1);   // one interior instant
+    if (!m->haveEst || prev.data != m->estPrev || curr.data != m->estCurr) return false;
+    if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || !m->samePitch(prev, curr)) return false;
+    if (m->fmt != Format::Rgba8) return false;
+    if (m->synthSets >= kSetRing) return false;
+    DeviceGuard g(m->device);
+    m->synthSets++;
+    if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
+    return m->blur(stream, prev, curr, out, t0, t1);
 }
 
 bool Interpolator::record(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t) {
@@ -1150,6 +1229,15 @@ int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, 
 int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* out,
                     float t) {
     return fg && prev && curr && out && fg->I.recordSynth((cudaStream_t)stream, fromC(prev), fromC(curr), fromC(out), t);
+}
+int fg_record_synth_blur(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
+                         const fg_frame* out, float t0, float t1) {
+    return fg && prev && curr && out &&
+           fg->I.recordSynthBlur((cudaStream_t)stream, fromC(prev), fromC(curr), fromC(out), t0, t1);
+}
+uint32_t fg_blur_plan(uint32_t samples, uint32_t weights, float t0, float t1, float* times, uint32_t* q) {
+    if (weights > 1u) return 0;
+    return Interpolator::blurPlan(samples, (BlurWeights)weights, t0, t1, times, q);
 }
 int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* out, float t) {
     return fg && prev && curr && out && fg->I.record((cudaStream_t)stream, fromC(prev), fromC(curr), fromC(out), t);

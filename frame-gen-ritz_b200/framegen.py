@@ -83,6 +83,9 @@ SIGNATURES = {
     "fg_record_estimate": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame)]),
     "fg_record_synth": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
     "fg_record": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
+    "fg_record_synth_blur": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F,
+                                  _F]),
+    "fg_blur_plan": (_U32, [_U32, _U32, _F, _F, _P, _P]),
     "fg_set_profiling": (_I, [_P, _I]),
     "fg_read_timings": (_I, [_P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint64), _U32,
                              ctypes.POINTER(_U32)]),
@@ -283,6 +286,12 @@ class Interpolator:
         return bool(lib().fg_record(self._h, _stream(stream), ctypes.byref(frame_of(prev)),
                                     ctypes.byref(frame_of(curr)), ctypes.byref(frame_of(out)), float(t)))
 
+    def record_synth_blur(self, prev, curr, out, t0, t1, stream=None):
+        """recordSynthBlur: the weighted average of settings.blurSamples sub-frames over [t0, t1]"""
+        return bool(lib().fg_record_synth_blur(self._h, _stream(stream), ctypes.byref(frame_of(prev)),
+                                               ctypes.byref(frame_of(curr)), ctypes.byref(frame_of(out)), float(t0),
+                                               float(t1)))
+
     def set_profiling(self, on):
         return bool(lib().fg_set_profiling(self._h, int(on)))
 
@@ -360,6 +369,17 @@ def read_trace(fg, stream=None):
     return {"seed_level": None if seed is None else int(l.seedLevel), "seed": seed,"luma": luma, "fields": fld, "sub": sub, "meds": f32(l.medOff, 2 * n).reshape(n, 2),
             "sads": f32(l.sadOff, bw0 * bh0).reshape(bh0, bw0), "pf": f32(l.pfOff, 2 * l.fw * l.fh).reshape(l.fh, l.fw, 2),
             "cut": bool(st[0]), "sad": float(st[1:2].view(np.float32)[0]), "sadSum256": int(st[2]), "err": int(st[3])}
+
+
+def blur_plan(samples, gaussian, t0, t1):
+    """Interpolator::blurPlan: ([t_k as float32], [q_k in units of 2^-16]) of a blur, or None if refused"""
+    times = (ctypes.c_float * 16)()
+    q = (ctypes.c_uint32 * 16)()
+    n = lib().fg_blur_plan(int(samples), int(bool(gaussian)), float(t0), float(t1), ctypes.addressof(times),
+                           ctypes.addressof(q))
+    if n == 0:
+        return None
+    return np.array(times[:n], np.float32), [int(v) for v in q[:n]]
 
 
 def record_synth_noalloc(prev, curr, out, field, cut, t, settings=None, view_format=VK_R8G8B8A8_UNORM, stream=None):

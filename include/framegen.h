@@ -10,7 +10,7 @@
 //   VkBuffer debug targets   -> device pointers
 //   VkFormat viewFormat      -> the same VkFormat numbers as plain uint32_t (kVkFormat* below; no Vulkan headers)
 // Out of scope here (rejected with a reason by settingsError / initError): MotionVersion V2 / Learned / V3, static-UI
-// protection modes other than Off, motion blur.
+// protection modes other than Off. Motion blur (recordSynthBlur): 8-bit RGBA / BGRA frames.
 //
 // Threading / streams: not thread-safe. All records of one Interpolator must go to ONE stream, in recording order:
 // its internal buffers are shared between records and only ordered by stream order.
@@ -73,7 +73,7 @@ struct Settings {
     uint32_t searchRadiusTop = 6;   // [1, 12]
     bool subpixel = true;
     UiProtection uiProtection = UiProtection::Off;   // Off only
-    uint32_t blurSamples = 0;                        // [0, 16]; recordSynthBlur is not part of this library
+    uint32_t blurSamples = 0;                        // [0, 16]: recordSynthBlur's sub-frames (< 2: blur off)
     BlurWeights blurWeights = BlurWeights::Gaussian;
     MotionVersion motionVersion = MotionVersion::V1; // V1 only
     // structural: init() or reconfigure()
@@ -127,6 +127,19 @@ public:
     bool recordEstimate(cudaStream_t stream, Frame prev, Frame curr);
     bool recordSynth(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t);
     bool record(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t = 0.5f);
+
+    // gpu/framegen.h:553-573: out = the weighted average of Settings::blurSamples (N) sub-frames of the latest
+    // estimate's pair at t_k = t0 + (t1 - t0)(k + 0.5) / N (double arithmetic, rounded to float, clamped to [t0, t1]),
+    // weights Settings::blurWeights (Gaussian: exp(-2 x_k^2), x_k = (2k + 1 - N) / N). A sub-frame is exactly the 8-bit
+    // frame recordSynth(t_k) gives (its scene-cut and whole-frame fallbacks included; prev / curr at t_k <= 0 / >= 1);
+    // the average is rounded once: out = (sum q_k v_k + 2^15) >> 16 per byte, q_k = the normalised weights in units
+    // of 2^-16 (largest-remainder rounding, blurPlan). N < 2 or t0 == t1: the single instant t1 (recordSynth(t1); a copy
+    // of prev / curr at t1 = 0 / 1). false (nothing recorded) unless 0 <= t0 <= t1 <= 1, and in recordSynth's cases;
+    // false for frames other than 8-bit RGBA / BGRA. Takes one synth of the ring; two launches whatever N is.
+    bool recordSynthBlur(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t0, float t1);
+    // the samples of a blur: their times and weights (units of 2^-16, summing to 2^16); returns their count (0 if
+    // refused: t0, t1 out of order or range)
+    static uint32_t blurPlan(uint32_t samples, BlurWeights weights, float t0, float t1, float* times, uint32_t* q);
 
     // gpu/framegen.h:705-717: CUDA events after every pass group; readTimings waits for them and returns the
     // group names and the nanoseconds of each group (the reference returns timestamp ticks; here 1 tick = 1 ns).

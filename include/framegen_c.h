@@ -86,6 +86,13 @@ int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, con
                     const fg_frame* out, float t);                                                        /* :550 */
 int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
               const fg_frame* out, float t);                                                              /* :551 */
+/* gpu/framegen.h:573 recordSynthBlur: the weighted average of settings.blurSamples sub-frames over [t0, t1]
+ * (framegen.h documents the samples, weights and rounding); 8-bit RGBA / BGRA frames */
+int fg_record_synth_blur(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
+                         const fg_frame* out, float t0, float t1);
+/* Interpolator::blurPlan (host only): the sample times and weights (units of 2^-16) of a blur into arrays of 16;
+ * weights 0 = Even, 1 = Gaussian; returns the number of samples, 0 if refused */
+uint32_t fg_blur_plan(uint32_t samples, uint32_t weights, float t0, float t1, float* times, uint32_t* q);
 
 int fg_set_profiling(fg_interpolator* fg, int on);                                   /* gpu/framegen.h:705 */
 /* gpu/framegen.h:717 readTimings: up to `capacity` names and nanoseconds; *count = the number of groups */

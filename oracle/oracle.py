@@ -8,6 +8,7 @@ Frames are numpy uint8 arrays (H, W, 4) in R,G,B,A order ("rgba"), (H, W, 4) B,G
 interp.py's own B,G,R order ("bgr"). Outputs keep the input's layout; alpha is the nearer real frame's.
 """
 import ctypes
+import math
 import os
 import subprocess
 from dataclasses import dataclass, field
@@ -176,6 +177,83 @@ def synth(a, c, est, t, settings=None, order="rgba", trace=False, threads=0):
     if trace:
         return {"out": out, "reason": REASONS[reason.value], "field_t": ft, "e": e, "untrusted": int(unt.value)}
     return out, REASONS[reason.value]
+
+
+# ---------------------------------------------------------------------------------------------- motion blur
+# recordSynthBlur (gpu/framegen.h:553-573, gpu/framegen.cpp:3534-3630): the weighted average of N sub-frames, each
+# exactly the frame recordSynth(t_k) gives. The reference's own check of it (gpu/blurtest.cpp:602-620, 757-806) takes
+# the sub-frames, weights them in double precision and rounds half up, allowing 1 level. This restatement fixes the
+# rounding: the normalised weights in units of 2^-16 (largest remainders), out = (sum q_k v_k + 2^15) >> 16.
+
+def blur_plan(samples, gaussian, t0, t1):
+    """(times as float32, weights q_k in units of 2^-16) of a blur over [t0, t1], or None if refused. Times: the
+    midpoints t0 + (t1 - t0)(k + 0.5) / N in double, rounded to float32 and clamped to [t0, t1]
+    (gpu/framegen.cpp:3552-3557); N < 2 or t0 == t1: the single instant t1. Weights: 1 (even) or exp(-2 x_k^2),
+    x_k = (2k + 1 - N) / N (gpu/blurtest.cpp:610-620, gpu/shaders/blur_resolve.comp:135-140)."""
+    t0, t1 = np.float32(t0), np.float32(t1)
+    if not (t0 >= 0 and t1 <= 1 and t0 <= t1):
+        return None
+    on = samples >= 2 and t0 < t1
+    n = min(int(samples), 16) if on else 1
+    d0, d1 = float(t0), float(t1)
+    times, w, tot_w = [], [], 0.0
+    for k in range(n):
+        t = d0 + (d1 - d0) * (k + 0.5) / n if on else d1
+        times.append(min(max(np.float32(t), t0), t1))
+        x = (2.0 * k + 1.0 - n) / n
+        w.append(math.exp(-2.0 * x * x) if gaussian else 1.0)
+        tot_w += w[-1]
+    q, frac = [], []
+    for v in w:
+        r = v / tot_w * 65536.0
+        q.append(math.floor(r))
+        frac.append(r - q[-1])
+    tot = sum(q)
+    while tot != 65536:   # the remaining units to the largest remainders, ties to the lower sample
+        best = 0
+        for k in range(1, n):
+            if (frac[k] > frac[best]) if tot < 65536 else (frac[k] < frac[best]):
+                best = k
+        if tot < 65536:
+            q[best] += 1
+            frac[best] -= 1.0
+            tot += 1
+        else:
+            q[best] -= 1
+            frac[best] += 1.0
+            tot -= 1
+    return np.array(times, np.float32), q
+
+
+def blur_subframes(a, c, est, t0, t1, samples, gaussian, settings=None, order="rgba"):
+    """the sub-frames of a blur: [(t_k, q_k, frame_k)], frame_k = synth(t_k)'s frame, a / c at t_k <= 0 / >= 1"""
+    plan = blur_plan(samples, gaussian, t0, t1)
+    if plan is None:
+        return None
+    out = []
+    for tk, qk in zip(*plan):
+        if tk <= 0:
+            f = a
+        elif tk >= 1:
+            f = c
+        else:
+            f, _ = synth(a, c, est, float(tk), settings, order)
+        out.append((float(tk), qk, f))
+    return out
+
+
+def synth_blur(a, c, est, t0, t1, samples, gaussian, settings=None, order="rgba"):
+    """recordSynthBlur's frame (None if refused): with blur off (N < 2) or t0 == t1 and t1 inside (0, 1), synth(t1);
+    otherwise (sum q_k frame_k + 2^15) >> 16 per byte"""
+    t0f, t1f = np.float32(t0), np.float32(t1)
+    if not (t0f >= 0 and t1f <= 1 and t0f <= t1f):
+        return None
+    if not (samples >= 2 and t0f < t1f) and 0 < t1f < 1:
+        return synth(a, c, est, float(t1f), settings, order)[0]
+    acc = np.zeros(np.shape(a), np.int64)
+    for _, qk, f in blur_subframes(a, c, est, t0, t1, samples, gaussian, settings, order):
+        acc += qk * f.astype(np.int64)
+    return ((acc + 32768) >> 16).astype(np.uint8)
 
 
 def mean_f32(a):
