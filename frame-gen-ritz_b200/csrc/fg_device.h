@@ -208,18 +208,21 @@ __device__ __forceinline__ SyCoef syFieldStage(const SynthParams& p, int X0, int
     hrow = g + GW * GH;                                    // GH x kSyE
     e = reinterpret_cast<uint8_t*>(hrow + GH * kSyE);      // kSyEH x kSyE
     hsum = reinterpret_cast<unsigned short*>(e + kSyEH * kSyE);   // kSyEH x kSyE (columns < kSyT used)
-    for (int r = ey0; r < GH; r += kSyThreads / kSyE)
-        for (int c = ex; c < GW; c += kSyE) {
-            const int qx = gx0 + c, qy = gy0 + r;
-            float2 v = __ldg(p.pf + (size_t)qy * p.fw + qx);
-            if (p.lookup) {
-                const float fx = (float)qx, fy = (float)qy;
+    // the region's GW x GH samples spread over all threads (GW is about half the CTA's width at flowScale 2): row
+    // r = floor((i + 0.5) / GW), exact in float for these sizes (the quotient stays >= 0.5 / GW from an integer)
+    const float invGW = 1.0f / (float)GW;
+    for (int i = tid; i < GW * GH; i += kSyThreads) {
+        const int r = (int)__fmul_rz(__int2float_rn(i) + 0.5f, invGW), c = i - r * GW;
+        const int qx = gx0 + c, qy = gy0 + r;
+        float2 v = __ldg(p.pf + (size_t)qy * p.fw + qx);
+        if (p.lookup) {
+            const float fx = (float)qx, fy = (float)qy;
 #pragma unroll
-                for (int it = 0; it < 2; it++)
-                    v = remapF2m(p.pf, p.fw, p.fh, __fsub_rn(fx, __fmul_rn(p.s, v.x)), __fsub_rn(fy, __fmul_rn(p.s, v.y)));
-            }
-            g[r * GW + c] = v;
+            for (int it = 0; it < 2; it++)
+                v = remapF2m(p.pf, p.fw, p.fh, __fsub_rn(fx, __fmul_rn(p.s, v.x)), __fsub_rn(fy, __fmul_rn(p.s, v.y)));
         }
+        g[r * GW + c] = v;
+    }
     __syncthreads();
     for (int r = ey0; r < GH; r += kSyThreads / kSyE) {
         const float2 s0 = g[r * GW + cx.i0], s1 = g[r * GW + cx.i1];
