@@ -705,8 +705,9 @@ __device__ __forceinline__ float2 tapPair(const float* __restrict__ ya, const fl
 
 __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     pdlEnter();
-    __shared__ int plane[kPfEH][kPfE];
-    __shared__ int hs[kPfEH][kPfE];
+    // rows padded by one word: the horizontal sums below read down the rows of a column group, one row per lane
+    __shared__ int plane[kPfEH][kPfE + 1];
+    __shared__ int hs[kPfEH][kPfE + 1];
     __shared__ float2 bv[kPfBY][kPfBX];
     __shared__ int2 bR[kPfBY][kPfBX];
     __shared__ float4 rowc[kPfEH];   // bilinear candidate, y: (row0, row1 relative to the block region, weights)
@@ -780,9 +781,10 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
             plane[ey][ex] = __float_as_int(__fmaf_rn(fabsf(t.x - t.y), 16.0f, 12582912.0f)) - 0x4B400000;   // E * 2^14
         }
         __syncthreads();
-        // 2. horizontal 5-sums: one region row, 8 output columns per thread (a running window)
+        // 2. horizontal 5-sums: one region row, 8 output columns per thread (a running window); the lanes of a warp
+        //    take the 32 rows of one column group (conflict-free with the padded rows)
         {
-            const int r = tid >> 3, c0 = (tid & 7) * 8;
+            const int r = tid & 31, c0 = (tid >> 5) * 8;
             const int* q = &plane[r][c0];
             int sum = q[0] + q[1] + q[2] + q[3] + q[4];
             hs[r][c0] = sum;
@@ -1234,15 +1236,12 @@ cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs) + kSyWarpBytes;
     return launchPdl(k_synth, dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), dim3(kSyThreads), smem, s, p);
 }
-cudaError_t launchSynthBlur(const BlurParams& bp, cudaStream_t s) {
+cudaError_t launchSynthBlur(const BlurParams& bp, int fix, cudaStream_t s) {
     const size_t smem = synthSmemBytes(bp.base.fs) + kSyWarpBytes;
     const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
     BlurParams p = bp;
-    p.fix = 0;
-    cudaError_t e = launchPdl(k_synth_blur, grid, dim3(kSyThreads), smem, s, p);
-    p.fix = 1;
-    if (e == cudaSuccess) e = launchPdl(k_synth_blur, grid, dim3(kSyThreads), smem, s, p);
-    return e;
+    p.fix = fix;
+    return launchPdl(k_synth_blur, grid, dim3(kSyThreads), smem, s, p);
 }
 cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s) {
     return launchPdl(k_synth_batch, dim3(grid), dim3(kSyThreads), smem, s, b);

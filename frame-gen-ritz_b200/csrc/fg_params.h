@@ -199,8 +199,8 @@ cudaError_t launchSynth(const SynthParams& p, cudaStream_t s);
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s);
 // batches (framegen.cpp Batch): many syntheses in one persistent launch, their fallbacks in one launch
 cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s);
-// the main pass (bp.fix = 0) then the fix-up (bp.fix = 1) of a motion blur, 8-bit RGBA frames
-cudaError_t launchSynthBlur(const BlurParams& bp, cudaStream_t s);
+// one pass of a motion blur, 8-bit RGBA frames: the main pass (fix = 0), then the fix-up (fix = 1)
+cudaError_t launchSynthBlur(const BlurParams& bp, int fix, cudaStream_t s);
 int synthBatchCtasPerSm(size_t smem);
 cudaError_t launchFallbackBatch(const FallbackParams* items, int nItems, cudaStream_t s);
 size_t synthKernelSmem(int fs);   // k_synth's / k_synth_batch's dynamic shared memory at this flow scale

@@ -244,6 +244,7 @@ struct Interpolator::Impl {
     std::vector<cudaEvent_t> events;
     std::vector<const char*> evNames;
     size_t evCount = 0;
+    uint32_t profileNo = 0, profileRead = 0, costSeq = 0;   // readCosts: profiles started, the last one read
 
     ~Impl() { freeAll(); }
 
@@ -399,7 +400,7 @@ struct Interpolator::Impl {
     bool estimate(cudaStream_t s, const Frame& prev, const Frame& curr) {
         const int n = (int)L.lv.size();
         const float lam = set.searchPenalty;
-        if (profiling) { evCount = 0; stamp(s, "start"); }
+        if (profiling) { evCount = 0; profileNo++; stamp(s, "start"); }
         // 1-2. luma + pyramid
         fgk::LumaPyrParams lp{};
         lp.a = (const uint8_t*)prev.data; lp.c = (const uint8_t*)curr.data; lp.pitch = prev.pitch;
@@ -559,8 +560,10 @@ struct Interpolator::Impl {
         bp.frac = (double)set.globalFallback;
         bp.cnt = blurCnt;
         if (!check(cudaMemsetAsync(blurCnt, 0, (size_t)fgk::kBlurMax * 4, s))) return false;
-        if (!check(fgk::launchSynthBlur(bp, s))) return false;
-        stamp(s, "blur");
+        if (!check(fgk::launchSynthBlur(bp, 0, s))) return false;
+        stamp(s, "blur resolve");
+        if (!check(fgk::launchSynthBlur(bp, 1, s))) return false;
+        stamp(s, "blur fixup");
         return true;
     }
 
@@ -818,6 +821,35 @@ bool Interpolator::readTimings(std::vector<const char*>& names, std::vector<uint
         names.push_back(m->evNames[i]);
         ticks.push_back((uint64_t)std::llround((double)ms * 1e6));
     }
+    return true;
+}
+
+bool Interpolator::readCosts(CostTimings& c) {
+    c = CostTimings{};
+    std::vector<const char*> names;
+    std::vector<uint64_t> ns;
+    if (!readTimings(names, ns)) return false;
+    static const char* const kEstimate[] = {"luma", "pyramid", "seed net", "subpixel", "pixel field"};
+    static const char* const kSynth[] = {"synth", "fallback", "blur resolve", "blur fixup"};
+    auto in = [](const char* n, const char* const* set, size_t k) {
+        for (size_t i = 0; i < k; i++)
+            if (std::strcmp(n, set[i]) == 0) return true;
+        return false;
+    };
+    uint64_t est = 0, syn = 0;
+    bool haveEst = false;
+    for (size_t i = 0; i < names.size(); i++) {
+        const char* n = names[i];
+        if (in(n, kEstimate, 5) || std::strncmp(n, "level ", 6) == 0) { est += ns[i]; haveEst = true; }
+        else if (in(n, kSynth, 4)) {
+            syn += ns[i];
+            if (std::strcmp(n, "synth") == 0 || std::strcmp(n, "blur resolve") == 0) c.synths++;
+        }
+    }
+    if (haveEst) c.estimateMs = (float)((double)est * 1e-6);
+    if (c.synths) c.synthMs = (float)((double)syn * 1e-6 / c.synths);
+    if (m->profileRead != m->profileNo || m->costSeq == 0) { m->costSeq++; m->profileRead = m->profileNo; }
+    c.seq = m->costSeq;
     return true;
 }
 
@@ -1243,6 +1275,13 @@ int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_
     return fg && prev && curr && out && fg->I.record((cudaStream_t)stream, fromC(prev), fromC(curr), fromC(out), t);
 }
 int fg_set_profiling(fg_interpolator* fg, int on) { return fg && fg->I.setProfiling(on != 0); }
+int fg_read_costs(fg_interpolator* fg, fg_costs* c) {
+    if (!fg || !c) return 0;
+    Interpolator::CostTimings t;
+    const bool ok = fg->I.readCosts(t);
+    c->estimate_ms = t.estimateMs; c->synth_ms = t.synthMs; c->seq = t.seq; c->synths = t.synths;
+    return ok;
+}
 int fg_read_timings(fg_interpolator* fg, const char** names, uint64_t* ns, uint32_t capacity, uint32_t* count) {
     if (!fg) return 0;
     std::vector<const char*> n;

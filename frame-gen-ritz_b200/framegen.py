@@ -61,6 +61,11 @@ class CTraceLayout(ctypes.Structure):
 
 # every symbol include/framegen_c.h declares, with (restype, argtypes)
 _P, _U32, _I, _F, _S = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float, ctypes.c_char_p
+
+
+class CCosts(ctypes.Structure):
+    _fields_ = [("estimate_ms", ctypes.c_float), ("synth_ms", ctypes.c_float), ("seq", ctypes.c_uint32),
+                ("synths", ctypes.c_uint32)]
 SIGNATURES = {
     "fg_abi_version": (_U32, []),
     "fg_default_settings": (None, [ctypes.POINTER(CSettings)]),
@@ -87,6 +92,7 @@ SIGNATURES = {
                                   _F]),
     "fg_blur_plan": (_U32, [_U32, _U32, _F, _F, _P, _P]),
     "fg_set_profiling": (_I, [_P, _I]),
+    "fg_read_costs": (_I, [_P, _P]),
     "fg_read_timings": (_I, [_P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint64), _U32,
                              ctypes.POINTER(_U32)]),
     "fg_record_debug_counters": (_I, [_P, _P, _P]),
@@ -303,6 +309,13 @@ class Interpolator:
         if not lib().fg_read_timings(self._h, names, ns, n, ctypes.byref(cnt)):
             return None
         return [(names[i].decode(), int(ns[i])) for i in range(min(cnt.value, n))]
+
+    def read_costs(self):
+        """readCosts: {estimate_ms, synth_ms, seq, synths} of the last profile (the pacer's cost-guard inputs), or None"""
+        c = CCosts()
+        if not lib().fg_read_costs(self._h, ctypes.byref(c)):
+            return None
+        return {"estimate_ms": c.estimate_ms, "synth_ms": c.synth_ms, "seq": c.seq, "synths": c.synths}
 
     def record_debug_counters(self, dst, stream=None):
         return bool(lib().fg_record_debug_counters(self._h, _stream(stream), dst.data_ptr()))

@@ -145,6 +145,15 @@ public:
     // group names and the nanoseconds of each group (the reference returns timestamp ticks; here 1 tick = 1 ns).
     bool setProfiling(bool on);
     bool readTimings(std::vector<const char*>& names, std::vector<uint64_t>& ticks);
+    // B200-build extension: the cost-guard inputs of gpu/pacing.h:869-871 (Pacer::Inputs::estimateMs / synthMs /
+    // costSeq) from the last profile: estimateMs = the estimate's pass groups (luma .. pixel field), synthMs = the
+    // synth-side groups (synth, fallback; blur resolve, blur fixup) per recorded synthesis; -1 where the profile has
+    // none; seq changes with every new profile read. false if profiling is off or nothing was recorded.
+    struct CostTimings {
+        float estimateMs = -1.0f, synthMs = -1.0f;
+        uint32_t seq = 0, synths = 0;
+    };
+    bool readCosts(CostTimings& c);
 
     // gpu/framegen.h:726-741: debug copies into device memory at dst (stream-ordered).
     bool recordDebugCounters(cudaStream_t stream, void* dst);   // 2 uint32: [untrusted px, finest SAD sum x 256]

@@ -98,6 +98,13 @@ int fg_set_profiling(fg_interpolator* fg, int on);                              
 /* gpu/framegen.h:717 readTimings: up to `capacity` names and nanoseconds; *count = the number of groups */
 int fg_read_timings(fg_interpolator* fg, const char** names, uint64_t* ns, uint32_t capacity, uint32_t* count);
 
+/* Interpolator::readCosts: the pacer's cost-guard inputs (gpu/pacing.h:869-871) from the last profile */
+typedef struct fg_costs {
+    float estimate_ms, synth_ms;   /* -1: none in the profile */
+    uint32_t seq, synths;          /* seq changes with every new profile; synths: syntheses in it */
+} fg_costs;
+int fg_read_costs(fg_interpolator* fg, fg_costs* c);
+
 int fg_record_debug_counters(fg_interpolator* fg, void* stream, void* dst);          /* gpu/framegen.h:726 */
 uint32_t fg_debug_sad_blocks(const fg_interpolator* fg);                             /* gpu/framegen.h:727 */
 int fg_get_debug_map_layout(const fg_interpolator* fg, fg_debug_map_layout* l);          /* gpu/framegen.h:740 */

@@ -96,4 +96,5 @@ def test_init_refusals_without_recording():
     # no estimate / not initialised: every record is refused and nothing is launched
     assert I.size_error(64, 64) == "not initialised"
     assert I.read_timings() is None
+    assert I.read_costs() is None
     I.close()

@@ -192,7 +192,9 @@ def test_blur_graph_capture_and_profiling():
     assert ctx.I.set_profiling(True)
     ctx.blur(0.2, 0.9, 6, True)
     names = [name for name, _ in ctx.I.read_timings()]
-    assert "blur" in names, names
+    assert names[-2:] == ["blur resolve", "blur fixup"], names
+    c = ctx.I.read_costs()
+    assert c["synths"] == 1 and c["synth_ms"] > 0, c
     ctx.close()
 
 

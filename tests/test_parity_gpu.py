@@ -181,6 +181,14 @@ def test_profiling_timings():
     assert names[:2] == ["luma", "pyramid"] and "subpixel" in names and "pixel field" in names
     assert names.count("synth") == 3 and names.count("fallback") == 3
     assert sum(ns for _, ns in tm) > 0
+    # the pacer's cost-guard inputs from the same profile (gpu/pacing.h:869-871)
+    c = I.read_costs()
+    est_ns = sum(ns for n, ns in tm if n in ("luma", "pyramid", "subpixel", "pixel field") or n.startswith("level "))
+    syn_ns = sum(ns for n, ns in tm if n in ("synth", "fallback"))
+    assert c["synths"] == 3 and abs(c["estimate_ms"] - est_ns * 1e-6) < 1e-6 and abs(c["synth_ms"] - syn_ns * 1e-6 / 3) < 1e-6
+    assert I.read_costs()["seq"] == c["seq"], "same profile, same sequence number"
+    assert I.record_estimate(a, cc)
+    assert I.read_costs()["seq"] == c["seq"] + 1 and I.read_costs()["synths"] == 0
     I.close()
 
 
