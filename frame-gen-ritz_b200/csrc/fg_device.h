@@ -136,6 +136,9 @@ constexpr int kSyE = 128, kSyEH = 32, kSyAp = 3;                 // 128 x 32 mis
 constexpr int kSyT = kSyE - 2 * kSyAp, kSyTH = kSyEH - 2 * kSyAp;
 constexpr int kSyThreads = 512, kSyK = kSyEH / (kSyThreads / kSyE);   // region rows per thread (512 = 128 columns x 4)
 constexpr size_t kSyWarpBytes = (size_t)2 * kSyTH * kSyE * 4;   // k_synth: both warps of the output rows, after the row sums
+// row strides of the mismatch plane e (bytes) and of its horizontal 7-sums (uint16): one word of padding per row, so
+// that the lanes of a warp can walk 32 different rows of one column group without bank conflicts
+constexpr int kSyES = kSyE + 4, kSyHS = kSyE + 2;
 
 // cv2.remap INTER_LINEAR / BORDER_REPLICATE of the 2-channel float field at (x, y): quantisation and weights paired
 // (exact), the taps' weighted sum as cv2 rounds it, ((p00 w00 + p01 w01) + p10 w10) + p11 w11 per channel
@@ -206,8 +209,8 @@ __device__ __forceinline__ SyCoef syFieldStage(const SynthParams& p, int X0, int
     const SyCoef cx = syCoef(ex, X0, p.W, uw, p.fw, gx0, invfs, 1.0f, true);
     float2* g = reinterpret_cast<float2*>(sm);             // GH x GW
     hrow = g + GW * GH;                                    // GH x kSyE
-    e = reinterpret_cast<uint8_t*>(hrow + GH * kSyE);      // kSyEH x kSyE
-    hsum = reinterpret_cast<unsigned short*>(e + kSyEH * kSyE);   // kSyEH x kSyE (columns < kSyT used)
+    e = reinterpret_cast<uint8_t*>(hrow + GH * kSyE);      // kSyEH rows of kSyES bytes
+    hsum = reinterpret_cast<unsigned short*>(e + kSyEH * kSyES);   // kSyEH rows of kSyHS (columns < kSyT used)
     // the region's GW x GH samples spread over all threads (GW is about half the CTA's width at flowScale 2): row
     // r = floor((i + 0.5) / GW), exact in float for these sizes (the quotient stays >= 0.5 / GW from an integer)
     const float invGW = 1.0f / (float)GW;
@@ -231,6 +234,21 @@ __device__ __forceinline__ SyCoef syFieldStage(const SynthParams& p, int X0, int
     }
     __syncthreads();
     return cx;
+}
+
+// Stage 3 of a synthesis tile: the horizontal 7-sums of the mismatch plane, one region row and 8 output columns per
+// thread (a running window); the lanes of a warp take the 32 rows of one column group (conflict-free strides)
+__device__ __forceinline__ void syRowSums(const uint8_t* e, unsigned short* hsum, int tid) {
+    const int r = tid & (kSyEH - 1), c0 = (tid / kSyEH) * 8;
+    const uint8_t* q = e + r * kSyES + c0;
+    unsigned short* o = hsum + r * kSyHS + c0;
+    unsigned int sum = q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6];
+    o[0] = (unsigned short)sum;
+#pragma unroll
+    for (int c = 1; c < 8; c++) {
+        if (c0 + c + 6 < kSyE) sum += q[c + 6] - q[c - 1];
+        o[c] = (unsigned short)sum;
+    }
 }
 
 // the half-vector of region row ey in this thread's column (vertical stage of the upsampling, x fs folded in)

@@ -337,22 +337,11 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
         float wa[3], wc[3];
         warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
         warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
-        e[ey * kSyE + ex] = (uint8_t)mismatch<F>(p.f, wa, wc);
+        e[ey * kSyES + ex] = (uint8_t)mismatch<F>(p.f, wa, wc);
     }
     __syncthreads();
     // 3. horizontal 7-sums (as k_synth)
-    {
-        const int r = tid >> 4, c0 = (tid & 15) * 8;
-        const uint8_t* q = e + r * kSyE + c0;
-        unsigned short* o = hsum + r * kSyE + c0;
-        unsigned int sum = q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6];
-        o[0] = (unsigned short)sum;
-#pragma unroll
-        for (int c = 1; c < 8; c++) {
-            if (c0 + c + 6 < kSyE) sum += q[c + 6] - q[c - 1];
-            o[c] = (unsigned short)sum;
-        }
-    }
+    syRowSums(e, hsum, tid);
     __syncthreads();
     // 4. output pixels: vertical 7-sum, trust, the warps again, blend, store
     unsigned int myCnt = 0;
@@ -362,8 +351,8 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
         for (int k = 0; k < kSyK; k++) {
             const int ey = ey0 + (kSyThreads / kSyE) * k, ly = ey - kSyAp, y = Y0 + ly;
             if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
-            const unsigned short* q = hsum + ly * kSyE + lx;
-            const int S = q[0] + q[kSyE] + q[2 * kSyE] + q[3 * kSyE] + q[4 * kSyE] + q[5 * kSyE] + q[6 * kSyE];
+            const unsigned short* q = hsum + ly * kSyHS + lx;
+            const int S = q[0] + q[kSyHS] + q[2 * kSyHS] + q[3 * kSyHS] + q[4 * kSyHS] + q[5 * kSyHS] + q[6 * kSyHS];
             const float eb = (float)((double)S * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
             const float u = clampF(__fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan), 0.0f, 1.0f);
             myCnt += u > 0.5f;
@@ -415,7 +404,7 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
                     else reinterpret_cast<unsigned short*>(oc)[x >> 1] = (unsigned short)(cb | (cr << 8));
                 }
             }
-            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[ey * kSyE + ex];
+            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[ey * kSyES + ex];
         }
     }
     if (myCnt) atomicAdd(&cnt, myCnt);

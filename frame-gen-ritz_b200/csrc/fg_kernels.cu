@@ -913,7 +913,7 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
     const SyCoef cx = syFieldStage(p, X0, Y0, tid, ex, ey0, rowc, gReg, sm, hrow, e, hsum);
     // 2. this thread's region column: half-vector (vertical stage, x fs folded in), both warps, mismatch. The warps
     //    wait in shared memory for the blend (in registers they would leave too few for the sample loads in flight).
-    uint32_t* sWA = reinterpret_cast<uint32_t*>(hsum + kSyEH * kSyE);   // the output rows: kSyTH x kSyE
+    uint32_t* sWA = reinterpret_cast<uint32_t*>(hsum + kSyEH * kSyHS);   // the output rows: kSyTH x kSyE
     uint32_t* sWC = sWA + kSyTH * kSyE;
     const float kA = p.mid ? 1.0f : p.ka, kC = p.mid ? 1.0f : p.kc;   // t = 0.5: the products by 1 are exact
 #pragma unroll
@@ -933,22 +933,11 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
             sWC[(ey - kSyAp) * kSyE + ex] = C;
         }
         const int m = max(max(abs(ca[0] - cc[0]), abs(ca[1] - cc[1])), abs(ca[2] - cc[2]));
-        e[ey * kSyE + ex] = (uint8_t)m;
+        e[ey * kSyES + ex] = (uint8_t)m;
     }
     __syncthreads();
     // 3. horizontal 7-sums: one region row and 16 output columns per thread, a running window
-    {
-        const int r = tid >> 4, c0 = (tid & 15) * 8;
-        const uint8_t* q = e + r * kSyE + c0;
-        unsigned short* o = hsum + r * kSyE + c0;
-        unsigned int sum = q[0] + q[1] + q[2] + q[3] + q[4] + q[5] + q[6];
-        o[0] = (unsigned short)sum;
-#pragma unroll
-        for (int c = 1; c < 8; c++) {
-            if (c0 + c + 6 < kSyE) sum += q[c + 6] - q[c - 1];
-            o[c] = (unsigned short)sum;
-        }
-    }
+    syRowSums(e, hsum, tid);
     __syncthreads();
     // 4. this thread's output pixels: vertical 7-sum, trust, blend, store
     unsigned int myCnt = 0;
@@ -958,8 +947,8 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
         for (int k = 0; k < kSyK; k++) {
             const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = Y0 + ly;
             if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
-            const unsigned short* q = hsum + ly * kSyE + lx;
-            const int S = q[0] + q[kSyE] + q[2 * kSyE] + q[3 * kSyE] + q[4 * kSyE] + q[5 * kSyE] + q[6 * kSyE];
+            const unsigned short* q = hsum + ly * kSyHS + lx;
+            const int S = q[0] + q[kSyHS] + q[2 * kSyHS] + q[3 * kSyHS] + q[4 * kSyHS] + q[5 * kSyHS] + q[6 * kSyHS];
             const uint32_t nq = __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
             const uint32_t wak = sWA[ly * kSyE + ex], wck = sWC[ly * kSyE + ex];
             uint32_t o;
@@ -1000,7 +989,7 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
             }
             o = (o & 0x00FFFFFFu) | (nq & 0xFF000000u);   // alpha (byte 3 in both pixel orders): the nearer frame's
             sink(k, x, y, ly, o);
-            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyE + ex];
+            if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[(ly + kSyAp) * kSyES + ex];
         }
     }
     if (myCnt) atomicAdd(&cnt, myCnt);
@@ -1227,7 +1216,7 @@ cudaError_t launchPixfield(const PixfieldParams& p, cudaStream_t s) {
 size_t synthSmemBytes(int fs) {  // declared in fg_params.h
     // worst-case field region of a tile (GW x GH float2) + its horizontal stage + mismatch + row sums
     const int gw = (kSyE + fs - 1) / fs + 3, gh = (kSyEH + fs - 1) / fs + 3;
-    return (size_t)gw * gh * 8 + (size_t)gh * kSyE * 8 + (size_t)kSyEH * kSyE + (size_t)kSyEH * kSyE * 2;
+    return (size_t)gw * gh * 8 + (size_t)gh * kSyE * 8 + (size_t)kSyEH * kSyES + (size_t)kSyEH * kSyHS * 2;
 }
 size_t synthKernelSmem(int fs) { return synthSmemBytes(fs) + kSyWarpBytes; }
 int synthTilesX(int W) { return (int)divUp(W, kSyT); }
