@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(256) k_down(const DownParams p) {
 // Search: every integer offset within +-R of the seed; the (8+2R)^2 windows of a and c (bilateral: a at q - v, c at
 // q + v) are staged in shared memory; lane i scores candidates i, i+32, ...; cost = SAD + lambda |d|_1; the warp
 // keeps the lowest (cost, raster index) pair, i.e. the first minimum in interp's (dy, dx) order.
+template <bool kLat>
 __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by, int lane, int& sx, int& sy);
 
 __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
     float* sC = sA + T * T;
     const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
     int sx, sy;
-    searchSeed(p, bx, by, lane, sx, sy);
+    searchSeed<false>(p, bx, by, lane, sx, sy);
     for (int i = lane; i < T * T; i += 32) {
         const int x = i % T, y = i / T;
         sA[i] = Lc(p.la, p.w, p.h, b0x - sx - R + x, b0y - sy - R + y);
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
 // The seed of a block (interp.seed_from :131-144 for one fine block), shared by both search kernels. A candidate equal
 // to an earlier one is skipped: its cost would equal that one's (or exceed it by lambda), so under the first-minimum
 // rule it could never be picked.
+template <bool kLat>
 __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by, int lane, int& sx, int& sy) {
     sx = 0;
     sy = 0;
@@ -200,34 +202,65 @@ __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by
         }
     }
     const int qx = b0x + (lane & 7), qy0 = b0y + (lane >> 3), qy1 = qy0 + 4;
+    if (!kLat) {   // large levels (throughput bound): candidates scored one after another, duplicates skipped
+        float best = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            bool dup = false;
+#pragma unroll
+            for (int j = 0; j < k; j++) dup |= cxs[j] == cxs[k] && cys[j] == cys[k];
+            if (dup) continue;   // warp-uniform
+            const int cx = cxs[k], cy = cys[k];
+            float s;
+            if (b0x - abs(cx) >= 0 && b0x + 7 + abs(cx) < p.w && b0y - abs(cy) >= 0 && b0y + 7 + abs(cy) < p.h) {
+                const float* ra = p.la + (size_t)(qy0 - cy) * p.w + (qx - cx);
+                const float* rc = p.lc + (size_t)(qy0 + cy) * p.w + (qx + cx);
+                s = fabsf(__ldg(ra) - __ldg(rc)) + fabsf(__ldg(ra + 4 * p.w) - __ldg(rc + 4 * p.w));
+            } else {
+                s = fabsf(Lc(p.la, p.w, p.h, qx - cx, qy0 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy0 + cy));
+                s += fabsf(Lc(p.la, p.w, p.h, qx - cx, qy1 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy1 + cy));
+            }
+            s = warpSum(s);   // exact: at most 24 significant bits
+            float cost = __fmul_rn(s, 1.0f / 64.0f);
+            if (k > 0 || pen0) cost = __fadd_rn(cost, p.lambda);
+            if (k == 0 || cost < best) { best = cost; sx = cx; sy = cy; }
+        }
+        return;
+    }
+    // small levels (latency bound): every candidate's two pixel pairs per lane are loaded before any is reduced
+    // (clamped addressing = the replicate border), so the six scores cost one memory round trip rather than six
+    bool dup[6];
+    float sk[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        dup[k] = false;
+#pragma unroll
+        for (int j = 0; j < k; j++) dup[k] |= cxs[j] == cxs[k] && cys[j] == cys[k];
+        const int cx = cxs[k], cy = cys[k];
+        sk[k] = fabsf(Lc(p.la, p.w, p.h, qx - cx, qy0 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy0 + cy)) +
+                fabsf(Lc(p.la, p.w, p.h, qx - cx, qy1 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy1 + cy));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)   // six warp sums side by side (exact: at most 24 significant bits)
+#pragma unroll
+        for (int k = 0; k < 6; k++) sk[k] += __shfl_xor_sync(0xffffffffu, sk[k], o);
     float best = 0.0f;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-        bool dup = false;
-#pragma unroll
-        for (int j = 0; j < k; j++) dup |= cxs[j] == cxs[k] && cys[j] == cys[k];
-        if (dup) continue;   // warp-uniform
-        const int cx = cxs[k], cy = cys[k];
-        float s;
-        if (b0x - abs(cx) >= 0 && b0x + 7 + abs(cx) < p.w && b0y - abs(cy) >= 0 && b0y + 7 + abs(cy) < p.h) {
-            const float* ra = p.la + (size_t)(qy0 - cy) * p.w + (qx - cx);
-            const float* rc = p.lc + (size_t)(qy0 + cy) * p.w + (qx + cx);
-            s = fabsf(__ldg(ra) - __ldg(rc)) + fabsf(__ldg(ra + 4 * p.w) - __ldg(rc + 4 * p.w));
-        } else {
-            s = fabsf(Lc(p.la, p.w, p.h, qx - cx, qy0 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy0 + cy));
-            s += fabsf(Lc(p.la, p.w, p.h, qx - cx, qy1 - cy) - Lc(p.lc, p.w, p.h, qx + cx, qy1 + cy));
-        }
-        s = warpSum(s);   // exact: at most 24 significant bits
-        float cost = __fmul_rn(s, 1.0f / 64.0f);
+        if (dup[k]) continue;   // warp-uniform
+        float cost = __fmul_rn(sk[k], 1.0f / 64.0f);
         if (k > 0 || pen0) cost = __fadd_rn(cost, p.lambda);
-        if (k == 0 || cost < best) { best = cost; sx = cx; sy = cy; }
+        if (k == 0 || cost < best) { best = cost; sx = cxs[k]; sy = cys[k]; }
     }
 }
+
+// levels of at most this many blocks are latency bound (a few CTAs per SM): their seeds load every candidate at once
+constexpr int kSearchLatBlocks = 2048;
 
 // interp.search at integer steps, radius R known at compile time (1..6), one warp per 8x8 block. The (8+2R)^2 windows
 // of a and c are staged in shared memory. Lane = (dy, block row y): it holds a's row y - dy and c's row y + dy in
 // registers and scores every dx from them; the 8 rows of a dy are summed by shuffles (all sums exact).
-template <int R>
+template <int R, bool kLat>
 __global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
     pdlEnter();
     constexpr int T = 8 + 2 * R, D = 2 * R + 1, NI = 8 * D, ROUNDS = (NI + 31) / 32;
@@ -240,7 +273,7 @@ __global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
     float* sad = sC + T * T;   // D x D window SADs (sums over the 64 pixels)
     const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
     int sx, sy;
-    searchSeed(p, bx, by, lane, sx, sy);
+    searchSeed<kLat>(p, bx, by, lane, sx, sy);
     const int ax0 = b0x - sx - R, ay0 = b0y - sy - R, cx0 = b0x + sx - R, cy0 = b0y + sy - R;
     if (ax0 >= 0 && ay0 >= 0 && ax0 + T <= p.w && ay0 + T <= p.h && cx0 >= 0 && cy0 >= 0 && cx0 + T <= p.w && cy0 + T <= p.h) {
         for (int i = lane; i < T * T; i += 32) {
@@ -402,6 +435,94 @@ __global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
         *p.done = 0;
     }
     for (int i = threadIdx.x; i < 2 * nb; i += 256) p.hist[i] = 0;
+}
+
+// k_median3 for a level small enough for one CTA (at most kMed1Blocks blocks; the histogram fits in shared memory):
+// the same medians and the same global median, with the histogram in shared memory and the order statistics read
+// off by the same CTA, so no global atomics, no fence and no last-block ticket stand in the estimate's critical path
+// (the coarse levels are latency bound).
+constexpr int kMed1Threads = 1024, kMed1Blocks = 2048, kMed1MaxBins = 4097;
+__global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Params p) {
+    pdlEnter();
+    extern __shared__ unsigned int hs1[];   // 2 * nb bins: x then y
+    __shared__ unsigned int part[32];
+    __shared__ int found[4];
+    const int nb = 2 * p.B + 1, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < 2 * nb; i += kMed1Threads) hs1[i] = 0;
+    if (tid < 4) found[tid] = 0;
+    __syncthreads();
+    const int n = p.bw * p.bh;
+#pragma unroll 2
+    for (int b = tid; b < n; b += kMed1Threads) {
+        const int bx = b % p.bw, by = b / p.bw;
+        float xs[9], ys[9];
+        int k = 0;
+#pragma unroll
+        for (int j = -1; j <= 1; j++)
+#pragma unroll
+            for (int i = -1; i <= 1; i++) {
+                const float2 v = p.in[clampi(by + j, 0, p.bh - 1) * p.bw + clampi(bx + i, 0, p.bw - 1)];
+                xs[k] = v.x;
+                ys[k] = v.y;
+                k++;
+            }
+        const float2 m = make_float2(med9(xs), med9(ys));
+        p.out[b] = m;
+        const int wx = bx < p.bw - 1 ? max(0, min(2, p.fbw - 2 * bx)) : max(0, p.fbw - 2 * bx);
+        const int wy = by < p.bh - 1 ? max(0, min(2, p.fbh - 2 * by)) : max(0, p.fbh - 2 * by);
+        const unsigned int wgt = (unsigned int)(wx * wy);
+        if (wgt) {
+            int ix = __float2int_rn(m.x) + p.B, iy = __float2int_rn(m.y) + p.B;
+            if (ix < 0 || ix > 2 * p.B || iy < 0 || iy > 2 * p.B) {
+                atomicOr(p.err, kErrHistRange);
+                ix = clampi(ix, 0, 2 * p.B);
+                iy = clampi(iy, 0, 2 * p.B);
+            }
+            atomicAdd(hs1 + ix, wgt);
+            atomicAdd(hs1 + nb + iy, wgt);
+        }
+    }
+    __syncthreads();
+    // order statistics k1 = (N - 1) / 2, k2 = N / 2 of each axis: chunk sums, a block-wide scan, a walk of the chunk
+    const unsigned int N = (unsigned int)(p.fbw * p.fbh), ks[2] = {(N - 1) / 2, N / 2};
+    const int per = (nb + kMed1Threads - 1) / kMed1Threads;
+    for (int axis = 0; axis < 2; axis++) {
+        const unsigned int* h = hs1 + axis * nb;
+        const int s0 = tid * per, s1 = min(s0 + per, nb);
+        unsigned int loc = 0;
+        for (int i = s0; i < s1; i++) loc += h[i];
+        unsigned int inc = loc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) part[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {   // the warps' totals -> their exclusive offsets
+            const unsigned int tot = part[lane];
+            unsigned int x = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int v = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += v;
+            }
+            part[lane] = x - tot;
+        }
+        __syncthreads();
+        unsigned int acc = part[wid] + inc - loc;
+        for (int i = s0; i < s1; i++) {
+            const unsigned int hv = h[i];
+            for (int q = 0; q < 2; q++)
+                if (acc <= ks[q] && ks[q] < acc + hv) found[axis * 2 + q] = i - p.B;
+            acc += hv;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        p.medOut[0] = (float)(found[0] + found[1]);
+        p.medOut[1] = (float)(found[2] + found[3]);
+    }
 }
 
 // ============================================================================================== scene-cut mean
@@ -1167,7 +1288,10 @@ cudaError_t launchDown(const DownParams& p, cudaStream_t s) {
 template <int R>
 static cudaError_t launchSearchR(const SearchParams& p, cudaStream_t s) {
     constexpr int T = 8 + 2 * R, D = 2 * R + 1;
-    return launchPdl(k_search_r<R>, dim3(divUp(p.bw * p.bh, 4)), dim3(128), (size_t)4 * (2 * T * T + D * D) * sizeof(float), s, p);
+    const dim3 grid(divUp(p.bw * p.bh, 4));
+    const size_t smem = (size_t)4 * (2 * T * T + D * D) * sizeof(float);
+    if (p.bw * p.bh <= kSearchLatBlocks) return launchPdl(k_search_r<R, true>, grid, dim3(128), smem, s, p);
+    return launchPdl(k_search_r<R, false>, grid, dim3(128), smem, s, p);
 }
 cudaError_t launchSearch(const SearchParams& p, cudaStream_t s) {
     switch (p.R) {
@@ -1184,6 +1308,9 @@ cudaError_t launchSearch(const SearchParams& p, cudaStream_t s) {
     }
 }
 cudaError_t launchMedian3(const Median3Params& p, cudaStream_t s) {
+    const int nb = 2 * p.B + 1;
+    if (p.doHist && p.bw * p.bh <= kMed1Blocks && nb <= kMed1MaxBins)
+        return launchPdl(k_median3_one, dim3(1), dim3(kMed1Threads), (size_t)2 * nb * 4, s, p);
     return launchPdl(k_median3, dim3(divUp(p.bw * p.bh, 256)), dim3(256), 0, s, p);
 }
 static size_t planBytes(const CutPlan& c) {
@@ -1192,6 +1319,8 @@ static size_t planBytes(const CutPlan& c) {
 }
 cudaError_t prepareKernels() {
     cudaError_t e = cudaFuncSetAttribute(k_subpix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_median3_one, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMed1MaxBins * 4);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cutmean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(synthSmemBytes(1) + kSyWarpBytes));
