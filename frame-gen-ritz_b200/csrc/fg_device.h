@@ -62,6 +62,11 @@ __device__ __forceinline__ int gray8(uint32_t px, int ri, int gi, int bi) {
     const int r = (px >> (8 * ri)) & 255, g = (px >> (8 * gi)) & 255, b = (px >> (8 * bi)) & 255;
     return (b * 3735 + g * 19235 + r * 9798 + 16384) >> 15;
 }
+// the same with the weights in 16-bit lanes for the two-way dot products (byte 0, byte 1) and (byte 2, byte 3) of a
+// pixel: wlo = w(byte 0) | w(byte 1) << 16, whi = w(byte 2) (byte 3, alpha, weighs 0); exact integer arithmetic
+__device__ __forceinline__ int gray8dp(uint32_t px, uint32_t wlo, uint32_t whi) {
+    return (int)(__dp2a_hi(whi, px, __dp2a_lo(wlo, px, 16384u)) >> 15);
+}
 
 // Paired fp32 multiply / add (two IEEE operations per instruction). The compiler may fuse a paired multiply and add into
 // one paired FMA whatever rounding is asked for, so these are used only where every product and sum is exact (dyadic

@@ -26,16 +26,18 @@ __global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
         // flowScale 2, 16-byte aligned rows, a full tile: thread = 4 frame pixels (one uint4) x 2 rows = 2 level-0
         // pixels; a warp reads 2 x 256 contiguous bytes per frame and row pair
         const int cg = threadIdx.x & 15, rp = threadIdx.x >> 4;
+        // luma weights by byte position for the dot-product form (G is byte 1 in both orders)
+        const uint32_t wlo = (p.ri == 0 ? 9798u : 3735u) | (19235u << 16), whi = p.ri == 0 ? 3735u : 9798u;
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             const int ly = rp + 16 * j, y = ty0 + ly;
             const size_t o0 = (size_t)(2 * y) * p.pitch + (size_t)(2 * tx0 + 4 * cg) * 4;
             const uint4 a0 = __ldg(reinterpret_cast<const uint4*>(p.a + o0)), a1 = __ldg(reinterpret_cast<const uint4*>(p.a + o0 + p.pitch));
             const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(p.c + o0)), c1 = __ldg(reinterpret_cast<const uint4*>(p.c + o0 + p.pitch));
-            const int sa0 = gray8(a0.x, p.ri, p.gi, p.bi) + gray8(a0.y, p.ri, p.gi, p.bi) + gray8(a1.x, p.ri, p.gi, p.bi) + gray8(a1.y, p.ri, p.gi, p.bi);
-            const int sa1 = gray8(a0.z, p.ri, p.gi, p.bi) + gray8(a0.w, p.ri, p.gi, p.bi) + gray8(a1.z, p.ri, p.gi, p.bi) + gray8(a1.w, p.ri, p.gi, p.bi);
-            const int sc0 = gray8(c0.x, p.ri, p.gi, p.bi) + gray8(c0.y, p.ri, p.gi, p.bi) + gray8(c1.x, p.ri, p.gi, p.bi) + gray8(c1.y, p.ri, p.gi, p.bi);
-            const int sc1 = gray8(c0.z, p.ri, p.gi, p.bi) + gray8(c0.w, p.ri, p.gi, p.bi) + gray8(c1.z, p.ri, p.gi, p.bi) + gray8(c1.w, p.ri, p.gi, p.bi);
+            const int sa0 = gray8dp(a0.x, wlo, whi) + gray8dp(a0.y, wlo, whi) + gray8dp(a1.x, wlo, whi) + gray8dp(a1.y, wlo, whi);
+            const int sa1 = gray8dp(a0.z, wlo, whi) + gray8dp(a0.w, wlo, whi) + gray8dp(a1.z, wlo, whi) + gray8dp(a1.w, wlo, whi);
+            const int sc0 = gray8dp(c0.x, wlo, whi) + gray8dp(c0.y, wlo, whi) + gray8dp(c1.x, wlo, whi) + gray8dp(c1.y, wlo, whi);
+            const int sc1 = gray8dp(c0.z, wlo, whi) + gray8dp(c0.w, wlo, whi) + gray8dp(c1.z, wlo, whi) + gray8dp(c1.w, wlo, whi);
             // sum * 0.25 (integer sums of 4 lumas: exact)
             const float2 va = make_float2(i2f(sa0) * 0.25f, i2f(sa1) * 0.25f), vc = make_float2(i2f(sc0) * 0.25f, i2f(sc1) * 0.25f);
             *reinterpret_cast<float2*>(p.la[0] + (size_t)y * fw + tx0 + 2 * cg) = va;
@@ -692,10 +694,26 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
         const int bx = b % p.bw, by = b / p.bw, b0x = bx * kBlock, b0y = by * kBlock;
         const float2 v0 = p.in[b];
         const int sx = __float2int_rn(v0.x), sy = __float2int_rn(v0.y);
-        for (int i = lane; i < kSubT * kSubT; i += 32) {
-            const int x = i % kSubT, y = i / kSubT;
-            tA[i] = Lc(p.la, p.w, p.h, b0x - sx - kSubO + x, b0y - sy - kSubO + y);
-            tC[i] = Lc(p.lc, p.w, p.h, b0x + sx - kSubO + x, b0y + sy - kSubO + y);
+        const int ax0 = b0x - sx - kSubO, ay0 = b0y - sy - kSubO, cx0 = b0x + sx - kSubO, cy0 = b0y + sy - kSubO;
+        if (ax0 >= 0 && ay0 >= 0 && ax0 + kSubT <= p.w && ay0 + kSubT <= p.h && cx0 >= 0 && cy0 >= 0 &&
+            cx0 + kSubT <= p.w && cy0 + kSubT <= p.h) {   // both windows inside the level: no clamps
+            const float* ra = p.la + (size_t)ay0 * p.w + ax0;
+            const float* rc = p.lc + (size_t)cy0 * p.w + cx0;
+#pragma unroll
+            for (int j = 0; j < (kSubT * kSubT + 31) / 32; j++) {
+                const int i = lane + 32 * j;
+                if (i < kSubT * kSubT) {
+                    const int x = i % kSubT, y = i / kSubT;
+                    tA[i] = __ldg(ra + y * p.w + x);
+                    tC[i] = __ldg(rc + y * p.w + x);
+                }
+            }
+        } else {
+            for (int i = lane; i < kSubT * kSubT; i += 32) {
+                const int x = i % kSubT, y = i / kSubT;
+                tA[i] = Lc(p.la, p.w, p.h, ax0 + x, ay0 + y);
+                tC[i] = Lc(p.lc, p.w, p.h, cx0 + x, cy0 + y);
+            }
         }
         __syncwarp();
         // lane constants: lattice column u = 3 x + (d + 1) (lanes 24..31 only help with the reductions)
