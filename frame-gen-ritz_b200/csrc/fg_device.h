@@ -137,9 +137,11 @@ __device__ __forceinline__ void lumaTower(const LumaPyrParams& p, float (*sl)[kT
 }
 
 // ============================================================================================== synthesis tile
-constexpr int kSyE = 128, kSyEH = 32, kSyAp = 3;                 // 128 x 32 mismatch region -> 122 x 26 output tile
+// 64 x 64 mismatch region -> 58 x 58 output tile: the square tile recomputes the least halo (1.22 region pixels per
+// output pixel, against 1.29 for 128 x 32) within the shared memory of 3 CTAs per SM
+constexpr int kSyE = 64, kSyEH = 64, kSyAp = 3;
 constexpr int kSyT = kSyE - 2 * kSyAp, kSyTH = kSyEH - 2 * kSyAp;
-constexpr int kSyThreads = 512, kSyK = kSyEH / (kSyThreads / kSyE);   // region rows per thread (512 = 128 columns x 4)
+constexpr int kSyThreads = 512, kSyK = kSyEH / (kSyThreads / kSyE);   // region rows per thread (512 = 64 columns x 8)
 constexpr size_t kSyWarpBytes = (size_t)2 * kSyTH * kSyE * 4;   // k_synth: both warps of the output rows, after the row sums
 // row strides of the mismatch plane e (bytes) and of its horizontal 7-sums (uint16): one word of padding per row, so
 // that the lanes of a warp can walk 32 different rows of one column group without bank conflicts

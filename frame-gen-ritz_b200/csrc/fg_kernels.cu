@@ -1075,7 +1075,7 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
         e[ey * kSyES + ex] = (uint8_t)m;
     }
     __syncthreads();
-    // 3. horizontal 7-sums: one region row and 16 output columns per thread, a running window
+    // 3. horizontal 7-sums: one region row and 8 output columns per thread, a running window
     syRowSums(e, hsum, tid);
     __syncthreads();
     // 4. this thread's output pixels: vertical 7-sum, trust, blend, store
