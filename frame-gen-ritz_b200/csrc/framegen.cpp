@@ -866,9 +866,10 @@ bool Interpolator::debugMapLayout(DebugMapLayout& l) const {
     if (!m || !m->W) return false;
     l.W = m->W; l.H = m->H; l.fw = m->L.fw; l.fh = m->L.fh;
     l.bw = m->L.lv[0].bw; l.bh = m->L.lv[0].bh; l.fscale = m->set.flowScale; l.eStride = (m->W + 3) / 4;
+    // contiguous, as gpu/framegen.cpp:2096-2099 lays it out: the bytes after an fgmaps header (gpu/fgtest.cpp:777-789)
     l.blockOff = 0;
-    l.pixOff = alignUp((uint64_t)l.bw * l.bh * 8, 256);
-    l.eOff = alignUp(l.pixOff + (uint64_t)l.fw * l.fh * 8, 256);
+    l.pixOff = (uint64_t)l.bw * l.bh * 8;
+    l.eOff = l.pixOff + (uint64_t)l.fw * l.fh * 8;
     l.size = l.eOff + (uint64_t)l.eStride * 4 * l.H;
     return true;
 }

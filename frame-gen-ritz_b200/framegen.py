@@ -355,6 +355,57 @@ class Interpolator:
         return None if v == 0xFFFFFFFF else v
 
 
+# ---------------------------------------------------------------------------------------------- debug wire formats
+# What the reference's test harness writes for its tooling (gpu/fgtest.cpp:25-33, 777-789; read by gpu/fgmaps.py and
+# bench/score): an .fgmaps file = a 64-byte header then Interpolator::recordDebugMaps' bytes, and one STATS line per
+# pair = recordDebugCounters' two counts with the block count and the pixel count.
+FGMAPS_MAGIC, FGMAPS_VERSION = 0x504D4746, 5   # 'FGMP'
+
+
+def fgmaps_header(layout, settings):
+    """the 64-byte fgmaps header: uint32 magic, version, W, H, fw, fh, bw, bh, fscale, eStride, float32 trustLow,
+    trustHigh, smoothBonus, hudBonus, uint32 motionVersion, v2Mode (0 here: V1 has no mode)"""
+    h = np.zeros(16, np.uint32)
+    h[:10] = [FGMAPS_MAGIC, FGMAPS_VERSION, layout.W, layout.H, layout.fw, layout.fh, layout.bw, layout.bh,
+              layout.fscale, layout.eStride]
+    h[10:14] = np.array([settings.trustLow, settings.trustHigh, settings.smoothBonus, settings.hudBonus],
+                        np.float32).view(np.uint32)
+    h[14] = settings.motionVersion
+    return h.tobytes()
+
+
+def fgmaps_bytes(fg, stream=None):
+    """an fgmaps file's bytes for the latest records of Interpolator fg (header + recordDebugMaps: the block field,
+    the per-pixel half-vector field, the packed mismatch of the latest synth recorded with setDebugCapture on)"""
+    import torch
+    l = fg.debug_map_layout()
+    if l is None:
+        raise RuntimeError("not initialised")
+    buf = torch.zeros(int(l.size), dtype=torch.uint8, device="cuda")
+    if not fg.record_debug_maps(buf, stream=stream):
+        raise RuntimeError("recordDebugMaps failed")
+    (stream or torch.cuda.current_stream()).synchronize()
+    return fgmaps_header(l, fg.settings()) + buf.cpu().numpy().tobytes()
+
+
+def write_fgmaps(fg, path, stream=None):
+    with open(path, "wb") as f:
+        f.write(fgmaps_bytes(fg, stream))
+
+
+def stats_line(fg, pair, stream=None):
+    """'STATS <pair> <untrusted px> <SAD sum x256> <SAD blocks> <W*H>': the whole-frame decision inputs of the latest
+    synth (recordDebugCounters), as the reference harness prints them for its scoring scripts"""
+    import torch
+    cnt = torch.zeros(2, dtype=torch.int32, device="cuda")
+    if not fg.record_debug_counters(cnt, stream=stream):
+        raise RuntimeError("recordDebugCounters failed")
+    (stream or torch.cuda.current_stream()).synchronize()
+    u, s = (int(v) & 0xFFFFFFFF for v in cnt.cpu().tolist())
+    l = fg.debug_map_layout()
+    return f"STATS {pair} {u} {s} {fg.debug_sad_blocks()} {l.W * l.H}"
+
+
 def read_trace(fg, stream=None):
     """Copy the latest estimate's intermediates to the host: a dict in the oracle's trace layout."""
     import torch
