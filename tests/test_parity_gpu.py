@@ -116,6 +116,16 @@ def test_4k_pair():
     check_against_oracle(p, c, [0.25, 0.5, 0.75])
 
 
+def test_8k_pair():
+    """7680x4320: six pyramid levels, the multi-CTA median3 on levels 2 and 1, the widest histograms (+-372 bins)"""
+    import workloads_gpu   # the CPU generator takes minutes at this size; the GPU one the same kind of content
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(8000)
+    d = workloads_gpu.flow_batch(1, 7680, 4320, gen)
+    p, c = d["prev"][0].cpu().numpy(), d["curr"][0].cpu().numpy()
+    check_against_oracle(p, c, [0.25, 0.5])
+
+
 def test_hard_cut_and_repeat_determinism():
     """A scene cut then a normal pair on the same interpolator: state resets between estimates (histograms,
     counters), and the same pair twice gives identical bytes."""
