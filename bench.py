@@ -45,6 +45,9 @@ def args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--pool", type=int, default=8, help="distinct 4K pairs cycled through (8 x 66 MB > L2)")
     ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--copy-streams", type=int, default=1,
+                    help="e2e: streams per copy direction, each frame split into that many row bands (on a B200 one "
+                         "stream already fills the PCIe link: 1.96 ms per pair with 1, 2.00-2.02 with 2-4)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--eager", type=int, default=0,
@@ -408,43 +411,55 @@ def main():
     dA = [torch.empty_like(base_a) for _ in range(2)]
     dC = [torch.empty_like(base_c) for _ in range(2)]
     douts = [[torch.empty_like(base_a) for _ in TS] for _ in range(2)]
-    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-    ev_in, ev_done, ev_out = ([torch.cuda.Event() for _ in range(2)] for _ in range(3))
+    nc = max(1, a.copy_streams)
+    s_in = [torch.cuda.Stream() for _ in range(nc)]
+    s_out = [torch.cuda.Stream() for _ in range(nc)]
+    ev_in = [[torch.cuda.Event() for _ in range(nc)] for _ in range(2)]
+    ev_out = [[torch.cuda.Event() for _ in range(nc)] for _ in range(2)]
+    ev_done = [torch.cuda.Event() for _ in range(2)]
+    bands = [(H4K * j // nc, H4K * (j + 1) // nc) for j in range(nc)]   # row bands, one per copy stream
     step_no = [0]
 
     def e2e_step():
         i = step_no[0]
         step_no[0] += 1
         k = i % 2
-        with torch.cuda.stream(s_in):
+        for j, (r0, r1) in enumerate(bands):
+            with torch.cuda.stream(s_in[j]):
+                if i >= 2:
+                    s_in[j].wait_event(ev_done[k])   # step i-2's compute has read these inputs
+                dA[k][r0:r1].copy_(ha[r0:r1], non_blocking=True)
+                dC[k][r0:r1].copy_(hc[r0:r1], non_blocking=True)
+                ev_in[k][j].record(s_in[j])
+            stream.wait_event(ev_in[k][j])
             if i >= 2:
-                s_in.wait_event(ev_done[k])   # step i-2's compute has read these inputs
-            dA[k].copy_(ha, non_blocking=True)
-            dC[k].copy_(hc, non_blocking=True)
-            ev_in[k].record(s_in)
-        stream.wait_event(ev_in[k])
-        if i >= 2:
-            stream.wait_event(ev_out[k])      # step i-2's outputs have left the device
+                stream.wait_event(ev_out[k][j])      # step i-2's outputs have left the device
         I.begin_frame()
         assert I.record_estimate(dA[k], dC[k], stream=stream)
         for o, t in zip(douts[k], TS):
             assert I.record_synth(dA[k], dC[k], o, t, stream=stream)
         ev_done[k].record(stream)
-        with torch.cuda.stream(s_out):
-            s_out.wait_event(ev_done[k])
-            for o, h in zip(douts[k], hout[k]):
-                h.copy_(o, non_blocking=True)
-            ev_out[k].record(s_out)
+        for j, (r0, r1) in enumerate(bands):
+            with torch.cuda.stream(s_out[j]):
+                s_out[j].wait_event(ev_done[k])
+                for o, h in zip(douts[k], hout[k]):
+                    h[r0:r1].copy_(o[r0:r1], non_blocking=True)
+                ev_out[k][j].record(s_out[j])
 
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ev0.record(s_in)
+    ev0.record(s_in[0])
+    for j in range(1, nc):
+        s_in[j].wait_event(ev0)
     for _ in range(a.e2e_steps):
         e2e_step()
-    ev1.record(s_out)
+    last_k = (step_no[0] - 1) % 2
+    for j in range(1, nc):
+        s_out[0].wait_event(ev_out[last_k][j])
+    ev1.record(s_out[0])
     torch.cuda.synchronize()
     e2e_ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
     e2e_value = e2e_ms / (a.e2e_steps * world)
