@@ -708,6 +708,9 @@ void Interpolator::beginFrame() {
     if (m) m->estSets = m->synthSets = 0;
 }
 
+void Interpolator::releaseUnusedUi() {}       // no UI-protection memory is ever held
+void Interpolator::releaseUnusedMotion() {}   // V1 is the only motion version
+
 bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
     if (!m || !m->W) return false;
     if (!m->frameOk(prev) || !m->frameOk(curr) || !m->samePitch(prev, curr)) return false;
@@ -1255,6 +1258,12 @@ void fg_get_settings(const fg_interpolator* fg, fg_settings* s) {
 }
 void fg_begin_frame(fg_interpolator* fg) {
     if (fg) fg->I.beginFrame();
+}
+void fg_release_unused_ui(fg_interpolator* fg) {
+    if (fg) fg->I.releaseUnusedUi();
+}
+void fg_release_unused_motion(fg_interpolator* fg) {
+    if (fg) fg->I.releaseUnusedMotion();
 }
 int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr) {
     return fg && prev && curr && fg->I.recordEstimate((cudaStream_t)stream, fromC(prev), fromC(curr));

@@ -85,6 +85,8 @@ SIGNATURES = {
     "fg_reconfigure": (_I, [_P, ctypes.POINTER(CSettings)]),
     "fg_get_settings": (None, [_P, ctypes.POINTER(CSettings)]),
     "fg_begin_frame": (None, [_P]),
+    "fg_release_unused_ui": (None, [_P]),
+    "fg_release_unused_motion": (None, [_P]),
     "fg_record_estimate": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame)]),
     "fg_record_synth": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
     "fg_record": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
@@ -279,6 +281,12 @@ class Interpolator:
 
     def begin_frame(self):
         lib().fg_begin_frame(self._h)
+
+    def release_unused_ui(self):
+        lib().fg_release_unused_ui(self._h)
+
+    def release_unused_motion(self):
+        lib().fg_release_unused_motion(self._h)
 
     def record_estimate(self, prev, curr, stream=None):
         return bool(lib().fg_record_estimate(self._h, _stream(stream), ctypes.byref(frame_of(prev)),

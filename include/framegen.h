@@ -120,6 +120,11 @@ public:
 
     // gpu/framegen.h:511: resets the per-submission record counts (kSetRing each)
     void beginFrame();
+    // gpu/framegen.h:693, 700: free the resources of UI-protection depths / motion versions no longer selected. This
+    // build holds only V1 and no UI-protection memory, so there is never anything unused: both are no-ops, kept so a
+    // host that calls them periodically links unchanged.
+    void releaseUnusedUi();
+    void releaseUnusedMotion();
 
     // gpu/framegen.h:549-551: passes 1-8 once per real pair, passes 9-11 per generated time t in (0, 1), or both.
     // false (and nothing recorded, out untouched) if not initialised, t outside (0, 1), a ring overflow since

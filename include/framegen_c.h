@@ -81,6 +81,8 @@ int fg_reconfigure(fg_interpolator* fg, const fg_settings* s);                  
 void fg_get_settings(const fg_interpolator* fg, fg_settings* s);                    /* gpu/framegen.h:507 */
 
 void fg_begin_frame(fg_interpolator* fg);                                           /* gpu/framegen.h:511 */
+void fg_release_unused_ui(fg_interpolator* fg);                                     /* gpu/framegen.h:693 (no-op here) */
+void fg_release_unused_motion(fg_interpolator* fg);                                 /* gpu/framegen.h:700 (no-op here) */
 int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr);   /* :549 */
 int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
                     const fg_frame* out, float t);                                                        /* :550 */

@@ -97,4 +97,6 @@ def test_init_refusals_without_recording():
     assert I.size_error(64, 64) == "not initialised"
     assert I.read_timings() is None
     assert I.read_costs() is None
+    I.release_unused_ui()        # gpu/framegen.h:693, 700: nothing is ever unused here (V1 only, no UI memory)
+    I.release_unused_motion()
     I.close()
