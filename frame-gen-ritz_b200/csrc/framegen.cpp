@@ -592,7 +592,18 @@ bool Interpolator::validate(const Settings& s) {
            s.pyramidMinSide >= 16 && s.pyramidMinSide <= 256 &&
            (uint32_t)s.uiProtection <= (uint32_t)UiProtection::CrosshairV2 &&
            (uint32_t)s.motionVersion <= (uint32_t)MotionVersion::V3 && s.blurSamples <= kBlurMaxSamples &&
-           (uint32_t)s.blurWeights <= (uint32_t)BlurWeights::Gaussian;
+           (uint32_t)s.blurWeights <= (uint32_t)BlurWeights::Gaussian &&
+           // the other versions' and UI protection's fields, with the reference's ranges (gpu/framegen.cpp:1688-1699)
+           (uint32_t)s.v2Mode <= (uint32_t)V2Mode::Performance && (uint32_t)s.v3Guard <= (uint32_t)V3Guard::V2Motion &&
+           (uint32_t)s.learnedNet < kLearnedNets && in(s.v3Smear, 0.0f, 1.0f) && in(s.v3OcclSoft, 0.25f, 4.0f) &&
+           in(s.v3Unsure, 0.25f, 4.0f) && in(s.v3SceneCut, 0.0f, 4.0f) && in(s.uiCrosshairArea, 0.0f, 1.0f) &&
+           s.uiCrosshairArea > 0.0f && in(s.uiBoxHeightFrac, 0.0f, 1.0f) && s.uiBoxWidth <= 16384 &&
+           s.uiBoxHeight <= 16384 && s.uiBoxOffsetX >= -16384 && s.uiBoxOffsetX <= 16384 && s.uiBoxOffsetY >= -16384 &&
+           s.uiBoxOffsetY <= 16384 && s.uiStillFrames >= 1 && s.uiStillFrames <= 255 &&
+           in(s.uiStillThreshold, 0.0f, 255.0f) && s.uiInpaintReach >= 1 && s.uiInpaintReach <= 16 &&
+           in(s.uiMaxStillFraction, 0.0f, 1.0f) && s.uiMaxStillFraction > 0.0f && in(s.uiContrastThreshold, 0.0f, 255.0f) &&
+           s.uiLeaveFrames >= 1 && s.uiLeaveFrames <= 255 && s.uiReentryFrames <= 255 && s.uiHistory >= 3 &&
+           s.uiHistory <= 65;
 }
 
 const char* Interpolator::settingsError(const Settings& s, Format f) {

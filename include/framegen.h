@@ -27,6 +27,12 @@ namespace framegen {
 enum class UiProtection : uint32_t { Off = 0, Crosshair = 1, WholeScreen = 2, CrosshairV2 = 3 };
 // gpu/framegen.h:28-59 (V1 is the only version this library runs)
 enum class MotionVersion : uint32_t { V1 = 0, V2 = 1, Learned = 2, V3 = 3 };
+// gpu/framegen.h:63-92 (the Learned version's nets: accepted, unused here)
+enum class LearnedNet : uint32_t { E2v3 = 0, E1v3 = 1, E2v4 = 2, E1v4 = 3, E2v5 = 4, E1v5 = 5, G2v2 = 6, G2v3 = 7, M2v2 = 8, M2v3 = 9 };
+constexpr uint32_t kLearnedNets = 10;
+// gpu/framegen.h:99-108, 115-121 (V2 / V3 options: accepted, unused here)
+enum class V2Mode : uint32_t { Quality = 0, Performance = 1 };
+enum class V3Guard : uint32_t { Off = 0, Guard = 1, V2Motion = 2 };
 // gpu/framegen.h:125-129
 enum class BlurWeights : uint32_t { Even = 0, Gaussian = 1 };
 // gpu/framegen.h:138
@@ -73,9 +79,37 @@ struct Settings {
     uint32_t searchRadiusTop = 6;   // [1, 12]
     bool subpixel = true;
     UiProtection uiProtection = UiProtection::Off;   // Off only
+    // the reference's UI-protection fields (gpu/framegen.h:196-300): validated with its ranges, unused here
+    uint32_t uiHistory = 3;                          // [3, 65]
+    float uiBoxHeightFrac = 0.025f;                  // [0, 1]
+    uint32_t uiBoxWidth = 0, uiBoxHeight = 0;        // [0, 16384]
+    float uiCrosshairArea = 0.03f;                   // (0, 1]
+    int32_t uiBoxOffsetX = 0, uiBoxOffsetY = 0;      // [-16384, 16384]
+    uint32_t uiStillFrames = 8;                      // [1, 255]
+    float uiStillThreshold = 3.5f;                   // [0, 255]
+    uint32_t uiInpaintReach = 12;                    // [1, 16]
+    float uiMaxStillFraction = 0.75f;                // (0, 1]
+    float uiContrastThreshold = 20.0f;               // [0, 255]
+    uint32_t uiLeaveFrames = 4;                      // [1, 255]
+    uint32_t uiReentryFrames = 2;                    // [0, 255]
+    bool uiEstimateFill = false;
     uint32_t blurSamples = 0;                        // [0, 16]: recordSynthBlur's sub-frames (< 2: blur off)
     BlurWeights blurWeights = BlurWeights::Gaussian;
     MotionVersion motionVersion = MotionVersion::V1; // V1 only
+    // the other versions' fields (gpu/framegen.h:310-380): validated with the reference's ranges, unused here
+    V2Mode v2Mode = V2Mode::Quality;
+    bool v2StaticMask = true;
+    float v3Smear = 0.35f;                           // [0, 1]
+    float v3OcclSoft = 1.0f;                         // [0.25, 4]
+    float v3Unsure = 1.0f;                           // [0.25, 4]
+    float v3SceneCut = 0.0f;                         // [0, 4]
+    bool v3ColourWindow = false;
+    bool v3DetailSplit = false;
+    V3Guard v3Guard = V3Guard::Off;
+    LearnedNet learnedNet = LearnedNet::E2v5;
+    bool learnedHalf = false;
+    bool learnedZeroTest = true;
+    bool learnedStaticGuard = false;
     // structural: init() or reconfigure()
     uint32_t flowScale = 2;         // 1, 2, 4
     uint32_t pyramidMinSide = 48;   // [16, 256]
