@@ -6,6 +6,9 @@ low-frequency noise scaled to max |v| = 24 px, prev = T, curr(p) = T(p - v(p)) b
 replicate), the ground truth at t = T(p - t v(p)); 5 % of pairs are scene cuts (curr an independent texture) and 5 %
 have 20 % of curr's area replaced by fresh noise. Random streams are torch's (seeded per batch), not numpy's, so the
 pairs are statistically like workloads.flow_pair's, not bit-identical to them.
+
+hdr_pair makes config 2's RgbaF16 linear-light pairs (log-uniform channels, a pan and rigid sprites) at 4K, which the
+numpy generators would take minutes for.
 """
 import math
 
@@ -84,3 +87,36 @@ def flow_batch(B, W, H, gen, ts=(), vmax=24.0, cut_frac=0.05, fresh_frac=0.05, d
             x0 = int(torch.randint(0, W - fw + 1, (1,), generator=gen, device=device))
             curr[b, y0:y0 + fh, x0:x0 + fw] = torch.rand(fh, fw, 3, generator=gen, device=device)
     return {"prev": to_rgba(tex), "curr": to_rgba(curr), "v": v, "kind": kind, "truth": truth}
+
+
+def hdr_pair(W, H, gen, pan=16.0, sprites=3, smin=128, smax=384, smove=32.0, device="cuda"):
+    """A config-2 pair: RgbaF16 linear light (scRGB), prev / curr (H, W, 4) float16 on the device, alpha 1. Each
+    channel is log-uniform in 1e-3..10 with 4-octave spatial correlation, 10^(-3 + 4 u) with u 4-octave value noise
+    normalised to [0, 1]; the background pans by a uniform (+-pan, +-pan) px and `sprites` rigid squares of side
+    smin..smax px (their own textures) move by up to +-smove px, composited over the background in both frames."""
+    def rnd(lo, hi):
+        return float(lo + (hi - lo) * torch.rand(1, generator=gen, device=device))
+
+    bg = value_noise(1, H + 2 * int(pan) + 2, W + 2 * int(pan) + 2, gen, octaves=4, base=128.0, device=device)[0]
+    dx, dy = rnd(-pan, pan), rnd(-pan, pan)
+    ys, xs = torch.meshgrid(torch.arange(H, device=device, dtype=torch.float32),
+                            torch.arange(W, device=device, dtype=torch.float32), indexing="ij")
+    o = float(int(pan) + 1)
+    prev = _bilinear(bg[None], (xs + o)[None], (ys + o)[None])[0]
+    curr = _bilinear(bg[None], (xs + o - dx)[None], (ys + o - dy)[None])[0]
+    for _ in range(sprites):
+        s = int(rnd(smin, smax))
+        tex = value_noise(1, s, s, gen, octaves=4, base=s / 4.0, device=device)
+        x0, y0 = rnd(0, W - s), rnd(0, H - s)
+        mx, my = rnd(-smove, smove), rnd(-smove, smove)
+        for img, (ox, oy) in ((prev, (x0, y0)), (curr, (x0 + mx, y0 + my))):
+            u, v = xs - ox, ys - oy
+            inside = (u >= 0) & (u <= s - 1) & (v >= 0) & (v <= s - 1)
+            val = _bilinear(tex, u.clamp(0, s - 1)[None], v.clamp(0, s - 1)[None])[0]
+            img[inside] = val[inside]
+
+    def lin(u):
+        rgb = torch.pow(10.0, -3.0 + 4.0 * u)
+        return torch.cat([rgb, torch.ones_like(rgb[..., :1])], dim=-1).to(torch.float16)
+
+    return lin(prev), lin(curr)

@@ -107,8 +107,12 @@ def sample_diff(name, got, ref, spec):
 
 
 def check(name, prev8, curr8, ts, settings=None, pad=0):
-    _, vk, spec, conv, extra = SPEC[name]
-    a, c = conv(prev8), conv(curr8)
+    conv = SPEC[name][3]
+    check_frames(name, conv(prev8), conv(curr8), ts, settings, pad)
+
+
+def check_frames(name, a, c, ts, settings=None, pad=0):
+    _, vk, spec, _, extra = SPEC[name]
     W, H = oracle.frame_size(a, spec)
     s = settings or oracle.Settings()
     fs = fg.Settings(**{k: getattr(s, k) for k in oracle.Settings.__dataclass_fields__})
@@ -174,6 +178,17 @@ def test_format_1080p(name):
     """1080p: four pyramid levels, the 2^-10 rounding of the coarse levels in play"""
     p, c, _ = workloads.flow_pair(1920, 1080, seed=21)
     check(name, p, c, [0.5, 0.25])
+
+
+def test_config2_4k_hdr():
+    """Config 2: 3840x2160 RgbaF16 linear scRGB (80 nits), t = 1/3 and 2/3; every channel log-uniform in 1e-3..10 with
+    4-octave correlation, a global pan of up to +-16 px and 3 rigid sprites of 128-384 px moving up to +-32 px
+    (workloads_gpu.hdr_pair, generated on the device)"""
+    import workloads_gpu
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(2 * 10 ** 6)
+    a, c = (x.cpu().numpy() for x in workloads_gpu.hdr_pair(3840, 2160, gen))
+    check_frames("f16_linear", a, c, [float(np.float32(1 / 3)), T23])
 
 
 def test_format_refusals():
