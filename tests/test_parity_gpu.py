@@ -116,6 +116,22 @@ def test_4k_pair():
     check_against_oracle(p, c, [0.25, 0.5, 0.75])
 
 
+@pytest.mark.parametrize("n,W,H", [(96, 640, 360), (24, 1920, 1080)])
+def test_config1_many_pairs(n, W, H):
+    """Config 1's kind of sequence, many pairs: smooth flows with scene cuts and fresh content mixed in (15 % each
+    here, so that every batch has some), each pair checked stage by stage and at t = 1/4, 1/2, 3/4"""
+    import workloads_gpu
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(10 ** 6 + n)
+    d = workloads_gpu.flow_batch(n, W, H, gen, cut_frac=0.15, fresh_frac=0.15)
+    kinds = d["kind"].tolist()
+    for i in range(n):
+        p, c = d["prev"][i].cpu().numpy(), d["curr"][i].cpu().numpy()
+        check_against_oracle(p, c, [0.25, 0.5, 0.75])
+    if n >= 24:
+        assert 1 in kinds and 2 in kinds and 0 in kinds, kinds
+
+
 def test_8k_pair():
     """7680x4320: six pyramid levels, the multi-CTA median3 on levels 2 and 1, the widest histograms (+-372 bins)"""
     import workloads_gpu   # the CPU generator takes minutes at this size; the GPU one the same kind of content
