@@ -141,13 +141,27 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """dram bytes per synth launch from the committed ncu summary (profiles/synth_4k.json), if present."""
+def ncu_synth():
+    """the committed ncu summary of one 4K synth launch (profiles/synth_4k.json): dram bytes, warp instructions"""
     try:
         with open(os.path.join(REPO, "profiles", "synth_4k.json")) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            return json.load(f)
     except (OSError, ValueError):
+        return {}
+
+
+def issue_roofline(prof, synth_us, clocks):
+    """the synth against the instruction-issue ceiling, the roofline that binds it: its ncu warp-instruction count
+    over its live duration, against one warp instruction per scheduler (4 per SM) per SM clock at the sampled clock"""
+    n, sms = prof.get("warp_instructions_per_launch"), prof.get("sms")
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+    if not n or not sms or not mhz or not synth_us:
         return None
+    achieved = n / (synth_us * 1e-6) / 1e12
+    peak = sms * 4 * mhz * 1e6 / 1e12
+    return {"kernel": "k_synth", "achieved": round(achieved, 4), "peak": round(peak, 4),
+            "unit": "T warp instructions/s", "frac": round(achieved / peak, 4), "warp_instructions": n,
+            "source": "ncu smsp__inst_executed of one 4K launch (profiles/synth_4k.json), live duration, sampled clock"}
 
 
 def run_reference(a):
@@ -481,7 +495,8 @@ def main():
 
     peak, peak_kind = measured_peak()
     achieved = SYNTH_BYTES / (synth_us * 1e-6) / 1e9
-    traffic = ncu_traffic()
+    prof = ncu_synth()
+    traffic = prof.get("dram_bytes_per_launch")
     del graphs
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": a.steps,
@@ -497,6 +512,7 @@ def main():
                 "roofline": {"bound": "hbm", "kernel": "k_synth", "achieved": round(achieved, 1),
                              "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                              "traffic": traffic, "algorithmic_bytes": SYNTH_BYTES, "duration_us": round(synth_us, 2)},
+                "issue_roofline": issue_roofline(prof, synth_us, clocks),
                 "breakdown_us": breakdown,
                 "gpu_launches": launches_per_step * a.steps,
                 "e2e": {"value": round(e2e_value, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 4 * W4K * H4K,
