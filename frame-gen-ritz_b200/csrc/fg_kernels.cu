@@ -8,6 +8,8 @@
 //     numpy's operation order with explicit round-to-nearest intrinsics (no contraction);
 //   - reductions whose rounding depends on order (the scene-cut mean) follow numpy's pairwise tree.
 // The whole library is compiled with -fmad=false as a second guard against contraction.
+#include <cooperative_groups.h>
+
 #include "fg_device.h"
 
 namespace fgk {
@@ -439,57 +441,52 @@ __global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
     for (int i = threadIdx.x; i < 2 * nb; i += 256) p.hist[i] = 0;
 }
 
-// k_median3 for a level small enough for one CTA (at most kMed1Blocks blocks; the histogram fits in shared memory):
-// the same medians and the same global median, with the histogram in shared memory and the order statistics read
-// off by the same CTA, so no global atomics, no fence and no last-block ticket stand in the estimate's critical path
-// (the coarse levels are latency bound).
+// One block of k_median3's work for the shared-memory forms below: the block's 3x3 medians (written to p.out), and
+// its own-parent weight added to the histogram hist (2 * nb bins in shared memory: x then y).
+__device__ __forceinline__ void med3Block(const Median3Params& p, int b, unsigned int* hist, int nb) {
+    const int bx = b % p.bw, by = b / p.bw;
+    float xs[9], ys[9];
+    int k = 0;
+#pragma unroll
+    for (int j = -1; j <= 1; j++)
+#pragma unroll
+        for (int i = -1; i <= 1; i++) {
+            const float2 v = p.in[clampi(by + j, 0, p.bh - 1) * p.bw + clampi(bx + i, 0, p.bw - 1)];
+            xs[k] = v.x;
+            ys[k] = v.y;
+            k++;
+        }
+    const float2 m = make_float2(med9(xs), med9(ys));
+    p.out[b] = m;
+    const int wx = bx < p.bw - 1 ? max(0, min(2, p.fbw - 2 * bx)) : max(0, p.fbw - 2 * bx);
+    const int wy = by < p.bh - 1 ? max(0, min(2, p.fbh - 2 * by)) : max(0, p.fbh - 2 * by);
+    const unsigned int wgt = (unsigned int)(wx * wy);
+    if (wgt) {
+        int ix = __float2int_rn(m.x) + p.B, iy = __float2int_rn(m.y) + p.B;
+        if (ix < 0 || ix > 2 * p.B || iy < 0 || iy > 2 * p.B) {
+            atomicOr(p.err, kErrHistRange);
+            ix = clampi(ix, 0, 2 * p.B);
+            iy = clampi(iy, 0, 2 * p.B);
+        }
+        atomicAdd(hist + ix, wgt);
+        atomicAdd(hist + nb + iy, wgt);
+    }
+}
+
 constexpr int kMed1Threads = 1024, kMed1Blocks = 2048, kMed1MaxBins = 4097;
-__global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Params p) {
-    pdlEnter();
-    extern __shared__ unsigned int hs1[];   // 2 * nb bins: x then y
+
+// The global median from a complete histogram in shared memory, by all kMed1Threads threads of the CTA: the order
+// statistics k1 = (N - 1) / 2, k2 = N / 2 of each axis (chunk sums, a block-wide scan, a walk of the chunk), written
+// as 2 x the median = v_k1 + v_k2 to p.medOut.
+__device__ __forceinline__ void medianFromHist(const Median3Params& p, const unsigned int* hist, int nb) {
     __shared__ unsigned int part[32];
     __shared__ int found[4];
-    const int nb = 2 * p.B + 1, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int i = tid; i < 2 * nb; i += kMed1Threads) hs1[i] = 0;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (tid < 4) found[tid] = 0;
-    __syncthreads();
-    const int n = p.bw * p.bh;
-#pragma unroll 2
-    for (int b = tid; b < n; b += kMed1Threads) {
-        const int bx = b % p.bw, by = b / p.bw;
-        float xs[9], ys[9];
-        int k = 0;
-#pragma unroll
-        for (int j = -1; j <= 1; j++)
-#pragma unroll
-            for (int i = -1; i <= 1; i++) {
-                const float2 v = p.in[clampi(by + j, 0, p.bh - 1) * p.bw + clampi(bx + i, 0, p.bw - 1)];
-                xs[k] = v.x;
-                ys[k] = v.y;
-                k++;
-            }
-        const float2 m = make_float2(med9(xs), med9(ys));
-        p.out[b] = m;
-        const int wx = bx < p.bw - 1 ? max(0, min(2, p.fbw - 2 * bx)) : max(0, p.fbw - 2 * bx);
-        const int wy = by < p.bh - 1 ? max(0, min(2, p.fbh - 2 * by)) : max(0, p.fbh - 2 * by);
-        const unsigned int wgt = (unsigned int)(wx * wy);
-        if (wgt) {
-            int ix = __float2int_rn(m.x) + p.B, iy = __float2int_rn(m.y) + p.B;
-            if (ix < 0 || ix > 2 * p.B || iy < 0 || iy > 2 * p.B) {
-                atomicOr(p.err, kErrHistRange);
-                ix = clampi(ix, 0, 2 * p.B);
-                iy = clampi(iy, 0, 2 * p.B);
-            }
-            atomicAdd(hs1 + ix, wgt);
-            atomicAdd(hs1 + nb + iy, wgt);
-        }
-    }
-    __syncthreads();
-    // order statistics k1 = (N - 1) / 2, k2 = N / 2 of each axis: chunk sums, a block-wide scan, a walk of the chunk
     const unsigned int N = (unsigned int)(p.fbw * p.fbh), ks[2] = {(N - 1) / 2, N / 2};
     const int per = (nb + kMed1Threads - 1) / kMed1Threads;
     for (int axis = 0; axis < 2; axis++) {
-        const unsigned int* h = hs1 + axis * nb;
+        const unsigned int* h = hist + axis * nb;
         const int s0 = tid * per, s1 = min(s0 + per, nb);
         unsigned int loc = 0;
         for (int i = s0; i < s1; i++) loc += h[i];
@@ -525,6 +522,54 @@ __global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Pa
         p.medOut[0] = (float)(found[0] + found[1]);
         p.medOut[1] = (float)(found[2] + found[3]);
     }
+}
+
+// k_median3 for a level small enough for one CTA (at most kMed1Blocks blocks; the histogram fits in shared memory):
+// the same medians and the same global median, with the histogram in shared memory and the order statistics read
+// off by the same CTA, so no global atomics, no fence and no last-block ticket stand in the estimate's critical path
+// (the coarse levels are latency bound).
+__global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Params p) {
+    pdlEnter();
+    extern __shared__ unsigned int hs1[];   // 2 * nb bins: x then y
+    const int nb = 2 * p.B + 1, tid = threadIdx.x;
+    for (int i = tid; i < 2 * nb; i += kMed1Threads) hs1[i] = 0;
+    __syncthreads();
+    const int n = p.bw * p.bh;
+#pragma unroll 2
+    for (int b = tid; b < n; b += kMed1Threads) med3Block(p, b, hs1, nb);
+    __syncthreads();
+    medianFromHist(p, hs1, nb);
+}
+
+// k_median3 for mid-size levels (at most kMedClBlocks blocks): a cluster of kMedCl CTAs, each with its own histogram
+// in shared memory; after the cluster barrier CTA 0 adds the others' histograms through distributed shared memory and
+// reads off the order statistics. No global atomics, no fence, no last-block ticket; the other CTAs stay resident
+// (a second cluster barrier) until CTA 0 has read their shared memory.
+constexpr int kMedCl = 8, kMedClBlocks = kMedCl * kMed1Threads * 2;
+__global__ void __cluster_dims__(kMedCl, 1, 1) __launch_bounds__(kMed1Threads, 1) k_median3_cluster(const Median3Params p) {
+    pdlEnter();
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ unsigned int hs1[];
+    const int nb = 2 * p.B + 1, tid = threadIdx.x;
+    const unsigned int rank = cl.block_rank();
+    for (int i = tid; i < 2 * nb; i += kMed1Threads) hs1[i] = 0;
+    __syncthreads();
+    const int n = p.bw * p.bh;
+#pragma unroll 2
+    for (int b = (int)rank * kMed1Threads + tid; b < n; b += kMedCl * kMed1Threads) med3Block(p, b, hs1, nb);
+    cl.sync();   // every CTA's histogram is complete
+    if (rank == 0) {
+        for (int i = tid; i < 2 * nb; i += kMed1Threads) {
+            unsigned int sum = hs1[i];
+#pragma unroll
+            for (int r = 1; r < kMedCl; r++) sum += cl.map_shared_rank(hs1, r)[i];
+            hs1[i] = sum;
+        }
+        __syncthreads();
+        medianFromHist(p, hs1, nb);
+    }
+    cl.sync();
 }
 
 // ============================================================================================== scene-cut mean
@@ -1329,6 +1374,8 @@ cudaError_t launchMedian3(const Median3Params& p, cudaStream_t s) {
     const int nb = 2 * p.B + 1;
     if (p.doHist && p.bw * p.bh <= kMed1Blocks && nb <= kMed1MaxBins)
         return launchPdl(k_median3_one, dim3(1), dim3(kMed1Threads), (size_t)2 * nb * 4, s, p);
+    if (p.doHist && p.bw * p.bh <= kMedClBlocks && nb <= kMed1MaxBins)
+        return launchPdl(k_median3_cluster, dim3(kMedCl), dim3(kMed1Threads), (size_t)2 * nb * 4, s, p);
     return launchPdl(k_median3, dim3(divUp(p.bw * p.bh, 256)), dim3(256), 0, s, p);
 }
 static size_t planBytes(const CutPlan& c) {
@@ -1339,6 +1386,8 @@ cudaError_t prepareKernels() {
     cudaError_t e = cudaFuncSetAttribute(k_subpix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_median3_one, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMed1MaxBins * 4);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_median3_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMed1MaxBins * 4);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cutmean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(synthSmemBytes(1) + kSyWarpBytes));
