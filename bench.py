@@ -198,7 +198,7 @@ def run_reference(a):
 def seed_net_arm(a, fg, pool, outs, stream, world, plain):
     """The CNN-seeded arm (Interpolator::setSeedNet at --seed-level, the trained weights): its graph-replayed ms per
     pair on the same pool as the plain path, and its PSNR against the plain path's on --psnr-pairs held-out 4K pairs
-    of the config-1 generator (ground truth at t = 1/4, 1/2, 3/4)."""
+    of the smooth-flow generator (ground truth at t = 1/4, 1/2, 3/4)."""
     import torch
     import torch.distributed as dist
     import replicas
@@ -255,7 +255,7 @@ def seed_net_arm(a, fg, pool, outs, stream, world, plain):
     return {"level": a.seed_level, "ms_per_pair": round(t_ms / (a.steps * world), 4),
             "psnr_db": round(float(np.mean(ps["cnn"])), 3), "plain_psnr_db": round(float(np.mean(ps["plain"])), 3),
             "psnr_delta_db": round(dp, 4), "within_0_1_db": abs(dp) <= 0.1, "psnr_frames": len(ps["cnn"]),
-            "data": "held-out config-1 pairs (workloads_gpu, seed 424242), 4K, ground truth at t = 1/4, 1/2, 3/4"}
+            "data": "held-out smooth-flow pairs (workloads_gpu, seed 424242), 4K, ground truth at t = 1/4, 1/2, 3/4"}
 
 
 def blur_arm(a, fg, pool, stream, world):

@@ -1,6 +1,6 @@
-"""Time the batched path on the config-3 workload: 64 frame pairs in one batch, sizes 1280x720 / 1920x1080 /
+"""Time the batched path on the mixed batch: 64 frame pairs in one batch, sizes 1280x720 / 1920x1080 /
 2560x1440 / 3840x2160 in ratio 8:4:2:1 (34 / 17 / 9 / 4), formats cycling Rgba8 / Rgb10 / Nv12 / P010, multipliers
-cycling 2 / 3 / 4, content from the config-1 generator (workloads_gpu, per-pair seeds).
+cycling 2 / 3 / 4, content from the smooth-flow generator (workloads_gpu, per-pair seeds).
 
     python frame-gen-ritz_b200/batch_bench.py [--reps 20]
     torchrun --nproc-per-node N --master-addr 127.0.0.1 frame-gen-ritz_b200/batch_bench.py
@@ -112,7 +112,7 @@ def main():
         frames, px = int(t[0]), int(t[1])
         dist.destroy_process_group()
     if rank == 0:
-        print(json.dumps({"workload": "config 3: 64 pairs, 34x720p / 17x1080p / 9x1440p / 4x2160p, Rgba8 / Rgb10 / "
+        print(json.dumps({"workload": "mixed batch: 64 pairs, 34x720p / 17x1080p / 9x1440p / 4x2160p, Rgba8 / Rgb10 / "
                                       "Nv12 / P010, 2x / 3x / 4x", "ranks": n, "generated_frames": frames,
                           "generated_megapixels": round(px / 1e6, 1), "ms_per_batch": res,
                           "shape_keys": "ctasPerSm_order_streams (ctasPerSm 0: one launch per synthesis)",

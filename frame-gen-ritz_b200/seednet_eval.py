@@ -1,4 +1,4 @@
-"""Evaluate the seed proposer: CNN-seeded against plain V1 on held-out config-1 pairs, against the ground truth.
+"""Evaluate the seed proposer: CNN-seeded against plain V1 on held-out smooth-flow pairs, against the ground truth.
 
     python frame-gen-ritz_b200/seednet_eval.py [--pairs 200] [--size 3840x2160] [--weights seednet_l1.bin] [--level 1]
 

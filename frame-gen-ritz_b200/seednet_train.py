@@ -8,7 +8,7 @@ batch of N x --batch), the ranks' gradients are summed by one all-reduce of the 
 in place in the net's gradient buffer, and the Adam step reads them times 1 / N (the mean gradient of the global
 batch); the ranks start from the same parameters and so stay identical. Rank 0 logs and writes the parameters.
 
-Data: 256x256 crops from the config-1 flow generator (workloads_gpu.flow_batch: smooth motion up to 24 px, 5 % scene
+Data: 256x256 crops from the smooth-flow generator (workloads_gpu.flow_batch: smooth motion up to 24 px, 5 % scene
 cuts, 5 % fresh content), 3125 steps x 64 crops = 200k crops, each crop new. Input: the crop pair's level-1 luma
 (64x64 at flowScale 2, the library's own luma pyramid, read back with recordTrace). Targets per 8x8 block of level 1:
   - candidate 1: the ground-truth half-vector, the block's mean of v / 8 (content displacement prev -> curr in

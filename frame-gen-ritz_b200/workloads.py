@@ -9,7 +9,7 @@ and motion statistics of the workloads the path is measured on:
                   low-frequency noise with |v| <= 24 px applied by bilinear backward warp; kind "cut" (two independent
                   textures) and "fresh" (20 % of the area replaced by fresh noise) exercise the fallbacks. Returns the
                   ground-truth frame at t as well (rendered from the same field).
-  flow_pair_seq   the 500-pair sequence of flow_pair with 5 % cuts and 5 % fresh pairs, seed = config * 10**6 + pair.
+  flow_pair_seq   the 500-pair sequence of flow_pair with 5 % cuts and 5 % fresh pairs, seed = stream * 10**6 + pair.
 
 Frames are (H, W, 4) uint8 in R,G,B,A order, alpha 255.
 """
@@ -109,14 +109,14 @@ def flow_pair(W=1920, H=1080, seed=0, kind="normal", t=0.5):
     return _to_rgba(prev), _to_rgba(curr), _to_rgba(truth)
 
 
-def pair_kind(config, pair):
+def pair_kind(stream, pair):
     """The kind of pair `pair` of a sequence: 5 % cuts, 5 % fresh, the rest normal (seeded per pair)."""
-    r = _rng(config * 10 ** 6 + pair).random()
+    r = _rng(stream * 10 ** 6 + pair).random()
     return "cut" if r < 0.05 else ("fresh" if r < 0.10 else "normal")
 
 
-def flow_pair_seq(config, pair, W=1920, H=1080, t=0.5):
-    return flow_pair(W, H, seed=config * 10 ** 6 + pair, kind=pair_kind(config, pair), t=t)
+def flow_pair_seq(stream, pair, W=1920, H=1080, t=0.5):
+    return flow_pair(W, H, seed=stream * 10 ** 6 + pair, kind=pair_kind(stream, pair), t=t)
 
 
 def contrast_texture(H, W, rng, cell=6):

@@ -1,4 +1,4 @@
-"""The config-1 flow-pair generator of workloads.py, batched on the GPU with torch (data generation only: training
+"""The smooth-flow pair generator of workloads.py (flow_pair), batched on the GPU with torch (data generation only: training
 and evaluating the seed proposer needs hundreds of thousands of pairs, which the numpy generator makes too slowly).
 
 Same construction as workloads.flow_pair: a 5-octave value-noise texture T, a smooth motion field v from 2-octave
@@ -7,7 +7,7 @@ replicate), the ground truth at t = T(p - t v(p)); 5 % of pairs are scene cuts (
 have 20 % of curr's area replaced by fresh noise. Random streams are torch's (seeded per batch), not numpy's, so the
 pairs are statistically like workloads.flow_pair's, not bit-identical to them.
 
-hdr_pair makes config 2's RgbaF16 linear-light pairs (log-uniform channels, a pan and rigid sprites) at 4K, which the
+hdr_pair makes the 4K HDR workload's RgbaF16 linear-light pairs (log-uniform channels, a pan and rigid sprites) at 4K, which the
 numpy generators would take minutes for.
 """
 import math
@@ -90,7 +90,7 @@ def flow_batch(B, W, H, gen, ts=(), vmax=24.0, cut_frac=0.05, fresh_frac=0.05, d
 
 
 def hdr_pair(W, H, gen, pan=16.0, sprites=3, smin=128, smax=384, smove=32.0, device="cuda"):
-    """A config-2 pair: RgbaF16 linear light (scRGB), prev / curr (H, W, 4) float16 on the device, alpha 1. Each
+    """A 4K HDR pair: RgbaF16 linear light (scRGB), prev / curr (H, W, 4) float16 on the device, alpha 1. Each
     channel is log-uniform in 1e-3..10 with 4-octave spatial correlation, 10^(-3 + 4 u) with u 4-octave value noise
     normalised to [0, 1]; the background pans by a uniform (+-pan, +-pan) px and `sprites` rigid squares of side
     smin..smax px (their own textures) move by up to +-smove px, composited over the background in both frames."""

@@ -56,7 +56,7 @@ def same(a, b):
 
 
 def c3_slots(scale=4, n=64):
-    """config 3's structure at 1/scale resolution: sizes 1280x720 / 1920x1080 / 2560x1440 / 3840x2160 in ratio
+    """the mixed batch's structure at 1/scale resolution: sizes 1280x720 / 1920x1080 / 2560x1440 / 3840x2160 in ratio
     8:4:2:1 (34 / 17 / 9 / 4 of 64), formats cycling Rgba8 / Rgb10 / Nv12 / P010, multipliers cycling 2 / 3 / 4"""
     sizes = [(1280, 720)] * 34 + [(1920, 1080)] * 17 + [(2560, 1440)] * 9 + [(3840, 2160)] * 4
     fmts = ["rgba8", "rgb10", "nv12", "p010"]

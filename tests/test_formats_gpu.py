@@ -180,8 +180,8 @@ def test_format_1080p(name):
     check(name, p, c, [0.5, 0.25])
 
 
-def test_config2_4k_hdr():
-    """Config 2: 3840x2160 RgbaF16 linear scRGB (80 nits), t = 1/3 and 2/3; every channel log-uniform in 1e-3..10 with
+def test_hdr_4k_f16_linear():
+    """The 4K HDR workload: 3840x2160 RgbaF16 linear scRGB (80 nits), t = 1/3 and 2/3; every channel log-uniform in 1e-3..10 with
     4-octave correlation, a global pan of up to +-16 px and 3 rigid sprites of 128-384 px moving up to +-32 px
     (workloads_gpu.hdr_pair, generated on the device)"""
     import workloads_gpu

@@ -2,7 +2,7 @@
 seednet_train.py run over NCCL, one process per GPU, on a B200 node.
 
   - frame pairs are partitioned, not exchanged: every rank computes the same partition alone, every pair lands on
-    exactly one rank, and the costliest rank stays within one pair of the mean (config 3's 64 mixed pairs);
+    exactly one rank, and the costliest rank stays within one pair of the mean (the mixed batch's 64 pairs);
   - the timing collective: the max of the ranks' spans over the pairs of all ranks;
   - data-parallel seed-net training: the all-reduced (summed) gradient of the ranks' half-batches, scaled by 1 / ranks,
     is the gradient of the whole batch (the float64 reference net), and one Adam step leaves the ranks' parameters
@@ -28,7 +28,7 @@ WORLD = 2
 
 
 def c3_costs():
-    """config 3's 64 pairs (34 x 720p, 17 x 1080p, 9 x 1440p, 4 x 2160p; multipliers 2 / 3 / 4 cycling): the
+    """the mixed batch's 64 pairs (34 x 720p, 17 x 1080p, 9 x 1440p, 4 x 2160p; multipliers 2 / 3 / 4 cycling): the
     pixels a pair moves, two frames in and m - 1 frames out"""
     sizes = [(1280, 720)] * 34 + [(1920, 1080)] * 17 + [(2560, 1440)] * 9 + [(3840, 2160)] * 4
     return [replicas.pair_cost(w, h, 2 + i % 3) for i, (w, h) in enumerate(sizes)]

@@ -117,8 +117,8 @@ def test_4k_pair():
 
 
 @pytest.mark.parametrize("n,W,H", [(96, 640, 360), (24, 1920, 1080)])
-def test_config1_many_pairs(n, W, H):
-    """Config 1's kind of sequence, many pairs: smooth flows with scene cuts and fresh content mixed in (15 % each
+def test_flow_pairs_many(n, W, H):
+    """A smooth-flow sequence, many pairs: smooth flows with scene cuts and fresh content mixed in (15 % each
     here, so that every batch has some), each pair checked stage by stage and at t = 1/4, 1/2, 3/4"""
     import workloads_gpu
     gen = torch.Generator(device="cuda")

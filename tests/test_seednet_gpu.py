@@ -25,7 +25,7 @@ def built():
 
 
 def level1_lumas(n, size=256, seed=0):
-    """(n, size/4, size/4) level-1 luma pairs of config-1-style flow pairs (the oracle's luma)"""
+    """(n, size/4, size/4) level-1 luma pairs of smooth-flow pairs (the oracle's luma)"""
     la, lc = [], []
     for i in range(n):
         p, c, _ = workloads.flow_pair(size, size, seed=seed + i)
