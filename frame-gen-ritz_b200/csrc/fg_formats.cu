@@ -307,16 +307,21 @@ __device__ __forceinline__ void copyNear(const SynthParams& p, int x, int y) {
 // interp.synth for one t in the other formats: the 8-bit path's tile (k_synth) with each format's warp, mismatch,
 // blend and store (resolve.comp:48-83). YUV: the chroma of each 2x2 block is written with its even-even pixel, warped
 // from the block centre with that pixel's half-vector and blended with that pixel's trust.
-template <int F>
-__global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
-    pdlEnter();
+//
+// synthFmtTile computes one output tile and hands every output value to a sink: word(k, x, y, w) for Rgb10 (the
+// packed pixel), half4(k, x, y, v) for RgbaF16 (four halves), luma(k, x, y, code) and chroma(k, x, y, cb, cr) for
+// YUV (codes; chroma for even-even pixels only); k is the thread's region-row slot. kCut: under a scene cut the tile is
+// a copy of the nearer frame (and the core returns); without kCut the caller has taken the cut into account. The
+// untrusted count goes to *p.untrusted unless that is null.
+template <int F, bool kCut, class Sink>
+__device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int by, Sink& sink) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ SyCoef rowc[kSyEH];
     __shared__ unsigned int cnt;
     __shared__ int gReg[4];
-    const int X0 = blockIdx.x * kSyT, Y0 = blockIdx.y * kSyTH;
+    const int X0 = bx * kSyT, Y0 = by * kSyTH;
     const int tid = threadIdx.x, ex = tid & (kSyE - 1), ey0 = tid / kSyE;
-    if (p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
+    if (kCut && p.st->cut) {   // scene cut (interp.py:225-226): the nearer real frame
         for (int i = tid; i < kSyT * kSyTH; i += kSyThreads) {
             const int x = X0 + (i % kSyT), y = Y0 + (i / kSyT);
             if (x < p.W && y < p.H) copyNear<F>(p, x, y);
@@ -348,6 +353,7 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
     const int lx = ex - kSyAp, x = X0 + lx;
     if ((unsigned)lx < (unsigned)kSyT && x < p.W) {
         const uint8_t* nearF = p.nearC ? p.c : p.a;
+#pragma unroll
         for (int k = 0; k < kSyK; k++) {
             const int ey = ey0 + (kSyThreads / kSyE) * k, ly = ey - kSyAp, y = Y0 + ly;
             if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
@@ -362,7 +368,6 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
             float wa[3], wc[3];
             warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
             warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
-            uint8_t* orow = p.out + (size_t)y * p.outPitch;
             if (F == kFmtRgb10) {
                 const uint32_t nw = ldw(nearF, p.pitch, x, y);
                 uint32_t ow = nw & 0xC0000000u;
@@ -373,23 +378,21 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
                     const int code = clampi((int)floorf(__fadd_rn(__fmul_rn(v, p.f.k10i), 0.5f)), 0, 1023);
                     ow |= (uint32_t)code << (p.f.rHigh ? 20 - 10 * c : 10 * c);
                 }
-                reinterpret_cast<uint32_t*>(orow)[x] = ow;
+                sink.word(k, x, y, ow);
             } else if (F == kFmtF16) {
                 const uint2 nq = __ldg(reinterpret_cast<const uint2*>(nearF + (size_t)y * p.pitch) + x);
                 const float n0 = h2f(nq.x & 0xFFFFu), n1 = h2f(nq.x >> 16), n2 = h2f(nq.y & 0xFFFFu);
                 const uint32_t o0 = __half_as_ushort(__float2half_rn(blendF(wa[0], wc[0], n0, u, iu, p)));
                 const uint32_t o1 = __half_as_ushort(__float2half_rn(blendF(wa[1], wc[1], n1, u, iu, p)));
                 const uint32_t o2 = __half_as_ushort(__float2half_rn(blendF(wa[2], wc[2], n2, u, iu, p)));
-                reinterpret_cast<uint2*>(orow)[x] = make_uint2(o0 | (o1 << 16), o2 | (nq.y & 0xFFFF0000u));
+                sink.half4(k, x, y, make_uint2(o0 | (o1 << 16), o2 | (nq.y & 0xFFFF0000u)));
             } else {
                 constexpr float ql = F == kFmtP010 ? 4.0f : 1.0f;   // 1 / YU_QL
                 constexpr int codes = F == kFmtP010 ? 1023 : 255;
                 float ny[3];
                 texel<F>(p.f, nearF, p.pitch, x, y, ny);
                 const float v = blendF(wa[0], wc[0], ny[0], u, iu, p);
-                const int code = clampi((int)floorf(__fadd_rn(__fmul_rn(v, ql), 0.5f)), 0, codes);
-                if (F == kFmtP010) reinterpret_cast<unsigned short*>(orow)[x] = (unsigned short)(code << 6);
-                else orow[x] = (uint8_t)code;
+                sink.luma(k, x, y, clampi((int)floorf(__fadd_rn(__fmul_rn(v, ql), 0.5f)), 0, codes));
                 if (((x | y) & 1) == 0) {   // the chroma of this 2x2 block, warped from its centre
                     const float bx = __fadd_rn(cx.pos, 0.5f), by = __fadd_rn(cy.pos, 0.5f);
                     const float2 ca = warpChroma<F>(p.ac, p.cpitch, p.W, p.H, rne32(__fsub_rn(bx, __fmul_rn(kA, h.x))),
@@ -399,9 +402,7 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
                     const float2 nc = ctexel<F>(p.nearC ? p.cc : p.ac, p.cpitch, x >> 1, y >> 1);
                     const int cb = clampi((int)floorf(__fadd_rn(__fmul_rn(blendF(ca.x, cc.x, nc.x, u, iu, p), ql), 0.5f)), 0, codes);
                     const int cr = clampi((int)floorf(__fadd_rn(__fmul_rn(blendF(ca.y, cc.y, nc.y, u, iu, p), ql), 0.5f)), 0, codes);
-                    uint8_t* oc = p.outc + (size_t)(y >> 1) * p.outCPitch;
-                    if (F == kFmtP010) reinterpret_cast<uint32_t*>(oc)[x >> 1] = ((uint32_t)cb << 6) | ((uint32_t)cr << 22);
-                    else reinterpret_cast<unsigned short*>(oc)[x >> 1] = (unsigned short)(cb | (cr << 8));
+                    sink.chroma(k, x, y, cb, cr);
                 }
             }
             if (p.emap) p.emap[(size_t)y * ((p.W + 3) & ~3) + x] = e[ey * kSyES + ex];
@@ -409,7 +410,195 @@ __global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
     }
     if (myCnt) atomicAdd(&cnt, myCnt);
     __syncthreads();
-    if (tid == 0 && cnt) atomicAdd(p.untrusted, cnt);
+    if (tid == 0 && cnt && p.untrusted) atomicAdd(p.untrusted, cnt);
+}
+
+// the store of a synthesis: the values go to p.out (and p.outc) in the format's layout
+template <int F>
+struct FmtStore {
+    const SynthParams& p;
+    __device__ __forceinline__ void word(int, int x, int y, uint32_t w) const {
+        reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = w;
+    }
+    __device__ __forceinline__ void half4(int, int x, int y, uint2 v) const {
+        reinterpret_cast<uint2*>(p.out + (size_t)y * p.outPitch)[x] = v;
+    }
+    __device__ __forceinline__ void luma(int, int x, int y, int code) const {
+        uint8_t* orow = p.out + (size_t)y * p.outPitch;
+        if (F == kFmtP010) reinterpret_cast<unsigned short*>(orow)[x] = (unsigned short)(code << 6);
+        else orow[x] = (uint8_t)code;
+    }
+    __device__ __forceinline__ void chroma(int, int x, int y, int cb, int cr) const {
+        uint8_t* oc = p.outc + (size_t)(y >> 1) * p.outCPitch;
+        if (F == kFmtP010) reinterpret_cast<uint32_t*>(oc)[x >> 1] = ((uint32_t)cb << 6) | ((uint32_t)cr << 22);
+        else reinterpret_cast<unsigned short*>(oc)[x >> 1] = (unsigned short)(cb | (cr << 8));
+    }
+};
+
+template <int F>
+__global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
+    pdlEnter();
+    FmtStore<F> store{p};
+    synthFmtTile<F, true>(p, blockIdx.x, blockIdx.y, store);
+}
+
+// ============================================================================================== motion blur
+// recordSynthBlur in the other formats (gpu/framegen.h:553-573): the weighted average of n sub-frames, each the
+// values recordSynth(t_k) stores, rounded once. Integer formats (Rgb10 codes, Nv12 / P010 luma and chroma codes):
+// sum q_k v_k with integer weights summing to 2^16, (acc + 2^15) >> 16, in any order (exact). RgbaF16: float32 sums of
+// fl32(w_k h_k), w_k = q_k 2^-16 (exact), in sample order, then rounded to half. A sample replaced by a real frame
+// (scene cut, flick, t <= 0 / >= 1) adds that frame's values at its place in the order. Alpha (Rgb10's 2 bits,
+// RgbaF16's half) is every sub-frame's nearer frame's, averaged the same way.
+template <int F>
+struct FmtAcc {
+    uint32_t (&ai)[kSyK][3];   // integer formats: codes (Rgb10 by bit position; YUV: Y, Cb, Cr)
+    float (&af)[kSyK][3];      // RgbaF16: the colour halves
+    uint32_t q;
+    float w;
+    __device__ __forceinline__ void word(int k, int, int, uint32_t v) const {
+#pragma unroll
+        for (int c = 0; c < 3; c++) ai[k][c] += q * ((v >> (10 * c)) & 1023u);
+    }
+    __device__ __forceinline__ void half4(int k, int, int, uint2 v) const {
+        af[k][0] = __fadd_rn(af[k][0], __fmul_rn(w, h2f(v.x & 0xFFFFu)));
+        af[k][1] = __fadd_rn(af[k][1], __fmul_rn(w, h2f(v.x >> 16)));
+        af[k][2] = __fadd_rn(af[k][2], __fmul_rn(w, h2f(v.y & 0xFFFFu)));
+    }
+    __device__ __forceinline__ void luma(int k, int, int, int code) const { ai[k][0] += q * (uint32_t)code; }
+    __device__ __forceinline__ void chroma(int k, int, int, int cb, int cr) const {
+        ai[k][1] += q * (uint32_t)cb;
+        ai[k][2] += q * (uint32_t)cr;
+    }
+};
+
+// the values a real frame (base pointers a: plane 0, ac: CbCr) holds at (x, y), handed to the sink as a synthesis
+// would hand them
+template <int F, class Sink>
+__device__ __forceinline__ void frameValues(const SynthParams& p, const uint8_t* a, const uint8_t* ac, int k, int x,
+                                            int y, Sink& sink) {
+    if (F == kFmtRgb10) {
+        sink.word(k, x, y, ldw(a, p.pitch, x, y));
+    } else if (F == kFmtF16) {
+        sink.half4(k, x, y, __ldg(reinterpret_cast<const uint2*>(a + (size_t)y * p.pitch) + x));
+    } else if (F == kFmtP010) {
+        sink.luma(k, x, y, __ldg(reinterpret_cast<const unsigned short*>(a + (size_t)y * p.pitch) + x) >> 6);
+        if (((x | y) & 1) == 0) {
+            const uint32_t cw = __ldg(reinterpret_cast<const uint32_t*>(ac + (size_t)(y >> 1) * p.cpitch) + (x >> 1));
+            sink.chroma(k, x, y, (int)((cw >> 6) & 1023u), (int)(cw >> 22));
+        }
+    } else {
+        sink.luma(k, x, y, __ldg(a + (size_t)y * p.pitch + x));
+        if (((x | y) & 1) == 0) {
+            const uint32_t cw = __ldg(reinterpret_cast<const unsigned short*>(ac + (size_t)(y >> 1) * p.cpitch) + (x >> 1));
+            sink.chroma(k, x, y, (int)(cw & 255u), (int)(cw >> 8));
+        }
+    }
+}
+
+template <int F>
+__global__ void __launch_bounds__(kSyThreads, 1) k_synth_blur_fmt(const BlurParams bp) {
+    pdlEnter();
+    __shared__ __align__(16) SynthParams sp;
+    __shared__ unsigned int sRepl, sRedo, sNearC;   // replaced samples; whether this pass has work; nearer = curr
+    __shared__ uint32_t sWap;                        // the weight of the samples whose nearer frame is prev
+    const int tid = threadIdx.x, ex = tid & (kSyE - 1), ey0 = tid / kSyE;
+    const SynthParams& b = bp.base;
+    if (tid == 0) {
+        const bool cut = b.st->cut != 0;
+        unsigned int repl = 0, flick = 0, nearc = 0;
+        uint32_t wap = 0;
+        for (int k = 0; k < bp.n; k++) {
+            const BlurSample& m = bp.smp[k];
+            const bool nc = m.mode == 2 || (m.mode == 0 && m.nearC);
+            bool r = m.mode != 0 || cut;
+            if (!r && bp.fix && (double)bp.cnt[k] / ((double)b.W * (double)b.H) > bp.frac) {
+                r = true;
+                flick |= 1u << k;
+            }
+            if (r) repl |= 1u << k;
+            if (nc) nearc |= 1u << k; else wap += m.q;
+        }
+        sRepl = repl;
+        sRedo = !bp.fix || flick != 0;
+        sNearC = nearc;
+        sWap = wap;
+    }
+    __syncthreads();
+    if (!sRedo) return;
+    const unsigned int repl = sRepl, nearc = sNearC;
+    uint32_t ai[kSyK][3];
+    float af[kSyK][3];
+#pragma unroll
+    for (int k = 0; k < kSyK; k++) {
+        ai[k][0] = ai[k][1] = ai[k][2] = 0u;
+        af[k][0] = af[k][1] = af[k][2] = 0.0f;
+    }
+    FmtAcc<F> acc{ai, af, 0u, 0.0f};
+    const int lx = ex - kSyAp, x = blockIdx.x * kSyT + lx;
+    const bool colOk = (unsigned)lx < (unsigned)kSyT && x < b.W;
+    for (int j = 0; j < bp.n; j++) {
+        acc.q = bp.smp[j].q;
+        acc.w = __fmul_rn((float)bp.smp[j].q, 1.0f / 65536.0f);
+        if ((repl >> j) & 1u) {   // a real frame in the sample's place (uniform over the CTA)
+            const bool nc = (nearc >> j) & 1u;
+            if (colOk) {
+#pragma unroll
+                for (int k = 0; k < kSyK; k++) {
+                    const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = blockIdx.y * kSyTH + ly;
+                    if ((unsigned)ly < (unsigned)kSyTH && y < b.H) frameValues<F>(b, nc ? b.c : b.a, nc ? b.cc : b.ac, k, x, y, acc);
+                }
+            }
+            continue;
+        }
+        static_assert(sizeof(SynthParams) % 4 == 0, "SynthParams copies as words");
+        for (int i = tid; i < (int)(sizeof(SynthParams) / 4); i += kSyThreads)
+            reinterpret_cast<uint32_t*>(&sp)[i] = reinterpret_cast<const uint32_t*>(&b)[i];
+        __syncthreads();
+        if (tid == 0) {
+            const BlurSample& m = bp.smp[j];
+            sp.lookup = m.lookup; sp.mid = m.mid; sp.nearC = m.nearC;
+            sp.s = m.s; sp.ka = m.ka; sp.kc = m.kc; sp.wA = m.wA; sp.wC = m.wC;
+            sp.untrusted = bp.fix ? nullptr : bp.cnt + j;
+            sp.emap = nullptr;
+        }
+        __syncthreads();
+        synthFmtTile<F, false>(sp, blockIdx.x, blockIdx.y, acc);
+        __syncthreads();   // the tile's shared memory and sp are free again
+    }
+    if (!colOk) return;
+    const uint32_t wap = sWap, wac = 65536u - wap;
+#pragma unroll
+    for (int k = 0; k < kSyK; k++) {
+        const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = blockIdx.y * kSyTH + ly;
+        if ((unsigned)ly >= (unsigned)kSyTH || y >= b.H) continue;
+        uint8_t* orow = b.out + (size_t)y * b.outPitch;
+        if (F == kFmtRgb10) {
+            const uint32_t pa = ldw(b.a, b.pitch, x, y) >> 30, pc = ldw(b.c, b.pitch, x, y) >> 30;
+            uint32_t w = ((wap * pa + wac * pc + 32768u) >> 16) << 30;
+#pragma unroll
+            for (int c = 0; c < 3; c++) w |= ((ai[k][c] + 32768u) >> 16) << (10 * c);
+            reinterpret_cast<uint32_t*>(orow)[x] = w;
+        } else if (F == kFmtF16) {
+            const float aa = h2f(__ldg(reinterpret_cast<const uint2*>(b.a + (size_t)y * b.pitch) + x).y >> 16);
+            const float ac = h2f(__ldg(reinterpret_cast<const uint2*>(b.c + (size_t)y * b.pitch) + x).y >> 16);
+            float al = 0.0f;   // alpha: the nearer frames' in sample order
+            for (int j = 0; j < bp.n; j++)
+                al = __fadd_rn(al, __fmul_rn(__fmul_rn((float)bp.smp[j].q, 1.0f / 65536.0f), ((nearc >> j) & 1u) ? ac : aa));
+            const uint32_t o0 = __half_as_ushort(__float2half_rn(af[k][0])), o1 = __half_as_ushort(__float2half_rn(af[k][1]));
+            const uint32_t o2 = __half_as_ushort(__float2half_rn(af[k][2])), o3 = __half_as_ushort(__float2half_rn(al));
+            reinterpret_cast<uint2*>(orow)[x] = make_uint2(o0 | (o1 << 16), o2 | (o3 << 16));
+        } else {
+            const uint32_t yc = (ai[k][0] + 32768u) >> 16;
+            if (F == kFmtP010) reinterpret_cast<unsigned short*>(orow)[x] = (unsigned short)(yc << 6);
+            else orow[x] = (uint8_t)yc;
+            if (((x | y) & 1) == 0) {
+                const uint32_t cb = (ai[k][1] + 32768u) >> 16, cr = (ai[k][2] + 32768u) >> 16;
+                uint8_t* oc = b.outc + (size_t)(y >> 1) * b.outCPitch;
+                if (F == kFmtP010) reinterpret_cast<uint32_t*>(oc)[x >> 1] = (cb << 6) | (cr << 22);
+                else reinterpret_cast<unsigned short*>(oc)[x >> 1] = (unsigned short)(cb | (cr << 8));
+            }
+        }
+    }
 }
 
 // interp.py:238-239 for the other formats: more than globalFallback of the pixels untrusted -> the nearer real frame
@@ -443,6 +632,10 @@ cudaError_t prepareFormatKernels() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     return e;
 }
 
@@ -471,6 +664,20 @@ cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
 
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s) {
     return launchPdl(k_fallback_fmt, dim3(148 * 4), dim3(256), 0, s, p);
+}
+
+cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s) {
+    const size_t smem = synthSmemBytes(bp.base.fs);
+    const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
+    BlurParams p = bp;
+    p.fix = fix;
+    switch (bp.base.f.format) {
+        case kFmtRgb10: return launchPdl(k_synth_blur_fmt<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
+        case kFmtF16: return launchPdl(k_synth_blur_fmt<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);
+        case kFmtNv12: return launchPdl(k_synth_blur_fmt<kFmtNv12>, grid, dim3(kSyThreads), smem, s, p);
+        case kFmtP010: return launchPdl(k_synth_blur_fmt<kFmtP010>, grid, dim3(kSyThreads), smem, s, p);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace fgk

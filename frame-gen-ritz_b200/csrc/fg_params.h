@@ -210,6 +210,8 @@ int synthTilesY(int H);
 cudaError_t prepareFormatKernels();
 cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s);
 cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s);
+// one pass of a motion blur in the other formats (bp.base.f.format): the main pass (fix = 0), then the fix-up
+cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s);
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s);
 
 }  // namespace fgk

@@ -560,9 +560,10 @@ struct Interpolator::Impl {
         bp.frac = (double)set.globalFallback;
         bp.cnt = blurCnt;
         if (!check(cudaMemsetAsync(blurCnt, 0, (size_t)fgk::kBlurMax * 4, s))) return false;
-        if (!check(fgk::launchSynthBlur(bp, 0, s))) return false;
+        const bool rgba8 = fmt == Format::Rgba8;
+        if (!check(rgba8 ? fgk::launchSynthBlur(bp, 0, s) : fgk::launchSynthBlurFmt(bp, 0, s))) return false;
         stamp(s, "blur resolve");
-        if (!check(fgk::launchSynthBlur(bp, 1, s))) return false;
+        if (!check(rgba8 ? fgk::launchSynthBlur(bp, 1, s) : fgk::launchSynthBlurFmt(bp, 1, s))) return false;
         stamp(s, "blur fixup");
         return true;
     }
@@ -785,7 +786,6 @@ bool Interpolator::recordSynthBlur(cudaStream_t stream, Frame prev, Frame curr, 
     if (!blur && t1 > 0.0f && t1 < 1.0f) return recordSynth(stream, prev, curr, out, t1);   // one interior instant
     if (!m->haveEst || prev.data != m->estPrev || curr.data != m->estCurr) return false;
     if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || !m->samePitch(prev, curr)) return false;
-    if (m->fmt != Format::Rgba8) return false;
     if (m->synthSets >= kSetRing) return false;
     DeviceGuard g(m->device);
     m->synthSets++;

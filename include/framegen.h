@@ -10,7 +10,7 @@
 //   VkBuffer debug targets   -> device pointers
 //   VkFormat viewFormat      -> the same VkFormat numbers as plain uint32_t (kVkFormat* below; no Vulkan headers)
 // Out of scope here (rejected with a reason by settingsError / initError): MotionVersion V2 / Learned / V3, static-UI
-// protection modes other than Off. Motion blur (recordSynthBlur): 8-bit RGBA / BGRA frames.
+// protection modes other than Off.
 //
 // Threading / streams: not thread-safe. All records of one Interpolator must go to ONE stream, in recording order:
 // its internal buffers are shared between records and only ordered by stream order.
@@ -173,8 +173,10 @@ public:
     // frame recordSynth(t_k) gives (its scene-cut and whole-frame fallbacks included; prev / curr at t_k <= 0 / >= 1);
     // the average is rounded once: out = (sum q_k v_k + 2^15) >> 16 per byte, q_k = the normalised weights in units
     // of 2^-16 (largest-remainder rounding, blurPlan). N < 2 or t0 == t1: the single instant t1 (recordSynth(t1); a copy
-    // of prev / curr at t1 = 0 / 1). false (nothing recorded) unless 0 <= t0 <= t1 <= 1, and in recordSynth's cases;
-    // false for frames other than 8-bit RGBA / BGRA. Takes one synth of the ring; two launches whatever N is.
+    // of prev / curr at t1 = 0 / 1). false (nothing recorded) unless 0 <= t0 <= t1 <= 1, and in recordSynth's cases.
+    // Other formats: the stored values are averaged the same way (Rgb10 / Nv12 / P010 codes, exact integer sums);
+    // RgbaF16 sums fl32(q_k 2^-16 h_k) in sample order in float32 and rounds to half once. Takes one synth of the ring;
+    // two launches whatever N is.
     bool recordSynthBlur(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t0, float t1);
     // the samples of a blur: their times and weights (units of 2^-16, summing to 2^16); returns their count (0 if
     // refused: t0, t1 out of order or range)

@@ -89,7 +89,7 @@ int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, con
 int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
               const fg_frame* out, float t);                                                              /* :551 */
 /* gpu/framegen.h:573 recordSynthBlur: the weighted average of settings.blurSamples sub-frames over [t0, t1]
- * (framegen.h documents the samples, weights and rounding); 8-bit RGBA / BGRA frames */
+ * (framegen.h documents the samples, weights and rounding), every format */
 int fg_record_synth_blur(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
                          const fg_frame* out, float t0, float t1);
 /* Interpolator::blurPlan (host only): the sample times and weights (units of 2^-16) of a blur into arrays of 16;

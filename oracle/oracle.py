@@ -403,6 +403,40 @@ def synth_fmt(a, c, est, t, spec, settings=None, trace=False, threads=0):
     return out, REASONS[reason.value]
 
 
+def synth_blur_fmt(a, c, est, t0, t1, samples, gaussian, spec, settings=None):
+    """recordSynthBlur's frame in the other formats (None if refused), from synth_fmt's sub-frames: Rgb10 codes (by bit
+    position, alpha's 2 bits included) and Nv12 / P010 luma and chroma codes averaged as (sum q_k v_k + 2^15) >> 16;
+    RgbaF16 summed in sample order as float32 sums of fl32(q_k 2^-16 h_k) per channel (alpha included), then rounded
+    to half. With blur off (N < 2) or t0 == t1 and t1 inside (0, 1): synth_fmt(t1)."""
+    t0f, t1f = np.float32(t0), np.float32(t1)
+    if not (t0f >= 0 and t1f <= 1 and t0f <= t1f):
+        return None
+    if not (samples >= 2 and t0f < t1f) and 0 < t1f < 1:
+        return synth_fmt(a, c, est, float(t1f), spec, settings)[0]
+    times, q = blur_plan(samples, gaussian, t0, t1)
+    subs = [a if tk <= 0 else c if tk >= 1 else synth_fmt(a, c, est, float(tk), spec, settings)[0]
+            for tk in times.tolist()]
+
+    def avg_codes(planes, shift):   # integer codes (after >> shift), then back
+        acc = sum(qk * (f.astype(np.int64) >> shift) for qk, f in zip(q, planes))
+        return ((acc + 32768) >> 16) << shift
+
+    if spec.format == "rgb10":
+        out = np.zeros_like(subs[0], dtype=np.uint32)
+        for pos, mask in ((0, 1023), (10, 1023), (20, 1023), (30, 3)):
+            acc = sum(qk * ((f.astype(np.int64) >> pos) & mask) for qk, f in zip(q, subs))
+            out |= (((acc + 32768) >> 16) << pos).astype(np.uint32)
+        return out
+    if spec.format == "f16":
+        acc = np.zeros(subs[0].shape, np.float32)
+        for qk, f in zip(q, subs):
+            acc = (acc + np.float32(qk / 65536.0) * f.astype(np.float32)).astype(np.float32)
+        return acc.astype(np.float16)
+    shift = 6 if spec.format == "p010" else 0
+    dt = subs[0][0].dtype
+    return (avg_codes([f[0] for f in subs], shift).astype(dt), avg_codes([f[1] for f in subs], shift).astype(dt))
+
+
 def pq255(v, white=80.0):
     """the oracle's PQ level of a linear value (format.glsl fgPq * 255)"""
     L = _fmt_lib()

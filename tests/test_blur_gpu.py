@@ -5,7 +5,8 @@ Bar: byte-exact. Cases follow the reference's own check (gpu/blurtest.cpp:757-80
 [.25, .75], [0, 1], [.1, .4], [.6, .9], even and Gaussian weights, the scene cut forced, the whole-frame flick forced
 on every sample and on some samples only (the fix-up pass); the single-instant cases, refusals, a CUDA graph, and at
 4K (too large for the oracle in seconds) the size-independent identity blur == the rounded mean of recordSynth
-outputs at the sample times.
+outputs at the sample times. The other formats (Rgb10, RgbaF16 linear and encoded, Nv12, P010) against
+oracle.synth_blur_fmt, with the cut and the flick forced.
 """
 import numpy as np
 import pytest
@@ -160,15 +161,44 @@ def test_blur_instants_and_refusals():
     I.close()
 
 
-def test_blur_other_formats_refused():
+BLUR_CASES = [(2, 0.0, 1.0, False), (3, 0.25, 0.75, True), (4, 0.1, 0.4, True), (5, 0.6, 0.9, False),
+              (8, 0.0, 1.0, True)]
+
+
+@pytest.mark.parametrize("variant", ["default", "cut", "flick"])
+@pytest.mark.parametrize("name", ["rgb10_argb", "f16_linear", "f16_encoded", "nv12_709_limited", "p010_2020_limited"])
+def test_blur_formats_match_oracle(name, variant):
+    """the other formats (odd size: ragged chroma), byte for byte against oracle.synth_blur_fmt: integer formats'
+    codes averaged with the 2^-16 weights, RgbaF16 float32 sums in sample order rounded to half; with the scene cut
+    forced and with every synthesis flicked (the fix-up pass)"""
+    from test_formats_gpu import SPEC, new_out as fmt_out, to_dev as fmt_dev, to_host
+    _, vk, spec, conv, extra = SPEC[name]
+    p8, c8, _ = workloads.flow_pair(203, 117, seed=17)
+    a, c = conv(p8), conv(c8)
+    s = {"default": oracle.Settings(), "cut": oracle.Settings(sceneCutSad=0.5),
+         "flick": oracle.Settings(globalFallback=0.0005)}[variant]
+    fs = to_fg(s)
     I = fg.Interpolator()
-    fs = fg.Settings()
-    fs.blurSamples = 4
-    assert I.init(64, 48, fg.VK_A2B10G10R10_UNORM, settings=fs), I.init_error()
-    x = torch.zeros((48, 64), dtype=torch.int32, device="cuda")
+    assert I.init(203, 117, vk, settings=fs, **extra), I.init_error()
+    da, dc = fmt_dev(a), fmt_dev(c)
     I.begin_frame()
-    assert I.record_estimate(x, x)
-    assert not I.record_synth_blur(x, x, torch.zeros_like(x), 0.2, 0.8)
+    assert I.record_estimate(da, dc)
+    est = oracle.estimate_fmt(a, c, spec, settings=s, trace=False)
+    assert bool(est["cut"]) == (variant == "cut")
+    bad = []
+    for n, t0, t1, g in BLUR_CASES:
+        fs.blurSamples, fs.blurWeights = n, int(g)
+        assert I.set_settings(fs)
+        I.begin_frame()
+        o = fmt_out(da)
+        assert I.record_synth_blur(da, dc, o, t0, t1), (n, t0, t1)
+        torch.cuda.synchronize()
+        got, want = to_host(o, a), oracle.synth_blur_fmt(a, c, est, t0, t1, n, g, spec, s)
+        planes = zip(got, want) if isinstance(got, tuple) else [(got, want)]
+        for gp, wp in planes:
+            if not np.array_equal(gp.view(np.uint8), wp.view(np.uint8)):
+                bad.append((n, t0, t1, g, int(np.count_nonzero(gp != wp))))
+    assert not bad, f"{name} {variant}: {bad}"
     I.close()
 
 

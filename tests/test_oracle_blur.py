@@ -106,3 +106,42 @@ def test_oracle_blur_instants(pair):
     assert np.array_equal(oracle.synth_blur(p, c, est, 1.0, 1.0, 4, False), c)       # a real-frame instant
     assert np.array_equal(oracle.synth_blur(p, c, est, 0.0, 0.0, 4, False), p)
     assert oracle.synth_blur(p, c, est, 0.7, 0.2, 4, False) is None
+
+
+@pytest.mark.parametrize("fmt", ["rgb10", "f16", "nv12", "p010"])
+def test_oracle_blur_formats(fmt):
+    """the other formats: instants are synth_fmt's frames; the average stays between the sub-frames' extremes and,
+    for the integer formats, within 1 code of the double-precision weighted mean of their codes"""
+    spec = {"rgb10": oracle.FormatSpec("rgb10"), "f16": oracle.FormatSpec("f16", linear=True, white=80.0),
+            "nv12": oracle.FormatSpec("nv12", matrix="bt709"), "p010": oracle.FormatSpec("p010", matrix="bt2020")}[fmt]
+    p8, c8, _ = workloads.flow_pair(96, 64, seed=23)
+    conv = {"rgb10": workloads.to_rgb10, "f16": lambda f: workloads.to_f16(f, linear=True),
+            "nv12": lambda f: workloads.to_yuv(f, 8, "bt709"), "p010": lambda f: workloads.to_yuv(f, 10, "bt2020")}[fmt]
+    a, c = conv(p8), conv(c8)
+    est = oracle.estimate_fmt(a, c, spec, trace=False)
+    planes = lambda f: list(f) if isinstance(f, tuple) else [f]
+    s30 = oracle.synth_fmt(a, c, est, float(np.float32(0.3)), spec)[0]
+    for got in (oracle.synth_blur_fmt(a, c, est, 0.3, 0.3, 8, True, spec),
+                oracle.synth_blur_fmt(a, c, est, 0.1, 0.3, 1, True, spec)):
+        assert all(np.array_equal(x, y) for x, y in zip(planes(got), planes(s30)))
+    assert all(np.array_equal(x, y) for x, y in zip(planes(oracle.synth_blur_fmt(a, c, est, 1.0, 1.0, 4, False, spec)),
+                                                    planes(c)))
+    assert oracle.synth_blur_fmt(a, c, est, 0.7, 0.2, 4, False, spec) is None
+    n, gaussian = 5, True
+    times, q = oracle.blur_plan(n, gaussian, 0.1, 0.9)
+    subs = [oracle.synth_fmt(a, c, est, float(t), spec)[0] for t in times.tolist()]
+    got = oracle.synth_blur_fmt(a, c, est, 0.1, 0.9, n, gaussian, spec)
+    for k, gp in enumerate(planes(got)):
+        sp = [planes(f)[k] for f in subs]
+        if fmt == "f16":
+            v = np.stack([x.astype(np.float64) for x in sp])
+            g = gp.astype(np.float64)
+            assert np.all(g >= v.min(0) - 1e-3 * np.abs(v.min(0))) and np.all(g <= v.max(0) + 1e-3 * np.abs(v.max(0)))
+            continue
+        shift = 6 if fmt == "p010" else 0
+        fields = [(0, 1023), (10, 1023), (20, 1023)] if fmt == "rgb10" else [(0, (1 << 16) - 1)]
+        for pos, mask in fields:
+            codes = np.stack([((x.astype(np.int64) >> shift) >> pos) & mask for x in sp])
+            want = np.tensordot(np.array(q, np.float64) / 65536.0, codes.astype(np.float64), axes=1)
+            gc = ((gp.astype(np.int64) >> shift) >> pos) & mask
+            assert np.abs(gc - want).max() <= 1.0
