@@ -238,9 +238,9 @@ class Interpolator:
         self._h = lib().fg_create()
 
     def close(self):
-        if self._h:
-            lib().fg_destroy(self._h)
-            self._h = None
+        if self._h and _lib is not None:   # (at interpreter exit the module's globals may already be gone)
+            _lib.fg_destroy(self._h)
+        self._h = None
 
     __del__ = close
 
