@@ -891,6 +891,7 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     pdlEnter();
     // rows padded by one word: the horizontal sums below read down the rows of a column group, one row per lane
     __shared__ int plane[kPfEH][kPfE + 1];
+    __shared__ int plane0[kPfEH][kPfE + 1];   // the zero candidate's errors, computed once
     __shared__ int hs[kPfEH][kPfE + 1];
     __shared__ float2 bv[kPfBY][kPfBX];
     __shared__ int2 bR[kPfBY][kPfBX];
@@ -937,8 +938,16 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     float best[kPfK];
     int bestk[kPfK];
     const double C = 0x1p-14 * (1.0 / 25.0);   // cv2's box scale with the 2^-14 units folded in (exact scaling)
+#pragma unroll
+    for (int j = 0; j < kPfK; j++) {   // the zero candidate: both taps at q itself (weights 32 x 32)
+        const int ey = ey0 + 4 * j;
+        const int qy = clampi(Y0 - kPfAp + ey, 0, p.h - 1);
+        const float ta = __fmul_rn(__ldg(p.ya + qy * p.w + qx), 1024.0f), tc = __fmul_rn(__ldg(p.yc + qy * p.w + qx), 1024.0f);
+        plane0[ey][ex] = __float_as_int(__fmaf_rn(fabsf(ta - tc), 16.0f, 12582912.0f)) - 0x4B400000;
+    }
     for (int k = 0; k < kPfNC; k++) {
-        // 1. candidate k's error at this thread's region pixels
+        // 1. candidate k's error at this thread's region pixels (the zero candidate's is plane0 already)
+        if (k < kPfNC - 1)
 #pragma unroll
         for (int j = 0; j < kPfK; j++) {
             const int ey = ey0 + 4 * j;
@@ -969,7 +978,7 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
         //    take the 32 rows of one column group (conflict-free with the padded rows)
         {
             const int r = tid & 31, c0 = (tid >> 5) * 8;
-            const int* q = &plane[r][c0];
+            const int* q = k == kPfNC - 1 ? &plane0[r][c0] : &plane[r][c0];
             int sum = q[0] + q[1] + q[2] + q[3] + q[4];
             hs[r][c0] = sum;
 #pragma unroll
