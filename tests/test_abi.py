@@ -100,3 +100,29 @@ def test_init_refusals_without_recording():
     I.release_unused_ui()        # gpu/framegen.h:693, 700: nothing is ever unused here (V1 only, no UI memory)
     I.release_unused_motion()
     I.close()
+
+
+NULL_PROBE = r"""
+import ctypes, sys
+sys.path[:0] = [sys.argv[1]]
+import framegen as fg
+L = fg.lib()
+for name in sorted(fg.SIGNATURES):
+    res, args = fg.SIGNATURES[name]
+    vals = [0.0 if a in (ctypes.c_float, ctypes.c_double) else
+            0 if a in (ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int64) else None for a in args]
+    print(name, flush=True)
+    getattr(L, name)(*vals)
+print("all returned", flush=True)
+"""
+
+
+def test_null_arguments_never_crash():
+    """every exported function called with null handles / pointers and zero sizes returns (the reference's API never
+    throws; a null object is 'not initialised', not a crash), run in a child process so a crash names the function"""
+    import subprocess
+    import sys
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "frame-gen-ritz_b200")
+    r = subprocess.run([sys.executable, "-c", NULL_PROBE, pkg], capture_output=True, text=True, timeout=120)
+    last = r.stdout.strip().splitlines()[-1] if r.stdout.strip() else "(nothing)"
+    assert r.returncode == 0 and last == "all returned", f"crashed in {last}: {r.stderr[-500:]}"
