@@ -131,10 +131,15 @@ extern "C" int fg_record_synth_noalloc(void* stream, uint32_t view_format, uint3
         return 0;
     }
     auto ok = [&](const fg_frame* f) {
-        return f && f->data && f->pitch >= (uint64_t)width * 4 && f->pitch % 4 == 0 && ((uintptr_t)f->data & 3) == 0;
+        return f && f->data && f->pitch >= (uint64_t)width * 4 && f->pitch % 4 == 0 && ((uintptr_t)f->data & 3) == 0 &&
+               f->pitch <= fgk::kMaxPlaneSpan && (uint64_t)(height - 1) * f->pitch + (uint64_t)width * 4 <= fgk::kMaxPlaneSpan;
     };
-    if (!ok(prev) || !ok(curr) || !ok(out) || prev->pitch != curr->pitch || !field) {
-        *err = "a frame is missing, misaligned or narrower than the width, or the field is null";
+    if (!ok(prev) || !ok(curr) || !ok(out) || prev->pitch != curr->pitch) {
+        *err = "a frame is missing, misaligned, narrower than the width or spans more than 2^34 bytes";
+        return 0;
+    }
+    if (!field) {
+        *err = "the per-pixel field is null";
         return 0;
     }
     int dev = 0;

@@ -12,6 +12,8 @@ constexpr int kMaxLevels = 16;
 constexpr int kPyrInKernel = 6;    // levels 0..5 come out of the luma kernel (a 32x32 tile of level 0 -> 1x1 of level 5)
 constexpr int kSeedNetOut = 8;    // seed net outputs per block: c1x, c1y, c2x, c2y, confidence logit, 3 unused
 constexpr int kMaxRadius = 12;     // Settings::searchRadius / searchRadiusTop upper bound (gpu/framegen.cpp validate)
+// the most bytes rows 0..H-1 of a frame's first plane may span: the 8-bit kernels form pixel offsets in 32-bit words
+constexpr size_t kMaxPlaneSpan = (size_t)1 << 34;
 
 // Device-side counters and small results of one estimate / synth (one allocation, zeroed at init).
 struct DevState {

@@ -365,11 +365,13 @@ struct Interpolator::Impl {
         return setupSeedNet();
     }
 
-    // a frame the kernels can address: plane 0 (and the CbCr plane of YUV) aligned to its sample size, rows wide enough
+    // a frame the kernels can address: plane 0 (and the CbCr plane of YUV) aligned to its sample size, rows wide enough,
+    // plane 0 within fgk::kMaxPlaneSpan bytes
     bool frameOk(const Frame& f) const {
         const size_t bpp = (size_t)planeBytes(fmt), cb = (size_t)chromaBytes(fmt);
         const size_t al = fmt == Format::Nv12 ? 1 : bpp;
         if (!f.data || f.pitch < (size_t)W * bpp || f.pitch % al || ((uintptr_t)f.data % al)) return false;
+        if (f.pitch > fgk::kMaxPlaneSpan || (size_t)(H - 1) * f.pitch + (size_t)W * bpp > fgk::kMaxPlaneSpan) return false;
         if (!cb) return true;
         return f.chroma && f.chromaPitch >= (size_t)((W + 1) / 2) * cb && f.chromaPitch % cb == 0 &&
                (uintptr_t)f.chroma % cb == 0;

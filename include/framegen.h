@@ -55,7 +55,9 @@ enum class Transfer : uint32_t { Encoded = 0, Linear = 1 };
 enum class YuvMatrix : uint32_t { Bt601 = 0, Bt709 = 1, Bt2020 = 2 };
 
 // gpu/framegen.h:154-159: one image as the library takes it. Device memory; rows `pitch` bytes apart (a multiple of
-// 4 for the 4-byte formats); pixels packed as the viewFormat says. The two-plane formats add the CbCr plane.
+// 4 for the 4-byte formats); pixels packed as the viewFormat says. The two-plane formats add the CbCr plane. A frame
+// whose first plane spans more than 2^34 bytes ((height - 1) * pitch + the row's bytes) is refused: the 8-bit kernels
+// address it in 32-bit words.
 struct Frame {
     void* data = nullptr;
     size_t pitch = 0;

@@ -25,7 +25,7 @@ typedef struct fg_settings {
     uint32_t flowScale, pyramidMinSide;
 } fg_settings;
 
-/* framegen::Frame (gpu/framegen.h:154-159) */
+/* framegen::Frame (gpu/framegen.h:154-159); the first plane spans at most 2^34 bytes */
 typedef struct fg_frame {
     void* data;
     uint64_t pitch;

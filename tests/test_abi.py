@@ -126,3 +126,28 @@ def test_null_arguments_never_crash():
     r = subprocess.run([sys.executable, "-c", NULL_PROBE, pkg], capture_output=True, text=True, timeout=120)
     last = r.stdout.strip().splitlines()[-1] if r.stdout.strip() else "(nothing)"
     assert r.returncode == 0 and last == "all returned", f"crashed in {last}: {r.stderr[-500:]}"
+
+
+def test_noalloc_frame_span_limit():
+    """fg_record_synth_noalloc refuses a frame whose first plane spans more than 2^34 bytes ((height - 1) * pitch + the
+    row's bytes; the 8-bit kernels address it in 32-bit words) and takes one that spans exactly 2^34. The pointers are
+    stand-ins that are never dereferenced: the frame checks and the null field refuse each call before CUDA is used."""
+    W = H = 16
+    limit = 1 << 34
+    at = (limit - 4 * W) // (H - 1)
+    assert at % 4 == 0 and (H - 1) * at + 4 * W == limit
+
+    def call(pitch):
+        f = fg.CFrame()
+        f.data, f.pitch = 1 << 20, pitch
+        err = ctypes.c_char_p()
+        ok = fg.lib().fg_record_synth_noalloc(None, fg.VK_R8G8B8A8_UNORM, W, H, ctypes.byref(f), ctypes.byref(f),
+                                              ctypes.byref(f), None, 0, 0.5, ctypes.byref(fg.Settings().to_c()),
+                                              ctypes.byref(err))
+        return ok, err.value.decode()
+
+    ok, msg = call(at)
+    assert not ok and "field is null" in msg, msg   # the frames passed
+    for pitch in (at + 4, limit + 4 * W, 1 << 62):
+        ok, msg = call(pitch)
+        assert not ok and "2^34" in msg, (pitch, msg)

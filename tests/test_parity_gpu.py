@@ -166,7 +166,7 @@ def test_hard_cut_and_repeat_determinism():
 
 def test_record_refusals():
     """gpu/framegen.h:532-549: false and nothing recorded for t outside (0, 1), no estimate, other frames, ring
-    overflow; beginFrame() resets the rings."""
+    overflow, a frame whose plane spans more than 2^34 bytes; beginFrame() resets the rings."""
     p, c = workloads.pan_pair(64, 48, seed=1)
     I = fg.Interpolator()
     assert I.init(64, 48, fg.VK_R8G8B8A8_UNORM)
@@ -176,6 +176,9 @@ def test_record_refusals():
     assert not I.record_synth(a, cc, o, 0.5)            # no estimate yet
     for t in (0.0, 1.0, -0.5, 1.5, float("nan")):
         assert not I.record(a, cc, o, t)
+    big = fg.frame_of(a)
+    big.pitch = 1 << 29                                  # 47 rows of 512 MiB: the plane spans more than 2^34 bytes
+    assert not fg.lib().fg_record_estimate(I._h, fg._stream(None), fg.ctypes.byref(big), fg.ctypes.byref(big))
     I.begin_frame()
     assert I.record_estimate(a, cc)
     other = to_dev(c)
