@@ -663,7 +663,7 @@ cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
 }
 
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s) {
-    return launchPdl(k_fallback_fmt, dim3(148 * 4), dim3(256), 0, s, p);
+    return launchPdl(k_fallback_fmt, dim3(smCount() * 4), dim3(256), 0, s, p);
 }
 
 cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s) {

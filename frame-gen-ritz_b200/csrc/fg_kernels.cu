@@ -8,6 +8,7 @@
 //     numpy's operation order with explicit round-to-nearest intrinsics (no contraction);
 //   - reductions whose rounding depends on order (the scene-cut mean) follow numpy's pairwise tree.
 // The whole library is compiled with -fmad=false as a second guard against contraction.
+#include <atomic>
 #include <cooperative_groups.h>
 
 #include "fg_device.h"
@@ -1449,10 +1450,28 @@ int synthBatchCtasPerSm(size_t smem) {   // resident k_synth_batch CTAs per SM w
     return occ;
 }
 cudaError_t launchFallbackBatch(const FallbackParams* items, int nItems, cudaStream_t s) {
-    return launchPdl(k_fallback_batch, dim3(148, nItems), dim3(256), 0, s, items);
+    return launchPdl(k_fallback_batch, dim3(smCount(), nItems), dim3(256), 0, s, items);
 }
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s) {
-    return launchPdl(k_fallback, dim3(148 * 4), dim3(256), 0, s, p);
+    return launchPdl(k_fallback, dim3(smCount() * 4), dim3(256), 0, s, p);
+}
+
+int smCount() {
+    constexpr int kDevices = 64;
+    static std::atomic<int> cached[kDevices];   // 0: not queried yet
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) {
+        cudaGetLastError();
+        return 148;   // the grid-stride kernels stay correct with any grid; B200's count is a fair size
+    }
+    int n = cached[dev].load(std::memory_order_relaxed);
+    if (n > 0) return n;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return 148;
+    }
+    cached[dev].store(n, std::memory_order_relaxed);
+    return n;
 }
 
 }  // namespace fgk

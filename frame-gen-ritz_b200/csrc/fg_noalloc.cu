@@ -9,18 +9,24 @@
 //
 // The scratch array (g_fgNoAllocScratch): a DevState (the scene-cut flag and the untrusted-pixel counters) and the
 // per-pixel field looked up at time t, for at most kNoAllocMaxFlowPixels flow pixels (3,145,728: 3840x2160 at
-// flowScale 2 needs 2,073,600). Every GPU that loads the library holds it (about 24 MiB) until the process exits.
-// All calls share it and it keeps the last call's contents: the counters are cleared by each call's first kernel, the
-// field is rewritten in full. Calls that overlap on the GPU (two streams, or two threads) race on it.
+// flowScale 2 needs 2,073,600). About 24 MiB on every GPU where it has been placed, held until the process exits.
+// The driver places it when this file's module is first used on a device: with CUDA's default lazy module loading
+// that is the first call's cudaGetSymbolAddress, so the first call on a device is where the 24 MiB are taken, and it
+// can fail there for lack of device memory. Hosts with a fixed memory budget make that first call at set-up time.
+// All calls share the array and it keeps the last call's contents: the counters are cleared by each call's first
+// kernel, the field is rewritten in full. Calls that overlap on the GPU (two streams, or two threads) race on it.
 //
 // Host code does not use the array's name as an address (in host code it is only a stand-in for the symbol): the first
 // call on a device, with that device current, looks the address up with cudaGetSymbolAddress and keeps it for that
-// device. That first call therefore does a little set-up work on the host and should come before any stream capture.
+// device (under a lock, so two host threads may make their first calls at once). That first call therefore does a
+// little set-up work on the host and should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 
 #include "fg_params.h"
 #include "framegen.h"
@@ -35,7 +41,9 @@ static_assert(sizeof(fgk::DevState) <= kNoAllocStateBytes, "DevState fits its sl
 static __device__ __align__(256) unsigned char g_fgNoAllocScratch[kNoAllocStateBytes + kNoAllocMaxFlowPixels * 8];
 
 constexpr int kMaxDevices = 64;
-unsigned char* g_scratchOfDevice[kMaxDevices];   // device address of g_fgNoAllocScratch per device (null: not set up)
+// device address of g_fgNoAllocScratch per device (null: not set up yet); written once, under g_setupLock
+std::atomic<unsigned char*> g_scratchOfDevice[kMaxDevices];
+std::mutex g_setupLock;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
@@ -78,20 +86,6 @@ __global__ void __launch_bounds__(256) k_noalloc_prepare(const float2* __restric
         }
         g[i] = v;
     }
-}
-
-// the 7x7 box sums below / above which the trust ramp is exactly 0 / 1 (see framegen.cpp Impl::updateTrust)
-void trustShortcuts(const framegen::Settings& set, int& sZero, int& sOne) {
-    const float t0 = set.trustLow, span = (float)((double)set.trustHigh - (double)set.trustLow);
-    auto u = [&](int S) {
-        const float eb = (float)((double)S * (1.0 / 49.0));
-        float v = (eb - t0) / span;
-        return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
-    };
-    sZero = -1;
-    for (int S = 0; S <= 49 * 255 && u(S) == 0.0f; S++) sZero = S;
-    sOne = 49 * 255 + 1;
-    for (int S = 49 * 255; S >= 0 && u(S) == 1.0f; S--) sOne = S;
 }
 
 }  // namespace
@@ -142,28 +136,39 @@ extern "C" int fg_record_synth_noalloc(void* stream, uint32_t view_format, uint3
         *err = "the per-pixel field is null";
         return 0;
     }
+    if (((uintptr_t)field & 7) != 0) {   // read as (x, y) pairs of floats
+        *err = "the per-pixel field is not 8-byte aligned";
+        return 0;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
         *err = "no usable CUDA device";
         return 0;
     }
-    if (!g_scratchOfDevice[dev]) {   // set-up, once per device (with that device current)
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_fgNoAllocScratch);
-        if (e != cudaSuccess || !ptr) {
-            cudaGetLastError();
-            *err = "cudaGetSymbolAddress of the no-allocation scratch failed";
-            return 0;
+    unsigned char* scratch = g_scratchOfDevice[dev].load(std::memory_order_acquire);
+    if (!scratch) {   // set-up, once per device (with that device current)
+        std::lock_guard<std::mutex> lock(g_setupLock);
+        scratch = g_scratchOfDevice[dev].load(std::memory_order_acquire);
+        if (!scratch) {
+            void* ptr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&ptr, g_fgNoAllocScratch);
+            if (e != cudaSuccess || !ptr) {
+                cudaGetLastError();
+                *err = "cudaGetSymbolAddress of the no-allocation scratch failed (the first call on a device places "
+                       "its 24 MiB array; is the device out of memory?)";
+                return 0;
+            }
+            if (fgk::prepareKernels() != cudaSuccess) {
+                cudaGetLastError();
+                *err = "the kernels' shared-memory limits could not be set";
+                return 0;
+            }
+            fgk::smCount();   // cached per device here, so later calls make no attribute query
+            scratch = static_cast<unsigned char*>(ptr);
+            g_scratchOfDevice[dev].store(scratch, std::memory_order_release);
         }
-        if (fgk::prepareKernels() != cudaSuccess) {
-            cudaGetLastError();
-            *err = "the kernels' shared-memory limits could not be set";
-            return 0;
-        }
-        g_scratchOfDevice[dev] = static_cast<unsigned char*>(ptr);
     }
-    unsigned char* scratch = g_scratchOfDevice[dev];
     fgk::DevState* st = reinterpret_cast<fgk::DevState*>(scratch);
     float2* g = reinterpret_cast<float2*>(scratch + kNoAllocStateBytes);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -171,7 +176,7 @@ extern "C" int fg_record_synth_noalloc(void* stream, uint32_t view_format, uint3
     const float sv = (float)(2.0 * td - 1.0);
     const int lookup = sv != 0.0f;
     const int n = fw * fh;
-    k_noalloc_prepare<<<(unsigned)std::min(148 * 8, (n + 255) / 256), 256, 0, s>>>(
+    k_noalloc_prepare<<<(unsigned)std::min(fgk::smCount() * 8, (n + 255) / 256), 256, 0, s>>>(
         reinterpret_cast<const float2*>(field), fw, fh, sv, lookup, cut, scratch);
     cudaError_t e = cudaGetLastError();
     const bool rgba = view_format == framegen::kVkFormatR8G8B8A8Unorm;
@@ -191,7 +196,7 @@ extern "C" int fg_record_synth_noalloc(void* stream, uint32_t view_format, uint3
     sp.wC = t;
     sp.trust0 = set.trustLow;
     sp.trustSpan = (float)((double)set.trustHigh - (double)set.trustLow);
-    trustShortcuts(set, sp.sZero, sp.sOne);
+    fgk::trustShortcuts(set.trustLow, set.trustHigh, sp.sZero, sp.sOne);
     sp.st = st;
     sp.untrusted = &st->untrusted[0];
     sp.emap = nullptr;

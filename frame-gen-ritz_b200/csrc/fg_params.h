@@ -216,4 +216,24 @@ cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s);
 cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s);
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s);
 
+// Streaming multiprocessors of the current device (cached per device); grids of the grid-stride kernels are sized in
+// multiples of it.
+int smCount();
+
+// The trust ramp of interp.py:236, u(S) = clip((float(S / 49) - trustLow) / (trustHigh - trustLow), 0, 1) for the 7x7
+// mismatch sums S = 0 .. 49 * 255, is monotone in S: S <= sZero gives exactly 0 and S >= sOne exactly 1 (the synthesis
+// kernels compute the ramp in between). Host-side, from the settings' thresholds.
+inline void trustShortcuts(float trustLow, float trustHigh, int& sZero, int& sOne) {
+    const float t0 = trustLow, span = (float)((double)trustHigh - (double)trustLow);
+    auto u = [&](int S) {
+        const float eb = (float)((double)S * (1.0 / 49.0));
+        float v = (eb - t0) / span;
+        return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+    };
+    sZero = -1;
+    for (int S = 0; S <= 49 * 255 && u(S) == 0.0f; S++) sZero = S;
+    sOne = 49 * 255 + 1;
+    for (int S = 49 * 255; S >= 0 && u(S) == 1.0f; S--) sOne = S;
+}
+
 }  // namespace fgk

@@ -285,20 +285,7 @@ struct Interpolator::Impl {
         haveEst = false;
     }
 
-    void updateTrust() {
-        // u(S) = clip((float(S / 49) - trustLow) / (trustHigh - trustLow), 0, 1) for 7x7 sums S = 0 .. 49 * 255 is
-        // monotone in S: S <= sZero gives 0, S >= sOne gives 1 (the kernel computes the ramp in between exactly).
-        const float t0 = set.trustLow, span = (float)((double)set.trustHigh - (double)set.trustLow);
-        auto u = [&](int S) {
-            const float eb = (float)((double)S * (1.0 / 49.0));
-            float v = (eb - t0) / span;
-            return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
-        };
-        sZero = -1;
-        for (int S = 0; S <= 49 * 255 && u(S) == 0.0f; S++) sZero = S;
-        sOne = 49 * 255 + 1;
-        for (int S = 49 * 255; S >= 0 && u(S) == 1.0f; S--) sOne = S;
-    }
+    void updateTrust() { fgk::trustShortcuts(set.trustLow, set.trustHigh, sZero, sOne); }
 
     // buffers of one size (createSizeDependent, gpu/framegen.cpp:994-1014)
     const char* allocSize(uint32_t w, uint32_t h) {

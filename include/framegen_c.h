@@ -175,13 +175,15 @@ int fg_seednet_adam_scaled(fg_seednet* net, void* stream, float lr, float grad_s
  * a compositor or overlay running inside another program's frame callback under that program's memory budget, a
  * real-time presentation thread that must not block on cudaMalloc / cudaFree, a plugin that is handed buffers but no
  * allocator. It allocates nothing and needs no fg_interpolator: the caller passes the two frames, the output, the
- * pair's per-pixel half-vector field (fw x fh float2 on the device, fw = rint(width / flowScale), fh likewise: the
- * field fg_record_estimate computes, e.g. read with fg_record_trace) and the pair's scene-cut decision; the rest lives
- * in one static device array inside the library, sized for at most 3,145,728 flow pixels (3840x2160 at flowScale 2).
- * Larger frames are refused with an error, before anything is launched. Every call shares that array and it keeps the
- * last call's contents; calls that overlap on the GPU race on it. The first call on a device looks the array's device
- * address up (host set-up work): make it before any stream capture. Returns 1 on success; 0 with *error (if error is
- * not null) set to a static message otherwise. view_format: 37 (R8G8B8A8) or 44 (B8G8R8A8); t in (0, 1). */
+ * pair's per-pixel half-vector field (fw x fh float2 on the device, 8-byte aligned, fw = rint(width / flowScale), fh
+ * likewise: the field fg_record_estimate computes, e.g. read with fg_record_trace) and the pair's scene-cut decision;
+ * the rest lives in one static device array inside the library (about 24 MiB), sized for at most 3,145,728 flow pixels
+ * (3840x2160 at flowScale 2). Larger frames are refused with an error, before anything is launched. Every call shares
+ * that array and it keeps the last call's contents; calls that overlap on the GPU race on it. The first call on a
+ * device looks the array's device address up (host set-up work), and with CUDA's lazy module loading that is also when
+ * the driver places the 24 MiB array on the device, so the first call can fail for lack of device memory: make it at
+ * set-up time, before any stream capture. Returns 1 on success; 0 with *error (if error is not null) set to a static
+ * message otherwise. view_format: 37 (R8G8B8A8) or 44 (B8G8R8A8); t in (0, 1). */
 int fg_record_synth_noalloc(void* stream, uint32_t view_format, uint32_t width, uint32_t height, const fg_frame* prev,
                             const fg_frame* curr, const fg_frame* out, const float* field, int cut, float t,
                             const fg_settings* settings, const char** error);

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generates the golden fixtures of the V1 path by running the reference's own proto/interp.py.
 
-Run in a checkout that has the reference (read-only) at $FGR_REF (default /root/reference); interp.py is imported from
+Run with FGR_REF set to a checkout of the reference (read-only); interp.py is imported from
 there, never copied, and its sha256 is pinned. Writes tests/golden/v1_golden.npz:
 
   per scene <name>:
@@ -54,7 +54,9 @@ def sha(*arrs):
 
 
 def load_interp():
-    ref = os.environ.get("FGR_REF", "/root/reference")
+    ref = os.environ.get("FGR_REF")
+    if not ref:
+        raise SystemExit("set FGR_REF to a checkout of the reference (the directory that holds proto/interp.py)")
     path = os.path.join(ref, "proto", "interp.py")
     digest = hashlib.sha256(open(path, "rb").read()).hexdigest()
     if digest != INTERP_SHA256:

@@ -137,12 +137,12 @@ def test_noalloc_frame_span_limit():
     at = (limit - 4 * W) // (H - 1)
     assert at % 4 == 0 and (H - 1) * at + 4 * W == limit
 
-    def call(pitch):
+    def call(pitch, field=None):
         f = fg.CFrame()
         f.data, f.pitch = 1 << 20, pitch
         err = ctypes.c_char_p()
         ok = fg.lib().fg_record_synth_noalloc(None, fg.VK_R8G8B8A8_UNORM, W, H, ctypes.byref(f), ctypes.byref(f),
-                                              ctypes.byref(f), None, 0, 0.5, ctypes.byref(fg.Settings().to_c()),
+                                              ctypes.byref(f), field, 0, 0.5, ctypes.byref(fg.Settings().to_c()),
                                               ctypes.byref(err))
         return ok, err.value.decode()
 
@@ -151,3 +151,6 @@ def test_noalloc_frame_span_limit():
     for pitch in (at + 4, limit + 4 * W, 1 << 62):
         ok, msg = call(pitch)
         assert not ok and "2^34" in msg, (pitch, msg)
+    # the field is read as float pairs: a 4-byte aligned stand-in pointer is refused before CUDA is used
+    ok, msg = call(at, field=(1 << 20) + 4)
+    assert not ok and "8-byte aligned" in msg, msg

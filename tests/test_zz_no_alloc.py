@@ -8,9 +8,11 @@ the frames and the output; the library's own scratch for this path is a fixed ar
 
 The test computes one estimate and a synth through the usual Interpolator entry points, then feeds the same frames,
 the estimate's field and its cut decision to fg_record_synth_noalloc twice in a row, and checks that both calls give
-the usual entry point's frame (bit-exact is expected; the tolerance of the parity tests, one level, is what is
-enforced). It also checks that a frame too large for the fixed scratch is refused with a clear message and that
-nothing is launched for it. This file is collected last so that a failure here cannot hide other tests' results.
+the usual entry point's frame, bit for bit (both run the same synthesis kernel on the same field). The second call
+must not change the device's free memory: after the first call on a device has placed the library's fixed array,
+nothing further is allocated. It also checks that a frame too large for the fixed scratch is refused with a clear
+message and that nothing is launched for it (the stream stays clean). This file is collected last so that a failure
+here cannot hide other tests' results.
 """
 import numpy as np
 import pytest
@@ -57,14 +59,18 @@ def test_noalloc_matches_synth_twice(kind, t):
     settings = fg.Settings()
     ref, field, cut = reference_synth(prev, curr, t, settings)
     a, c = to_dev(prev), to_dev(curr)
+    outs = [new_out(a) for _ in range(2)]
     for call in range(2):   # two calls in a row on the shared scratch
-        o = new_out(a)
-        ok, err = fg.record_synth_noalloc(a, c, o, field, cut, t, settings)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        ok, err = fg.record_synth_noalloc(a, c, outs[call], field, cut, t, settings)
         assert ok, err
         torch.cuda.synchronize()
-        got = o.cpu().numpy()
+        if call == 1:   # the first call may place the fixed array; the next one allocates nothing at all
+            assert torch.cuda.mem_get_info()[0] == free_before, "the second call changed the device's free memory"
+        got = outs[call].cpu().numpy()
         mx, mean, nd = frame_diff(got, ref)
-        assert mx <= TOL, f"call {call}: max diff {mx}, mean {mean}, {nd} bytes differ"
+        assert mx <= TOL and nd == 0, f"call {call}: max diff {mx}, mean {mean}, {nd} bytes differ"
 
 
 def test_noalloc_refuses_frames_beyond_its_scratch():
@@ -81,3 +87,12 @@ def test_noalloc_refuses_frames_beyond_its_scratch():
     # t outside (0, 1) is refused too, with its own reason
     ok, msg = fg.record_synth_noalloc(small, small, small, field, 0, 1.0)
     assert not ok and "outside" in msg
+    # nothing was launched for either call: the device is idle, and a valid call right after succeeds (the entry point
+    # reads cudaGetLastError after its first launch, so an error left pending by the refused calls would fail it)
+    torch.cuda.synchronize()
+    prev, curr = workloads.pan_pair(32, 32, seed=5)
+    a, c = to_dev(prev), to_dev(curr)
+    f16 = torch.zeros((16, 16, 2), dtype=torch.float32, device="cuda")
+    ok, msg = fg.record_synth_noalloc(a, c, new_out(a), f16, 0, 0.5)
+    assert ok, msg
+    torch.cuda.synchronize()
