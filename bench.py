@@ -11,7 +11,10 @@ pinned memory, records the estimate and 3 synths, and copies the 3 frames back.
 `roofline` is the dominant kernel (the fused synth) against the measured HBM copy bandwidth, its duration from the
 library's own per-pass CUDA events. `cpu_baseline` is the oracle (a plain-C restatement of proto/interp.py) on this
 host's cores. --impl reference times that CPU implementation itself (rank 0 only).
-Multi-GPU: every rank runs its own pairs (weak scaling, no collective on the data path).
+Multi-GPU: every rank runs its own pairs (weak scaling, no collective on the data path). `--gpus N` without a
+launcher starts the N ranks itself (one process per GPU, the launcher's environment variables, rendezvous on
+127.0.0.1); under torchrun the launcher's ranks are used and must number N. `value` is then the whole job's time per
+pair (the slowest rank's span over the pairs of all ranks) and `per_rank_ms_per_pair` the slowest rank's latency.
 """
 import argparse
 import json
@@ -58,7 +61,37 @@ def args():
     ap.add_argument("--no-seed-net", action="store_true")
     ap.add_argument("--psnr-pairs", type=int, default=8, help="held-out 4K pairs of the CNN-vs-plain PSNR check")
     ap.add_argument("--blur-samples", type=int, default=4, help="sub-frames of the motion-blur line (0: no line)")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="the rank plumbing only, on CPU with gloo: a stand-in host step, no GPU (for the CPU tests)")
     return ap.parse_args()
+
+
+def dry_run(a, world, rank):
+    """The rank logic of the timed region without a GPU: gloo, a barrier on both sides, a stand-in host step per pair,
+    the max of the ranks' spans; rank 0 prints a line shaped like the real one."""
+    import datetime
+    import torch.distributed as dist
+    import replicas
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    x = np.arange(1 << 16, dtype=np.float64)
+    for _ in range(a.warmup):
+        np.sort(x[::-1])
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        np.sort(x[::-1])
+    span = (time.perf_counter() - t0) * 1e3
+    if world > 1:
+        dist.barrier()
+    t_ms = replicas.max_over_ranks(span)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": round(t_ms / (a.steps * world), 6), "unit": "ms",
+                          "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                          "per_rank_ms_per_pair": round(t_ms / a.steps, 6), "dry_run": True}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def workload_pair():
@@ -309,11 +342,18 @@ def blur_arm(a, fg, pool, stream, world):
 
 def main():
     a = args()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ and not (a.impl == "reference" and not a.dry_run):
+        import replicas
+        sys.exit(replicas.spawn_ranks(os.path.abspath(__file__), sys.argv[1:], a.gpus))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference(a)
+    if world != a.gpus:
+        raise SystemExit(f"bench.py: --gpus {a.gpus} but the launcher started {world} rank(s)")
+    if a.dry_run:
+        return dry_run(a, world, rank)
     import torch
     import torch.distributed as dist
     import datetime
@@ -394,8 +434,8 @@ def main():
         dist.barrier()
     clocks = clock_summary(clk)
     t_ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
-    ms_per_step = t_ms / a.steps
-    value = t_ms / (a.steps * world)
+    ms_per_step = t_ms / a.steps          # the slowest rank's time per step (one pair on every rank)
+    value = t_ms / (a.steps * world)      # the whole job's time per pair
 
     # ---- per-pass device times (the library's CUDA events on its stream; the launches queue behind a sleep so the
     # events see back-to-back execution, not host gaps)
@@ -501,6 +541,8 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
+                "per_rank_ms_per_pair": round(ms_per_step, 4),
+                "value_is": "the whole job's device time per pair: the slowest rank's span / the pairs of all ranks",
                 "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
                 "config": {"workload": "V1 plain, 3840x2160 Rgba8, 4x (estimate + synths at t=1/4, 1/2, 3/4), "
                                        "flowScale 2, radii 6/2, subpixel on",

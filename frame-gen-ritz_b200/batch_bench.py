@@ -2,8 +2,8 @@
 2560x1440 / 3840x2160 in ratio 8:4:2:1 (34 / 17 / 9 / 4), formats cycling Rgba8 / Rgb10 / Nv12 / P010, multipliers
 cycling 2 / 3 / 4, content from the smooth-flow generator (workloads_gpu, per-pair seeds).
 
-    python frame-gen-ritz_b200/batch_bench.py [--reps 20]
-    torchrun --nproc-per-node N --master-addr 127.0.0.1 frame-gen-ritz_b200/batch_bench.py
+    python frame-gen-ritz_b200/batch_bench.py [--reps 20] [--gpus N]
+    torchrun --nproc-per-node N --master-addr 127.0.0.1 frame-gen-ritz_b200/batch_bench.py --gpus N
 
 Each launch shape is timed as a CUDA graph of one whole-batch record (device time, CUDA events, median of --reps
 replays); tune() then picks its shape. Prints one JSON line. Under torchrun the 64 pairs are partitioned over the ranks
@@ -56,7 +56,13 @@ def like(d):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--gpus", type=int, default=1, help="ranks, one per GPU (started here unless a launcher did)")
     a = ap.parse_args()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(replicas.spawn_ranks(os.path.abspath(__file__), sys.argv[1:], a.gpus))
+    if int(os.environ.get("WORLD_SIZE", "1")) != a.gpus:
+        raise SystemExit(f"batch_bench.py: --gpus {a.gpus} but the launcher started {os.environ.get('WORLD_SIZE')} "
+                         "rank(s)")
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:

@@ -8,6 +8,11 @@ Every function works on any torch.distributed backend (NCCL on GPUs; gloo on CPU
 single-process case when no process group is initialised.
 """
 import heapq
+import os
+import socket
+import subprocess
+import sys
+import time
 
 import torch
 import torch.distributed as dist
@@ -85,3 +90,32 @@ class GradSync:
     def rank_seed(self, seed):
         """the data seed of this rank (distinct crops per rank; the parameter initialisation uses the shared seed)"""
         return seed + 7919 * self.rank
+
+
+def free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def spawn_ranks(script, argv, n):
+    """A script asked for n GPUs without a launcher: run n copies of it, rank r on GPU r, with the variables a launcher
+    sets (RANK, LOCAL_RANK, WORLD_SIZE, LOCAL_WORLD_SIZE, MASTER_ADDR = 127.0.0.1, MASTER_PORT). If a rank fails, the
+    others are stopped after a grace period (their process group would otherwise end them by its timeout). Returns
+    the worst exit code."""
+    port = free_port()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, script] + list(argv), env=env))
+    failed_at = None
+    while any(p.poll() is None for p in procs):
+        if failed_at is None and any(p.returncode not in (None, 0) for p in procs):
+            failed_at = time.monotonic()
+        if failed_at is not None and time.monotonic() - failed_at > 30:
+            for p in procs:
+                if p.poll() is None:
+                    p.kill()
+        time.sleep(0.2)
+    return max(abs(p.returncode) for p in procs)

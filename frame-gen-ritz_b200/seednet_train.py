@@ -1,7 +1,7 @@
 """Train the seed proposer (csrc/fg_seednet.cu) on the GPU with the library's own kernels.
 
     python frame-gen-ritz_b200/seednet_train.py [--steps 3125] [--batch 64] [--lr 1e-3] [--out seednet_l1.bin]
-    torchrun --nproc-per-node N --master-addr 127.0.0.1 frame-gen-ritz_b200/seednet_train.py --batch 64 ...
+    python frame-gen-ritz_b200/seednet_train.py --gpus N ...   (or torchrun --nproc-per-node N ... --gpus N)
 
 Data-parallel under torchrun (one process per GPU, NCCL): every rank draws its own crops (--batch per rank, a global
 batch of N x --batch), the ranks' gradients are summed by one all-reduce of the 39,912 float32 values per step,
@@ -99,7 +99,13 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default=os.path.join(HERE, "seednet_l1.bin"))
     ap.add_argument("--log", default=None)
+    ap.add_argument("--gpus", type=int, default=1, help="ranks, one per GPU (started here unless a launcher did)")
     a = ap.parse_args()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(replicas.spawn_ranks(os.path.abspath(__file__), sys.argv[1:], a.gpus))
+    if int(os.environ.get("WORLD_SIZE", "1")) != a.gpus:
+        raise SystemExit(f"seednet_train.py: --gpus {a.gpus} but the launcher started {os.environ.get('WORLD_SIZE')} "
+                         "rank(s)")
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:

@@ -138,3 +138,21 @@ def test_reference_arm_on_a_nonzero_rank_exits_quietly():
                        env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_bench_spawns_its_ranks():
+    """`bench.py --gpus 2` without torchrun starts its two ranks itself (the rank plumbing of the timed region: gloo,
+    barriers, the max of the spans) and reports n_gpus 2; a launcher with a different rank count is refused."""
+    import json
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--gpus", "2", "--dry-run", "--steps", "5",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=240)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["steps"] == 5 and line["warmup"] == 3
+    assert line["value"] * 2 == pytest.approx(line["per_rank_ms_per_pair"], rel=1e-3)
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--gpus", "2", "--dry-run", "--steps", "2"],
+                       capture_output=True, text=True, timeout=240, env=env)
+    assert r.returncode != 0 and "--gpus 2" in r.stderr
