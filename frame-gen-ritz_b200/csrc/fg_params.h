@@ -27,7 +27,7 @@ struct DevState {
     unsigned int err;                  // sticky error bits (bound checks that could only fail on a library bug)
 };
 
-enum : unsigned int { kErrHistRange = 1u, kErrPlan = 2u };
+enum : unsigned int { kErrHistRange = 1u, kErrPlan = 2u, kErrSeedNet = 4u };
 
 // Frame formats other than 8-bit RGBA (framegen::Format) and their constants, computed on the host from InitInfo
 enum : int { kFmtRgba8 = 0, kFmtRgb10 = 1, kFmtF16 = 2, kFmtNv12 = 3, kFmtP010 = 4 };

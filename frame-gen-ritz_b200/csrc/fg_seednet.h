@@ -48,12 +48,26 @@ struct SnAdamArgs {
     float gscale;                                // the gradient is read as grad * gscale (1 / ranks after a sum)
 };
 
+// the fused forward (fg_seednet_tc.cu, tensor cores): B images of h x w float luma (prev, curr) -> per block 8 floats
+struct SnFusedArgs {
+    const float* la; const float* lc;   // [B][h][w] each
+    const void* wb;                     // bf16 parameters (the flat array)
+    const float* p;                     // float parameters (the biases)
+    void* y3;                           // layer 3's output, bf16 [B][h3][w3][32]
+    float* out;                         // [B][h3][w3][kSnOut]
+    int B, h, w, h1, w1, h2, w2, h3, w3;
+    unsigned int* err;                  // kErrSeedNet is or-ed in when a tensor-core wait gave up
+};
+cudaError_t prepareSeedNetFused();
+cudaError_t launchSnFused(const SnFusedArgs& a, cudaStream_t s);
+
 cudaError_t launchSnPack(const float* la, const float* lc, int n, void* x, cudaStream_t s);
 cudaError_t launchSnConv(int layer, const SnConvArgs& a, cudaStream_t s);
-// the forward of a net (fg_seednet_host.cpp) for the Interpolator: one image of h x w from its float luma planes;
-// *why = the failure's message
+// the forward of a net (fg_seednet_host.cpp) for the Interpolator: one image of h x w from its float luma planes, on
+// the fused tensor-core kernels; kErrSeedNet is or-ed into *err if a tensor-core wait gave up; *why = the failure's
+// message
 bool seedNetForwardLuma(::fg_seednet* n, cudaStream_t s, const float* la, const float* lc, int h, int w, float* out,
-                        const char** why);
+                        unsigned int* err, const char** why);
 cudaError_t launchSnBackward(int layer, const SnBackArgs& a, bool needDx, cudaStream_t s);
 cudaError_t launchSnLoss(const float* out, const float* tgt, int n, float* dout, float* loss, float scale, cudaStream_t s);
 cudaError_t launchSnAdam(const SnAdamArgs& a, cudaStream_t s);

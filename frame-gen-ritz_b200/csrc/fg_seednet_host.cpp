@@ -60,6 +60,7 @@ struct fg_seednet {
     float* grad = nullptr;
     float* loss = nullptr;
     void* act[kSnLayers - 1] = {};   // bf16 outputs of layers 1..5
+    unsigned int* errFlags = nullptr;   // the fused forward's sticky error bits (kErrSeedNet) when no other is given
     float* out = nullptr;            // last layer (float)
     float* dA = nullptr;             // gradient ping-pong buffers (float)
     float* dB = nullptr;
@@ -109,6 +110,18 @@ struct fg_seednet {
         return true;
     }
 
+    // the fused forward on the tensor cores (two launches, fg_seednet_tc.cu) from the float luma planes
+    bool forwardFused(cudaStream_t s, int B, int H, int W, float* dst, const float* la, const float* lc,
+                      unsigned int* errOut) {
+        const SnDims d(H, W);
+        SnFusedArgs a{};
+        a.la = la; a.lc = lc; a.wb = wb; a.p = p; a.y3 = act[2]; a.out = dst;
+        a.B = B; a.h = H; a.w = W;
+        a.h1 = d.h[1]; a.w1 = d.w[1]; a.h2 = d.h[2]; a.w2 = d.w[2]; a.h3 = d.h[3]; a.w3 = d.w[3];
+        a.err = errOut ? errOut : errFlags;
+        return ok(launchSnFused(a, s), "fused forward");
+    }
+
     bool backward(cudaStream_t s, const void* x, int B, int H, int W, const float* targets) {
         const SnDims d(H, W);
         const int nb = B * d.h[kSnLayers] * d.w[kSnLayers];
@@ -134,10 +147,10 @@ struct fg_seednet {
 
 namespace fgk {
 bool seedNetForwardLuma(::fg_seednet* n, cudaStream_t s, const float* la, const float* lc, int h, int w, float* out,
-                        const char** why) {
+                        unsigned int* err, const char** why) {
     if (!n || !n->fits(1, h, w)) { *why = "seed net workspace too small"; return false; }
     DevScope g(n->device);
-    if (n->forward(s, nullptr, 1, h, w, out, la, lc)) return true;
+    if (n->forwardFused(s, 1, h, w, out, la, lc, err)) return true;
     *why = n->err;
     return false;
 }
@@ -168,6 +181,7 @@ fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w) {
         maxGrad = std::max(maxGrad, e);
     }
     const size_t oOut = take((size_t)max_batch * d.h[kSnLayers] * d.w[kSnLayers] * kSnOut * 4);
+    const size_t oErr = take(4);
     const size_t oDA = take(maxGrad * 4), oDB = take(maxGrad * 4);
     if (cudaMalloc(&n->mem, off) != cudaSuccess) {
         cudaGetLastError();
@@ -180,6 +194,14 @@ fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w) {
     n->v = (float*)(n->mem + oV); n->grad = (float*)(n->mem + oG); n->loss = (float*)(n->mem + oL);
     for (int l = 0; l < kSnLayers - 1; l++) n->act[l] = n->mem + oAct[l];
     n->out = (float*)(n->mem + oOut);
+    n->errFlags = (unsigned int*)(n->mem + oErr);
+    if (prepareSeedNetFused() != cudaSuccess) {   // the fused kernels' shared-memory limits
+        cudaGetLastError();
+        cudaFree(n->mem);
+        delete n;
+        cudaSetDevice(old);
+        return nullptr;
+    }
     n->dA = (float*)(n->mem + oDA); n->dB = (float*)(n->mem + oDB);
     cudaDeviceSynchronize();
     cudaSetDevice(old);
@@ -242,6 +264,21 @@ int fg_seednet_forward_luma(fg_seednet* n, void* stream, const float* luma_prev,
     if (!n || !luma_prev || !luma_curr || !out || !n->fits(batch, h, w)) return 0;
     DevScope g(n->device);
     return n->forward((cudaStream_t)stream, nullptr, batch, h, w, out, luma_prev, luma_curr);
+}
+
+int fg_seednet_forward_fused(fg_seednet* n, void* stream, const float* luma_prev, const float* luma_curr, int batch,
+                            int h, int w, float* out) {
+    if (!n || !luma_prev || !luma_curr || !out || !n->fits(batch, h, w)) return 0;
+    DevScope g(n->device);
+    return n->forwardFused((cudaStream_t)stream, batch, h, w, out, luma_prev, luma_curr, nullptr);
+}
+
+uint32_t fg_seednet_fused_errors(fg_seednet* n) {
+    if (!n) return UINT32_MAX;
+    DevScope g(n->device);
+    uint32_t v = 0;
+    if (!n->ok(cudaMemcpy(&v, n->errFlags, 4, cudaMemcpyDeviceToHost))) return UINT32_MAX;
+    return v;
 }
 
 int fg_seednet_backward(fg_seednet* n, void* stream, const void* x, int batch, int h, int w, const float* targets,

@@ -415,7 +415,7 @@ struct Interpolator::Impl {
         stamp(s, "pyramid");
         if (snK >= 0) {   // the seed net on level snK
             const Level& lk = L.lv[snK];
-            if (!fgk::seedNetForwardLuma(snet, s, luma + lk.lumaA, luma + lk.lumaC, lk.h, lk.w, snOut, &lastErr))
+            if (!fgk::seedNetForwardLuma(snet, s, luma + lk.lumaA, luma + lk.lumaC, lk.h, lk.w, snOut, &st->err, &lastErr))
                 return false;
             stamp(s, "seed net");
         }

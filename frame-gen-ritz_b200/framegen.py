@@ -131,6 +131,8 @@ SIGNATURES = {
     "fg_seednet_pack": (_I, [_P, _P, _P, _I, _P]),
     "fg_seednet_forward": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "fg_seednet_forward_luma": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
+    "fg_seednet_forward_fused": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
+    "fg_seednet_fused_errors": (_U32, [_P]),
     "fg_seednet_backward": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
     "fg_seednet_zero_grads": (_I, [_P, _P]),
     "fg_seednet_adam": (_I, [_P, _P, _F]),
@@ -530,6 +532,20 @@ class SeedNet:
         self._ok(lib().fg_seednet_forward_luma(self._h, _stream(stream), luma_prev.data_ptr(), luma_curr.data_ptr(), B,
                                                h, w, out.data_ptr()))
         return out
+
+    def forward_fused(self, luma_prev, luma_curr, out=None, stream=None):
+        """the fused tensor-core forward (two launches; the Interpolator's) from (B, h, w) float32 luma planes"""
+        import torch
+        B, h, w = luma_prev.shape
+        if out is None:
+            out = torch.empty((B, (h + 7) // 8, (w + 7) // 8, self.N_OUT), dtype=torch.float32, device=luma_prev.device)
+        self._ok(lib().fg_seednet_forward_fused(self._h, _stream(stream), luma_prev.data_ptr(), luma_curr.data_ptr(),
+                                                B, h, w, out.data_ptr()))
+        return out
+
+    def fused_errors(self):
+        """the fused forward's sticky error bits (4: a tensor-core wait gave up); synchronous"""
+        return int(lib().fg_seednet_fused_errors(self._h))
 
     def backward(self, x, targets, loss=None, stream=None):
         B, h, w = x.shape[:3]

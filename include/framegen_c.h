@@ -160,6 +160,12 @@ int fg_seednet_forward(fg_seednet* net, void* stream, const void* x, int batch, 
 int fg_seednet_forward_luma(fg_seednet* net, void* stream, const float* luma_prev, const float* luma_curr, int batch, int h,
                            int w, float* out);
 /* forward + loss + backward: adds dLoss/dParams to the gradient; *loss (device float, optional) = the batch's loss */
+/* The same forward as fg_seednet_forward_luma, fused into two launches on the tensor cores (tcgen05, accumulators in
+ * tensor memory); the Interpolator's seed net runs this one. Same outputs up to the order of the f32 accumulation. */
+int fg_seednet_forward_fused(fg_seednet* net, void* stream, const float* luma_prev, const float* luma_curr, int batch,
+                            int h, int w, float* out);
+/* The fused forward's sticky error bits (4: a tensor-core wait gave up) on the net's own flag; synchronous. */
+uint32_t fg_seednet_fused_errors(fg_seednet* net);
 int fg_seednet_backward(fg_seednet* net, void* stream, const void* x, int batch, int h, int w, const float* targets,
                         float* loss);
 int fg_seednet_zero_grads(fg_seednet* net, void* stream);

@@ -180,3 +180,37 @@ def test_forward_from_luma_equals_packed_forward():
     torch.cuda.synchronize()
     assert torch.equal(a, b)
     net.close()
+
+
+@pytest.mark.parametrize("B,h,w,seed", [(2, 64, 64, 1), (1, 135, 240, 2), (3, 37, 51, 3), (1, 8, 8, 4),
+                                        (1, 540, 960, 5)])
+def test_fused_forward_matches_layers_and_fp64(B, h, w, seed):
+    """The Interpolator's fused forward (two launches, tcgen05 implicit GEMMs with accumulators in tensor memory)
+    against the per-layer forward (mma.sync) and the float64 reference. Same bf16 weights, inputs and activation
+    rounding; only the f32 accumulation order differs, so an activation can round to the other neighbouring bf16
+    now and then. Tolerances: against the per-layer forward max |diff| <= 0.02 * max(1, max |logit|) with the mean
+    |diff| below 1e-3 of that scale; against float64 the per-layer forward's own bound (0.03 * scale). The measured
+    errors are printed. Sizes: a 256x256 crop's level 1, a 1080p frame's level 1, odd sizes, one block, and a 4K
+    frame's level 1 (960x540, 144 encoder tiles)."""
+    rng = np.random.default_rng(seed)
+    la = (rng.random((B, h, w)) * 255).round(2).astype(np.float32)
+    lc = np.roll(la, (1, 2), axis=(1, 2)) + rng.normal(0, 2, (B, h, w)).astype(np.float32)
+    p = params(seed)
+    net = fg.SeedNet(B, h, w)
+    net.set_params(p)
+    ta, tc = torch.from_numpy(la).cuda(), torch.from_numpy(lc).cuda()
+    fused = net.forward_fused(ta, tc)
+    layers = net.forward_luma(ta, tc)
+    torch.cuda.synchronize()
+    assert net.fused_errors() == 0
+    f, l = fused.cpu().numpy().astype(np.float64), layers.cpu().numpy().astype(np.float64)
+    scale = max(1.0, np.abs(l).max())
+    d = np.abs(f - l)
+    print(f"fused vs per-layer: max {d.max():.4g} mean {d.mean():.3g} (scale {scale:.3g})")
+    assert d.max() <= 0.02 * scale and d.mean() <= 1e-3 * scale
+    if h * w <= 64 * 64 * 4:
+        want = ref.forward(ref.unflatten(p), ref.pack(la, lc)).detach().numpy()
+        err = np.abs(f - want).max()
+        print(f"fused vs float64: max {err:.4g}")
+        assert err <= 0.03 * max(1.0, np.abs(want).max())
+    net.close()
