@@ -1,0 +1,184 @@
+"""Known-answer check of the formats other than 8-bit RGBA against the reference's own output, not the oracle's
+restatement: the golden scenes' 8-bit content, encoded into each format as the reference's own format tests encode it,
+run through this library's format path, decoded back to 8-bit levels and compared with proto/interp.py's frames.
+
+interp.py is 8-bit only, so no reference output exists in these formats; what the reference holds them to is their
+distance from the 8-bit path on the same content. Its gates, restated here:
+  - gpu/formattest.cpp:117-175 (encode), :177-220 (decode), :957-960: Rgb10 (codes lround(v * 1023 / 255)) and
+    RgbaF16 encoded (v / 255) within >= 40 dB of the Rgba8 output of the same scene; RgbaF16 linear
+    ((v / 255)^2.2 * 4, linearWhiteNits 80) and BT.709 limited Nv12 / P010 (2x2 mean chroma) within >= 25 dB;
+  - webgl/tests/hdr.mjs:8, :25 with webgl/tests/hdr_pairs.py:1-8 (the "id" encoding, 8-bit values / 255 as half floats
+    against the 8-bit library output): mean absolute error <= 0.5 levels, at most 1 % of pixels more than 4 levels off;
+  - every format: the scene-cut and whole-frame decisions of interp.py.
+The 8-bit frames are interp.py's: stored in tests/golden/v1_golden.npz, or, where the fixture keeps only their sha256,
+this library's Rgba8 output checked against that digest first.
+"""
+import numpy as np
+import pytest
+import torch
+
+import framegen as fg
+from golden_io import golden, scene_inputs, scene_names, sha, times
+from gpu_util import decision
+
+pytestmark = pytest.mark.gpu
+
+KR, KB = 0.2126, 0.0722   # BT.709
+WHY = {None: 0, "cut": 1, "untrusted": 2}
+LIN_PEAK, LIN_GAMMA = 4.0, 2.2
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    import build
+    build.build()
+
+
+def lround(x):
+    return np.floor(x + 0.5)
+
+
+def encode(kind, rgba):
+    v = rgba[..., :3].astype(np.float64)
+    H, W = v.shape[:2]
+    if kind == "rgb10":
+        c = lround(v * 1023.0 / 255.0).astype(np.uint32)
+        return ((np.uint32(3) << 30) | (c[..., 2] << 20) | (c[..., 1] << 10) | c[..., 0]).view(np.int32)
+    if kind in ("f16_encoded", "f16_linear"):
+        e = (v / 255.0).astype(np.float32)   # the reference divides in float
+        if kind == "f16_linear":
+            e = (e.astype(np.float64) ** LIN_GAMMA * LIN_PEAK).astype(np.float32)
+        out = np.ones((H, W, 4), np.float16)
+        out[..., :3] = e.astype(np.float16)
+        return out.view(np.int16)
+    p010 = kind == "p010"
+    sc, top = (4.0, 1023.0) if p010 else (1.0, 255.0)
+    R, G, B = v[..., 0], v[..., 1], v[..., 2]
+    Y = KR * R + (1 - KR - KB) * G + KB * B
+    yc = lround(np.clip((16 + Y * 219.0 / 255.0) * sc, 0, top))
+    cb = 128 + (B - Y) / (2 * (1 - KB)) * 224.0 / 255.0
+    cr = 128 + (R - Y) / (2 * (1 - KR)) * 224.0 / 255.0
+    ch, cw = (H + 1) // 2, (W + 1) // 2
+    ys = np.minimum(np.arange(2 * ch), H - 1)[:, None]
+    xs = np.minimum(np.arange(2 * cw), W - 1)[None, :]
+
+    def mean2(p):   # the 2x2 mean, the last row / column repeated for odd sizes
+        return p[ys, xs].reshape(ch, 2, cw, 2).mean(axis=(1, 3))
+
+    cbc = lround(np.clip(mean2(cb) * sc, 0, top))
+    crc = lround(np.clip(mean2(cr) * sc, 0, top))
+    C = np.stack([cbc, crc], axis=2)
+    if p010:
+        return ((yc.astype(np.uint16) << 6).view(np.int16), (C.astype(np.uint16) << 6).view(np.int16))
+    return yc.astype(np.uint8), C.astype(np.uint8)
+
+
+def decode(kind, out, W, H):
+    """the output -> float RGB levels (H, W, 3), as gpu/formattest.cpp decodes it"""
+    if kind == "rgb10":
+        w = out.view(np.uint32)
+        return np.stack([((w >> (10 * c)) & 1023).astype(np.float64) * 255.0 / 1023.0 for c in range(3)], axis=2)
+    if kind in ("f16_encoded", "f16_linear"):
+        v = out.view(np.float16)[..., :3].astype(np.float64)
+        if kind == "f16_linear":
+            return 255.0 * (np.maximum(v, 0.0) / LIN_PEAK) ** (1.0 / LIN_GAMMA)
+        return v * 255.0
+    y, c = out
+    if kind == "p010":
+        Y = (y.view(np.uint16) >> 6) / 4.0
+        cb = (c.view(np.uint16)[..., 0] >> 6) / 4.0
+        cr = (c.view(np.uint16)[..., 1] >> 6) / 4.0
+    else:
+        Y, cb, cr = y.astype(np.float64), c[..., 0].astype(np.float64), c[..., 1].astype(np.float64)
+    cb = np.repeat(np.repeat(cb, 2, axis=0), 2, axis=1)[:H, :W]
+    cr = np.repeat(np.repeat(cr, 2, axis=0), 2, axis=1)[:H, :W]
+    yf, bb, rr = (Y - 16) * 255.0 / 219.0, (cb - 128) * 255.0 / 224.0, (cr - 128) * 255.0 / 224.0
+    R, B = yf + 2 * (1 - KR) * rr, yf + 2 * (1 - KB) * bb
+    G = (yf - KR * R - KB * B) / (1 - KR - KB)
+    return np.stack([R, G, B], axis=2)
+
+
+KINDS = {
+    "rgb10": (fg.VK_A2B10G10R10_UNORM, {}, 40.0),
+    "f16_encoded": (fg.VK_R16G16B16A16_SFLOAT, {"transfer": 0}, 40.0),
+    "f16_linear": (fg.VK_R16G16B16A16_SFLOAT, {"transfer": 1, "linear_white_nits": 80.0}, 25.0),
+    "nv12": (fg.VK_R8_UNORM, {"yuv_matrix": 1, "yuv_full_range": False}, 25.0),
+    "p010": (fg.VK_R16_UNORM, {"yuv_matrix": 1, "yuv_full_range": False}, 25.0),
+}
+
+
+def dev(x):
+    return tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in x) if isinstance(x, tuple) else \
+        torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def like(d):
+    return tuple(torch.zeros_like(p) for p in d) if isinstance(d, tuple) else torch.zeros_like(d)
+
+
+def host(d):
+    return tuple(p.cpu().numpy() for p in d) if isinstance(d, tuple) else d.cpu().numpy()
+
+
+def interp_frames(name, prev, curr):
+    """interp.py's 8-bit frames (R, G, B levels) at every fixture time: stored, or this library's Rgba8 output pinned
+    by the fixture's sha256 of interp.py's frame"""
+    G = golden()
+    H, W = prev.shape[:2]
+    I = fg.Interpolator()
+    assert I.init(W, H, fg.VK_R8G8B8A8_UNORM), I.init_error()
+    a, c = dev(prev), dev(curr)
+    I.begin_frame()
+    assert I.record_estimate(a, c)
+    frames = []
+    for k, t in enumerate(times()):
+        o = torch.zeros_like(a)
+        assert I.record_synth(a, c, o, t)
+        got = o.cpu().numpy()
+        if f"{name}/out_t{k}" in G:   # interp.py's BGR frame
+            frames.append(G[f"{name}/out_t{k}"][..., [2, 1, 0]].astype(np.float64))
+        else:
+            bgr = np.ascontiguousarray(got[..., [2, 1, 0]])
+            assert np.array_equal(sha(bgr), G[f"{name}/outsha_t{k}"]), f"{name}: the Rgba8 output at t={t} is not interp.py's"
+            frames.append(got[..., :3].astype(np.float64))
+    I.close()
+    return frames
+
+
+@pytest.mark.parametrize("kind", list(KINDS))
+def test_format_against_interp(kind):
+    vk, extra, min_db = KINDS[kind]
+    worst_db, worst_mae, worst_pct = 99.0, 0.0, 0.0
+    rows = []
+    for name in scene_names():
+        prev, curr = scene_inputs(name)
+        H, W = prev.shape[:2]
+        ref = interp_frames(name, prev, curr)
+        I = fg.Interpolator()
+        assert I.init(W, H, vk, **extra), I.init_error()
+        a, c = dev(encode(kind, prev)), dev(encode(kind, curr))
+        I.begin_frame()
+        assert I.record_estimate(a, c), I.last_error()
+        cnt = torch.zeros(2, dtype=torch.int32, device="cuda")
+        for k, t in enumerate(times()):
+            o = like(a)
+            assert I.record_synth(a, c, o, t), I.last_error()
+            assert I.record_debug_counters(cnt)
+            torch.cuda.synchronize()
+            tr = fg.read_trace(I)
+            got = decode(kind, host(o), W, H)
+            d = np.abs(got - ref[k])
+            mse = float(np.mean(d ** 2))
+            db = 99.0 if mse == 0 else 10 * np.log10(255.0 ** 2 / mse)
+            mae, pct4 = float(d.mean()), 100.0 * float(np.mean(d.max(axis=2) > 4.0))
+            # the whole-frame decision (none / scene cut / untrusted share) against interp.py's
+            mine = WHY[decision(tr["cut"], int(cnt[0]), W, H)]
+            assert mine == int(golden()[f"{name}/why_t{k}"][0]), f"{kind} {name} t={t}: decision differs from interp.py's"
+            worst_db, worst_mae, worst_pct = min(worst_db, db), max(worst_mae, mae), max(worst_pct, pct4)
+            rows.append((name, t, round(db, 2), round(mae, 3), round(pct4, 3)))
+        I.close()
+    print(f"{kind}: worst PSNR against interp.py {worst_db:.2f} dB, worst MAE {worst_mae:.3f} levels, "
+          f"worst share > 4 levels {worst_pct:.3f} %")
+    assert worst_db >= min_db, rows
+    if kind == "f16_encoded":   # the "id" encoding of webgl/tests/hdr.mjs
+        assert worst_mae <= 0.5 and worst_pct <= 1.0, rows
