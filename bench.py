@@ -37,7 +37,6 @@ FW, FH = W4K // 2, H4K // 2
 # algorithmic bytes of one fused synth launch: both frames read, the per-pixel field read, the output written
 SYNTH_BYTES = 2 * 4 * W4K * H4K + 8 * FW * FH + 4 * W4K * H4K
 PAIR_BYTES = 2 * 4 * W4K * H4K + 8 * FW * FH + 3 * SYNTH_BYTES     # (A): 431,308,800 B per pair
-CPU_CROP = (960, 540)   # the CPU sample: 1/16 of the 4K area
 
 
 def args():
@@ -52,7 +51,9 @@ def args():
                     help="e2e: streams per copy direction, each frame split into that many row bands (on a B200 one "
                          "stream already fills the PCIe link: 1.96 ms per pair with 1, 2.00-2.02 with 2-4)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (the oracle's timing and the parity checks)")
+    ap.add_argument("--parity-c1-pairs", type=int, default=100, help="1080p pairs of the parity check (config 1)")
+    ap.add_argument("--parity-c2-pairs", type=int, default=2, help="4K RgbaF16 pairs of the parity check (config 2)")
     ap.add_argument("--eager", type=int, default=0,
                     help="profiling mode: run this many eager steps (no graphs, no timing, no JSON) and exit")
     ap.add_argument("--seed-net", default=os.path.join(REPO, "frame-gen-ritz_b200", "seednet_l1.bin"),
@@ -100,26 +101,223 @@ def workload_pair():
     return p, c
 
 
-def cpu_sample(p, c, seconds, threads=0):
-    """The oracle on 960x540 crops of the 4K pair (estimate + 3 synths each), repeated for about `seconds`; returns
-    (ms per 4K pair, crops timed). Time scales with area: x16."""
+def frame_stats(got, ref):
+    d = np.abs(got.astype(np.int32) - ref.astype(np.int32))
+    return int(d.max()), float(d.sum()), d.size, int(np.count_nonzero(d))
+
+
+class ParityTally:
+    """max / mean absolute difference, differing bytes and decision agreement over many frames"""
+
+    def __init__(self):
+        self.mx, self.sum, self.n, self.nd, self.frames, self.pairs, self.dec_ok, self.dec_n = 0, 0.0, 0, 0, 0, 0, 0, 0
+
+    def add(self, got, ref):
+        mx, sm, n, nd = frame_stats(got, ref)
+        self.mx, self.sum, self.n, self.nd, self.frames = max(self.mx, mx), self.sum + sm, self.n + n, self.nd + nd, \
+            self.frames + 1
+
+    def decision(self, same):
+        self.dec_n += 1
+        self.dec_ok += int(bool(same))
+
+    def report(self, **extra):
+        return dict({"pairs": self.pairs, "frames": self.frames, "max_abs_diff": self.mx,
+                     "mean_abs_diff": round(self.sum / max(self.n, 1), 9), "bytes_differing": self.nd,
+                     "decisions_agree": f"{self.dec_ok}/{self.dec_n}"}, **extra)
+
+
+def gpu_decision(cut, untrusted, W, H, frac=0.15):
+    if cut:
+        return "cut"
+    return "untrusted" if untrusted / (W * H) > float(np.float32(frac)) else None
+
+
+def cpu_leg(pool, outs, seconds):
+    """The CPU baseline on the metric's own workload: the oracle (the plain-C port of proto/interp.py, all host
+    threads) runs estimate + 3 synths on full 3840x2160 pairs of the pool, for about `seconds` (at least every pool
+    pair once); returns (median ms per pair, pairs timed, parity of the GPU's outputs of those pairs against the
+    oracle's: the oracle is the checker here, its outputs are compared with what the graphs left in `outs`)."""
     import oracle
-    cw, ch = CPU_CROP
     times = []
+    tally = ParityTally()
+    host = [(pool[k][0].cpu().numpy(), pool[k][1].cpu().numpy()) for k in range(len(pool))]
+    got = [[o.cpu().numpy() for o in outs[k]] for k in range(len(pool))]
     t_end = time.perf_counter() + seconds
     k = 0
     while True:
-        y0, x0 = (k * 540) % (H4K - ch + 1), (k * 960) % (W4K - cw + 1)
-        a, cc = np.ascontiguousarray(p[y0:y0 + ch, x0:x0 + cw]), np.ascontiguousarray(c[y0:y0 + ch, x0:x0 + cw])
+        j = k % len(pool)
+        p, c = host[j]
         t0 = time.perf_counter()
-        est = oracle.estimate(a, cc, trace=False, threads=threads)
-        for t in TS:
-            oracle.synth(a, cc, est, t, threads=threads)
+        est = oracle.estimate(p, c, trace=False)
+        res = [oracle.synth(p, c, est, t) for t in TS]
         times.append(time.perf_counter() - t0)
+        if k < len(pool):
+            tally.pairs += 1
+            for (ref, _), g in zip(res, got[j]):
+                tally.add(g, ref)
         k += 1
-        if time.perf_counter() > t_end and k >= 2:
+        if time.perf_counter() > t_end and k >= len(pool):
             break
-    return statistics.median(times) * 1e3 * (W4K * H4K) / (cw * ch), k
+    return statistics.median(times) * 1e3, k, tally
+
+
+def parity_configs(a, fg):
+    """Every workload configuration of the path against the oracle (rank 0, N = 1; part of the CPU leg: the oracle
+    runs on the host for each): config 0 (640x360, 2x, one pair, also its device latency), config 1 (1080p 4x, a sample
+    of --parity-c1-pairs of the 500), config 2 (4K RgbaF16 linear 3x, --parity-c2-pairs of the 200), config 3 (the
+    full 64-pair mixed batch: every slot against a standalone Interpolator, the Rgba8 slots against the oracle)."""
+    import torch
+    import oracle
+    import workloads
+    import workloads_gpu
+    out = {}
+    cnt = torch.zeros(2, dtype=torch.int32, device="cuda")
+
+    def pair_through(I, da, dc, ts):
+        I.begin_frame()
+        assert I.record_estimate(da, dc)
+        tr = fg.read_trace(I)
+        res = []
+        for t in ts:
+            o = torch.empty_like(da)
+            assert I.record_synth(da, dc, o, t)
+            assert I.record_debug_counters(cnt)
+            torch.cuda.synchronize()
+            res.append((o.cpu().numpy(), int(cnt[0])))
+        return tr, res
+
+    # config 0
+    p, c = workloads.pan_pair()
+    I = fg.Interpolator()
+    assert I.init(640, 360, fg.VK_R8G8B8A8_UNORM), I.init_error()
+    da, dc = torch.from_numpy(p).cuda(), torch.from_numpy(c).cuda()
+    tr, res = pair_through(I, da, dc, [0.5])
+    tally = ParityTally()
+    tally.pairs = 1
+    est = oracle.estimate(p, c, trace=False)
+    ref, why = oracle.synth(p, c, est, 0.5)
+    tally.add(res[0][0], ref)
+    tally.decision(gpu_decision(tr["cut"], res[0][1], 640, 360) == why and tr["sad"] == est["sad"])
+    o = torch.empty_like(da)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        I.begin_frame()
+        I.record_estimate(da, dc, stream=s)
+        I.record_synth(da, dc, o, 0.5, stream=s)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            I.begin_frame()
+            I.record_estimate(da, dc, stream=s)
+            I.record_synth(da, dc, o, 0.5, stream=s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lat = []
+        for _ in range(50):
+            e0.record(s)
+            g.replay()
+            e1.record(s)
+            torch.cuda.synchronize()
+            lat.append(e0.elapsed_time(e1) * 1e3)
+    del g
+    I.close()
+    out["config0"] = tally.report(workload="640x360 Rgba8 2x (t = 1/2), the panning pair with sprite and HUD",
+                                  latency_us=round(statistics.median(lat), 2),
+                                  latency_method="median of 50 CUDA-graph replays of estimate + synth, device time")
+    # config 1
+    tally = ParityTally()
+    I = fg.Interpolator()
+    assert I.init(1920, 1080, fg.VK_R8G8B8A8_UNORM), I.init_error()
+    gen = torch.Generator(device="cuda")
+    kinds = [0, 0, 0]
+    n1 = a.parity_c1_pairs
+    for b in range((n1 + 9) // 10):
+        gen.manual_seed(1 * 10 ** 6 + b)
+        d = workloads_gpu.flow_batch(10, 1920, 1080, gen)
+        for k in range(min(10, n1 - 10 * b)):
+            da, dc = d["prev"][k].contiguous(), d["curr"][k].contiguous()
+            kinds[int(d["kind"][k])] += 1
+            tr, res = pair_through(I, da, dc, TS)
+            p, c = da.cpu().numpy(), dc.cpu().numpy()
+            est = oracle.estimate(p, c, trace=False)
+            tally.pairs += 1
+            for (g_out, u), t in zip(res, TS):
+                ref, why = oracle.synth(p, c, est, t)
+                tally.add(g_out, ref)
+                tally.decision(gpu_decision(tr["cut"], u, 1920, 1080) == why and tr["sad"] == est["sad"])
+    I.close()
+    out["config1"] = tally.report(workload=f"1920x1080 Rgba8 4x, {n1} of the 500 smooth-flow pairs ({kinds[1]} cuts, "
+                                           f"{kinds[2]} fresh); all 500 run in tests/test_configs_gpu.py")
+    # config 2
+    spec = oracle.FormatSpec("f16", linear=True, white=80.0)
+    ts2 = (float(np.float32(1 / 3)), float(np.float32(2 / 3)))
+    I = fg.Interpolator()
+    assert I.init(3840, 2160, fg.VK_R16G16B16A16_SFLOAT, transfer=1, linear_white_nits=80.0), I.init_error()
+    worst, ndiff, frames, dec_ok, dec_n = 0.0, 0, 0, 0, 0
+    for k in range(a.parity_c2_pairs):
+        gen.manual_seed(2 * 10 ** 6 + k)
+        da, dc = workloads_gpu.hdr_pair(3840, 2160, gen)
+        tr, res = pair_through(I, da, dc, ts2)
+        ah, ch = da.cpu().numpy(), dc.cpu().numpy()
+        est = oracle.estimate_fmt(ah, ch, spec)
+        for (got, u), t in zip(res, ts2):
+            ref = oracle.synth_fmt(ah, ch, est, t, spec, trace=True)
+            nd = got.view(np.uint16) != ref["out"].view(np.uint16)
+            ndiff += int(np.count_nonzero(nd))
+            frames += 1
+            dec_n += 1
+            dec_ok += int(gpu_decision(tr["cut"], u, 3840, 2160) == ref["reason"])
+            if nd.any():
+                pq = np.vectorize(lambda v: oracle.pq255(v, 80.0))
+                worst = max(worst, float(np.abs(pq(got[nd].astype(np.float32)) - pq(ref["out"][nd].astype(np.float32))).max()))
+    I.close()
+    out["config2"] = {"pairs": a.parity_c2_pairs, "frames": frames, "max_abs_diff_pq_levels": worst,
+                      "half_floats_differing": ndiff, "decisions_agree": f"{dec_ok}/{dec_n}",
+                      "workload": f"3840x2160 RgbaF16 linear 3x, {a.parity_c2_pairs} of the 200 HDR pairs; 16 run in "
+                                  "tests/test_configs_gpu.py"}
+    # config 3
+    import batch_bench
+    slots = batch_bench.slots()
+    B = fg.Batch()
+    prev, curr, bouts, rgba = [], [], [], {}
+    for i, (w, h, fmt, m) in enumerate(slots):
+        assert B.add(w, h, batch_bench.VK[fmt], multiplier=m) == i, B.error()
+        gen.manual_seed(3 * 10 ** 6 + i)
+        d = workloads_gpu.flow_batch(1, w, h, gen)
+        if fmt == "rgba8":
+            rgba[i] = (d["prev"][0].cpu().numpy(), d["curr"][0].cpu().numpy())
+        prev.append(batch_bench.to_dev(fmt, d["prev"][0].contiguous()))
+        curr.append(batch_bench.to_dev(fmt, d["curr"][0].contiguous()))
+        bouts += [batch_bench.like(prev[-1]) for _ in range(m - 1)]
+    assert B.record(prev, curr, bouts), B.error()
+    torch.cuda.synchronize()
+    st, orc = ParityTally(), ParityTally()
+    j = 0
+    for i, (w, h, fmt, m) in enumerate(slots):
+        I = fg.Interpolator()
+        assert I.init(w, h, batch_bench.VK[fmt]), I.init_error()
+        I.begin_frame()
+        assert I.record_estimate(prev[i], curr[i])
+        st.pairs += 1
+        est = oracle.estimate(*rgba[i], trace=False) if fmt == "rgba8" else None
+        orc.pairs += est is not None
+        for t in fg.Batch.times(m):
+            o = batch_bench.like(prev[i])
+            assert I.record_synth(prev[i], curr[i], o, t)
+            torch.cuda.synchronize()
+            for x, y in zip(o if isinstance(o, tuple) else (o,), bouts[j] if isinstance(bouts[j], tuple) else (bouts[j],)):
+                st.add(y.cpu().numpy(), x.cpu().numpy())
+            if est is not None:
+                ref, _ = oracle.synth(*rgba[i], est, t)
+                orc.add(bouts[j].cpu().numpy(), ref)
+            j += 1
+        I.close()
+    rs, ro = st.report(), orc.report()
+    rs.pop("decisions_agree")
+    ro.pop("decisions_agree")
+    out["config3"] = {"workload": "the 64-pair mixed batch at full size, one Batch record in its default shape",
+                      "vs_standalone": rs, "rgba8_vs_oracle": ro}
+    return out
 
 
 def clock_sampler(local_rank):
@@ -174,13 +372,30 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def sources_sha(paths):
+    import hashlib
+    h = hashlib.sha256()
+    for rel in paths:
+        with open(os.path.join(REPO, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
 def ncu_synth():
-    """the committed ncu summary of one 4K synth launch (profiles/synth_4k.json): dram bytes, warp instructions"""
+    """the committed ncu summary of one 4K synth launch (profiles/synth_4k.json): dram bytes, warp instructions. It
+    records the sha256 of the kernel sources it was captured from; when they have changed since, the figures are
+    stale and are not reported ({"stale": True})."""
     try:
         with open(os.path.join(REPO, "profiles", "synth_4k.json")) as f:
-            return json.load(f)
+            prof = json.load(f)
     except (OSError, ValueError):
         return {}
+    try:
+        if sources_sha(prof["sources"]) != prof["source_sha256"]:
+            return {"stale": True}
+    except (KeyError, OSError):
+        return {"stale": True}
+    return prof
 
 
 def issue_roofline(prof, synth_us, clocks):
@@ -198,26 +413,26 @@ def issue_roofline(prof, synth_us, clocks):
 
 
 def run_reference(a):
+    """The reference arm: the CPU implementation of the path (the oracle port of proto/interp.py, all host threads) on
+    the metric's workload itself, full 3840x2160 pairs, estimate + 3 synths per step (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import oracle
     p, c = workload_pair()
     cores = os.cpu_count()
-    cw, ch = CPU_CROP
-    scale = (W4K * H4K) / (cw * ch)
-    import oracle
     step_ms = []
     for i in range(a.warmup + a.steps):
-        y0, x0 = (i * 540) % (H4K - ch + 1), (i * 960) % (W4K - cw + 1)
-        pa, pc = np.ascontiguousarray(p[y0:y0 + ch, x0:x0 + cw]), np.ascontiguousarray(c[y0:y0 + ch, x0:x0 + cw])
+        k = i % 4   # four distinct pairs: the same content rolled, as the GPU arm's pool
+        pa, pc = np.roll(p, (53 * k, 97 * k), axis=(0, 1)), np.roll(c, (53 * k, 97 * k), axis=(0, 1))
         t0 = time.perf_counter()
         est = oracle.estimate(pa, pc, trace=False)
         for t in TS:
             oracle.synth(pa, pc, est, t)
         if i >= a.warmup:
-            step_ms.append((time.perf_counter() - t0) * 1e3 * scale)
+            step_ms.append((time.perf_counter() - t0) * 1e3)
     v = statistics.median(step_ms)
-    sample = f"{cw}x{ch} crops of the 4K pair (1/16 area), estimate + 3 synths per step, time x16; oracle, {cores} threads"
+    sample = f"full 3840x2160 pairs (4 distinct, cycled), estimate + 3 synths per step; oracle, {cores} threads"
     print(json.dumps({"metric": METRIC, "value": round(v, 3), "unit": "ms", "impl": "reference", "n_gpus": a.gpus,
                       "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
                       "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
@@ -521,22 +736,32 @@ def main():
         last = (step_no[0] - 1) % 2
         assert all(torch.equal(h, e.cpu()) for h, e in zip(hout[last], eager0)), "e2e output differs"
 
+    # the CPU leg (rank 0, N = 1): every pool slot's plain outputs once more, then the oracle on the same pairs
+    cpu = parity = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        with torch.cuda.stream(stream):
+            for g in graphs:
+                g.replay()
+        torch.cuda.synchronize()
+        v, n, tally = cpu_leg(pool, outs, a.cpu_seconds)
+        cpu = {"value": round(v, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n} full 3840x2160 pairs of the pool, estimate + 3 synths each, median; oracle (plain-C "
+                         f"restatement of proto/interp.py, OpenMP, all host threads)"}
+        parity = {"metric_workload": tally.report(workload="the bench's 4K pool: the GPU's graph outputs against the "
+                                                            "oracle's")}
+        parity["metric_workload"].pop("decisions_agree")
+        parity.update(parity_configs(a, fg))
+
     blur = blur_arm(a, fg, pool, stream, world) if a.blur_samples >= 2 else None
     seed = None
     if not a.no_seed_net and os.path.exists(a.seed_net):
         seed = seed_net_arm(a, fg, pool, outs, stream, world, I)
 
-    cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu:
-        v, n = cpu_sample(p_np, c_np, a.cpu_seconds)
-        cpu = {"value": round(v, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{n} 960x540 crops of the 4K pair (1/16 area each), estimate + 3 synths, median x16; "
-                         f"oracle (plain-C restatement of proto/interp.py, OpenMP)"}
 
     peak, peak_kind = measured_peak()
     achieved = SYNTH_BYTES / (synth_us * 1e-6) / 1e9
     prof = ncu_synth()
-    traffic = prof.get("dram_bytes_per_launch")
+    traffic = prof.get("dram_bytes_per_launch")   # None when the capture is stale
     del graphs
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": a.steps,
@@ -553,13 +778,14 @@ def main():
                 "hbm_gbs_per_pair": round(PAIR_BYTES / (value * 1e-3) / 1e9 / world, 1),
                 "roofline": {"bound": "hbm", "kernel": "k_synth", "achieved": round(achieved, 1),
                              "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                             "traffic": traffic, "algorithmic_bytes": SYNTH_BYTES, "duration_us": round(synth_us, 2)},
+                             "traffic": traffic, "traffic_stale": bool(prof.get("stale")),
+                             "algorithmic_bytes": SYNTH_BYTES, "duration_us": round(synth_us, 2)},
                 "issue_roofline": issue_roofline(prof, synth_us, clocks),
                 "breakdown_us": breakdown,
                 "gpu_launches": launches_per_step * a.steps,
                 "e2e": {"value": round(e2e_value, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 4 * W4K * H4K,
                         "d2h_bytes_per_step": len(TS) * 4 * W4K * H4K},
-                "cpu_baseline": cpu, "clocks": clocks, "seed_net": seed, "motion_blur": blur}
+                "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "seed_net": seed, "motion_blur": blur}
         print(json.dumps(line), flush=True)
     I.close()
     if world > 1:
