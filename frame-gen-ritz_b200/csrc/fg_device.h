@@ -76,6 +76,24 @@ __device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
 // round-half-even(x * 32) for |x * 32| < 2^22 (cv2's saturate_cast<int>(x * INTER_TAB_SIZE)), as the float's bits
+// CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl): does the bilinear tap whose position rounded to
+// 1/32 px is (X, Y) (in 1/32 px) read, with a non-zero weight, a pixel that the UI mask m (header + bytes, fg_params.h
+// UiV2Params) marks? The tap reads lo = (X >> 5, Y >> 5) .. lo + (the fraction is not 0) per axis.
+__device__ __forceinline__ bool uiHitMask(const uint32_t* __restrict__ m, int X, int Y) {
+    const uint32_t wh = __ldg(m + 2);
+    if (wh == 0u) return false;
+    const uint32_t o = __ldg(m + 1);
+    const int ox = (int)(o & 0xFFFFu), oy = (int)(o >> 16), w = (int)(wh & 0xFFFFu), h = (int)(wh >> 16);
+    const int stride = (int)__ldg(m + 3);
+    const int lx = X >> 5, ly = Y >> 5;
+    const int x0 = max(lx - ox, 0), y0 = max(ly - oy, 0);
+    const int x1 = min(lx + ((X & 31) != 0) - ox, w - 1), y1 = min(ly + ((Y & 31) != 0) - oy, h - 1);
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++)
+            if ((__ldg(m + 4 + y * stride + (x >> 2)) >> (8 * (x & 3))) & 255u) return true;
+    return false;
+}
+
 __device__ __forceinline__ float2 rne32bits(float2 v) {
     return __ffma2_rn(v, make_float2(32.0f, 32.0f), make_float2(12582912.0f, 12582912.0f));
 }

@@ -1074,7 +1074,7 @@ __device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, u
 // (alpha = the nearer frame's). The untrusted count is added to *p.untrusted unless that is null. kCut: under a scene
 // cut the tile is a copy of the nearer frame to p.out (and the core returns at once); without kCut the caller has
 // taken the cut into account.
-template <bool kCut, class Sink>
+template <bool kCut, bool kUi = false, class Sink>
 __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int by, Sink&& sink) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ SyCoef rowc[kSyEH];
@@ -1121,7 +1121,20 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
         const float2 ba = rne32bits(make_float2(__fsub_rn(cx.pos, __fmul_rn(kA, hx)), __fsub_rn(cy.pos, __fmul_rn(kA, hy))));
         const float2 bc = rne32bits(make_float2(__fadd_rn(cx.pos, __fmul_rn(kC, hx)), __fadd_rn(cy.pos, __fmul_rn(kC, hy))));
         int ca[3], cc[3];
-        const uint32_t A = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y, ca), C = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y, cc);
+        uint32_t A = sampleU8(fa32, pw, p.W, p.H, ba.x, ba.y, ca), C = sampleU8(fc32, pw, p.W, p.H, bc.x, bc.y, cc);
+        if (kUi) {   // CrosshairV2: a tap on its own frame's UI takes the other frame's tap (both or neither: kept)
+            const bool ha = p.uiA && uiHitMask(p.uiA, __float_as_int(ba.x) - 0x4B400000, __float_as_int(ba.y) - 0x4B400000);
+            const bool hc = p.uiC && uiHitMask(p.uiC, __float_as_int(bc.x) - 0x4B400000, __float_as_int(bc.y) - 0x4B400000);
+            if (ha != hc) {
+                if (ha) {
+                    A = C;
+                    ca[0] = cc[0]; ca[1] = cc[1]; ca[2] = cc[2];
+                } else {
+                    C = A;
+                    cc[0] = ca[0]; cc[1] = ca[1]; cc[2] = ca[2];
+                }
+            }
+        }
         if ((unsigned)(ey - kSyAp) < (unsigned)kSyTH) {   // warp-uniform
             sWA[(ey - kSyAp) * kSyE + ex] = A;
             sWC[(ey - kSyAp) * kSyE + ex] = C;
@@ -1192,8 +1205,9 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
 }
 
 // one output tile of one synthesis, stored to p.out
+template <bool kUi = false>
 __device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) {
-    synthTileCore<true>(p, bx, by, [&](int, int x, int y, int, uint32_t o) {
+    synthTileCore<true, kUi>(p, bx, by, [&](int, int x, int y, int, uint32_t o) {
         reinterpret_cast<uint32_t*>(p.out + (size_t)y * p.outPitch)[x] = o;
     });
 }
@@ -1201,6 +1215,12 @@ __device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) 
 __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
     pdlEnter();
     synthTile(p, blockIdx.x, blockIdx.y);
+}
+
+// the same with CrosshairV2's warp-tap rejection (p.uiA / p.uiC); a separate kernel so the plain one is unchanged
+__global__ void __launch_bounds__(kSyThreads) k_synth_ui(const SynthParams p) {
+    pdlEnter();
+    synthTile<true>(p, blockIdx.x, blockIdx.y);
 }
 
 // Motion blur (gpu/framegen.h:553-573, gpu/shaders/blur_resolve.comp): out = round(sum_k w_k frame_k), frame_k the
@@ -1211,7 +1231,8 @@ __global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
 // mean of prev's and curr's alpha. A flick (more than globalFallback of a sample's pixels untrusted) is known only
 // when every tile has counted: the main pass (fix = 0) assumes none and counts per sample; the fix-up pass (fix = 1)
 // exits at once unless some synthesized sample flicked, and then redoes every tile with those samples replaced.
-__global__ void __launch_bounds__(kSyThreads, 2) k_synth_blur(const BlurParams bp) {
+template <bool kUi>
+__global__ void __launch_bounds__(kSyThreads, 2) k_synth_blur_t(const BlurParams bp) {
     pdlEnter();
     __shared__ __align__(16) SynthParams sp;
     __shared__ unsigned int sRepl, sRedo;   // samples replaced by a real frame; whether this pass has work
@@ -1261,7 +1282,7 @@ __global__ void __launch_bounds__(kSyThreads, 2) k_synth_blur(const BlurParams b
         }
         __syncthreads();
         const uint32_t q = bp.smp[j].q;
-        synthTileCore<false>(sp, blockIdx.x, blockIdx.y, [&](int k, int, int, int, uint32_t o) {
+        synthTileCore<false, kUi>(sp, blockIdx.x, blockIdx.y, [&](int k, int, int, int, uint32_t o) {
             acc[k][0] += q * (o & 255u);
             acc[k][1] += q * ((o >> 8) & 255u);
             acc[k][2] += q * ((o >> 16) & 255u);
@@ -1405,8 +1426,13 @@ cudaError_t prepareKernels() {
         e = cudaFuncSetAttribute(k_synth_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(synthSmemBytes(1) + kSyWarpBytes));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_synth_blur, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(k_synth_blur_t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(synthSmemBytes(1) + kSyWarpBytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_blur_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(synthSmemBytes(1) + kSyWarpBytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_ui, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(synthSmemBytes(1) + kSyWarpBytes));
     return e;
 }
 cudaError_t launchSubpix(const SubpixParams& p, cudaStream_t s) {
@@ -1429,14 +1455,17 @@ int synthTilesX(int W) { return (int)divUp(W, kSyT); }
 int synthTilesY(int H) { return (int)divUp(H, kSyTH); }
 cudaError_t launchSynth(const SynthParams& p, cudaStream_t s) {
     const size_t smem = synthSmemBytes(p.fs) + kSyWarpBytes;
-    return launchPdl(k_synth, dim3(divUp(p.W, kSyT), divUp(p.H, kSyTH)), dim3(kSyThreads), smem, s, p);
+    const dim3 grid(divUp(p.W, kSyT), divUp(p.H, kSyTH));
+    if (p.uiA || p.uiC) return launchPdl(k_synth_ui, grid, dim3(kSyThreads), smem, s, p);
+    return launchPdl(k_synth, grid, dim3(kSyThreads), smem, s, p);
 }
 cudaError_t launchSynthBlur(const BlurParams& bp, int fix, cudaStream_t s) {
     const size_t smem = synthSmemBytes(bp.base.fs) + kSyWarpBytes;
     const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
     BlurParams p = bp;
     p.fix = fix;
-    return launchPdl(k_synth_blur, grid, dim3(kSyThreads), smem, s, p);
+    if (p.base.uiA || p.base.uiC) return launchPdl(k_synth_blur_t<true>, grid, dim3(kSyThreads), smem, s, p);
+    return launchPdl(k_synth_blur_t<false>, grid, dim3(kSyThreads), smem, s, p);
 }
 cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s) {
     return launchPdl(k_synth_batch, dim3(grid), dim3(kSyThreads), smem, s, b);

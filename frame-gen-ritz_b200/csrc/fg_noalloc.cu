@@ -98,7 +98,7 @@ extern "C" int fg_record_synth_noalloc(void* stream, uint32_t view_format, uint3
     *err = nullptr;
     framegen::Settings set;
     if (settings) {
-        fg_settings c = *settings;
+        const fg_settings& c = *settings;   // the V1 fields only (a caller's struct may end after pyramidMinSide)
         set.trustLow = c.trustLow; set.trustHigh = c.trustHigh; set.globalFallback = c.globalFallback;
         set.sceneCutSad = c.sceneCutSad; set.hudBonus = c.hudBonus; set.smoothBonus = c.smoothBonus;
         set.searchPenalty = c.searchPenalty; set.searchRadius = c.searchRadius; set.searchRadiusTop = c.searchRadiusTop;

@@ -142,6 +142,9 @@ struct SynthParams {
     FmtConst f;
     const uint8_t* ac; const uint8_t* cc; size_t cpitch;
     uint8_t* outc; size_t outCPitch;
+    // CrosshairV2's warp-tap rejection (8-bit RGBA): the UI masks of prev and curr (header + bytes, see UiV2Params);
+    // both null = off
+    const uint32_t* uiA; const uint32_t* uiC;
 };
 
 struct SynthBatchArgs {             // k_synth_batch: a work list of syntheses
@@ -215,6 +218,35 @@ cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s);
 // one pass of a motion blur in the other formats (bp.base.f.format): the main pass (fix = 0), then the fix-up
 cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s);
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s);
+
+// CrosshairV2 static-UI protection (gpu/shaders/ui_v2_update.comp, ui_v2_mask.comp, ui_patch.comp), 8-bit RGBA.
+// State: 4 words per pixel of the work rectangle (the box grown by 1 px, clamped to the frame):
+//   w0 = previous original (r | g << 8 | b << 16) | still-and-contrasty count << 24
+//   w1 = last confirmed colour | flags << 24 (bit 0 in the mask, bit 1 has a stored colour, bit 2 still in this pair)
+//   w2 = consecutive changed frames while in the mask | consecutive stored-colour matches while out of it << 8
+// Mask buffer of one kept frame: header words [1] = x | y << 16, [2] = w | h << 16, [3] = words per row; from word 4
+// the bytes (4 pixels per word): 255 = UI and unchanged in this pair (pasted), 64 = UI but changed, 0 = not UI.
+constexpr int kUiMaskHeader = 4;
+struct UiV2Params {
+    const uint8_t* frame; size_t pitch;
+    int W, H, ri, gi, bi;
+    int bx, by, bw, bh;            // the box (detection)
+    int wx, wy, ww, wh;            // the work rectangle (state and mask)
+    uint32_t* st;
+    int reset;                     // the state describes no previous frame
+    float thr, cthr;               // uiStillThreshold, uiContrastThreshold (8-bit levels)
+    int still, leave, reentry;     // uiStillFrames, uiLeaveFrames, uiReentryFrames
+    uint32_t* mask;                // observe: this frame's mask buffer; recordTrack: null
+    int maskStride;                // words per mask row
+};
+struct UiPatchParams {
+    const uint8_t* curr; size_t pitch;
+    uint8_t* out; size_t outPitch;
+    const uint32_t* mask;
+};
+cudaError_t launchUiV2Update(const UiV2Params& p, cudaStream_t s);
+cudaError_t launchUiV2Mask(const UiV2Params& p, cudaStream_t s);
+cudaError_t launchUiPatch(const UiPatchParams& p, int wx, int wy, int ww, int wh, cudaStream_t s);
 
 // Streaming multiprocessors of the current device (cached per device); grids of the grid-stride kernels are sized in
 // multiples of it.

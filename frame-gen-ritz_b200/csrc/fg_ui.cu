@@ -1,0 +1,173 @@
+// Static-UI protection, CrosshairV2 mode, for 8-bit RGBA / BGRA frames: the passes of recordObserve / recordTrack and
+// the paste-back after a synthesis. The warp-tap rejection between them lives in the synthesis kernels (uiHitMask in
+// fg_device.h). Restates the reference's Vulkan shaders gpu/shaders/ui_v2_update.comp, ui_v2_mask.comp and
+// ui_patch.comp (binary paste); layouts in fg_params.h (UiV2Params).
+//
+//   k_ui_v2_update  one thread per pixel of the work rectangle: the per-pixel state machine (still / contrasty / in the
+//                   mask / leave and re-entry counters). The local contrast, max channel |I - median7x7(I)|, is found
+//                   only where it can matter (out of the mask and still or matching its stored colour): per channel a
+//                   binary search on the value for the smallest m with at least 25 of the 49 levels <= m, the window's
+//                   49 pixels packed one word each in registers.
+//   k_ui_v2_mask    one thread per mask word (4 pixels): in the mask or within 1 px of it -> 255 if still in this pair,
+//                   else 64; writes the rectangle into the header.
+//   k_ui_patch      one thread per work-rectangle pixel: out = the real curr pixel (colour channels) where the byte is
+//                   255.
+// The work rectangle of a 4K frame's default box is 56 x 56 pixels: these passes are latency-sized, not bandwidth-sized.
+#include <cstdint>
+
+#include "fg_device.h"
+#include "fg_params.h"
+
+namespace fgk {
+namespace {
+
+constexpr int kUiTX = 16, kUiTY = 8;   // threads per CTA of the update and patch passes
+
+__device__ __forceinline__ uint32_t uiPixel(const UiV2Params& p, int x, int y) {   // r | g << 8 | b << 16, clamped
+    x = min(max(x, 0), p.W - 1);
+    y = min(max(y, 0), p.H - 1);
+    const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(p.frame + (size_t)y * p.pitch) + x);
+    return ((v >> (8 * p.ri)) & 255u) | (((v >> (8 * p.gi)) & 255u) << 8) | (((v >> (8 * p.bi)) & 255u) << 16);
+}
+
+__device__ __forceinline__ int maxAbsDiff(uint32_t a, uint32_t b) {
+    int m = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) m = max(m, abs((int)((a >> (8 * c)) & 255u) - (int)((b >> (8 * c)) & 255u)));
+    return m;
+}
+
+// max channel |v - median7x7| at (x, y)
+__device__ int contrastAt(const UiV2Params& p, int x, int y, uint32_t v) {
+    uint32_t w[49];
+#pragma unroll
+    for (int j = 0; j < 7; j++)
+#pragma unroll
+        for (int i = 0; i < 7; i++) w[j * 7 + i] = uiPixel(p, x + i - 3, y + j - 3);
+    int d = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        int lo = 0, hi = 255;
+        for (int it = 0; it < 8; it++) {
+            const int mid = (lo + hi) >> 1;
+            int cnt = 0;
+#pragma unroll
+            for (int j = 0; j < 49; j++) cnt += (int)((w[j] >> (8 * c)) & 255u) <= mid;
+            if (cnt >= 25) hi = mid;
+            else lo = mid + 1;
+        }
+        d = max(d, abs((int)((v >> (8 * c)) & 255u) - lo));
+    }
+    return d;
+}
+
+__global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_v2_update(const UiV2Params p) {
+    pdlEnter();
+    const int x = blockIdx.x * kUiTX + threadIdx.x, y = blockIdx.y * kUiTY + threadIdx.y;
+    if (x >= p.ww || y >= p.wh) return;
+    const int sx = p.wx + x, sy = p.wy + y;
+    const uint32_t now = uiPixel(p, sx, sy);
+    uint32_t* s = p.st + ((size_t)y * p.ww + x) * 4;
+    const int ix = sx - p.bx, iy = sy - p.by;
+    if (ix < 0 || iy < 0 || ix >= p.bw || iy >= p.bh) {   // the margin ring: only the pair gate
+        uint32_t ring = 0;
+        if (!p.reset && (float)maxAbsDiff(now, s[0] & 0xFFFFFFu) <= p.thr) ring = 4u;
+        s[0] = now;
+        s[1] = ring << 24;
+        s[2] = 0u;
+        return;
+    }
+    uint32_t cnt = 0, flags = 0, leave = 0, match = 0, stored = 0;
+    if (!p.reset) {
+        const uint32_t w0 = s[0], w1 = s[1], w2 = s[2];
+        flags = w1 >> 24;
+        stored = w1 & 0xFFFFFFu;
+        leave = w2 & 255u;
+        match = (w2 >> 8) & 255u;
+        const bool still = (float)maxAbsDiff(now, w0 & 0xFFFFFFu) <= p.thr;
+        bool inMask = (flags & 1u) != 0u, hasStored = (flags & 2u) != 0u;
+        const bool matchS = !inMask && hasStored && p.reentry > 0 && (float)maxAbsDiff(now, stored) <= p.thr;
+        bool contrasty = p.cthr <= 0.0f;
+        if (!inMask && !contrasty && (still || matchS)) contrasty = (float)contrastAt(p, sx, sy, now) >= p.cthr;
+        if (inMask) {
+            leave = still ? 0u : min(leave + 1u, 255u);
+            if (still) stored = now;
+            if ((int)leave >= p.leave) {
+                inMask = false;
+                leave = 0u;
+                match = 0u;
+            }
+            cnt = 0u;
+        } else {
+            cnt = (still && contrasty) ? min((w0 >> 24) + 1u, 255u) : 0u;
+            match = (matchS && contrasty) ? min(match + 1u, 255u) : 0u;
+            if ((int)cnt >= p.still || (p.reentry > 0 && hasStored && (int)match >= p.reentry)) {
+                inMask = true;
+                hasStored = true;
+                stored = now;
+                leave = 0u;
+                match = 0u;
+            }
+        }
+        flags = (inMask ? 1u : 0u) | (hasStored ? 2u : 0u) | (still ? 4u : 0u);
+    }
+    s[0] = now | (cnt << 24);
+    s[1] = stored | (flags << 24);
+    s[2] = leave | (match << 8);
+}
+
+__device__ __forceinline__ uint32_t uiFlagsAt(const UiV2Params& p, int x, int y) {
+    if (x < 0 || y < 0 || x >= p.ww || y >= p.wh) return 0u;
+    return p.st[((size_t)y * p.ww + x) * 4 + 1] >> 24;
+}
+
+__global__ void __launch_bounds__(128) k_ui_v2_mask(const UiV2Params p) {
+    pdlEnter();
+    const int g = blockIdx.x * 128 + threadIdx.x;
+    if (g >= p.maskStride * p.wh) return;
+    const int gx = g % p.maskStride, gy = g / p.maskStride;
+    uint32_t word = 0;
+    for (int k = 0; k < 4; k++) {
+        const int x = gx * 4 + k;
+        if (x >= p.ww) break;
+        bool near = false;
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) near = near || (uiFlagsAt(p, x + dx, gy + dy) & 1u) != 0u;
+        uint32_t a = 0;
+        if (near) a = (uiFlagsAt(p, x, gy) & 4u) != 0u ? 255u : 64u;
+        word |= a << (8 * k);
+    }
+    p.mask[kUiMaskHeader + g] = word;
+    if (g == 0) {
+        p.mask[0] = 0u;
+        p.mask[1] = (uint32_t)p.wx | ((uint32_t)p.wy << 16);
+        p.mask[2] = (uint32_t)p.ww | ((uint32_t)p.wh << 16);
+        p.mask[3] = (uint32_t)p.maskStride;
+    }
+}
+
+__global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_patch(const UiPatchParams p, int wx, int wy, int ww, int wh) {
+    pdlEnter();
+    const int x = blockIdx.x * kUiTX + threadIdx.x, y = blockIdx.y * kUiTY + threadIdx.y;
+    if (x >= ww || y >= wh) return;
+    const int stride = (int)p.mask[3];
+    const uint32_t a = (p.mask[kUiMaskHeader + y * stride + (x >> 2)] >> (8 * (x & 3))) & 255u;
+    if (a != 255u) return;
+    uint32_t* o = reinterpret_cast<uint32_t*>(p.out + (size_t)(wy + y) * p.outPitch) + wx + x;
+    const uint32_t real = __ldg(reinterpret_cast<const uint32_t*>(p.curr + (size_t)(wy + y) * p.pitch) + wx + x);
+    *o = (real & 0x00FFFFFFu) | (*o & 0xFF000000u);   // colour channels from the real frame, alpha kept
+}
+
+}  // namespace
+
+cudaError_t launchUiV2Update(const UiV2Params& p, cudaStream_t s) {
+    return launchPdl(k_ui_v2_update, dim3(divUp(p.ww, kUiTX), divUp(p.wh, kUiTY)), dim3(kUiTX, kUiTY), 0, s, p);
+}
+cudaError_t launchUiV2Mask(const UiV2Params& p, cudaStream_t s) {
+    return launchPdl(k_ui_v2_mask, dim3(divUp(p.maskStride * p.wh, 128)), dim3(128), 0, s, p);
+}
+cudaError_t launchUiPatch(const UiPatchParams& p, int wx, int wy, int ww, int wh, cudaStream_t s) {
+    return launchPdl(k_ui_patch, dim3(divUp(ww, kUiTX), divUp(wh, kUiTY)), dim3(kUiTX, kUiTY), 0, s, p, wx, wy, ww, wh);
+}
+
+}  // namespace fgk

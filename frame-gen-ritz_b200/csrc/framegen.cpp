@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -136,7 +137,9 @@ size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 const char* kErrSettings = "invalid settings: a field is out of range or not finite (see Interpolator::validate)";
 const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
-const char* kErrUi = "static-UI protection is not built into this library (Settings::uiProtection must be Off)";
+const char* kErrUi = "static-UI protection: only CrosshairV2 is built into this library (Crosshair and WholeScreen are not)";
+const char* kErrUiFormat = "static-UI protection (CrosshairV2) is built for the 8-bit RGBA / BGRA formats only";
+const char* kErrUiFill = "static-UI protection: uiEstimateFill is not built into this library";
 const char* kErrNoFormat = "unsupported viewFormat (see framegen::Format)";
 const char* kErrYuvMatrix = "yuvMatrix must be Bt601, Bt709 or Bt2020";
 const char* kErrNits = "linearWhiteNits must be in (0, 10000]";
@@ -239,6 +242,23 @@ struct Interpolator::Impl {
     int snLevelReq = -1, snK = -1;
     fg_seednet* snet = nullptr;
     float* snOut = nullptr;    // its output, bw x bh x kSeedNetOut floats
+    // static-UI protection, CrosshairV2 (recordObserve / recordTrack): the box and work rectangle of this size and
+    // settings, the per-pixel state of the work rectangle, and the kept frames' masks (LRU by observe order)
+    struct UiEntry {
+        const void* key = nullptr;    // the frame (device pointer); null = free
+        uint32_t* mask = nullptr;     // header + bytes (fg_params.h UiV2Params)
+        uint64_t stamp = 0;           // observe order
+    };
+    std::vector<UiEntry> uiE;
+    uint32_t* uiState = nullptr;
+    int32_t uiBox[4] = {}, uiWork[4] = {};
+    int uiStride = 0;
+    bool uiReset = true, uiExplicit = false;
+    const void* uiLast = nullptr;
+    uint64_t uiClock = 0;
+    bool estUi = false;
+    int estEnt[2] = {-1, -1};
+    uint64_t estStamp[2] = {0, 0};
     // profiling
     bool profiling = false;
     std::vector<cudaEvent_t> events;
@@ -273,8 +293,139 @@ struct Interpolator::Impl {
         return nullptr;
     }
 
+    bool uiOn() const { return set.uiProtection == UiProtection::CrosshairV2; }
+
+    void uiFree() {
+        DeviceGuard g(device);
+        for (UiEntry& e : uiE)
+            if (e.mask) cudaFree(e.mask);
+        uiE.clear();
+        if (uiState) cudaFree(uiState);
+        uiState = nullptr;
+        uiWork[2] = uiWork[3] = 0;
+        uiReset = true;
+        uiLast = nullptr;
+        estUi = false;
+    }
+
+    // the protection's buffers for the current size and settings (outside any capture; only ever allocates, except
+    // when the work rectangle changes): the state of the work rectangle, uiHistory masks. A new rectangle (size or box
+    // change) or `restart` (protection switched on) starts the state afresh and forgets every kept frame.
+    const char* uiSetup(bool restart) {
+        if (!uiOn() || !W) return nullptr;
+        int32_t box[4], work[4];
+        Interpolator::boxRect(set, W, H, box);
+        Interpolator::workRect(set, W, H, work);
+        const bool same = uiState && std::equal(work, work + 4, uiWork) && std::equal(box, box + 4, uiBox);
+        DeviceGuard g(device);
+        if (!same) {
+            uiFree();
+            std::copy(box, box + 4, uiBox);
+            std::copy(work, work + 4, uiWork);
+            uiStride = (work[2] + 3) / 4;
+            if (cudaMalloc((void**)&uiState, (size_t)work[2] * work[3] * 16) != cudaSuccess) {
+                cudaGetLastError();
+                uiState = nullptr;
+                uiWork[2] = uiWork[3] = 0;
+                return kErrAlloc;
+            }
+            restart = true;
+        }
+        if (restart) {
+            uiReset = true;
+            uiLast = nullptr;
+            for (UiEntry& e : uiE) e.key = nullptr;
+            estUi = false;
+        }
+        const size_t words = (size_t)fgk::kUiMaskHeader + (size_t)uiStride * uiWork[3];
+        while (uiE.size() < set.uiHistory) {
+            UiEntry e;
+            if (cudaMalloc((void**)&e.mask, words * 4) != cudaSuccess) {
+                cudaGetLastError();
+                return kErrAlloc;
+            }
+            uiE.push_back(e);
+        }
+        uiEvict(set.uiHistory);
+        return nullptr;
+    }
+
+    int uiCount() const {
+        int n = 0;
+        for (const UiEntry& e : uiE) n += e.key != nullptr;
+        return n;
+    }
+    // forget the least recently observed frames until at most `keep` are kept
+    void uiEvict(uint32_t keep) {
+        while ((uint32_t)uiCount() > keep) {
+            UiEntry* old = nullptr;
+            for (UiEntry& e : uiE)
+                if (e.key && (!old || e.stamp < old->stamp)) old = &e;
+            old->key = nullptr;
+        }
+    }
+    int uiFind(const void* key) const {
+        for (size_t i = 0; i < uiE.size(); i++)
+            if (uiE[i].key == key) return (int)i;
+        return -1;
+    }
+
+    // one observed (track = false) or tracked frame: the state update, then (observe) the frame's mask in its entry
+    bool uiObserve(cudaStream_t s, const Frame& f, bool track) {
+        fgk::UiV2Params p{};
+        p.frame = (const uint8_t*)f.data; p.pitch = f.pitch;
+        p.W = (int)W; p.H = (int)H; p.ri = ri; p.gi = gi; p.bi = bi;
+        p.bx = uiBox[0]; p.by = uiBox[1]; p.bw = uiBox[2]; p.bh = uiBox[3];
+        p.wx = uiWork[0]; p.wy = uiWork[1]; p.ww = uiWork[2]; p.wh = uiWork[3];
+        p.st = uiState;
+        p.reset = uiReset;
+        p.thr = set.uiStillThreshold; p.cthr = set.uiContrastThreshold;
+        p.still = (int)set.uiStillFrames; p.leave = (int)set.uiLeaveFrames; p.reentry = (int)set.uiReentryFrames;
+        p.maskStride = uiStride;
+        int slot = uiFind(f.data);
+        if (track) {
+            if (slot >= 0) uiE[slot].key = nullptr;   // the frame holds new pixels: its kept mask is stale
+        } else if (slot < 0) {
+            uiEvict(set.uiHistory - 1);
+            slot = uiFind(nullptr);
+        }
+        p.mask = track ? nullptr : uiE[slot].mask;
+        if (!check(fgk::launchUiV2Update(p, s))) return false;
+        if (!track) {
+            if (!check(fgk::launchUiV2Mask(p, s))) return false;
+            uiE[slot].key = f.data;
+            uiE[slot].stamp = ++uiClock;
+            uiLast = f.data;
+        }
+        uiReset = false;
+        stamp(s, track ? "ui track" : "ui observe");
+        return true;
+    }
+
+    // the kept masks the latest estimate's pair uses, if they are still the same entries (else a synthesis refuses)
+    bool uiPairMasks(const uint32_t*& ma, const uint32_t*& mc) const {
+        ma = mc = nullptr;
+        if (!uiOn() || !estUi) return true;
+        for (int k = 0; k < 2; k++) {
+            if (estEnt[k] < 0 || estEnt[k] >= (int)uiE.size()) return false;
+            const UiEntry& e = uiE[estEnt[k]];
+            if (e.key != (k ? estCurr : estPrev) || e.stamp != estStamp[k]) return false;
+        }
+        ma = uiE[estEnt[0]].mask;
+        mc = uiE[estEnt[1]].mask;
+        return true;
+    }
+
+    bool uiPatch(cudaStream_t s, const Frame& curr, const Frame& out, const uint32_t* mc) {
+        fgk::UiPatchParams pp{(const uint8_t*)curr.data, curr.pitch, (uint8_t*)out.data, out.pitch, mc};
+        if (!check(fgk::launchUiPatch(pp, uiWork[0], uiWork[1], uiWork[2], uiWork[3], s))) return false;
+        stamp(s, "ui patch");
+        return true;
+    }
+
     void freeAll() {
         DeviceGuard g(device);
+        uiFree();
         freeSeedNet();
         if (arena) cudaFree(arena);
         arena = nullptr;
@@ -349,7 +500,8 @@ struct Interpolator::Impl {
         W = w;
         H = h;
         haveEst = false;
-        return setupSeedNet();
+        if (const char* e = setupSeedNet()) return e;
+        return uiSetup(true);
     }
 
     // a frame the kernels can address: plane 0 (and the CbCr plane of YUV) aligned to its sample size, rows wide enough,
@@ -526,7 +678,8 @@ struct Interpolator::Impl {
 
     // recordSynthBlur (gpu/framegen.cpp:3534-3630): every sample's synthesis parameters as recordSynth(t_k) builds
     // them, the per-sample counters zeroed, then the blur's main and fix-up passes
-    bool blur(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t0, float t1) {
+    bool blur(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t0, float t1,
+              const uint32_t* ma, const uint32_t* mc) {
         float tk[Interpolator::kBlurMaxSamples];
         uint32_t q[Interpolator::kBlurMaxSamples];
         const int n = (int)Interpolator::blurPlan(set.blurSamples, set.blurWeights, t0, t1, tk, q);
@@ -534,6 +687,8 @@ struct Interpolator::Impl {
         fgk::BlurParams bp{};
         bp.base = synthParams(prev, curr, out, 0.5f, nullptr);
         bp.base.emap = nullptr;
+        bp.base.uiA = ma;
+        bp.base.uiC = mc;
         for (int k = 0; k < n; k++) {
             fgk::BlurSample& m = bp.smp[k];
             m.q = q[k];
@@ -554,11 +709,16 @@ struct Interpolator::Impl {
         stamp(s, "blur resolve");
         if (!check(rgba8 ? fgk::launchSynthBlur(bp, 1, s) : fgk::launchSynthBlurFmt(bp, 1, s))) return false;
         stamp(s, "blur fixup");
-        return true;
+        return !mc || uiPatch(s, curr, out, mc);
     }
 
-    bool synth(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t) {
-        const fgk::SynthParams sp = synthParams(prev, curr, out, t, &st->untrusted[parity]);
+    // ma / mc: the pair's UI masks (CrosshairV2) or null: the tap rejection in the synthesis, then curr's UI pixels
+    // pasted back over the finished frame
+    bool synth(cudaStream_t s, const Frame& prev, const Frame& curr, const Frame& out, float t, const uint32_t* ma,
+               const uint32_t* mc) {
+        fgk::SynthParams sp = synthParams(prev, curr, out, t, &st->untrusted[parity]);
+        sp.uiA = ma;
+        sp.uiC = mc;
         if (!check(fmt == Format::Rgba8 ? fgk::launchSynth(sp, s) : fgk::launchSynthFmt(sp, s))) return false;
         stamp(s, "synth");
         const fgk::FallbackParams fp = fallbackParams(sp, &st->untrusted[parity ^ 1u]);
@@ -566,7 +726,7 @@ struct Interpolator::Impl {
         stamp(s, "fallback");
         lastParity = parity;
         parity ^= 1u;
-        return true;
+        return !mc || uiPatch(s, curr, out, mc);
     }
 };
 
@@ -599,8 +759,9 @@ bool Interpolator::validate(const Settings& s) {
 const char* Interpolator::settingsError(const Settings& s, Format f) {
     if (!validate(s)) return kErrSettings;
     if (s.motionVersion != MotionVersion::V1) return kErrVersion;
-    if (s.uiProtection != UiProtection::Off) return kErrUi;
-    (void)f;
+    if (s.uiProtection != UiProtection::Off && s.uiProtection != UiProtection::CrosshairV2) return kErrUi;
+    if (s.uiProtection == UiProtection::CrosshairV2 && f != Format::Rgba8) return kErrUiFormat;
+    if (s.uiProtection == UiProtection::CrosshairV2 && s.uiEstimateFill) return kErrUiFill;
     return nullptr;
 }
 
@@ -684,9 +845,23 @@ bool Interpolator::resize(uint32_t w, uint32_t h, uint32_t viewFormat) {
     return m->allocSize(w, h) == nullptr;
 }
 
+// A change of static-UI protection's mode or box restarts its state and drops the current estimate (gpu/framegen.h:590-592)
+static bool uiGeometryChanged(const Settings& a, const Settings& b) {
+    return a.uiProtection != b.uiProtection || a.uiBoxHeightFrac != b.uiBoxHeightFrac || a.uiBoxWidth != b.uiBoxWidth ||
+           a.uiBoxHeight != b.uiBoxHeight || a.uiCrosshairArea != b.uiCrosshairArea || a.uiBoxOffsetX != b.uiBoxOffsetX ||
+           a.uiBoxOffsetY != b.uiBoxOffsetY;
+}
+
 bool Interpolator::setSettings(const Settings& s) {
     if (!m || settingsError(s) || s.flowScale != m->set.flowScale || s.pyramidMinSide != m->set.pyramidMinSide) return false;
+    const Settings old = m->set;
+    const bool restart = uiGeometryChanged(old, s);
     m->set = s;
+    if (m->uiSetup(restart)) {   // the allocation failed: nothing changed
+        m->set = old;
+        return false;
+    }
+    if (restart) m->haveEst = m->estUi = false;
     m->updateTrust();
     return true;
 }
@@ -699,6 +874,10 @@ bool Interpolator::reconfigure(const Settings& s) {
     m->updateTrust();
     if (structural && m->W) {
         if (m->allocSize(m->W, m->H)) { m->set = old; m->updateTrust(); m->allocSize(m->W, m->H); return false; }
+    } else if (m->W) {
+        const bool restart = uiGeometryChanged(old, s);
+        if (m->uiSetup(restart)) { m->set = old; m->updateTrust(); return false; }
+        if (restart) m->haveEst = m->estUi = false;
     }
     return true;
 }
@@ -709,7 +888,25 @@ void Interpolator::beginFrame() {
     if (m) m->estSets = m->synthSets = 0;
 }
 
-void Interpolator::releaseUnusedUi() {}       // no UI-protection memory is ever held
+void Interpolator::releaseUnusedUi() {
+    if (!m) return;
+    DeviceGuard g(m->device);
+    if (!m->uiOn()) {
+        m->uiFree();
+        return;
+    }
+    // free the masks beyond uiHistory (uiEvict already keeps at most uiHistory frames): the forgotten entries go
+    for (size_t i = m->uiE.size(); i-- > 0 && m->uiE.size() > m->set.uiHistory;) {
+        if (m->uiE[i].key) continue;
+        if (m->uiE[i].mask) cudaFree(m->uiE[i].mask);
+        m->uiE.erase(m->uiE.begin() + (long)i);
+    }
+    if (m->estUi) {   // the kept entries moved: the estimate's pair by key (same stamps, or the synthesis refuses)
+        m->estEnt[0] = m->uiFind(m->estPrev);
+        m->estEnt[1] = m->uiFind(m->estCurr);
+        m->estUi = m->estEnt[0] >= 0 && m->estEnt[1] >= 0;
+    }
+}
 void Interpolator::releaseUnusedMotion() {}   // V1 is the only motion version
 
 bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
@@ -719,11 +916,94 @@ bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
     DeviceGuard g(m->device);
     m->estSets++;
     m->haveEst = false;
+    m->estUi = false;
+    if (m->uiOn() && !m->uiExplicit && m->uiState) {   // the implicit observe (gpu/framegen.h:602-609)
+        if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
+        if (m->uiFind(prev.data) < 0 && !m->uiObserve(stream, prev, false)) return false;
+        if (m->uiLast != curr.data && !m->uiObserve(stream, curr, false)) return false;
+    }
     if (!m->estimate(stream, prev, curr)) return false;
     m->haveEst = true;
     m->estPrev = prev.data;
     m->estCurr = curr.data;
+    if (m->uiOn()) {   // the pair is protected if both frames are kept
+        m->estEnt[0] = m->uiFind(prev.data);
+        m->estEnt[1] = m->uiFind(curr.data);
+        m->estUi = m->estEnt[0] >= 0 && m->estEnt[1] >= 0;
+        if (m->estUi) {
+            m->estStamp[0] = m->uiE[m->estEnt[0]].stamp;
+            m->estStamp[1] = m->uiE[m->estEnt[1]].stamp;
+        }
+    }
     return true;
+}
+
+bool Interpolator::recordObserve(cudaStream_t stream, Frame frame) {
+    if (!m || !m->W) return false;
+    if (!m->uiOn()) return true;
+    if (!m->frameOk(frame) || !m->uiState) return false;
+    DeviceGuard g(m->device);
+    m->uiExplicit = true;
+    if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
+    return m->uiObserve(stream, frame, false);
+}
+
+bool Interpolator::recordTrack(cudaStream_t stream, Frame frame) {
+    if (!m || !m->W) return false;
+    if (!m->uiOn()) return true;
+    if (!m->frameOk(frame) || !m->uiState) return false;
+    DeviceGuard g(m->device);
+    if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
+    return m->uiObserve(stream, frame, true);
+}
+
+size_t Interpolator::uiTraceBytes() const {
+    if (!m || !m->uiOn() || !m->uiState) return 0;
+    return (size_t)m->uiWork[2] * m->uiWork[3] * 16 + ((size_t)fgk::kUiMaskHeader + (size_t)m->uiStride * m->uiWork[3]) * 4;
+}
+
+bool Interpolator::uiTrace(cudaStream_t stream, const void* frame, void* dst) {
+    const size_t total = uiTraceBytes();
+    if (!total || !dst) return false;
+    DeviceGuard g(m->device);
+    const size_t sb = (size_t)m->uiWork[2] * m->uiWork[3] * 16;
+    char* d = static_cast<char*>(dst);
+    if (!m->check(cudaMemcpyAsync(d, m->uiState, sb, cudaMemcpyDeviceToDevice, stream))) return false;
+    const int k = frame ? m->uiFind(frame) : -1;
+    return m->check(k >= 0 ? cudaMemcpyAsync(d + sb, m->uiE[k].mask, total - sb, cudaMemcpyDeviceToDevice, stream)
+                           : cudaMemsetAsync(d + sb, 0, total - sb, stream));
+}
+
+void Interpolator::boxSize(const Settings& set, uint32_t w, uint32_t h, uint32_t* boxW, uint32_t* boxH) {
+    const int fw = (int)w, fh = (int)h;
+    int side;
+    if (set.uiBoxHeightFrac > 0.0f)
+        side = std::min(std::max((int)std::lround((double)h * set.uiBoxHeightFrac), 8), std::min(fw, fh));
+    else   // the legacy area fraction
+        side = std::min(std::max((int)std::lround(std::sqrt((double)set.uiCrosshairArea * fw * fh)), 32), std::min(fw, fh));
+    *boxW = set.uiBoxWidth ? (uint32_t)std::min(std::max((int)set.uiBoxWidth, 4), fw) : (uint32_t)side;
+    *boxH = set.uiBoxHeight ? (uint32_t)std::min(std::max((int)set.uiBoxHeight, 4), fh) : (uint32_t)side;
+}
+
+void Interpolator::boxRect(const Settings& set, uint32_t w, uint32_t h, int32_t r[4]) {
+    uint32_t bw, bh;
+    boxSize(set, w, h, &bw, &bh);
+    r[2] = (int32_t)bw;
+    r[3] = (int32_t)bh;
+    r[0] = std::min(std::max(((int)w - r[2]) / 2 + set.uiBoxOffsetX, 0), (int)w - r[2]);
+    r[1] = std::min(std::max(((int)h - r[3]) / 2 + set.uiBoxOffsetY, 0), (int)h - r[3]);
+}
+
+uint32_t Interpolator::boxMargin(const Settings& set) {
+    return set.uiProtection == UiProtection::Crosshair ? 2u : set.uiProtection == UiProtection::CrosshairV2 ? 1u : 0u;
+}
+
+void Interpolator::workRect(const Settings& set, uint32_t w, uint32_t h, int32_t r[4]) {
+    boxRect(set, w, h, r);
+    const int mg = (int)boxMargin(set);
+    const int x0 = std::max(r[0] - mg, 0), y0 = std::max(r[1] - mg, 0);
+    const int x1 = std::min(r[0] + r[2] + mg, (int)w), y1 = std::min(r[1] + r[3] + mg, (int)h);
+    r[0] = x0; r[1] = y0; r[2] = x1 - x0; r[3] = y1 - y0;
 }
 
 bool Interpolator::recordSynth(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t) {
@@ -731,10 +1011,12 @@ bool Interpolator::recordSynth(cudaStream_t stream, Frame prev, Frame curr, Fram
     if (!m->haveEst || prev.data != m->estPrev || curr.data != m->estCurr) return false;
     if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || !m->samePitch(prev, curr)) return false;
     if (m->synthSets >= kSetRing) return false;
+    const uint32_t *ma, *mc;
+    if (!m->uiPairMasks(ma, mc)) return false;   // an entry the estimate used was evicted or replaced since
     DeviceGuard g(m->device);
     m->synthSets++;
     if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
-    return m->synth(stream, prev, curr, out, t);
+    return m->synth(stream, prev, curr, out, t, ma, mc);
 }
 
 uint32_t Interpolator::blurPlan(uint32_t samples, BlurWeights weights, float t0, float t1, float* times, uint32_t* q) {
@@ -776,10 +1058,12 @@ bool Interpolator::recordSynthBlur(cudaStream_t stream, Frame prev, Frame curr, 
     if (!m->haveEst || prev.data != m->estPrev || curr.data != m->estCurr) return false;
     if (!m->frameOk(prev) || !m->frameOk(curr) || !m->frameOk(out) || !m->samePitch(prev, curr)) return false;
     if (m->synthSets >= kSetRing) return false;
+    const uint32_t *ma, *mc;
+    if (!m->uiPairMasks(ma, mc)) return false;
     DeviceGuard g(m->device);
     m->synthSets++;
     if (m->profiling && m->evCount == 0) m->stamp(stream, "start");
-    return m->blur(stream, prev, curr, out, t0, t1);
+    return m->blur(stream, prev, curr, out, t0, t1, ma, mc);
 }
 
 bool Interpolator::record(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t) {
@@ -1188,6 +1472,14 @@ static Settings fromC(const fg_settings* c) {
     s.subpixel = c->subpixel != 0; s.uiProtection = (UiProtection)c->uiProtection; s.blurSamples = c->blurSamples;
     s.blurWeights = (BlurWeights)c->blurWeights; s.motionVersion = (MotionVersion)c->motionVersion;
     s.flowScale = c->flowScale; s.pyramidMinSide = c->pyramidMinSide;
+    if (c->size >= offsetof(fg_settings, uiEstimateFill) + sizeof(c->uiEstimateFill)) {   // the UI fields
+        s.uiHistory = c->uiHistory; s.uiBoxHeightFrac = c->uiBoxHeightFrac; s.uiBoxWidth = c->uiBoxWidth;
+        s.uiBoxHeight = c->uiBoxHeight; s.uiCrosshairArea = c->uiCrosshairArea; s.uiBoxOffsetX = c->uiBoxOffsetX;
+        s.uiBoxOffsetY = c->uiBoxOffsetY; s.uiStillFrames = c->uiStillFrames; s.uiStillThreshold = c->uiStillThreshold;
+        s.uiInpaintReach = c->uiInpaintReach; s.uiMaxStillFraction = c->uiMaxStillFraction;
+        s.uiContrastThreshold = c->uiContrastThreshold; s.uiLeaveFrames = c->uiLeaveFrames;
+        s.uiReentryFrames = c->uiReentryFrames; s.uiEstimateFill = c->uiEstimateFill != 0;
+    }
     return s;
 }
 static void toC(const Settings& s, fg_settings* c) {
@@ -1198,6 +1490,12 @@ static void toC(const Settings& s, fg_settings* c) {
     c->subpixel = s.subpixel; c->uiProtection = (uint32_t)s.uiProtection; c->blurSamples = s.blurSamples;
     c->blurWeights = (uint32_t)s.blurWeights; c->motionVersion = (uint32_t)s.motionVersion;
     c->flowScale = s.flowScale; c->pyramidMinSide = s.pyramidMinSide;
+    c->uiHistory = s.uiHistory; c->uiBoxHeightFrac = s.uiBoxHeightFrac; c->uiBoxWidth = s.uiBoxWidth;
+    c->uiBoxHeight = s.uiBoxHeight; c->uiCrosshairArea = s.uiCrosshairArea; c->uiBoxOffsetX = s.uiBoxOffsetX;
+    c->uiBoxOffsetY = s.uiBoxOffsetY; c->uiStillFrames = s.uiStillFrames; c->uiStillThreshold = s.uiStillThreshold;
+    c->uiInpaintReach = s.uiInpaintReach; c->uiMaxStillFraction = s.uiMaxStillFraction;
+    c->uiContrastThreshold = s.uiContrastThreshold; c->uiLeaveFrames = s.uiLeaveFrames;
+    c->uiReentryFrames = s.uiReentryFrames; c->uiEstimateFill = s.uiEstimateFill;
 }
 static Frame fromC(const fg_frame* f) {
     return f ? Frame(f->data, (size_t)f->pitch, f->chroma, (size_t)f->chroma_pitch) : Frame();
@@ -1267,6 +1565,29 @@ void fg_release_unused_motion(fg_interpolator* fg) {
 }
 int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr) {
     return fg && prev && curr && fg->I.recordEstimate((cudaStream_t)stream, fromC(prev), fromC(curr));
+}
+uint64_t fg_ui_trace_bytes(const fg_interpolator* fg) { return fg ? (uint64_t)fg->I.uiTraceBytes() : 0; }
+int fg_ui_trace(fg_interpolator* fg, void* stream, const void* frame, void* dst) {
+    return fg && fg->I.uiTrace((cudaStream_t)stream, frame, dst);
+}
+int fg_record_observe(fg_interpolator* fg, void* stream, const fg_frame* f) {
+    return fg && f && fg->I.recordObserve((cudaStream_t)stream, fromC(f));
+}
+int fg_record_track(fg_interpolator* fg, void* stream, const fg_frame* f) {
+    return fg && f && fg->I.recordTrack((cudaStream_t)stream, fromC(f));
+}
+void fg_box_size(const fg_settings* s, uint32_t w, uint32_t h, uint32_t* bw, uint32_t* bh) {
+    uint32_t a = 0, b = 0;
+    Interpolator::boxSize(fromC(s), w, h, &a, &b);
+    if (bw) *bw = a;
+    if (bh) *bh = b;
+}
+void fg_box_rect(const fg_settings* s, uint32_t w, uint32_t h, int32_t rect[4]) {
+    if (rect) Interpolator::boxRect(fromC(s), w, h, rect);
+}
+uint32_t fg_box_margin(const fg_settings* s) { return Interpolator::boxMargin(fromC(s)); }
+void fg_work_rect(const fg_settings* s, uint32_t w, uint32_t h, int32_t rect[4]) {
+    if (rect) Interpolator::workRect(fromC(s), w, h, rect);
 }
 int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr, const fg_frame* out,
                     float t) {

@@ -31,7 +31,13 @@ class CSettings(ctypes.Structure):
                                               "smoothBonus", "searchPenalty")] + \
                [(n, ctypes.c_uint32) for n in ("searchRadius", "searchRadiusTop", "subpixel", "uiProtection",
                                                "blurSamples", "blurWeights", "motionVersion", "flowScale",
-                                               "pyramidMinSide")]
+                                               "pyramidMinSide")] + \
+               [("uiHistory", ctypes.c_uint32), ("uiBoxHeightFrac", ctypes.c_float), ("uiBoxWidth", ctypes.c_uint32),
+                ("uiBoxHeight", ctypes.c_uint32), ("uiCrosshairArea", ctypes.c_float), ("uiBoxOffsetX", ctypes.c_int32),
+                ("uiBoxOffsetY", ctypes.c_int32), ("uiStillFrames", ctypes.c_uint32), ("uiStillThreshold", ctypes.c_float),
+                ("uiInpaintReach", ctypes.c_uint32), ("uiMaxStillFraction", ctypes.c_float),
+                ("uiContrastThreshold", ctypes.c_float), ("uiLeaveFrames", ctypes.c_uint32),
+                ("uiReentryFrames", ctypes.c_uint32), ("uiEstimateFill", ctypes.c_uint32)]
 
 
 class CFrame(ctypes.Structure):
@@ -88,6 +94,14 @@ SIGNATURES = {
     "fg_release_unused_ui": (None, [_P]),
     "fg_release_unused_motion": (None, [_P]),
     "fg_record_estimate": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame)]),
+    "fg_record_observe": (_I, [_P, _P, ctypes.POINTER(CFrame)]),
+    "fg_record_track": (_I, [_P, _P, ctypes.POINTER(CFrame)]),
+    "fg_box_size": (None, [ctypes.POINTER(CSettings), _U32, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "fg_box_rect": (None, [ctypes.POINTER(CSettings), _U32, _U32, ctypes.POINTER(ctypes.c_int32)]),
+    "fg_box_margin": (_U32, [ctypes.POINTER(CSettings)]),
+    "fg_work_rect": (None, [ctypes.POINTER(CSettings), _U32, _U32, ctypes.POINTER(ctypes.c_int32)]),
+    "fg_ui_trace_bytes": (ctypes.c_uint64, [_P]),
+    "fg_ui_trace": (_I, [_P, _P, _P, _P]),
     "fg_record_synth": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
     "fg_record": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F]),
     "fg_record_synth_blur": (_I, [_P, _P, ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), ctypes.POINTER(CFrame), _F,
@@ -176,6 +190,21 @@ class Settings:
     motionVersion: int = 0
     flowScale: int = 2
     pyramidMinSide: int = 48
+    uiHistory: int = 3
+    uiBoxHeightFrac: float = 0.025
+    uiBoxWidth: int = 0
+    uiBoxHeight: int = 0
+    uiCrosshairArea: float = 0.03
+    uiBoxOffsetX: int = 0
+    uiBoxOffsetY: int = 0
+    uiStillFrames: int = 8
+    uiStillThreshold: float = 3.5
+    uiInpaintReach: int = 12
+    uiMaxStillFraction: float = 0.75
+    uiContrastThreshold: float = 20.0
+    uiLeaveFrames: int = 4
+    uiReentryFrames: int = 2
+    uiEstimateFill: bool = False
 
     def to_c(self):
         c = CSettings()
@@ -289,6 +318,14 @@ class Interpolator:
 
     def release_unused_motion(self):
         lib().fg_release_unused_motion(self._h)
+
+    def record_observe(self, frame, stream=None):
+        """recordObserve: static-UI protection (CrosshairV2) advances its state with this real frame and keeps its mask"""
+        return bool(lib().fg_record_observe(self._h, _stream(stream), ctypes.byref(frame_of(frame))))
+
+    def record_track(self, frame, stream=None):
+        """recordTrack: the state update only, for a real frame passed through without generating"""
+        return bool(lib().fg_record_track(self._h, _stream(stream), ctypes.byref(frame_of(frame))))
 
     def record_estimate(self, prev, curr, stream=None):
         return bool(lib().fg_record_estimate(self._h, _stream(stream), ctypes.byref(frame_of(prev)),
@@ -633,3 +670,43 @@ class Batch:
 
     def set_shape(self, ctas_per_sm, order, streams=8):
         return bool(lib().fg_batch_set_shape(self._h, int(ctas_per_sm), int(order), int(streams)))
+
+
+def box_rect(settings, W, H):
+    """Interpolator::boxRect: (x, y, w, h) of the static-UI box of a W x H frame"""
+    r = (ctypes.c_int32 * 4)()
+    lib().fg_box_rect(ctypes.byref(settings.to_c()), W, H, r)
+    return tuple(r)
+
+
+def work_rect(settings, W, H):
+    """Interpolator::workRect: the box grown by boxMargin, clamped to the frame"""
+    r = (ctypes.c_int32 * 4)()
+    lib().fg_work_rect(ctypes.byref(settings.to_c()), W, H, r)
+    return tuple(r)
+
+
+def box_margin(settings):
+    return int(lib().fg_box_margin(ctypes.byref(settings.to_c())))
+
+
+def read_ui(I, frame, settings, W, H, stream=None):
+    """the CrosshairV2 state of an Interpolator and the kept mask of `frame` (a CUDA tensor; its data pointer is the
+    key): dict with w0, w1, w2 ((wh, ww) uint32 each), mask ((wh, ww) uint8), header (4 words), rect"""
+    import numpy as np
+    import torch
+    n = int(lib().fg_ui_trace_bytes(I._h))
+    if not n:
+        return None
+    buf = torch.empty(n, dtype=torch.uint8, device="cuda")
+    key = frame[0].data_ptr() if isinstance(frame, tuple) else frame.data_ptr()
+    assert lib().fg_ui_trace(I._h, _stream(stream), key, buf.data_ptr())
+    torch.cuda.synchronize()
+    raw = buf.cpu().numpy()
+    wx, wy, ww, wh = work_rect(settings, W, H)
+    st = raw[:ww * wh * 16].view(np.uint32).reshape(wh, ww, 4)
+    mk = raw[ww * wh * 16:].view(np.uint32)
+    stride = (ww + 3) // 4
+    mask = mk[4:4 + stride * wh].view(np.uint8).reshape(wh, stride * 4)[:, :ww]
+    return {"w0": st[..., 0], "w1": st[..., 1], "w2": st[..., 2], "mask": mask, "header": mk[:4].copy(),
+            "rect": (wx, wy, ww, wh)}

@@ -80,8 +80,11 @@ struct Settings {
     uint32_t searchRadius = 2;      // [1, 12]
     uint32_t searchRadiusTop = 6;   // [1, 12]
     bool subpixel = true;
-    UiProtection uiProtection = UiProtection::Off;   // Off only
-    // the reference's UI-protection fields (gpu/framegen.h:196-300): validated with its ranges, unused here
+    // Static-UI protection (gpu/framegen.h:196-305): Off, or CrosshairV2 for the 8-bit RGBA / BGRA formats (the box
+    // fields, uiHistory, uiStillFrames, uiStillThreshold, uiContrastThreshold, uiLeaveFrames, uiReentryFrames apply).
+    // Crosshair, WholeScreen, uiEstimateFill and the other formats are refused by settingsError with a reason;
+    // uiInpaintReach and uiMaxStillFraction (Crosshair / WholeScreen fields) are validated with the reference's ranges.
+    UiProtection uiProtection = UiProtection::Off;
     uint32_t uiHistory = 3;                          // [3, 65]
     float uiBoxHeightFrac = 0.025f;                  // [0, 1]
     uint32_t uiBoxWidth = 0, uiBoxHeight = 0;        // [0, 16384]
@@ -156,11 +159,37 @@ public:
 
     // gpu/framegen.h:511: resets the per-submission record counts (kSetRing each)
     void beginFrame();
-    // gpu/framegen.h:693, 700: free the resources of UI-protection depths / motion versions no longer selected. This
-    // build holds only V1 and no UI-protection memory, so there is never anything unused: both are no-ops, kept so a
-    // host that calls them periodically links unchanged.
+    // gpu/framegen.h:693: frees the kept-frame masks Settings::uiHistory no longer keeps (they stay allocated when it is
+    // lowered; everything when protection is off). Every earlier record must have retired. gpu/framegen.h:700: V1 is
+    // the only motion version here, so releaseUnusedMotion has nothing to free (kept so a host that calls it links).
     void releaseUnusedUi();
     void releaseUnusedMotion();
+
+    // Static-UI protection, CrosshairV2 (gpu/framegen.h:576-691). recordObserve(stream, frame): once per new real
+    // frame, in presentation order, after its pixels are final and before the recordEstimate that uses it: advances
+    // the per-pixel state of the box (still / contrasty / in the mask, with hysteresis and fast re-entry) and keeps
+    // the frame's mask (the frame's device pointer is the key; LRU by observe order, Settings::uiHistory frames kept).
+    // recordTrack: the same state update for a frame passed through without generating, no mask kept (and an entry
+    // of the same frame forgotten). A host that never calls recordObserve gets the implicit observe in recordEstimate
+    // (prev if not kept, curr if it is not the most recently observed frame). A synthesis of a pair whose frames are
+    // both kept rejects warp taps that land on a frame's own UI pixels and pastes curr's UI pixels that did not change
+    // in the pair; a pair without both entries is interpolated unprotected. recordSynth returns false if an entry the
+    // estimate used was evicted or replaced since. Protection Off: both return true and record nothing. false: not
+    // initialised, a bad frame, or the first-use allocation failed.
+    bool recordObserve(cudaStream_t stream, Frame frame);
+    bool recordTrack(cudaStream_t stream, Frame frame);
+    // gpu/framegen.h:484-494: the box size, the box rectangle {x, y, w, h} (centred plus the offsets, clamped into the
+    // frame), the margin past it the mode protects (1 for CrosshairV2, 2 Crosshair, 0 otherwise) and the work
+    // rectangle (the box grown by the margin, clamped to the frame). They do not check validity.
+    static void boxSize(const Settings&, uint32_t w, uint32_t h, uint32_t* boxW, uint32_t* boxH);
+    static void boxRect(const Settings&, uint32_t w, uint32_t h, int32_t rect[4]);
+    static uint32_t boxMargin(const Settings&);
+    static void workRect(const Settings&, uint32_t w, uint32_t h, int32_t rect[4]);
+    // B200-build extension (no reference counterpart; for parity tests): the size of uiTrace's output, and a copy
+    // (on `stream`) of the protection's per-pixel state (4 words per work-rectangle pixel) followed by the kept mask
+    // of `frame` (header + bytes; zeros if that frame is not kept). false if the protection is off or unallocated.
+    size_t uiTraceBytes() const;
+    bool uiTrace(cudaStream_t stream, const void* frame, void* dst);
 
     // gpu/framegen.h:549-551: passes 1-8 once per real pair, passes 9-11 per generated time t in (0, 1), or both.
     // false (and nothing recorded, out untouched) if not initialised, t outside (0, 1), a ring overflow since

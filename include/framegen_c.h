@@ -16,13 +16,26 @@ extern "C" {
 
 typedef struct fg_interpolator fg_interpolator;
 
-/* framegen::Settings (gpu/framegen.h:167-409, the V1 fields). `size` = sizeof(fg_settings) for ABI growth. */
+/* framegen::Settings (gpu/framegen.h:167-409, the V1 fields and the static-UI protection fields). `size` =
+ * sizeof(fg_settings) for ABI growth: a caller built against the shorter struct (ending at pyramidMinSide) gets the
+ * UI fields' defaults. */
 typedef struct fg_settings {
     uint32_t size;
     float trustLow, trustHigh, globalFallback, sceneCutSad, hudBonus, smoothBonus, searchPenalty;
     uint32_t searchRadius, searchRadiusTop, subpixel;
     uint32_t uiProtection, blurSamples, blurWeights, motionVersion;
     uint32_t flowScale, pyramidMinSide;
+    /* static-UI protection (gpu/framegen.h:196-305) */
+    uint32_t uiHistory;
+    float uiBoxHeightFrac;
+    uint32_t uiBoxWidth, uiBoxHeight;
+    float uiCrosshairArea;
+    int32_t uiBoxOffsetX, uiBoxOffsetY;
+    uint32_t uiStillFrames;
+    float uiStillThreshold;
+    uint32_t uiInpaintReach;
+    float uiMaxStillFraction, uiContrastThreshold;
+    uint32_t uiLeaveFrames, uiReentryFrames, uiEstimateFill;
 } fg_settings;
 
 /* framegen::Frame (gpu/framegen.h:154-159); the first plane spans at most 2^34 bytes */
@@ -81,9 +94,20 @@ int fg_reconfigure(fg_interpolator* fg, const fg_settings* s);                  
 void fg_get_settings(const fg_interpolator* fg, fg_settings* s);                    /* gpu/framegen.h:507 */
 
 void fg_begin_frame(fg_interpolator* fg);                                           /* gpu/framegen.h:511 */
-void fg_release_unused_ui(fg_interpolator* fg);                                     /* gpu/framegen.h:693 (no-op here) */
+void fg_release_unused_ui(fg_interpolator* fg);                                     /* gpu/framegen.h:693 */
 void fg_release_unused_motion(fg_interpolator* fg);                                 /* gpu/framegen.h:700 (no-op here) */
 int fg_record_estimate(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr);   /* :549 */
+/* Static-UI protection, CrosshairV2: gpu/framegen.h:610 recordObserve, :691 recordTrack (Interpolator::recordObserve) */
+int fg_record_observe(fg_interpolator* fg, void* stream, const fg_frame* frame);
+int fg_record_track(fg_interpolator* fg, void* stream, const fg_frame* frame);
+/* gpu/framegen.h:484-494: Interpolator::boxSize / boxRect / boxMargin / workRect (rect = {x, y, w, h}) */
+void fg_box_size(const fg_settings* s, uint32_t w, uint32_t h, uint32_t* box_w, uint32_t* box_h);
+void fg_box_rect(const fg_settings* s, uint32_t w, uint32_t h, int32_t rect[4]);
+uint32_t fg_box_margin(const fg_settings* s);
+void fg_work_rect(const fg_settings* s, uint32_t w, uint32_t h, int32_t rect[4]);
+/* B200-build extension (parity tests): Interpolator::uiTraceBytes / uiTrace, the CrosshairV2 state and a kept mask */
+uint64_t fg_ui_trace_bytes(const fg_interpolator* fg);
+int fg_ui_trace(fg_interpolator* fg, void* stream, const void* frame, void* dst);
 int fg_record_synth(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,
                     const fg_frame* out, float t);                                                        /* :550 */
 int fg_record(fg_interpolator* fg, void* stream, const fg_frame* prev, const fg_frame* curr,

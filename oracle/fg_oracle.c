@@ -570,9 +570,48 @@ void fgo_i_field_at(const float* pf, int w, int h, float sf, float* out) {
 /* interp.synth: the frame at time t from the estimate. out has the input's pixel layout (alpha = the nearer
  * frame's). reason: 0 = interpolated, 1 = scene cut, 2 = untrusted share. Optional: field_t (fw*fh*2, the field
  * at t), emap (W*H bytes: the per-pixel mismatch before the 7x7 box), *untrusted (pixels with trust past 0.5). */
+/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl; gpu/shaders/motion_v1.glsl:117-129): the UI mask of a
+ * frame over its rectangle (bytes, 0 = not UI). A tap at p reads the pixels lo..hi with X = roundEven(32 p),
+ * lo = X >> 5, hi = lo + (X & 31 != 0) per axis; does any of them lie on the mask? */
+typedef struct { const uint8_t* m; int x, y, w, h, stride; } fgo_uimask;
+
+static int ui_hit(const fgo_uimask* u, float px, float py) {
+    if (!u || !u->m || u->w <= 0 || u->h <= 0) return 0;
+    int X = (int)nearbyintf(px * 32.0f), Y = (int)nearbyintf(py * 32.0f);
+    int lx = X >> 5, ly = Y >> 5, hx = lx + ((X & 31) != 0), hy = ly + ((Y & 31) != 0);
+    int x0 = lx - u->x, y0 = ly - u->y, x1 = hx - u->x, y1 = hy - u->y;
+    if (x0 < 0) x0 = 0;
+    if (y0 < 0) y0 = 0;
+    if (x1 > u->w - 1) x1 = u->w - 1;
+    if (y1 > u->h - 1) y1 = u->h - 1;
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++)
+            if (u->m[(size_t)y * u->stride + x]) return 1;
+    return 0;
+}
+
+static int synth_impl(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                      const float* pf, int cut, float t, uint8_t* out, int out_pitch, float* field_t, uint8_t* emap,
+                      long long* untrusted, int* reason, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc);
+
 int fgo_synth(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
               const float* pf, int cut, float t, uint8_t* out, int out_pitch, float* field_t, uint8_t* emap,
               long long* untrusted, int* reason, int nthreads) {
+    return synth_impl(a8, c8, W, H, pitch, order, s, pf, cut, t, out, out_pitch, field_t, emap, untrusted, reason, nthreads,
+                      NULL, NULL);
+}
+
+/* fgo_synth with CrosshairV2's tap rejection: ua / uc are prev's / curr's UI masks (either may be NULL) */
+int fgo_synth_ui(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                 const float* pf, int cut, float t, uint8_t* out, int out_pitch, float* field_t, uint8_t* emap,
+                 long long* untrusted, int* reason, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc) {
+    return synth_impl(a8, c8, W, H, pitch, order, s, pf, cut, t, out, out_pitch, field_t, emap, untrusted, reason, nthreads,
+                      ua, uc);
+}
+
+static int synth_impl(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                      const float* pf, int cut, float t, uint8_t* out, int out_pitch, float* field_t, uint8_t* emap,
+                      long long* untrusted, int* reason, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #else
@@ -613,12 +652,20 @@ int fgo_synth(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int
             float hx = hv[((size_t)sy * uw + sx) * 2] * (float)fs, hy = hv[((size_t)sy * uw + sx) * 2 + 1] * (float)fs;
             int* wa = wab + ((size_t)y * W + x) * 8;
             int* wc = wa + 4;
+            float pax, pay, pcx, pcy;
             if (mid) {
-                remap_u8(&A, (float)x - hx, (float)y - hy, wa);
-                remap_u8(&C, (float)x + hx, (float)y + hy, wc);
+                pax = (float)x - hx; pay = (float)y - hy; pcx = (float)x + hx; pcy = (float)y + hy;
             } else {
-                remap_u8(&A, (float)x - ka * hx, (float)y - ka * hy, wa);
-                remap_u8(&C, (float)x + kc * hx, (float)y + kc * hy, wc);
+                pax = (float)x - ka * hx; pay = (float)y - ka * hy; pcx = (float)x + kc * hx; pcy = (float)y + kc * hy;
+            }
+            remap_u8(&A, pax, pay, wa);
+            remap_u8(&C, pcx, pcy, wc);
+            if (ua || uc) {   /* a tap on its own frame's UI takes the other frame's tap; both or neither: unchanged */
+                int ha = ui_hit(ua, pax, pay), hc = ui_hit(uc, pcx, pcy);
+                if (ha != hc) {
+                    if (ha) memcpy(wa, wc, 4 * sizeof(int));
+                    else memcpy(wc, wa, 4 * sizeof(int));
+                }
             }
             int m = 0;
             int ch[3] = {A.ri, A.gi, A.bi};

@@ -76,6 +76,8 @@ def lib():
         L.fgo_synth.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CSettings),
                                 P, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, P, P, P, P, ctypes.c_int]
         L.fgo_synth.restype = ctypes.c_int
+        L.fgo_synth_ui.argtypes = L.fgo_synth.argtypes + [ctypes.POINTER(_CUiMask), ctypes.POINTER(_CUiMask)]
+        L.fgo_synth_ui.restype = ctypes.c_int
         L.fgo_mean_f32.argtypes = [P, ctypes.c_long]
         L.fgo_mean_f32.restype = ctypes.c_float
         _lib = L
@@ -158,9 +160,25 @@ def estimate(a, c, settings=None, order="rgba", trace=True, threads=0, seed_net=
     return est
 
 
-def synth(a, c, est, t, settings=None, order="rgba", trace=False, threads=0):
+class _CUiMask(ctypes.Structure):   # fgo_uimask: a UI mask over its rectangle
+    _fields_ = [("m", ctypes.c_void_p), ("x", ctypes.c_int), ("y", ctypes.c_int), ("w", ctypes.c_int),
+                ("h", ctypes.c_int), ("stride", ctypes.c_int)]
+
+
+def _uimask(m):
+    """(mask bytes (h, w), (x, y, w, h)) -> (fgo_uimask, the array it points into), or (None, None)"""
+    if m is None:
+        return None, None
+    mask, (x, y, w, h) = m
+    mask = np.ascontiguousarray(mask, np.uint8)
+    return _CUiMask(mask.ctypes.data, x, y, w, h, mask.strides[0]), mask
+
+
+def synth(a, c, est, t, settings=None, order="rgba", trace=False, threads=0, ui=None):
     """interp.synth(a, c, est, t, why=True): returns (frame, reason) or, with trace, a dict that adds field_t,
-    e (the per-pixel mismatch before the 7x7 box) and untrusted (pixels whose trust is past 0.5)."""
+    e (the per-pixel mismatch before the 7x7 box) and untrusted (pixels whose trust is past 0.5).
+    ui = (prev's mask, curr's mask), each (bytes, rect) or None: CrosshairV2's warp-tap rejection (no paste-back here;
+    ui_v2.patch does that)."""
     s = settings or Settings()
     a, W, H, pitch = _frame_args(a, order)
     c, _, _, _ = _frame_args(c, order)
@@ -170,8 +188,13 @@ def synth(a, c, est, t, settings=None, order="rgba", trace=False, threads=0):
     ft = np.zeros((L.fh, L.fw, 2), np.float32) if trace else None
     e = np.zeros((H, W), np.uint8) if trace else None
     unt, reason = ctypes.c_longlong(), ctypes.c_int()
-    r = lib().fgo_synth(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), _p(pf), int(est["cut"]),
-                        float(t), _p(out), out.strides[0], _p(ft), _p(e), ctypes.byref(unt), ctypes.byref(reason), threads)
+    args = (_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), _p(pf), int(est["cut"]), float(t), _p(out),
+            out.strides[0], _p(ft), _p(e), ctypes.byref(unt), ctypes.byref(reason), threads)
+    if ui is not None:
+        (ma, ka), (mc, kc) = _uimask(ui[0]), _uimask(ui[1])
+        r = lib().fgo_synth_ui(*args, ctypes.byref(ma) if ma else None, ctypes.byref(mc) if mc else None)
+    else:
+        r = lib().fgo_synth(*args)
     if r != 0:
         raise ValueError("fgo_synth failed (t outside (0, 1)?)")
     if trace:

@@ -34,7 +34,7 @@ def test_every_declared_symbol_is_exported_and_bound():
 
 
 def test_struct_sizes_match_header():
-    assert ctypes.sizeof(fg.CSettings) == 4 * 17
+    assert ctypes.sizeof(fg.CSettings) == 4 * (17 + 15)   # the V1 fields, then the 15 static-UI protection fields
     assert ctypes.sizeof(fg.CFrame) == 32
     ii = fg.CInitInfo()
     fg.lib().fg_default_init_info(ctypes.byref(ii))
@@ -51,6 +51,12 @@ def test_defaults_are_interp_constants():
     assert (s.trustLow, s.trustHigh, s.globalFallback, s.sceneCutSad) == (12.0, 40.0, pytest.approx(0.15), 30.0)
     assert (s.hudBonus, s.smoothBonus, s.searchPenalty) == (1.0, 0.5, 0.5)
     assert (s.searchRadius, s.searchRadiusTop, s.subpixel, s.flowScale, s.pyramidMinSide) == (2, 6, True, 2, 48)
+    # gpu/framegen.h:220-305: the static-UI protection defaults
+    assert (s.uiProtection, s.uiHistory, s.uiBoxWidth, s.uiBoxHeight, s.uiBoxOffsetX, s.uiBoxOffsetY) == (0, 3, 0, 0, 0, 0)
+    assert (s.uiBoxHeightFrac, s.uiCrosshairArea) == (pytest.approx(0.025), pytest.approx(0.03))
+    assert (s.uiStillFrames, s.uiStillThreshold, s.uiContrastThreshold, s.uiLeaveFrames, s.uiReentryFrames) == \
+        (8, 3.5, 20.0, 4, 2)
+    assert (s.uiInpaintReach, s.uiMaxStillFraction, s.uiEstimateFill) == (12, 0.75, False)
     ii = fg.CInitInfo()
     fg.lib().fg_default_init_info(ctypes.byref(ii))
     assert ii.view_format == fg.VK_B8G8R8A8_UNORM and ii.linear_white_nits == 80.0 and ii.device == -1
@@ -77,8 +83,29 @@ def test_validate_ranges(field, value, ok):
 def test_settings_error_names_unbuilt_parts():
     s = fg.Settings(motionVersion=1)
     assert fg.validate(s) and "V1 only" in fg.settings_error(s)
-    s = fg.Settings(uiProtection=1)
-    assert fg.validate(s) and "uiProtection must be Off" in fg.settings_error(s)
+    for mode in (1, 2):   # Crosshair, WholeScreen
+        s = fg.Settings(uiProtection=mode)
+        assert fg.validate(s) and "only CrosshairV2" in fg.settings_error(s)
+    s = fg.Settings(uiProtection=3)   # CrosshairV2: built for the 8-bit RGBA formats, without uiEstimateFill
+    assert fg.validate(s) and fg.settings_error(s) is None
+    assert "8-bit RGBA" in fg.settings_error(s, fmt="Rgb10")
+    assert "uiEstimateFill" in fg.settings_error(fg.Settings(uiProtection=3, uiEstimateFill=True))
+
+
+def test_box_geometry():
+    """Interpolator::boxSize / boxRect / boxMargin / workRect against gpu/framegen.cpp:1041-1075, restated in
+    oracle/ui_v2.py"""
+    import ui_v2
+    cases = [fg.Settings(uiProtection=3), fg.Settings(uiProtection=3, uiBoxWidth=40, uiBoxHeight=6),
+             fg.Settings(uiProtection=3, uiBoxOffsetX=5000, uiBoxOffsetY=-7), fg.Settings(uiProtection=3, uiBoxHeightFrac=0.0),
+             fg.Settings(uiProtection=0), fg.Settings(uiProtection=1, uiBoxHeightFrac=0.3)]
+    for s in cases:
+        for W, H in ((3840, 2160), (640, 360), (17, 16), (101, 999)):
+            assert fg.box_rect(s, W, H) == ui_v2.box_rect(s, W, H), (s, W, H)
+            m = {0: 0, 1: 2, 2: 0, 3: 1}[s.uiProtection]
+            assert fg.box_margin(s) == m
+            assert fg.work_rect(s, W, H) == ui_v2.work_rect(s, W, H, m), (s, W, H)
+    assert fg.box_rect(fg.Settings(), 3840, 2160) == (1893, 1053, 54, 54)   # round(2160 * 0.025) = 54
 
 
 def test_format_of():
