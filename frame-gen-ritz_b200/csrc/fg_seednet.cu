@@ -16,7 +16,8 @@
 // K = 9 cin (layer 1: 18, zero-padded to 32); a CTA = 4 warps x 16 output pixels, the layer's weights staged once in
 // shared memory. The GEMMs are small (a 4K frame's level 1: 1.2 GFLOP in all), so warp-level MMA with
 // register-gathered A fragments is enough; no TMEM / TMA staging.
-// Training (backward, Adam): CUDA-core kernels, bf16 operands and float32 accumulation and gradients.
+// Training: the backward's weight and input gradients are tcgen05 implicit GEMMs (fg_seednet_bwd.cu); the loss and
+// Adam are elementwise kernels here. bf16 operands, float32 accumulation, gradients and master weights.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -174,72 +175,6 @@ __global__ void __launch_bounds__(128) k_sn_conv(const SnConvArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------- training kernels
-// dX of one layer, masked by the previous layer's ReLU: dpre_in[q][ci] = [x[q][ci] > 0] * sum_{tap, co} w[co][tap][ci]
-// dpre_out[p][co] over the output pixels p with STRIDE p + tap - 1 = q. One thread per (q, ci).
-template <int CIN, int COUT, int STRIDE>
-__global__ void __launch_bounds__(256) k_sn_dx(const SnBackArgs a) {
-    __shared__ float wsh[COUT * 9 * CIN];
-    const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
-    for (int i = threadIdx.x; i < COUT * 9 * CIN; i += 256) wsh[i] = __bfloat162float(w[i]);
-    __syncthreads();
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    const int n = a.B * a.H * a.W * CIN;
-    if (i >= n) return;
-    const int ci = i % CIN, q = i / CIN;
-    const int b = q / (a.H * a.W), rem = q % (a.H * a.W), qy = rem / a.W, qx = rem % a.W;
-    const bf16* __restrict__ x = reinterpret_cast<const bf16*>(a.x);
-    if (!(__bfloat162float(x[i]) > 0.0f)) { a.dx[i] = 0.0f; return; }
-    float s = 0.0f;
-#pragma unroll
-    for (int tap = 0; tap < 9; tap++) {
-        const int ty = qy + 1 - tap / 3, tx = qx + 1 - tap % 3;   // STRIDE * p = t
-        if (ty < 0 || tx < 0 || ty % STRIDE || tx % STRIDE) continue;
-        const int py = ty / STRIDE, px = tx / STRIDE;
-        if (py >= a.Ho || px >= a.Wo) continue;
-        const float* g = a.dy + ((size_t)(b * a.Ho + py) * a.Wo + px) * COUT;
-#pragma unroll 8
-        for (int co = 0; co < COUT; co++) s += g[co] * wsh[(co * 9 + tap) * CIN + ci];
-    }
-    a.dx[i] = s;
-}
-
-// dW[co][tap][ci] += sum_p x[STRIDE p + tap - 1][ci] dpre[p][co] and db[co] += sum_p dpre[p][co], over a slice of the
-// output pixels per CTA (grid.y slices); one CTA row per (co, tap), threads = (pixel lane, ci)
-template <int CIN, int COUT, int STRIDE>
-__global__ void __launch_bounds__(256) k_sn_dw(const SnBackArgs a) {
-    constexpr int LANES = 256 / CIN;
-    __shared__ float red[256];
-    __shared__ float redb[256];
-    const int co = blockIdx.x / 9, tap = blockIdx.x % 9;
-    const int ci = threadIdx.x % CIN, lane = threadIdx.x / CIN;
-    const int npix = a.B * a.Ho * a.Wo;
-    const int per = (npix + gridDim.y - 1) / gridDim.y;
-    const int p0 = blockIdx.y * per, p1 = min(npix, p0 + per);
-    const bf16* __restrict__ x = reinterpret_cast<const bf16*>(a.x);
-    float s = 0.0f, sb = 0.0f;
-    for (int p = p0 + lane; p < p1; p += LANES) {
-        const float g = a.dy[(size_t)p * COUT + co];
-        if (g == 0.0f) continue;
-        if (tap == 0 && ci == 0) sb += g;
-        const int b = p / (a.Ho * a.Wo), rem = p % (a.Ho * a.Wo);
-        const int iy = (rem / a.Wo) * STRIDE - 1 + tap / 3, ix = (rem % a.Wo) * STRIDE - 1 + tap % 3;
-        if ((unsigned)iy >= (unsigned)a.H || (unsigned)ix >= (unsigned)a.W) continue;
-        s += g * __bfloat162float(x[((size_t)(b * a.H + iy) * a.W + ix) * CIN + ci]);
-    }
-    red[threadIdx.x] = s;
-    redb[threadIdx.x] = sb;
-    __syncthreads();
-    for (int h = 128; h >= CIN; h >>= 1) {
-        if (threadIdx.x < h) {
-            red[threadIdx.x] += red[threadIdx.x + h];
-            redb[threadIdx.x] += redb[threadIdx.x + h];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x < CIN) atomicAdd(a.dw + (co * 9 + tap) * CIN + threadIdx.x, red[threadIdx.x]);
-    if (threadIdx.x == 0 && tap == 0) atomicAdd(a.db + co, redb[0]);
-}
-
 // the loss of one batch and its gradient at the last layer's output (per block: huber(c1 - truth) +
 // huber(c2 - search) + BCE(confidence, |c1 - truth|_inf < 1), each block weighted by its target's weight; scale =
 // 1 / blocks: the batch mean)
@@ -303,31 +238,6 @@ cudaError_t launchSnConv(int layer, const SnConvArgs& a, cudaStream_t s) {
         case 5: return launchPdl(k_sn_conv<32, kSnOut, 1, true>, grid, dim3(128), 0, s, a);
         default: return cudaErrorInvalidValue;
     }
-}
-
-cudaError_t launchSnBackward(int layer, const SnBackArgs& a, bool needDx, cudaStream_t s) {
-    const int npix = a.B * a.Ho * a.Wo;
-    const unsigned slices = (unsigned)std::max(1, std::min(64, npix / 2048));
-    const unsigned nx = divUp(a.B * a.H * a.W * 32, 256);
-    switch (layer) {
-        case 0: k_sn_dw<2, 32, 2><<<dim3(32 * 9, slices), 256, 0, s>>>(a); break;
-        case 1:
-        case 2:
-            k_sn_dw<32, 32, 2><<<dim3(32 * 9, slices), 256, 0, s>>>(a);
-            if (needDx) k_sn_dx<32, 32, 2><<<nx, 256, 0, s>>>(a);
-            break;
-        case 3:
-        case 4:
-            k_sn_dw<32, 32, 1><<<dim3(32 * 9, slices), 256, 0, s>>>(a);
-            if (needDx) k_sn_dx<32, 32, 1><<<nx, 256, 0, s>>>(a);
-            break;
-        case 5:
-            k_sn_dw<32, kSnOut, 1><<<dim3(kSnOut * 9, slices), 256, 0, s>>>(a);
-            if (needDx) k_sn_dx<32, kSnOut, 1><<<nx, 256, 0, s>>>(a);
-            break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
 }
 
 cudaError_t launchSnLoss(const float* out, const float* tgt, int n, float* dout, float* loss, float scale, cudaStream_t s) {

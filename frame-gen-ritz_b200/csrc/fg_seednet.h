@@ -68,7 +68,10 @@ cudaError_t launchSnConv(int layer, const SnConvArgs& a, cudaStream_t s);
 // message
 bool seedNetForwardLuma(::fg_seednet* n, cudaStream_t s, const float* la, const float* lc, int h, int w, float* out,
                         unsigned int* err, const char** why);
-cudaError_t launchSnBackward(int layer, const SnBackArgs& a, bool needDx, cudaStream_t s);
+// one layer's weight / bias gradient (and its input gradient when needDx) on the tensor cores (fg_seednet_bwd.cu);
+// kErrSeedNet into *err if a tensor-core wait gave up
+cudaError_t prepareSeedNetBackward();
+cudaError_t launchSnBackwardTc(int layer, const SnBackArgs& a, bool needDx, unsigned int* err, cudaStream_t s);
 cudaError_t launchSnLoss(const float* out, const float* tgt, int n, float* dout, float* loss, float scale, cudaStream_t s);
 cudaError_t launchSnAdam(const SnAdamArgs& a, cudaStream_t s);
 

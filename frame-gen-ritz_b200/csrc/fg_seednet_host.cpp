@@ -138,7 +138,7 @@ struct fg_seednet {
             a.dw = grad + snWeightOff(l);
             a.db = grad + snBiasOff(l);
             a.B = B; a.H = d.h[l]; a.W = d.w[l]; a.Ho = d.h[l + 1]; a.Wo = d.w[l + 1];
-            if (!ok(launchSnBackward(l, a, l > 0, s), "backward", l)) return false;
+            if (!ok(launchSnBackwardTc(l, a, l > 0, errFlags, s), "backward", l)) return false;
             dy = a.dx;
         }
         return true;
@@ -195,7 +195,7 @@ fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w) {
     for (int l = 0; l < kSnLayers - 1; l++) n->act[l] = n->mem + oAct[l];
     n->out = (float*)(n->mem + oOut);
     n->errFlags = (unsigned int*)(n->mem + oErr);
-    if (prepareSeedNetFused() != cudaSuccess) {   // the fused kernels' shared-memory limits
+    if (prepareSeedNetFused() != cudaSuccess || prepareSeedNetBackward() != cudaSuccess) {   // shared-memory limits
         cudaGetLastError();
         cudaFree(n->mem);
         delete n;
