@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 struct fg_seednet;   // the C ABI's handle (framegen_c.h)
 
 namespace fgk {
@@ -51,6 +53,8 @@ struct SnAdamArgs {
 // the fused forward (fg_seednet_tc.cu, tensor cores): B images of h x w float luma (prev, curr) -> per block 8 floats
 struct SnFusedArgs {
     const float* la; const float* lc;   // [B][h][w] each
+    const uint32_t* xp;                 // or (when set) the packed input [B][h][w] (bf16 prev | bf16 curr << 16)
+    void* act[5];                       // optional (training): layers 1-5's bf16 outputs [B][h_l][w_l][32]
     const void* wb;                     // bf16 parameters (the flat array)
     const float* p;                     // float parameters (the biases)
     void* y3;                           // layer 3's output, bf16 [B][h3][w3][32]

@@ -110,12 +110,16 @@ struct fg_seednet {
         return true;
     }
 
-    // the fused forward on the tensor cores (two launches, fg_seednet_tc.cu) from the float luma planes
+    // the fused forward on the tensor cores (two launches, fg_seednet_tc.cu) from the float luma planes or (xp) the
+    // packed input; keep: also store layers 1-5's outputs (the backward's inputs)
     bool forwardFused(cudaStream_t s, int B, int H, int W, float* dst, const float* la, const float* lc,
-                      unsigned int* errOut) {
+                      unsigned int* errOut, const void* xp = nullptr, bool keep = false) {
         const SnDims d(H, W);
         SnFusedArgs a{};
         a.la = la; a.lc = lc; a.wb = wb; a.p = p; a.y3 = act[2]; a.out = dst;
+        a.xp = static_cast<const uint32_t*>(xp);
+        if (keep)
+            for (int l = 0; l < kSnLayers - 1; l++) a.act[l] = act[l];
         a.B = B; a.h = H; a.w = W;
         a.h1 = d.h[1]; a.w1 = d.w[1]; a.h2 = d.h[2]; a.w2 = d.w[2]; a.h3 = d.h[3]; a.w3 = d.w[3];
         a.err = errOut ? errOut : errFlags;
@@ -125,7 +129,7 @@ struct fg_seednet {
     bool backward(cudaStream_t s, const void* x, int B, int H, int W, const float* targets) {
         const SnDims d(H, W);
         const int nb = B * d.h[kSnLayers] * d.w[kSnLayers];
-        if (!forward(s, x, B, H, W, out)) return false;
+        if (!forwardFused(s, B, H, W, out, nullptr, nullptr, nullptr, x, true)) return false;   // keeps layers 1-5
         if (!ok(cudaMemsetAsync(loss, 0, sizeof(float), s))) return false;
         float* dy = dA;
         if (!ok(launchSnLoss(out, targets, nb, dy, loss, 1.0f / (float)nb, s), "loss")) return false;

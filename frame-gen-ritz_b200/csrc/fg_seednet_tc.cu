@@ -9,6 +9,9 @@
 //             outputs stay in shared memory, only layer 3's goes to global memory (bf16, NHWC).
 //   k_sn_head layers 4-6 (stride 1, on the block grid): one CTA per tile of 10 x 8 cells; loads the 16 x 14 cells of
 //             layer 3 around it, computes layer 4 on 14 x 12, layer 5 on 12 x 10, layer 6 on the tile (float out).
+// For training the same two kernels also store layers 1, 2, 4 and 5 (the backward's inputs): each CTA the part of
+// every layer that its tile owns (the tiles partition the block grid, so their footprints partition every layer),
+// and may read the packed bf16 input instead of the float luma.
 //
 // Each layer is an implicit GEMM: M = output pixels (chunks of 128 rows), N = 32 output channels (layer 6: 16, of
 // which 8 are the net's outputs), K = 9 taps x 32 input channels, issued as 18 MMAs of K = 16.
@@ -200,15 +203,17 @@ __global__ void __launch_bounds__(kEncThreads, 1) k_sn_enc(const SnFusedArgs a) 
     // the luma region, normalised ((v - 128) / 64, bf16), zero outside the level
     {
         const int ly0 = 8 * cy0 - 7, lx0 = 8 * cx0 - 7;
-        const float* __restrict__ la = a.la + (size_t)bz * a.h * a.w;
-        const float* __restrict__ lc = a.lc + (size_t)bz * a.h * a.w;
+        const float* __restrict__ la = a.xp ? nullptr : a.la + (size_t)bz * a.h * a.w;
+        const float* __restrict__ lc = a.xp ? nullptr : a.lc + (size_t)bz * a.h * a.w;
         for (int i = tid; i < kR0y * kP0; i += kEncThreads) {
             const int y = i / kP0, x = i % kP0, gy = ly0 + y, gx = lx0 + x;
             uint32_t v = 0;
             if (x < kR0x && gy >= 0 && gy < a.h && gx >= 0 && gx < a.w) {
                 const size_t o = (size_t)gy * a.w + gx;
-                v = packBf2(__fmul_rn(__fsub_rn(__ldg(la + o), 128.0f), 1.0f / 64.0f),
-                            __fmul_rn(__fsub_rn(__ldg(lc + o), 128.0f), 1.0f / 64.0f));
+                if (a.xp) v = __ldg(a.xp + (size_t)bz * a.h * a.w + o);
+                else
+                    v = packBf2(__fmul_rn(__fsub_rn(__ldg(la + o), 128.0f), 1.0f / 64.0f),
+                                __fmul_rn(__fsub_rn(__ldg(lc + o), 128.0f), 1.0f / 64.0f));
             }
             luma[i] = v;
         }
@@ -248,7 +253,10 @@ __global__ void __launch_bounds__(kEncThreads, 1) k_sn_enc(const SnFusedArgs a) 
             const int gy = 4 * cy0 - 3 + oy, gx = 4 * cx0 - 3 + ox;
             const bool in = gy >= 0 && gy < a.h1 && gx >= 0 && gx < a.w1;
             const int ph = ((oy & 1) << 1) | (ox & 1);
-            pl2[(ph * 4 + part) * kPl2 + (oy >> 1) * kP2 + (ox >> 1)] = actPack(v, bias + 8 * part, in);
+            const uint4 val = actPack(v, bias + 8 * part, in);
+            pl2[(ph * 4 + part) * kPl2 + (oy >> 1) * kP2 + (ox >> 1)] = val;
+            if (a.act[0] && in && gy >= 4 * cy0 && gy < 4 * (cy0 + kEncTY) && gx >= 4 * cx0 && gx < 4 * (cx0 + kEncTX))
+                reinterpret_cast<uint4*>(a.act[0])[(((size_t)bz * a.h1 + gy) * a.w1 + gx) * 4 + part] = val;
         }
     };
     prep1(0, 0);
@@ -277,7 +285,10 @@ __global__ void __launch_bounds__(kEncThreads, 1) k_sn_enc(const SnFusedArgs a) 
             const int gy = 2 * cy0 - 1 + oy, gx = 2 * cx0 - 1 + ox;
             const bool in = gy >= 0 && gy < a.h2 && gx >= 0 && gx < a.w2;
             const int ph = ((oy & 1) << 1) | (ox & 1);
-            pl3[(ph * 4 + part) * kPl3 + (oy >> 1) * kP3 + (ox >> 1)] = actPack(v, bias + 32 + 8 * part, in);
+            const uint4 val = actPack(v, bias + 32 + 8 * part, in);
+            pl3[(ph * 4 + part) * kPl3 + (oy >> 1) * kP3 + (ox >> 1)] = val;
+            if (a.act[1] && in && gy >= 2 * cy0 && gy < 2 * (cy0 + kEncTY) && gx >= 2 * cx0 && gx < 2 * (cx0 + kEncTX))
+                reinterpret_cast<uint4*>(a.act[1])[(((size_t)bz * a.h2 + gy) * a.w2 + gx) * 4 + part] = val;
         }
     };
     auto none = [&](int, int) {};
@@ -362,21 +373,27 @@ __global__ void __launch_bounds__(kHeadThreads) k_sn_head(const SnFusedArgs a) {
         }
     };
     // layers 4, 5: the layer's region starts d cells before the tile; columns >= validX are the padded raster's
-    auto epiS1 = [&](uint4* dst, int plLen, int M, int d, int validX, const float* b, int c, int acc) {
+    auto epiS1 = [&](uint4* dst, int plLen, int M, int d, int validX, const float* b, void* act, int c, int acc) {
         float v[16];
         tmemLd16(tbase + tlane + 32 * acc + 16 * part, v);
         const int m = chunkStart(c, M) + row, oy = m / kHP, ox = m % kHP;
         const int gy = cy0 - d + oy, gx = cx0 - d + ox;
         const bool in = ox < validX && gy >= 0 && gy < a.h3 && gx >= 0 && gx < a.w3;
-        dst[(2 * part) * plLen + m] = actPack(v, b + 16 * part, in);
-        dst[(2 * part + 1) * plLen + m] = actPack(v + 8, b + 16 * part + 8, in);
+        const uint4 v0 = actPack(v, b + 16 * part, in), v1 = actPack(v + 8, b + 16 * part + 8, in);
+        dst[(2 * part) * plLen + m] = v0;
+        dst[(2 * part + 1) * plLen + m] = v1;
+        if (act && in && gy >= cy0 && gy < cy0 + kHTY && gx >= cx0 && gx < cx0 + kHTX) {
+            uint4* o = reinterpret_cast<uint4*>(act) + (((size_t)bz * a.h3 + gy) * a.w3 + gx) * 4 + 2 * part;
+            o[0] = v0;
+            o[1] = v1;
+        }
     };
     auto none = [&](int, int) {};
     auto issue4 = [&](int c, int acc) { issueS1(pin, kPin, reinterpret_cast<const uint4*>(sm + kHOffW4), 32, chunkStart(c, kM4), acc); };
-    auto epi4 = [&](int c, int acc) { epiS1(p4, kPl4, kM4, 2, kHP - 2, bias, c, acc); };
+    auto epi4 = [&](int c, int acc) { epiS1(p4, kPl4, kM4, 2, kHP - 2, bias, a.act[3], c, acc); };
     bool ok = chunkLoop((kM4 + 127) / 128, bars, phase, issue4, epi4, none);
     auto issue5 = [&](int c, int acc) { issueS1(p4, kPl4, reinterpret_cast<const uint4*>(sm + kHOffW5), 32, chunkStart(c, kM5), acc); };
-    auto epi5 = [&](int c, int acc) { epiS1(p5, kPl5, kM5, 1, kHP - 4, bias + 32, c, acc); };
+    auto epi5 = [&](int c, int acc) { epiS1(p5, kPl5, kM5, 1, kHP - 4, bias + 32, a.act[4], c, acc); };
     if (ok) ok = chunkLoop((kM5 + 127) / 128, bars, phase, issue5, epi5, none);
     auto issue6 = [&](int, int acc) { issueS1(p5, kPl5, reinterpret_cast<const uint4*>(sm + kHOffW6), 16, 0, acc); };
     auto epi6 = [&](int, int acc) {
