@@ -54,6 +54,7 @@ def args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (the oracle's timing and the parity checks)")
     ap.add_argument("--parity-c1-pairs", type=int, default=100, help="1080p pairs of the parity check (config 1)")
     ap.add_argument("--parity-c2-pairs", type=int, default=2, help="4K RgbaF16 pairs of the parity check (config 2)")
+    ap.add_argument("--batch-reps", type=int, default=10, help="graph replays of the config-3 batch per shape (0: no line)")
     ap.add_argument("--eager", type=int, default=0,
                     help="profiling mode: run this many eager steps (no graphs, no timing, no JSON) and exit")
     ap.add_argument("--seed-net", default=os.path.join(REPO, "frame-gen-ritz_b200", "seednet_l1.bin"),
@@ -162,7 +163,73 @@ def cpu_leg(pool, outs, seconds):
     return statistics.median(times) * 1e3, k, tally
 
 
-def parity_configs(a, fg):
+def config3_inputs(fg):
+    """the 64-pair mixed batch at full size (34 x 720p, 17 x 1080p, 9 x 1440p, 4 x 2160p; Rgba8 / Rgb10 / Nv12 / P010;
+    2x / 3x / 4x), content from the smooth-flow generator seeded per pair: (slots, Batch, prev, curr, outs, rgba pairs)"""
+    import torch
+    import batch_bench
+    import workloads_gpu
+    slots = batch_bench.slots()
+    B = fg.Batch()
+    prev, curr, outs, rgba = [], [], [], {}
+    gen = torch.Generator(device="cuda")
+    for i, (w, h, fmt, m) in enumerate(slots):
+        assert B.add(w, h, batch_bench.VK[fmt], multiplier=m) == i, B.error()
+        gen.manual_seed(3 * 10 ** 6 + i)
+        d = workloads_gpu.flow_batch(1, w, h, gen)
+        if fmt == "rgba8":
+            rgba[i] = (d["prev"][0], d["curr"][0])
+        prev.append(batch_bench.to_dev(fmt, d["prev"][0].contiguous()))
+        curr.append(batch_bench.to_dev(fmt, d["curr"][0].contiguous()))
+        outs += [batch_bench.like(prev[-1]) for _ in range(m - 1)]
+    return slots, B, prev, curr, outs, rgba
+
+
+def batch_arm(a, b3):
+    """Config 3 timed: one Batch record of all 64 pairs (127 generated frames, 259 megapixels) as a CUDA graph, device
+    time (CUDA events), median of --batch-reps replays, in the single-stream per-synthesis shape and in the shape
+    Batch::tune picks on the device"""
+    import torch
+    slots, B, prev, curr, outs, _ = b3
+    s = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed():
+        with torch.cuda.stream(s):
+            assert B.record(prev, curr, outs, stream=s), B.error()
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                assert B.record(prev, curr, outs, stream=s)
+            for _ in range(2):
+                g.replay()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(a.batch_reps):
+                e0.record(s)
+                g.replay()
+                e1.record(s)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        del g
+        return statistics.median(ts)
+
+    assert B.set_shape(0, 0, 1)
+    base = timed()
+    with torch.cuda.stream(s):
+        best = B.tune(prev, curr, outs, reps=3, stream=s)
+    shape = B.shape()
+    tuned = timed()
+    px = sum(w * h * (m - 1) for w, h, _, m in slots)
+    return {"workload": "config 3: 64 pairs, 34 x 720p / 17 x 1080p / 9 x 1440p / 4 x 2160p, Rgba8 / Rgb10 / Nv12 / "
+                        "P010, 2x / 3x / 4x; one Batch record per step, graph-replayed",
+            "generated_frames": len(outs), "generated_megapixels": round(px / 1e6, 1),
+            "ms_per_batch_per_synthesis_1_stream": round(base, 3), "ms_per_batch_tuned": round(tuned, 3),
+            "tuned_shape": {"ctas_per_sm": shape[0], "order": shape[1], "streams": shape[2], "index": best},
+            "megapixels_per_s_tuned": round(px / 1e6 / (tuned * 1e-3), 1), "reps": a.batch_reps}
+
+
+def parity_configs(a, fg, b3):
     """Every workload configuration of the path against the oracle (rank 0, N = 1; part of the CPU leg: the oracle
     runs on the host for each): config 0 (640x360, 2x, one pair, also its device latency), config 1 (1080p 4x, a sample
     of --parity-c1-pairs of the 500), config 2 (4K RgbaF16 linear 3x, --parity-c2-pairs of the 200), config 3 (the
@@ -275,20 +342,10 @@ def parity_configs(a, fg):
                       "half_floats_differing": ndiff, "decisions_agree": f"{dec_ok}/{dec_n}",
                       "workload": f"3840x2160 RgbaF16 linear 3x, {a.parity_c2_pairs} of the 200 HDR pairs; 16 run in "
                                   "tests/test_configs_gpu.py"}
-    # config 3
+    # config 3: the batch as the batch arm left it (its tuned shape); every slot against a standalone Interpolator
     import batch_bench
-    slots = batch_bench.slots()
-    B = fg.Batch()
-    prev, curr, bouts, rgba = [], [], [], {}
-    for i, (w, h, fmt, m) in enumerate(slots):
-        assert B.add(w, h, batch_bench.VK[fmt], multiplier=m) == i, B.error()
-        gen.manual_seed(3 * 10 ** 6 + i)
-        d = workloads_gpu.flow_batch(1, w, h, gen)
-        if fmt == "rgba8":
-            rgba[i] = (d["prev"][0].cpu().numpy(), d["curr"][0].cpu().numpy())
-        prev.append(batch_bench.to_dev(fmt, d["prev"][0].contiguous()))
-        curr.append(batch_bench.to_dev(fmt, d["curr"][0].contiguous()))
-        bouts += [batch_bench.like(prev[-1]) for _ in range(m - 1)]
+    slots, B, prev, curr, bouts, rgba = b3
+    rgba = {k: (p.cpu().numpy(), c.cpu().numpy()) for k, (p, c) in rgba.items()}
     assert B.record(prev, curr, bouts), B.error()
     torch.cuda.synchronize()
     st, orc = ParityTally(), ParityTally()
@@ -315,7 +372,7 @@ def parity_configs(a, fg):
     rs, ro = st.report(), orc.report()
     rs.pop("decisions_agree")
     ro.pop("decisions_agree")
-    out["config3"] = {"workload": "the 64-pair mixed batch at full size, one Batch record in its default shape",
+    out["config3"] = {"workload": "the 64-pair mixed batch at full size, one Batch record in the tuned shape",
                       "vs_standalone": rs, "rgba8_vs_oracle": ro}
     return out
 
@@ -736,6 +793,12 @@ def main():
         last = (step_no[0] - 1) % 2
         assert all(torch.equal(h, e.cpu()) for h, e in zip(hout[last], eager0)), "e2e output differs"
 
+    # config 3, the batched path (rank 0, N = 1)
+    b3 = batch = None
+    if rank == 0 and world == 1 and (a.batch_reps > 0 or not a.no_cpu):
+        b3 = config3_inputs(fg)
+        if a.batch_reps > 0:
+            batch = batch_arm(a, b3)
     # the CPU leg (rank 0, N = 1): every pool slot's plain outputs once more, then the oracle on the same pairs
     cpu = parity = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -750,7 +813,7 @@ def main():
         parity = {"metric_workload": tally.report(workload="the bench's 4K pool: the GPU's graph outputs against the "
                                                             "oracle's")}
         parity["metric_workload"].pop("decisions_agree")
-        parity.update(parity_configs(a, fg))
+        parity.update(parity_configs(a, fg, b3))
 
     blur = blur_arm(a, fg, pool, stream, world) if a.blur_samples >= 2 else None
     seed = None
@@ -785,7 +848,8 @@ def main():
                 "gpu_launches": launches_per_step * a.steps,
                 "e2e": {"value": round(e2e_value, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 4 * W4K * H4K,
                         "d2h_bytes_per_step": len(TS) * 4 * W4K * H4K},
-                "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "seed_net": seed, "motion_blur": blur}
+                "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "seed_net": seed, "motion_blur": blur,
+                "batch": batch}
         print(json.dumps(line), flush=True)
     I.close()
     if world > 1:
