@@ -244,6 +244,16 @@ struct UiPatchParams {
     uint8_t* out; size_t outPitch;
     const uint32_t* mask;
 };
+// the estimate fill (Settings::uiEstimateFill): level-0 luma cells holding UI pixels re-averaged over their not-UI
+// pixels, prev's (mask ma, luma la) and curr's (mc, lc); cells of the rectangle (cx0, cy0) .. + (ncx, ncy)
+struct UiFillParams {
+    const uint8_t* a; const uint8_t* c; size_t pitch;
+    int W, H, ri, gi, bi, fs, fw, fh;
+    const uint32_t* ma; const uint32_t* mc;
+    float* la; float* lc;
+    int cx0, cy0, ncx, ncy;
+};
+cudaError_t launchUiFill(const UiFillParams& p, cudaStream_t s);
 cudaError_t launchUiV2Update(const UiV2Params& p, cudaStream_t s);
 cudaError_t launchUiV2Mask(const UiV2Params& p, cudaStream_t s);
 cudaError_t launchUiPatch(const UiPatchParams& p, int wx, int wy, int ww, int wh, cudaStream_t s);

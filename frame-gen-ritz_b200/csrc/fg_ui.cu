@@ -158,7 +158,56 @@ __global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_patch(const UiPatchParams 
     *o = (real & 0x00FFFFFFu) | (*o & 0xFF000000u);   // colour channels from the real frame, alpha kept
 }
 
+// is the frame pixel (x, y) a UI pixel of the mask (header + bytes)?
+__device__ __forceinline__ bool uiPx(const uint32_t* __restrict__ m, int x, int y) {
+    const uint32_t o = __ldg(m + 1), wh = __ldg(m + 2);
+    x -= (int)(o & 0xFFFFu);
+    y -= (int)(o >> 16);
+    if (x < 0 || y < 0 || x >= (int)(wh & 0xFFFFu) || y >= (int)(wh >> 16)) return false;
+    return ((__ldg(m + kUiMaskHeader + y * (int)__ldg(m + 3) + (x >> 2)) >> (8 * (x & 3))) & 255u) != 0u;
+}
+
+// The estimate fill (gpu/shaders/ui_v2_lumafill.comp), one thread per level-0 cell of the mask rectangle, z = 0 prev,
+// 1 curr: a cell holding a UI pixel takes the mean gray level (cv2's weights, the library's level-0 source) of its
+// not-UI pixels, the window widened by fs px per side per step up to 8 px while there are none, rounded half up to the
+// level-0 grid (multiples of 1 / fs^2) so the estimate's sums stay exact.
+__global__ void __launch_bounds__(64) k_ui_v2_fill(const UiFillParams p) {
+    pdlEnter();
+    const int cx = p.cx0 + (int)(blockIdx.x * 8 + (threadIdx.x & 7)), cy = p.cy0 + (int)(blockIdx.y * 8 + (threadIdx.x >> 3));
+    if (cx >= p.cx0 + p.ncx || cy >= p.cy0 + p.ncy || cx >= p.fw || cy >= p.fh) return;
+    const bool isC = blockIdx.z != 0;
+    const uint32_t* __restrict__ m = isC ? p.mc : p.ma;
+    const uint8_t* f = isC ? p.c : p.a;
+    const int fs = p.fs, px = cx * fs, py = cy * fs;
+    bool has = false;
+    for (int j = 0; j < fs && !has; j++)
+        for (int i = 0; i < fs; i++)
+            if (px + i < p.W && py + j < p.H && uiPx(m, px + i, py + j)) {
+                has = true;
+                break;
+            }
+    if (!has) return;
+    for (int k = 0; k <= 8; k += fs) {
+        int sum = 0, n = 0;
+        for (int y = py - k; y < py + fs + k; y++)
+            for (int x = px - k; x < px + fs + k; x++) {
+                if (x < 0 || y < 0 || x >= p.W || y >= p.H || uiPx(m, x, y)) continue;
+                sum += gray8(__ldg(reinterpret_cast<const uint32_t*>(f + (size_t)y * p.pitch) + x), p.ri, p.gi, p.bi);
+                n++;
+            }
+        if (n > 0) {
+            const int s2 = fs * fs;
+            (isC ? p.lc : p.la)[(size_t)cy * p.fw + cx] = (float)((2 * sum * s2 + n) / (2 * n)) / (float)s2;
+            return;
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launchUiFill(const UiFillParams& p, cudaStream_t s) {
+    return launchPdl(k_ui_v2_fill, dim3(divUp(p.ncx, 8), divUp(p.ncy, 8), 2), dim3(64), 0, s, p);
+}
 
 cudaError_t launchUiV2Update(const UiV2Params& p, cudaStream_t s) {
     return launchPdl(k_ui_v2_update, dim3(divUp(p.ww, kUiTX), divUp(p.wh, kUiTY)), dim3(kUiTX, kUiTY), 0, s, p);

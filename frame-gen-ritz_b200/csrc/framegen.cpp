@@ -139,7 +139,6 @@ const char* kErrSettings = "invalid settings: a field is out of range or not fin
 const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
 const char* kErrUi = "static-UI protection: only CrosshairV2 is built into this library (Crosshair and WholeScreen are not)";
 const char* kErrUiFormat = "static-UI protection (CrosshairV2) is built for the 8-bit RGBA / BGRA formats only";
-const char* kErrUiFill = "static-UI protection: uiEstimateFill is not built into this library";
 const char* kErrNoFormat = "unsupported viewFormat (see framegen::Format)";
 const char* kErrYuvMatrix = "yuvMatrix must be Bt601, Bt709 or Bt2020";
 const char* kErrNits = "linearWhiteNits must be in (0, 10000]";
@@ -257,6 +256,7 @@ struct Interpolator::Impl {
     const void* uiLast = nullptr;
     uint64_t uiClock = 0;
     bool estUi = false;
+    const uint32_t* fillMask[2] = {nullptr, nullptr};   // the estimate fill's masks of the pair being estimated
     int estEnt[2] = {-1, -1};
     uint64_t estStamp[2] = {0, 0};
     // profiling
@@ -559,7 +559,21 @@ struct Interpolator::Impl {
         if (prev.pitch != curr.pitch) return false;
         if (!check(fmt == Format::Rgba8 ? fgk::launchLumaPyr(lp, s) : fgk::launchLumaFmt(lp, s))) return false;
         stamp(s, "luma");
-        for (int l = fgk::kPyrInKernel; l <= top; l++) {
+        const bool fill = fillMask[0] && fillMask[1];
+        if (fill) {   // CrosshairV2's estimate fill of level 0; the pyramid is then rebuilt from the filled level 0
+            fgk::UiFillParams fp{};
+            fp.a = lp.a; fp.c = lp.c; fp.pitch = lp.pitch;
+            fp.W = (int)W; fp.H = (int)H; fp.ri = ri; fp.gi = gi; fp.bi = bi; fp.fs = (int)set.flowScale;
+            fp.fw = L.lv[0].w; fp.fh = L.lv[0].h;
+            fp.ma = fillMask[0]; fp.mc = fillMask[1];
+            fp.la = luma + L.lv[0].lumaA; fp.lc = luma + L.lv[0].lumaC;
+            fp.cx0 = uiWork[0] / fp.fs; fp.cy0 = uiWork[1] / fp.fs;
+            fp.ncx = (uiWork[0] + uiWork[2] - 1) / fp.fs - fp.cx0 + 1;
+            fp.ncy = (uiWork[1] + uiWork[3] - 1) / fp.fs - fp.cy0 + 1;
+            if (!check(fgk::launchUiFill(fp, s))) return false;
+            stamp(s, "ui fill");
+        }
+        for (int l = fill ? 1 : fgk::kPyrInKernel; l <= top; l++) {
             fgk::DownParams dp{luma + L.lv[l - 1].lumaA, luma + L.lv[l - 1].lumaC, L.lv[l - 1].w, L.lv[l - 1].h,
                                luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h, fmt != Format::Rgba8};
             if (!check(fgk::launchDown(dp, s))) return false;
@@ -761,7 +775,6 @@ const char* Interpolator::settingsError(const Settings& s, Format f) {
     if (s.motionVersion != MotionVersion::V1) return kErrVersion;
     if (s.uiProtection != UiProtection::Off && s.uiProtection != UiProtection::CrosshairV2) return kErrUi;
     if (s.uiProtection == UiProtection::CrosshairV2 && f != Format::Rgba8) return kErrUiFormat;
-    if (s.uiProtection == UiProtection::CrosshairV2 && s.uiEstimateFill) return kErrUiFill;
     return nullptr;
 }
 
@@ -922,18 +935,27 @@ bool Interpolator::recordEstimate(cudaStream_t stream, Frame prev, Frame curr) {
         if (m->uiFind(prev.data) < 0 && !m->uiObserve(stream, prev, false)) return false;
         if (m->uiLast != curr.data && !m->uiObserve(stream, curr, false)) return false;
     }
-    if (!m->estimate(stream, prev, curr)) return false;
+    bool ui = false;
+    int ep = -1, ec = -1;
+    if (m->uiOn()) {   // the pair is protected if both frames are kept
+        ep = m->uiFind(prev.data);
+        ec = m->uiFind(curr.data);
+        ui = ep >= 0 && ec >= 0;
+    }
+    m->fillMask[0] = ui && m->set.uiEstimateFill ? m->uiE[ep].mask : nullptr;
+    m->fillMask[1] = ui && m->set.uiEstimateFill ? m->uiE[ec].mask : nullptr;
+    const bool ok = m->estimate(stream, prev, curr);
+    m->fillMask[0] = m->fillMask[1] = nullptr;
+    if (!ok) return false;
     m->haveEst = true;
     m->estPrev = prev.data;
     m->estCurr = curr.data;
-    if (m->uiOn()) {   // the pair is protected if both frames are kept
-        m->estEnt[0] = m->uiFind(prev.data);
-        m->estEnt[1] = m->uiFind(curr.data);
-        m->estUi = m->estEnt[0] >= 0 && m->estEnt[1] >= 0;
-        if (m->estUi) {
-            m->estStamp[0] = m->uiE[m->estEnt[0]].stamp;
-            m->estStamp[1] = m->uiE[m->estEnt[1]].stamp;
-        }
+    m->estUi = ui;
+    if (ui) {
+        m->estEnt[0] = ep;
+        m->estEnt[1] = ec;
+        m->estStamp[0] = m->uiE[ep].stamp;
+        m->estStamp[1] = m->uiE[ec].stamp;
     }
     return true;
 }

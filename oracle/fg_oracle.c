@@ -438,6 +438,66 @@ static void pixel_field(const float* v, int bw, int bh, const float* ya, const f
 
 /* ---------------------------------------------------------------------------------------------- estimate */
 
+/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl; gpu/shaders/motion_v1.glsl:117-129): the UI mask of a
+ * frame over its rectangle (bytes, 0 = not UI). A tap at p reads the pixels lo..hi with X = roundEven(32 p),
+ * lo = X >> 5, hi = lo + (X & 31 != 0) per axis; does any of them lie on the mask? */
+typedef struct { const uint8_t* m; int x, y, w, h, stride; } fgo_uimask;
+
+static int ui_hit(const fgo_uimask* u, float px, float py) {
+    if (!u || !u->m || u->w <= 0 || u->h <= 0) return 0;
+    int X = (int)nearbyintf(px * 32.0f), Y = (int)nearbyintf(py * 32.0f);
+    int lx = X >> 5, ly = Y >> 5, hx = lx + ((X & 31) != 0), hy = ly + ((Y & 31) != 0);
+    int x0 = lx - u->x, y0 = ly - u->y, x1 = hx - u->x, y1 = hy - u->y;
+    if (x0 < 0) x0 = 0;
+    if (y0 < 0) y0 = 0;
+    if (x1 > u->w - 1) x1 = u->w - 1;
+    if (y1 > u->h - 1) y1 = u->h - 1;
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++)
+            if (u->m[(size_t)y * u->stride + x]) return 1;
+    return 0;
+}
+
+/* CrosshairV2's estimate fill (Settings::uiEstimateFill; gpu/shaders/ui_v2_lumafill.comp), restated for this
+ * library's level-0 luma: every flow cell of the mask rectangle's cells that holds a UI pixel (mask byte != 0) takes
+ * the mean gray level of its not-UI pixels, the window widened by S px on every side per step, up to 8 px, while it has
+ * none (no such pixel within 8 px: the cell keeps its luma). The mean is rounded half up to the level-0 grid (a
+ * multiple of 1 / S^2), where the reference keeps it unrounded, so the estimate's sums stay exact in any order. */
+static int ui_px(const fgo_uimask* u, int x, int y) {
+    x -= u->x;
+    y -= u->y;
+    return x >= 0 && y >= 0 && x < u->w && y < u->h && u->m[(size_t)y * u->stride + x] != 0;
+}
+
+static void ui_fill(const img8* m, const fgo_uimask* u, int fs, float* L0, int fw, int fh) {
+    if (!u || !u->m || u->w <= 0 || u->h <= 0) return;
+    const int cx0 = u->x / fs, cx1 = (u->x + u->w - 1) / fs, cy0 = u->y / fs, cy1 = (u->y + u->h - 1) / fs;
+    for (int cy = cy0; cy <= cy1 && cy < fh; cy++)
+        for (int cx = cx0; cx <= cx1 && cx < fw; cx++) {
+            const int px = cx * fs, py = cy * fs;
+            int has = 0;
+            for (int j = 0; j < fs && !has; j++)
+                for (int i = 0; i < fs; i++)
+                    if (px + i < m->W && py + j < m->H && ui_px(u, px + i, py + j)) { has = 1; break; }
+            if (!has) continue;
+            for (int k = 0; k <= 8; k += fs) {
+                long sum = 0;
+                int n = 0;
+                for (int y = py - k; y < py + fs + k; y++)
+                    for (int x = px - k; x < px + fs + k; x++) {
+                        if (x < 0 || y < 0 || x >= m->W || y >= m->H || ui_px(u, x, y)) continue;
+                        sum += gray8(m, x, y);
+                        n++;
+                    }
+                if (n > 0) {
+                    const long s2 = (long)fs * fs;
+                    L0[(size_t)cy * fw + cx] = (float)((2 * sum * s2 + n) / (2 * (long)n)) / (float)s2;
+                    break;
+                }
+            }
+        }
+}
+
 /* interp.estimate (flow + the cut test + pixel_field). Output buffers (any may be NULL except pf):
  *   luma   : per level l, a (lw*lh floats) then c
  *   fields : per level l, the search output then the median3 output (2*bw*bh floats each); then sub1 and sub2
@@ -459,9 +519,28 @@ int fgo_estimate(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, 
 
 /* fgo_estimate with the seed net's output at level cnnLevel (cnn: that level's bw*bh x 8 floats, NULL = plain): the
  * levels above it are skipped and its search is seeded by seed_cnn */
+static int estimate_impl(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                         int cnnLevel, const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads,
+                         float* pf, float* sad_mean, int* cut, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc);
+
 int fgo_estimate_cnn(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
                      int cnnLevel, const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads,
                      float* pf, float* sad_mean, int* cut, int nthreads) {
+    return estimate_impl(a8, c8, W, H, pitch, order, s, cnnLevel, cnn, luma, fields, seeds, meds, sads, pf, sad_mean, cut,
+                         nthreads, NULL, NULL);
+}
+
+/* fgo_estimate with CrosshairV2's estimate fill of prev's / curr's level-0 luma from their UI masks */
+int fgo_estimate_ui(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                    float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean, int* cut,
+                    int nthreads, const fgo_uimask* ua, const fgo_uimask* uc) {
+    return estimate_impl(a8, c8, W, H, pitch, order, s, -1, NULL, luma, fields, seeds, meds, sads, pf, sad_mean, cut,
+                         nthreads, ua, uc);
+}
+
+static int estimate_impl(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
+                         int cnnLevel, const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads,
+                         float* pf, float* sad_mean, int* cut, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #else
@@ -476,6 +555,8 @@ int fgo_estimate_cnn(const uint8_t* a8, const uint8_t* c8, int W, int H, int pit
         for (int k = 0; k < 2; k++) L[l][k] = malloc(sizeof(float) * (size_t)lw[l] * lh[l]);
     luma_area(&A, s->flowScale, L[0][0], fw, fh);
     luma_area(&C, s->flowScale, L[0][1], fw, fh);
+    ui_fill(&A, ua, s->flowScale, L[0][0], fw, fh);
+    ui_fill(&C, uc, s->flowScale, L[0][1], fw, fh);
     for (int l = 1; l < n; l++)
         for (int k = 0; k < 2; k++) fgo_i_area_half(L[l - 1][k], lw[l - 1], lh[l - 1], L[l][k], lw[l], lh[l], 0);
     int r = fgo_i_estimate_levels(L, n, lw, lh, s, cnnLevel, cnn, luma, fields, seeds, meds, sads, pf, sad_mean, cut);
@@ -570,26 +651,6 @@ void fgo_i_field_at(const float* pf, int w, int h, float sf, float* out) {
 /* interp.synth: the frame at time t from the estimate. out has the input's pixel layout (alpha = the nearer
  * frame's). reason: 0 = interpolated, 1 = scene cut, 2 = untrusted share. Optional: field_t (fw*fh*2, the field
  * at t), emap (W*H bytes: the per-pixel mismatch before the 7x7 box), *untrusted (pixels with trust past 0.5). */
-/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl; gpu/shaders/motion_v1.glsl:117-129): the UI mask of a
- * frame over its rectangle (bytes, 0 = not UI). A tap at p reads the pixels lo..hi with X = roundEven(32 p),
- * lo = X >> 5, hi = lo + (X & 31 != 0) per axis; does any of them lie on the mask? */
-typedef struct { const uint8_t* m; int x, y, w, h, stride; } fgo_uimask;
-
-static int ui_hit(const fgo_uimask* u, float px, float py) {
-    if (!u || !u->m || u->w <= 0 || u->h <= 0) return 0;
-    int X = (int)nearbyintf(px * 32.0f), Y = (int)nearbyintf(py * 32.0f);
-    int lx = X >> 5, ly = Y >> 5, hx = lx + ((X & 31) != 0), hy = ly + ((Y & 31) != 0);
-    int x0 = lx - u->x, y0 = ly - u->y, x1 = hx - u->x, y1 = hy - u->y;
-    if (x0 < 0) x0 = 0;
-    if (y0 < 0) y0 = 0;
-    if (x1 > u->w - 1) x1 = u->w - 1;
-    if (y1 > u->h - 1) y1 = u->h - 1;
-    for (int y = y0; y <= y1; y++)
-        for (int x = x0; x <= x1; x++)
-            if (u->m[(size_t)y * u->stride + x]) return 1;
-    return 0;
-}
-
 static int synth_impl(const uint8_t* a8, const uint8_t* c8, int W, int H, int pitch, int order, const fgo_settings* s,
                       const float* pf, int cut, float t, uint8_t* out, int out_pitch, float* field_t, uint8_t* emap,
                       long long* untrusted, int* reason, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc);

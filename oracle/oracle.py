@@ -78,6 +78,10 @@ def lib():
         L.fgo_synth.restype = ctypes.c_int
         L.fgo_synth_ui.argtypes = L.fgo_synth.argtypes + [ctypes.POINTER(_CUiMask), ctypes.POINTER(_CUiMask)]
         L.fgo_synth_ui.restype = ctypes.c_int
+        L.fgo_estimate_ui.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(_CSettings), P, P, P, P, P, P, P, P, ctypes.c_int,
+                                      ctypes.POINTER(_CUiMask), ctypes.POINTER(_CUiMask)]
+        L.fgo_estimate_ui.restype = ctypes.c_int
         L.fgo_mean_f32.argtypes = [P, ctypes.c_long]
         L.fgo_mean_f32.restype = ctypes.c_float
         _lib = L
@@ -113,10 +117,11 @@ def _frame_args(a, order):
     return a, a.shape[1], a.shape[0], a.strides[0]
 
 
-def estimate(a, c, settings=None, order="rgba", trace=True, threads=0, seed_net=None):
+def estimate(a, c, settings=None, order="rgba", trace=True, threads=0, seed_net=None, ui_fill=None):
     """interp.estimate(a, c) plus every intermediate: returns a dict with sad (the float32 mean as a Python float),
     cut (bool), pf (fh, fw, 2) and, with trace, luma/fields/seeds/meds/sads per level. seed_net = (level, output):
-    the CNN-seeded estimate from the seed net's output (bh, bw, 8) at that level (no counterpart in interp.py)."""
+    the CNN-seeded estimate from the seed net's output (bh, bw, 8) at that level (no counterpart in interp.py).
+    ui_fill = (prev's mask, curr's mask), each (bytes, rect): CrosshairV2's estimate fill of the level-0 luma."""
     s = settings or Settings()
     a, W, H, pitch = _frame_args(a, order)
     c, _, _, _ = _frame_args(c, order)
@@ -133,9 +138,15 @@ def estimate(a, c, settings=None, order="rgba", trace=True, threads=0, seed_net=
     pf = np.zeros((L.fh, L.fw, 2), np.float32)
     mean, cut = ctypes.c_float(), ctypes.c_int()
     lvl, cnn = (-1, None) if seed_net is None else (int(seed_net[0]), np.ascontiguousarray(seed_net[1], np.float32))
-    n = lib().fgo_estimate_cnn(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), lvl, _p(cnn), _p(luma),
-                               _p(fields), _p(seeds), _p(meds), _p(sads), _p(pf), ctypes.byref(mean), ctypes.byref(cut),
-                               threads)
+    if ui_fill is not None:
+        (ma, ka), (mc, kc) = _uimask(ui_fill[0]), _uimask(ui_fill[1])
+        n = lib().fgo_estimate_ui(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), _p(luma), _p(fields),
+                                  _p(seeds), _p(meds), _p(sads), _p(pf), ctypes.byref(mean), ctypes.byref(cut), threads,
+                                  ctypes.byref(ma) if ma else None, ctypes.byref(mc) if mc else None)
+    else:
+        n = lib().fgo_estimate_cnn(_p(a), _p(c), W, H, pitch, ORDERS[order], ctypes.byref(_cs(s)), lvl, _p(cnn),
+                                   _p(luma), _p(fields), _p(seeds), _p(meds), _p(sads), _p(pf), ctypes.byref(mean),
+                                   ctypes.byref(cut), threads)
     if n != len(L.levels):
         raise RuntimeError("fgo_estimate failed")
     est = {"sad": float(mean.value), "cut": bool(cut.value), "pf": pf, "layout": L,

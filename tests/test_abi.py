@@ -86,10 +86,10 @@ def test_settings_error_names_unbuilt_parts():
     for mode in (1, 2):   # Crosshair, WholeScreen
         s = fg.Settings(uiProtection=mode)
         assert fg.validate(s) and "only CrosshairV2" in fg.settings_error(s)
-    s = fg.Settings(uiProtection=3)   # CrosshairV2: built for the 8-bit RGBA formats, without uiEstimateFill
+    s = fg.Settings(uiProtection=3)   # CrosshairV2: built for the 8-bit RGBA formats, with or without uiEstimateFill
     assert fg.validate(s) and fg.settings_error(s) is None
+    assert fg.settings_error(fg.Settings(uiProtection=3, uiEstimateFill=True)) is None
     assert "8-bit RGBA" in fg.settings_error(s, fmt="Rgb10")
-    assert "uiEstimateFill" in fg.settings_error(fg.Settings(uiProtection=3, uiEstimateFill=True))
 
 
 def test_box_geometry():

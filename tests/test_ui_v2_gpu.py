@@ -109,12 +109,15 @@ def run_sequence(frames, s, ts=(0.5, 0.25), observe=True, blur=None):
     return [o.cpu().numpy() for o in outs], I, dev
 
 
-@pytest.mark.parametrize("case", ["defaults", "fast_reentry_off", "no_contrast_gate", "offset_box"])
+@pytest.mark.parametrize("case", ["defaults", "fast_reentry_off", "no_contrast_gate", "offset_box", "estimate_fill",
+                                  "estimate_fill_fs1"])
 def test_state_and_outputs_match_the_oracle(case):
     W, H = 160, 96
     kw = {"defaults": {}, "fast_reentry_off": dict(uiReentryFrames=0, uiLeaveFrames=1),
           "no_contrast_gate": dict(uiContrastThreshold=0.0, uiStillFrames=3),
-          "offset_box": dict(uiBoxWidth=24, uiBoxHeight=20, uiBoxOffsetX=-9, uiBoxOffsetY=5)}[case]
+          "offset_box": dict(uiBoxWidth=24, uiBoxHeight=20, uiBoxOffsetX=-9, uiBoxOffsetY=5),
+          "estimate_fill": dict(uiEstimateFill=True, uiBoxWidth=20, uiBoxHeight=18),
+          "estimate_fill_fs1": dict(uiEstimateFill=True, flowScale=1)}[case]
     s = v2_settings(**kw)
     frames, _ = grain_scene(W, H, 12)
     # a disturbance: frame 6 flashes a square over the plus (the leave counter runs, the plus may leave and re-enter)
@@ -137,11 +140,14 @@ def test_state_and_outputs_match_the_oracle(case):
         wx, wy, ww, wh = st.work
         assert tuple(int(v) for v in got["header"][1:]) == (wx | (wy << 16), ww | (wh << 16), (ww + 3) // 4)
     assert (masks[11] == 255).sum() > 0, "the plus was never detected"
-    # the last pair: rejection + paste, against the oracle
+    # the last pair: (the estimate fill,) rejection + paste, against the oracle
     I.begin_frame()
     assert I.record_estimate(dev[10], dev[11])
-    est = oracle.estimate(frames[10], frames[11], settings=oracle_settings(s), trace=False)
     rect = st.work
+    fill = ((masks[10], rect), (masks[11], rect)) if s.uiEstimateFill else None
+    est = oracle.estimate(frames[10], frames[11], settings=oracle_settings(s), trace=True, ui_fill=fill)
+    from gpu_util import assert_estimate_equal
+    assert_estimate_equal(fg.read_trace(I), est)
     for t in (0.5, 0.25, float(np.float32(2 / 3))):
         o = torch.empty_like(dev[0])
         assert I.record_synth(dev[10], dev[11], o, t)
@@ -180,11 +186,9 @@ def artifacts(ui, out, ref, cx, cy, r=40, tol=24):
 
 def test_doubled_crosshair_gates():
     """gpu/formattest.cpp:611-690, 1100-1111: a grain background panning (14, 6) px per frame, a static 12x12 cyan
-    plus. Off copies the plus along the pan (>= 15 artifact pixels: the check has teeth); CrosshairV2 pastes the plus
-    pixel-exact at t = 0.5 and leaves few artifact pixels around it, at t = 0.5 and in the blurred output. The
-    reference's gate of 8 artifact pixels is measured with its uiEstimateFill on; this library does not build the
-    fill (what is left without it is flow noise from the plus's vote for the zero vector), so the count is printed and
-    held to 24."""
+    plus. Off copies the plus along the pan (>= 15 artifact pixels: the check has teeth); CrosshairV2 with the estimate
+    fill (as the reference measures it) pastes the plus pixel-exact at t = 0.5 and leaves at most 8 artifact pixels
+    around it, at t = 0.5 and in the blurred output. The count without the fill is printed beside it."""
     W, H = 320, 192
     frames, ui = grain_scene(W, H, 12)
     clean, _ = grain_scene(W, H, 12, plus=False)
@@ -192,15 +196,18 @@ def test_doubled_crosshair_gates():
     blur = (0.3, 0.7)
     ref, Ir, _ = run_sequence(clean, fg.Settings(blurSamples=3), ts=(0.5,), blur=blur)
     off, Io, _ = run_sequence(frames, fg.Settings(blurSamples=3), ts=(0.5,), blur=blur)
-    v2, Iv, _ = run_sequence(frames, v2_settings(blurSamples=3), ts=(0.5,), blur=blur)
+    v2, Iv, _ = run_sequence(frames, v2_settings(blurSamples=3, uiEstimateFill=True), ts=(0.5,), blur=blur)
+    nofill, In, _ = run_sequence(frames, v2_settings(blurSamples=3), ts=(0.5,), blur=blur)
     a_off = [artifacts(ui, o, r, cx, cy) for o, r in zip(off, ref)]
     a_v2 = [artifacts(ui, o, r, cx, cy) for o, r in zip(v2, ref)]
+    a_nf = [artifacts(ui, o, r, cx, cy) for o, r in zip(nofill, ref)]
     plus_bad = int(np.count_nonzero(np.abs(v2[0][..., :3].astype(int) - frames[-1][..., :3].astype(int)).max(axis=2)[ui] > 1))
-    print(f"artifact px around the plus (t = 0.5 / blurred): Off {a_off}, CrosshairV2 {a_v2}; plus pixels wrong {plus_bad}")
+    print(f"artifact px around the plus (t = 0.5 / blurred): Off {a_off}, CrosshairV2 + fill {a_v2}, without the fill "
+          f"{a_nf}; plus pixels wrong {plus_bad}")
     assert min(a_off) >= 15
     assert plus_bad == 0
-    assert max(a_v2) <= 24
-    for I in (Ir, Io, Iv):
+    assert max(a_v2) <= 8
+    for I in (Ir, Io, Iv, In):
         I.close()
 
 
