@@ -134,6 +134,17 @@ def gpu_decision(cut, untrusted, W, H, frac=0.15):
     return "untrusted" if untrusted / (W * H) > float(np.float32(frac)) else None
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_leg(pool, outs, seconds):
     """The CPU baseline on the metric's own workload: the oracle (the plain-C port of proto/interp.py, all host
     threads) runs estimate + 3 synths on full 3840x2160 pairs of the pool, for about `seconds` (at least every pool
@@ -495,7 +506,8 @@ def run_reference(a):
                       "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
                       "config": {"workload": "V1 plain, 3840x2160 Rgba8, 4x (estimate + 3 synths), flowScale 2",
                                  "cpu_impl": "oracle port (plain C, OpenMP) of proto/interp.py"},
-                      "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
+                      "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "port", "sample": sample,
+                                       "cpu_model": cpu_model()},
                       "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
           flush=True)
 
@@ -807,7 +819,7 @@ def main():
                 g.replay()
         torch.cuda.synchronize()
         v, n, tally = cpu_leg(pool, outs, a.cpu_seconds)
-        cpu = {"value": round(v, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+        cpu = {"value": round(v, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port", "cpu_model": cpu_model(),
                "sample": f"{n} full 3840x2160 pairs of the pool, estimate + 3 synths each, median; oracle (plain-C "
                          f"restatement of proto/interp.py, OpenMP, all host threads)"}
         parity = {"metric_workload": tally.report(workload="the bench's 4K pool: the GPU's graph outputs against the "
