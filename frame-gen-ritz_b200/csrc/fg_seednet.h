@@ -40,7 +40,10 @@ struct SnBackArgs {
     float* dw;         // += dL/dW, float [cout][9][cin]
     float* db;         // += dL/db, float [cout]
     int B, H, W, Ho, Wo;
+    float* part;       // the weight gradient's per-CTA partial sums (kSnPartFloats per CTA, up to partCtas CTAs)
+    int partCtas;
 };
+constexpr int kSnPartFloats = (9 * 32 + 1) * 32;   // rows (tap, ci) + the bias row, times cout, of the widest layer
 
 struct SnAdamArgs {
     float* p; float* m; float* v; float* grad;   // float32 master parameters, moments, gradients (zeroed here)

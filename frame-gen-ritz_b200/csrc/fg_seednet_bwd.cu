@@ -5,8 +5,8 @@
 //   k_sn_dw_tc<CIN, COUT, S>  dW[co][tap][ci] += sum_p x[S p + tap - 1][ci] dpre[p][co], db[co] += sum_p dpre[p][co]
 //       GEMM D[m][n] = sum_k A[m][k] B[n][k] with m = tap * CIN + ci (plus one row of ones at m = 9 CIN, which makes
 //       that row of D the bias gradient), n = co, k = output pixel. Every CTA reduces a contiguous slice of the output
-//       pixels in chunks of 64 (4 MMAs of K = 16 per 128-row chunk of m), the operands double-buffered, and adds its
-//       partial D into dW / db with float atomics.
+//       pixels in chunks of 64 (4 MMAs of K = 16 per 128-row chunk of m), the operands double-buffered, and stores its
+//       partial D; k_sn_dw_sum then adds the partials into dW / db in CTA order, so the gradient is deterministic.
 //   k_sn_dx_tc<CIN, COUT, S>  dpre_in[q][ci] = [x[q][ci] > 0] sum_{tap, co} w[co][tap][ci] dpre[p(q, tap)][co], the
 //       output pixels p with S p + tap - 1 = q: GEMM with m = input pixel q (128 per chunk), n = ci, k = tap * COUT + co
 //       (padded to a multiple of 16); the weights are staged once per CTA.
@@ -160,11 +160,10 @@ __global__ void __launch_bounds__(kBwdThreads) k_sn_dw_tc(const SnBackArgs a, in
             float v[16];
             if (Sh::NP / 2 == 16) tmemLd16(ta, v);
             else tmemLd8(ta, v);
+            float* part = a.part + (size_t)blockIdx.x * kSnPartFloats;
             for (int j = 0; j < Sh::NP / 2; j++) {
                 const int co = half * (Sh::NP / 2) + j;
-                if (co >= COUT) continue;
-                if (m < 9 * CIN) atomicAdd(a.dw + (co * 9 + m / CIN) * CIN + m % CIN, v[j]);
-                else if (m == 9 * CIN) atomicAdd(a.db + co, v[j]);
+                if (co < COUT && m <= 9 * CIN) part[m * COUT + co] = v[j];
             }
         }
     }
@@ -175,6 +174,18 @@ __global__ void __launch_bounds__(kBwdThreads) k_sn_dw_tc(const SnBackArgs a, in
         tcFenceAfter();
         tmemFree(tbase, Sh::TCOLS);
     }
+}
+
+// dW / db += the sum of the CTAs' partial products, in CTA order (one thread per (row, co))
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(256) k_sn_dw_sum(const SnBackArgs a, int ctas) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= (9 * CIN + 1) * COUT) return;
+    const int m = i / COUT, co = i % COUT;
+    float s = 0.0f;
+    for (int b = 0; b < ctas; b++) s += a.part[(size_t)b * kSnPartFloats + i];
+    if (m < 9 * CIN) a.dw[(co * 9 + m / CIN) * CIN + m % CIN] += s;
+    else a.db[co] += s;
 }
 
 template <int CIN, int COUT>
@@ -302,9 +313,11 @@ cudaError_t dwLaunch(const SnBackArgs& a, unsigned int* err, cudaStream_t s) {
     static_assert(Sh::SMEM <= 227 * 1024, "shared memory");
     const int npix = a.B * a.Ho * a.Wo;
     const int nchunks = (npix + kDwK - 1) / kDwK;
-    const int ctas = std::min(nchunks, 2 * smCount());
+    const int ctas = std::min(nchunks, a.partCtas);
     const int per = (nchunks + ctas - 1) / ctas;
-    k_sn_dw_tc<CIN, COUT, S><<<(nchunks + per - 1) / per, kBwdThreads, Sh::SMEM, s>>>(a, per, err);
+    const int grid = (nchunks + per - 1) / per;
+    k_sn_dw_tc<CIN, COUT, S><<<grid, kBwdThreads, Sh::SMEM, s>>>(a, per, err);
+    k_sn_dw_sum<CIN, COUT><<<divUp((9 * CIN + 1) * COUT, 256), 256, 0, s>>>(a, grid);
     return cudaGetLastError();
 }
 

@@ -61,6 +61,8 @@ struct fg_seednet {
     float* loss = nullptr;
     void* act[kSnLayers - 1] = {};   // bf16 outputs of layers 1..5
     unsigned int* errFlags = nullptr;   // the fused forward's sticky error bits (kErrSeedNet) when no other is given
+    float* part = nullptr;              // the weight gradient's per-CTA partial sums
+    int partCtas = 0;
     float* out = nullptr;            // last layer (float)
     float* dA = nullptr;             // gradient ping-pong buffers (float)
     float* dB = nullptr;
@@ -142,6 +144,7 @@ struct fg_seednet {
             a.dw = grad + snWeightOff(l);
             a.db = grad + snBiasOff(l);
             a.B = B; a.H = d.h[l]; a.W = d.w[l]; a.Ho = d.h[l + 1]; a.Wo = d.w[l + 1];
+            a.part = part; a.partCtas = partCtas;
             if (!ok(launchSnBackwardTc(l, a, l > 0, errFlags, s), "backward", l)) return false;
             dy = a.dx;
         }
@@ -186,6 +189,10 @@ fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w) {
     }
     const size_t oOut = take((size_t)max_batch * d.h[kSnLayers] * d.w[kSnLayers] * kSnOut * 4);
     const size_t oErr = take(4);
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device) != cudaSuccess) { cudaGetLastError(); sms = 148; }
+    n->partCtas = 2 * sms;
+    const size_t oPart = take((size_t)n->partCtas * kSnPartFloats * 4);
     const size_t oDA = take(maxGrad * 4), oDB = take(maxGrad * 4);
     if (cudaMalloc(&n->mem, off) != cudaSuccess) {
         cudaGetLastError();
@@ -199,6 +206,7 @@ fg_seednet* fg_seednet_create(int device, int max_batch, int max_h, int max_w) {
     for (int l = 0; l < kSnLayers - 1; l++) n->act[l] = n->mem + oAct[l];
     n->out = (float*)(n->mem + oOut);
     n->errFlags = (unsigned int*)(n->mem + oErr);
+    n->part = (float*)(n->mem + oPart);
     if (prepareSeedNetFused() != cudaSuccess || prepareSeedNetBackward() != cudaSuccess) {   // shared-memory limits
         cudaGetLastError();
         cudaFree(n->mem);
