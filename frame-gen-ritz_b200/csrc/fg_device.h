@@ -161,6 +161,9 @@ constexpr int kSyE = 64, kSyEH = 64, kSyAp = 3;
 constexpr int kSyT = kSyE - 2 * kSyAp, kSyTH = kSyEH - 2 * kSyAp;
 constexpr int kSyThreads = 512, kSyK = kSyEH / (kSyThreads / kSyE);   // region rows per thread (512 = 64 columns x 8)
 constexpr size_t kSyWarpBytes = (size_t)2 * kSyTH * kSyE * 4;   // k_synth: both warps of the output rows, after the row sums
+// the output row (tile coordinates) of a thread's k-th output pixel: thread rows ey0 = 0..7 take kSyK consecutive rows
+// each (the last only kSyTH - 7 kSyK of them), so the vertical 7-sums run as a sliding window
+__device__ __forceinline__ int syOutRow(int ey0, int k) { return ey0 * kSyK + k; }
 // row strides of the mismatch plane e (bytes) and of its horizontal 7-sums (uint16): one word of padding per row, so
 // that the lanes of a warp can walk 32 different rows of one column group without bank conflicts
 constexpr int kSyES = kSyE + 4, kSyHS = kSyE + 2;

@@ -989,14 +989,17 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
             }
         }
         __syncthreads();
-        // 3. vertical 5-sums, the cost, the running first minimum
+        // 3. vertical 5-sums (a running window down this thread's kPfK consecutive output rows), the cost, the running
+        //    first minimum
         const int lx = ex - kPfAp;
         if ((unsigned)lx < (unsigned)kPfTW) {
+            const int ly0 = ey0 * kPfK;
+            int S = hs[ly0][lx] + hs[ly0 + 1][lx] + hs[ly0 + 2][lx] + hs[ly0 + 3][lx];
 #pragma unroll
             for (int j = 0; j < kPfK; j++) {
-                const int ly = ey0 + 4 * j - kPfAp;
-                if ((unsigned)ly >= (unsigned)kPfTH) continue;
-                const int S = hs[ly][lx] + hs[ly + 1][lx] + hs[ly + 2][lx] + hs[ly + 3][lx] + hs[ly + 4][lx];
+                const int ly = ly0 + j;
+                if (ly >= kPfTH) break;   // uniform over the warp; later rows are out too
+                S += hs[ly + 4][lx] - (j ? hs[ly - 1][lx] : 0);
                 float c = (float)(__dadd_rn(__hiloint2double(0x43300000, S), -4503599627370496.0) * C);
                 if (k == 0) c = __fsub_rn(c, p.smooth);
                 if (k == kPfNC - 1) c = __fsub_rn(c, p.zero);
@@ -1009,8 +1012,8 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     if ((unsigned)lx >= (unsigned)kPfTW || x >= p.w) return;
 #pragma unroll
     for (int j = 0; j < kPfK; j++) {
-        const int ey = ey0 + 4 * j, ly = ey - kPfAp, y = Y0 + ly;
-        if ((unsigned)ly >= (unsigned)kPfTH || y >= p.h) continue;
+        const int ly = ey0 * kPfK + j, ey = ly + kPfAp, y = Y0 + ly;
+        if (ly >= kPfTH || y >= p.h) break;
         const int k = bestk[j];
         float2 v;
         if (k == 0) {
@@ -1042,27 +1045,29 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
 // the conversion units; the bilinear taps run two channels per 32-bit multiply (R|B lanes, G) and the mismatch and the
 // t = 0.5 blend use byte-SIMD instructions.
 
-// one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame at the position whose
-// rne32 bits are (bx, by): channels 0..2 of the result (byte 3 = 0; also unpacked in ch). Horizontal stage two channels per multiply (16-bit
-// lanes hold at most 255 * 32), vertical stage per channel; (v + 512) >> 10 == cv2's (32 v + 2^14) >> 15.
+// one cv2.remap INTER_LINEAR / BORDER_REPLICATE sample of a 4-byte-per-pixel 8-bit frame of at least 2 x 2 pixels
+// at the position whose rne32 bits are (bx, by): channels 0..2 of the result (byte 3 = 0; also unpacked in ch).
+// Borders: the 1/32-pixel position is clamped to [0, 32 (W - 1)], the left tap is min(X >> 5, W - 2) and the right
+// weight X - 32 ix (0..32): at the right edge the taps (W - 2, W - 1) with weights (0, 32), the same products as cv2's
+// (W - 1, W - 1) pair, so the four taps are always (ix, iy) + {0, 1}^2 (one address, fixed offsets). Filter: cv2's
+// 15-bit weights of 5-bit bilinear fractions are 32 wx wy, and (sum p 32 wx wy + 2^14) >> 15 == (sum p wx wy + 512) >> 10
+// with wx wy <= 1024; per channel two 16-bit x 8-bit dot products (dp2a) on tap bytes gathered by byte permutes, exact
+// in 32 bits.
 __device__ __forceinline__ uint32_t sampleU8(const uint32_t* __restrict__ img, uint32_t pw, int W, int H, float bxf, float byf,
                                              int ch[3]) {
-    const int X = __float_as_int(bxf) - 0x4B400000, Y = __float_as_int(byf) - 0x4B400000;
-    const int ix = X >> 5, iy = Y >> 5;
-    const uint32_t fx = (uint32_t)X & 31u, fy = (uint32_t)Y & 31u;
-    // taps clamped one by one, without a branch, so the loads of the samples a thread takes can all be in flight
-    // together (pw: row pitch in 4-byte words)
-    const uint32_t x0 = (uint32_t)clampi(ix, 0, W - 1), x1 = (uint32_t)clampi(ix + 1, 0, W - 1);
-    const uint32_t r0 = (uint32_t)clampi(iy, 0, H - 1) * pw, r1 = (uint32_t)clampi(iy + 1, 0, H - 1) * pw;
-    const uint32_t p00 = __ldg(img + r0 + x0), p01 = __ldg(img + r0 + x1);
-    const uint32_t p10 = __ldg(img + r1 + x0), p11 = __ldg(img + r1 + x1);
-    const uint32_t M = 0x00FF00FFu, wx0 = 32u - fx, wy0 = 32u - fy;
-    const uint32_t rb0 = (p00 & M) * wx0 + (p01 & M) * fx, rb1 = (p10 & M) * wx0 + (p11 & M) * fx;
-    const uint32_t g0 = __byte_perm(p00, 0, 0x4441) * wx0 + __byte_perm(p01, 0, 0x4441) * fx;
-    const uint32_t g1 = __byte_perm(p10, 0, 0x4441) * wx0 + __byte_perm(p11, 0, 0x4441) * fx;
-    const uint32_t c0 = ((rb0 & 0xFFFFu) * wy0 + (rb1 & 0xFFFFu) * fy + 512u) >> 10;
-    const uint32_t c2 = ((rb0 >> 16) * wy0 + (rb1 >> 16) * fy + 512u) >> 10;
-    const uint32_t c1 = (g0 * wy0 + g1 * fy + 512u) >> 10;
+    const int X = clampi(__float_as_int(bxf) - 0x4B400000, 0, 32 * (W - 1));
+    const int Y = clampi(__float_as_int(byf) - 0x4B400000, 0, 32 * (H - 1));
+    const int ix = min(X >> 5, W - 2), iy = min(Y >> 5, H - 2);
+    const uint32_t fx = (uint32_t)(X - 32 * ix), fy = (uint32_t)(Y - 32 * iy);
+    const uint32_t* q = img + ((uint32_t)iy * pw + (uint32_t)ix);
+    const uint32_t p00 = __ldg(q), p01 = __ldg(q + 1), p10 = __ldg(q + pw), p11 = __ldg(q + pw + 1);
+    const uint32_t wx = (32u - fx) | (fx << 16);            // (left, right) weights as 16-bit lanes
+    const uint32_t w0 = wx * (32u - fy), w1 = wx * fy;      // (w00, w01), (w10, w11): lanes <= 1024, no carry
+    const uint32_t rg0 = __byte_perm(p00, p01, 0x5140), rg1 = __byte_perm(p10, p11, 0x5140);   // R00 R01 G00 G01
+    const uint32_t b0 = __byte_perm(p00, p01, 0x0062), b1 = __byte_perm(p10, p11, 0x6200);     // B00 B01 / - - B10 B11
+    const uint32_t c0 = __dp2a_lo(w1, rg1, __dp2a_lo(w0, rg0, 512u)) >> 10;
+    const uint32_t c1 = __dp2a_hi(w1, rg1, __dp2a_hi(w0, rg0, 512u)) >> 10;
+    const uint32_t c2 = __dp2a_hi(w1, b1, __dp2a_lo(w0, b0, 512u)) >> 10;
     ch[0] = (int)c0;
     ch[1] = (int)c1;
     ch[2] = (int)c2;
@@ -1146,16 +1151,18 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
     // 3. horizontal 7-sums: one region row and 8 output columns per thread, a running window
     syRowSums(e, hsum, tid);
     __syncthreads();
-    // 4. this thread's output pixels: vertical 7-sum, trust, blend, store
+    // 4. this thread's output pixels, kSyK consecutive rows of one column: vertical 7-sum (a running window), trust,
+    //    blend, store
     unsigned int myCnt = 0;
     const int lx = ex - kSyAp, x = X0 + lx;
     if ((unsigned)lx < (unsigned)kSyT && x < p.W) {
+        const unsigned short* q = hsum + syOutRow(ey0, 0) * kSyHS + lx;
+        int S = q[0] + q[kSyHS] + q[2 * kSyHS] + q[3 * kSyHS] + q[4 * kSyHS] + q[5 * kSyHS];
 #pragma unroll
         for (int k = 0; k < kSyK; k++) {
-            const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = Y0 + ly;
-            if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
-            const unsigned short* q = hsum + ly * kSyHS + lx;
-            const int S = q[0] + q[kSyHS] + q[2 * kSyHS] + q[3 * kSyHS] + q[4 * kSyHS] + q[5 * kSyHS] + q[6 * kSyHS];
+            const int ly = syOutRow(ey0, k), y = Y0 + ly;
+            if (ly >= kSyTH || y >= p.H) break;   // uniform over the warp; later rows are out too
+            S += q[(k + 6) * kSyHS] - (k ? q[(k - 1) * kSyHS] : 0);
             const uint32_t nq = __ldg(reinterpret_cast<const uint32_t*>(nearF + (size_t)y * pitch) + x);
             const uint32_t wak = sWA[ly * kSyE + ex], wck = sWC[ly * kSyE + ex];
             uint32_t o;
@@ -1295,9 +1302,9 @@ __global__ void __launch_bounds__(kSyThreads, 2) k_synth_blur_t(const BlurParams
     const int lx = ex - kSyAp, x = blockIdx.x * kSyT + lx;
     if ((unsigned)lx >= (unsigned)kSyT || x >= b.W) return;
 #pragma unroll
-    for (int k = 0; k < kSyK; k++) {
-        const int ly = ey0 + (kSyThreads / kSyE) * k - kSyAp, y = blockIdx.y * kSyTH + ly;
-        if ((unsigned)ly >= (unsigned)kSyTH || y >= b.H) continue;
+    for (int k = 0; k < kSyK; k++) {   // the pixels synthTileCore gave this thread's slot k
+        const int ly = syOutRow(ey0, k), y = blockIdx.y * kSyTH + ly;
+        if (ly >= kSyTH || y >= b.H) break;
         const uint32_t pa = __ldg(reinterpret_cast<const uint32_t*>(b.a + (size_t)y * pitch) + x);
         const uint32_t pc = __ldg(reinterpret_cast<const uint32_t*>(b.c + (size_t)y * pitch) + x);
         uint32_t o = 0;

@@ -126,12 +126,18 @@ __device__ __forceinline__ uint4 actPack(const float v[8], const float* b, bool 
 
 // a 32 -> N layer's bf16 weights [n][9][32] (global) into the canonical K-major layout [kc = k / 8][n][8]; rows
 // n >= nValid are zero
-template <int N>
-__device__ __forceinline__ void stageW32(const bf16* __restrict__ w, int nValid, uint4* dst, int tid, int nthreads) {
-    for (int i = tid; i < 36 * N; i += nthreads) {
-        const int kc = i / N, n = i % N;
-        dst[kc * N + n] = n < nValid ? *reinterpret_cast<const uint4*>(w + (size_t)n * 288 + kc * 8) : make_uint4(0, 0, 0, 0);
+template <int N, int kThreads>
+__device__ __forceinline__ void stageW32(const bf16* __restrict__ w, int nValid, uint4* dst, int tid) {
+    constexpr int kIt = (36 * N + kThreads - 1) / kThreads;
+    uint4 v[kIt];
+#pragma unroll
+    for (int j = 0; j < kIt; j++) {   // all loads in flight before the first store
+        const int i = tid + j * kThreads, kc = i / N, n = i % N;
+        v[j] = i < 36 * N && n < nValid ? __ldg(reinterpret_cast<const uint4*>(w + (size_t)n * 288 + kc * 8)) : make_uint4(0, 0, 0, 0);
     }
+#pragma unroll
+    for (int j = 0; j < kIt; j++)
+        if (tid + j * kThreads < 36 * N) dst[tid + j * kThreads] = v[j];
 }
 
 // chunk schedule: 128-row chunks covering [0, M), the last one moved back to end at M (rows recomputed, not read past)
@@ -191,13 +197,18 @@ __global__ void __launch_bounds__(kEncThreads, 1) k_sn_enc(const SnFusedArgs a) 
     // weights and biases (not produced by the preceding kernels)
     {
         const bf16* __restrict__ wg = reinterpret_cast<const bf16*>(a.wb);
-        for (int i = tid; i < 4 * 32 * 8; i += kEncThreads) {   // layer 1: K = 18 (tap * 2 + ci), padded to 32
-            const int kc = i >> 8, n = (i >> 3) & 31, e = i & 7, k = kc * 8 + e;
-            w1[i] = k < 18 ? wg[kW[0] + n * 18 + k] : __float2bfloat16(0.0f);
+        bf16 v1[2];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {   // layer 1: K = 18 (tap * 2 + ci), padded to 32; 4 x 32 x 8 = 2 x 512 entries
+            const int i = tid + j * kEncThreads, kc = i >> 8, n = (i >> 3) & 31, e = i & 7, k = kc * 8 + e;
+            v1[j] = k < 18 ? wg[kW[0] + n * 18 + k] : __float2bfloat16(0.0f);
         }
-        stageW32<32>(wg + kW[1], 32, reinterpret_cast<uint4*>(sm + kOffW2), tid, kEncThreads);
-        stageW32<32>(wg + kW[2], 32, reinterpret_cast<uint4*>(sm + kOffW3), tid, kEncThreads);
-        if (tid < 96) bias[tid] = a.p[(tid < 32 ? kB[0] : tid < 64 ? kB[1] : kB[2]) + (tid & 31)];
+        const float bv = tid < 96 ? a.p[(tid < 32 ? kB[0] : tid < 64 ? kB[1] : kB[2]) + (tid & 31)] : 0.0f;
+        stageW32<32, kEncThreads>(wg + kW[1], 32, reinterpret_cast<uint4*>(sm + kOffW2), tid);
+        stageW32<32, kEncThreads>(wg + kW[2], 32, reinterpret_cast<uint4*>(sm + kOffW3), tid);
+        w1[tid] = v1[0];
+        w1[tid + kEncThreads] = v1[1];
+        if (tid < 96) bias[tid] = bv;
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
     // the luma region, normalised ((v - 128) / 64, bf16), zero outside the level
@@ -205,17 +216,31 @@ __global__ void __launch_bounds__(kEncThreads, 1) k_sn_enc(const SnFusedArgs a) 
         const int ly0 = 8 * cy0 - 7, lx0 = 8 * cx0 - 7;
         const float* __restrict__ la = a.xp ? nullptr : a.la + (size_t)bz * a.h * a.w;
         const float* __restrict__ lc = a.xp ? nullptr : a.lc + (size_t)bz * a.h * a.w;
-        for (int i = tid; i < kR0y * kP0; i += kEncThreads) {
-            const int y = i / kP0, x = i % kP0, gy = ly0 + y, gx = lx0 + x;
-            uint32_t v = 0;
-            if (x < kR0x && gy >= 0 && gy < a.h && gx >= 0 && gx < a.w) {
-                const size_t o = (size_t)gy * a.w + gx;
-                if (a.xp) v = __ldg(a.xp + (size_t)bz * a.h * a.w + o);
-                else
-                    v = packBf2(__fmul_rn(__fsub_rn(__ldg(la + o), 128.0f), 1.0f / 64.0f),
-                                __fmul_rn(__fsub_rn(__ldg(lc + o), 128.0f), 1.0f / 64.0f));
+        constexpr int kIt = (kR0y * kP0 + kEncThreads - 1) / kEncThreads;
+        float va[kIt], vc[kIt];
+        uint32_t vx[kIt];
+#pragma unroll
+        for (int j = 0; j < kIt; j++) {   // every load first, then the conversions and stores
+            const int i = tid + j * kEncThreads, y = i / kP0, x = i % kP0, gy = ly0 + y, gx = lx0 + x;
+            const bool in = i < kR0y * kP0 && x < kR0x && gy >= 0 && gy < a.h && gx >= 0 && gx < a.w;
+            const size_t o = in ? (size_t)gy * a.w + gx : 0;
+            vx[j] = 0u;
+            va[j] = vc[j] = 128.0f;   // (v - 128) / 64 = 0 outside the level
+            if (in) {
+                if (a.xp) vx[j] = __ldg(a.xp + (size_t)bz * a.h * a.w + o);
+                else {
+                    va[j] = __ldg(la + o);
+                    vc[j] = __ldg(lc + o);
+                }
             }
-            luma[i] = v;
+        }
+#pragma unroll
+        for (int j = 0; j < kIt; j++) {
+            const int i = tid + j * kEncThreads;
+            if (i < kR0y * kP0)
+                luma[i] = a.xp ? vx[j]
+                               : packBf2(__fmul_rn(__fsub_rn(va[j], 128.0f), 1.0f / 64.0f),
+                                         __fmul_rn(__fsub_rn(vc[j], 128.0f), 1.0f / 64.0f));
         }
     }
     tcFenceBefore();
@@ -336,22 +361,29 @@ __global__ void __launch_bounds__(kHeadThreads) k_sn_head(const SnFusedArgs a) {
     }
     {
         const bf16* __restrict__ wg = reinterpret_cast<const bf16*>(a.wb);
-        stageW32<32>(wg + kW[3], 32, reinterpret_cast<uint4*>(sm + kHOffW4), tid, kHeadThreads);
-        stageW32<32>(wg + kW[4], 32, reinterpret_cast<uint4*>(sm + kHOffW5), tid, kHeadThreads);
-        stageW32<16>(wg + kW[5], kSnOut, reinterpret_cast<uint4*>(sm + kHOffW6), tid, kHeadThreads);
-        if (tid < 64) bias[tid] = a.p[(tid < 32 ? kB[3] : kB[4]) + (tid & 31)];
-        else if (tid < 64 + kSnOut) bias[tid] = a.p[kB[5] + tid - 64];
+        const float bv = tid < 64 ? a.p[(tid < 32 ? kB[3] : kB[4]) + (tid & 31)] : tid < 64 + kSnOut ? a.p[kB[5] + tid - 64] : 0.0f;
+        stageW32<32, kHeadThreads>(wg + kW[3], 32, reinterpret_cast<uint4*>(sm + kHOffW4), tid);
+        stageW32<32, kHeadThreads>(wg + kW[4], 32, reinterpret_cast<uint4*>(sm + kHOffW5), tid);
+        stageW32<16, kHeadThreads>(wg + kW[5], kSnOut, reinterpret_cast<uint4*>(sm + kHOffW6), tid);
+        if (tid < 64 + kSnOut) bias[tid] = bv;
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
     // layer 3's cells around the tile
     {
         const uint4* __restrict__ y3 = reinterpret_cast<const uint4*>(a.y3);
-        for (int i = tid; i < (kHTY + 6) * kHP * 4; i += kHeadThreads) {
-            const int c8 = i & 3, pix = i >> 2, y = pix / kHP, x = pix % kHP;
+        constexpr int kN = (kHTY + 6) * kHP * 4, kIt = (kN + kHeadThreads - 1) / kHeadThreads;
+        uint4 v[kIt];
+#pragma unroll
+        for (int j = 0; j < kIt; j++) {   // every load first, then the stores
+            const int i = tid + j * kHeadThreads, c8 = i & 3, pix = i >> 2, y = pix / kHP, x = pix % kHP;
             const int gy = cy0 - 3 + y, gx = cx0 - 3 + x;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (gy >= 0 && gy < a.h3 && gx >= 0 && gx < a.w3) v = y3[(((size_t)bz * a.h3 + gy) * a.w3 + gx) * 4 + c8];
-            pin[c8 * kPin + pix] = v;
+            v[j] = make_uint4(0, 0, 0, 0);
+            if (i < kN && gy >= 0 && gy < a.h3 && gx >= 0 && gx < a.w3) v[j] = y3[(((size_t)bz * a.h3 + gy) * a.w3 + gx) * 4 + c8];
+        }
+#pragma unroll
+        for (int j = 0; j < kIt; j++) {
+            const int i = tid + j * kHeadThreads;
+            if (i < kN) pin[(i & 3) * kPin + (i >> 2)] = v[j];
         }
     }
     tcFenceBefore();
