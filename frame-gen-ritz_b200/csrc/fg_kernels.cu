@@ -888,6 +888,58 @@ __device__ __forceinline__ float2 tapPair(const float* __restrict__ ya, const fl
     return __ffma2_rn(h1, wy1, pmul(h0, wy0));
 }
 
+// the horizontal stage of one tap row of both frames: a at row ra (columns ax0, ax1), c at row rc (cx0, cx1), rows
+// clamped; returns 32 x the row's value of each (tapPair's h0 / h1)
+__device__ __forceinline__ float2 tapRowPair(const float* __restrict__ ya, const float* __restrict__ yc, int w, int h,
+                                             int ra, int rc, int ax0, int ax1, int cx0, int cx1, float2 wx0, float2 wx1) {
+    const float* qa = ya + clampi(ra, 0, h - 1) * w;
+    const float* qc = yc + clampi(rc, 0, h - 1) * w;
+    return __ffma2_rn(make_float2(__ldg(qa + ax1), __ldg(qc + cx1)), wx1, pmul(make_float2(__ldg(qa + ax0), __ldg(qc + cx0)), wx0));
+}
+
+// Candidates 1..5 (the vector of the pixel's own block or of a 4-neighbour) are constant over a block: the thread walks
+// down kPfK consecutive region rows of its column with one set of taps and weights per block, each row's lower tap row
+// being the next row's upper one (the rows are the same for every lane, so the branches are uniform). Same taps,
+// weights and operation order as tapPair.
+__device__ __forceinline__ void pfBlockCandidate(const PixfieldParams& p, int k, int qx, int Y0, int ey0, int ex, int bx0,
+                                                 int by0, const int2 (*bR)[kPfBX], int (*plane)[kPfE + 1]) {
+    const int dxk = k == 4 ? -1 : (k == 5 ? 1 : 0), dyk = k == 2 ? -1 : (k == 3 ? 1 : 0);
+    const int bx = clampi((qx >> 3) + dxk, 0, p.bw - 1) - bx0;
+    int ax0 = 0, ax1 = 0, cx0 = 0, cx1 = 0, dya = 0, dyc = 0, by = -1, qyPrev = -1, E = 0;
+    float2 wx0 = make_float2(0.0f, 0.0f), wx1 = wx0, wy0 = wx0, wy1 = wx0, top = wx0, bot = wx0;
+#pragma unroll
+    for (int j = 0; j < kPfK; j++) {
+        const int ey = ey0 * kPfK + j;
+        const int qy = clampi(Y0 - kPfAp + ey, 0, p.h - 1);
+        if (qy != qyPrev) {   // a clamped row repeats the previous one
+            const int b = clampi((qy >> 3) + dyk, 0, p.bh - 1) - by0;
+            if (b != by) {    // a new block row: this lane's vector, taps and weights; both tap rows
+                by = b;
+                const int2 R = bR[b][bx];
+                const int ia = qx + ((-R.x) >> 5), ic = qx + (R.x >> 5);
+                ax0 = clampi(ia, 0, p.w - 1);
+                ax1 = clampi(ia + 1, 0, p.w - 1);
+                cx0 = clampi(ic, 0, p.w - 1);
+                cx1 = clampi(ic + 1, 0, p.w - 1);
+                dya = (-R.y) >> 5;
+                dyc = R.y >> 5;
+                wx1 = make_float2(i2f((-R.x) & 31), i2f(R.x & 31));
+                wy1 = make_float2(i2f((-R.y) & 31), i2f(R.y & 31));
+                wx0 = padd(make_float2(32.0f, 32.0f), make_float2(-wx1.x, -wx1.y));
+                wy0 = padd(make_float2(32.0f, 32.0f), make_float2(-wy1.x, -wy1.y));
+                top = tapRowPair(p.ya, p.yc, p.w, p.h, qy + dya, qy + dyc, ax0, ax1, cx0, cx1, wx0, wx1);
+            } else {
+                top = bot;    // qy = qyPrev + 1 in the same block row
+            }
+            bot = tapRowPair(p.ya, p.yc, p.w, p.h, qy + dya + 1, qy + dyc + 1, ax0, ax1, cx0, cx1, wx0, wx1);
+            const float2 t = __ffma2_rn(bot, wy1, pmul(top, wy0));
+            E = __float_as_int(__fmaf_rn(fabsf(t.x - t.y), 16.0f, 12582912.0f)) - 0x4B400000;   // E * 2^14
+            qyPrev = qy;
+        }
+        plane[ey][ex] = E;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     pdlEnter();
     // rows padded by one word: the horizontal sums below read down the rows of a column group, one row per lane
@@ -948,31 +1000,23 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     }
     for (int k = 0; k < kPfNC; k++) {
         // 1. candidate k's error at this thread's region pixels (the zero candidate's is plane0 already)
-        if (k < kPfNC - 1)
+        if (k == 0) {   // the upsampled field: a vector per pixel
 #pragma unroll
-        for (int j = 0; j < kPfK; j++) {
-            const int ey = ey0 + 4 * j;
-            const int qy = clampi(Y0 - kPfAp + ey, 0, p.h - 1);
-            int2 R;
-            if (k == 0) {
+            for (int j = 0; j < kPfK; j++) {
+                const int ey = ey0 + 4 * j;
+                const int qy = clampi(Y0 - kPfAp + ey, 0, p.h - 1);
                 const float4 ry = rowc[ey];
                 const int r0 = __float_as_int(ry.x), r1 = __float_as_int(ry.y);
                 const float2 h0 = padd(pmul(bv[r0][cx0], make_float2(ca0, ca0)), pmul(bv[r0][cx1], make_float2(ca1, ca1)));
                 const float2 h1 = padd(pmul(bv[r1][cx0], make_float2(ca0, ca0)), pmul(bv[r1][cx1], make_float2(ca1, ca1)));
                 const float2 r = rne32bits(padd(pmul(h0, make_float2(ry.z, ry.z)), pmul(h1, make_float2(ry.w, ry.w))));
-                R = make_int2(__float_as_int(r.x) - 0x4B400000, __float_as_int(r.y) - 0x4B400000);
-            } else if (k == kPfNC - 1) {
-                R = make_int2(0, 0);
-            } else {
-                const int byq = (qy >> 3) - by0;
-                const int dx = k == 4 ? -1 : (k == 5 ? 1 : 0), dy = k == 2 ? -1 : (k == 3 ? 1 : 0);
-                const int bx = clampi((qx >> 3) + dx, 0, p.bw - 1) - bx0, by = clampi((qy >> 3) + dy, 0, p.bh - 1) - by0;
-                R = bR[by][bx];
-                (void)byq;
+                const int2 R = make_int2(__float_as_int(r.x) - 0x4B400000, __float_as_int(r.y) - 0x4B400000);
+                const int qy32 = 32 * qy;
+                const float2 t = tapPair(p.ya, p.yc, p.w, p.h, qx32 - R.x, qy32 - R.y, qx32 + R.x, qy32 + R.y);
+                plane[ey][ex] = __float_as_int(__fmaf_rn(fabsf(t.x - t.y), 16.0f, 12582912.0f)) - 0x4B400000;   // E * 2^14
             }
-            const int qy32 = 32 * qy;
-            const float2 t = tapPair(p.ya, p.yc, p.w, p.h, qx32 - R.x, qy32 - R.y, qx32 + R.x, qy32 + R.y);
-            plane[ey][ex] = __float_as_int(__fmaf_rn(fabsf(t.x - t.y), 16.0f, 12582912.0f)) - 0x4B400000;   // E * 2^14
+        } else if (k < kPfNC - 1) {
+            pfBlockCandidate(p, k, qx, Y0, ey0, ex, bx0, by0, bR, plane);
         }
         __syncthreads();
         // 2. horizontal 5-sums: one region row, 8 output columns per thread (a running window); the lanes of a warp
@@ -1147,15 +1191,22 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
         const int m = max(max(abs(ca[0] - cc[0]), abs(ca[1] - cc[1])), abs(ca[2] - cc[2]));
         e[ey * kSyES + ex] = (uint8_t)m;
     }
+    const int lx = ex - kSyAp, x = X0 + lx;
+    const bool colOk = (unsigned)lx < (unsigned)kSyT && x < p.W;   // this thread's output column
     __syncthreads();
     // 3. horizontal 7-sums: one region row and 8 output columns per thread, a running window
     syRowSums(e, hsum, tid);
     __syncthreads();
-    // 4. this thread's output pixels, kSyK consecutive rows of one column: vertical 7-sum (a running window), trust,
-    //    blend, store
+    // 4. this thread's output pixels: vertical 7-sum (a running window), trust, blend, store
     unsigned int myCnt = 0;
-    const int lx = ex - kSyAp, x = X0 + lx;
-    if ((unsigned)lx < (unsigned)kSyT && x < p.W) {
+    // Weights that are multiples of 1/256 (t = k/256: 1/4, 3/4, ...) make every step of the blend exact (8-bit x 8-bit
+    // products, sums below 2^17), so fl(fl(wA a) + fl(wC c)) + 0.5 floored is (WA a + WC c + 128) >> 8 with WA = 256 wA,
+    // WC = 256 wC: two channels per 32-bit multiply-add (16-bit lanes, no carry while WA + WC <= 256)
+    const float wa256 = __fmul_rn(p.wA, 256.0f), wc256 = __fmul_rn(p.wC, 256.0f);
+    const bool dyad = !p.mid && wa256 == truncf(wa256) && wc256 == truncf(wc256) && wa256 >= 0.0f && wc256 >= 0.0f &&
+                      __fadd_rn(wa256, wc256) <= 256.0f;
+    const uint32_t WA = dyad ? (uint32_t)wa256 : 0u, WC = dyad ? (uint32_t)wc256 : 0u;
+    if (colOk) {
         const unsigned short* q = hsum + syOutRow(ey0, 0) * kSyHS + lx;
         int S = q[0] + q[kSyHS] + q[2 * kSyHS] + q[3 * kSyHS] + q[4 * kSyHS] + q[5 * kSyHS];
 #pragma unroll
@@ -1170,6 +1221,11 @@ __device__ __forceinline__ void synthTileCore(const SynthParams& p, int bx, int 
                 if (p.mid) {
                     // floor(0.5 (a + c) + 0.5) per byte: (a | c) - ((a ^ c) >> 1), no borrow between bytes
                     o = (wak | wck) - (((wak ^ wck) >> 1) & 0x7F7F7F7Fu);
+                } else if (dyad) {
+                    const uint32_t M = 0x00FF00FFu;
+                    const uint32_t rb = (wak & M) * WA + ((wck & M) * WC + 0x00800080u);
+                    const uint32_t g = ((wak >> 8) & M) * WA + (((wck >> 8) & M) * WC + 0x00800080u);
+                    o = ((rb >> 8) & M) | (g & 0x0000FF00u);
                 } else {
                     // fl32(fl32((1 - t) a) + fl32(t c)) + 0.5, floored (never above 255.5 here, so no clamp is needed): the
                     // products come from the tables, the adds are paired (adds alone cannot be fused), the floor is a
@@ -1219,13 +1275,13 @@ __device__ __forceinline__ void synthTile(const SynthParams& p, int bx, int by) 
     });
 }
 
-__global__ void __launch_bounds__(kSyThreads) k_synth(const SynthParams p) {
+__global__ void __launch_bounds__(kSyThreads, 3) k_synth(const SynthParams p) {
     pdlEnter();
     synthTile(p, blockIdx.x, blockIdx.y);
 }
 
 // the same with CrosshairV2's warp-tap rejection (p.uiA / p.uiC); a separate kernel so the plain one is unchanged
-__global__ void __launch_bounds__(kSyThreads) k_synth_ui(const SynthParams p) {
+__global__ void __launch_bounds__(kSyThreads, 3) k_synth_ui(const SynthParams p) {
     pdlEnter();
     synthTile<true>(p, blockIdx.x, blockIdx.y);
 }
