@@ -274,8 +274,10 @@ __device__ __forceinline__ int mismatch(const FmtConst& f, const float wa[3], co
 }
 
 // resolve.comp: m = 0.5 (a + c) at t = 0.5, else (1 - t) a + t c; out = m (1 - u) + n u
-__device__ __forceinline__ float blendF(float a, float c, float n, float u, float iu, const SynthParams& p) {
-    const float m = p.mid ? __fmul_rn(0.5f, __fadd_rn(a, c)) : __fadd_rn(__fmul_rn(p.wA, a), __fmul_rn(p.wC, c));
+__device__ __forceinline__ float mixF(float a, float c, const SynthParams& p) {
+    return p.mid ? __fmul_rn(0.5f, __fadd_rn(a, c)) : __fadd_rn(__fmul_rn(p.wA, a), __fmul_rn(p.wC, c));
+}
+__device__ __forceinline__ float blendM(float m, float n, float u, float iu) {
     return __fadd_rn(__fmul_rn(m, iu), __fmul_rn(n, u));
 }
 
@@ -334,7 +336,14 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
     unsigned short* hsum;
     const SyCoef cx = syFieldStage(p, X0, Y0, tid, ex, ey0, rowc, gReg, sm, hrow, e, hsum);
     const float kA = p.mid ? 1.0f : p.ka, kC = p.mid ? 1.0f : p.kc;
-    // 2. the mismatch over the region
+    constexpr bool kYuv = F == kFmtNv12 || F == kFmtP010;
+    // the blend inputs m of the output pixels, kept from stage 2 for stage 4 (the warps are computed once): per channel
+    // planes of kSyTH x kSyE floats (YUV: the luma plane, then the block-centre chroma (Cb, Cr) of the even-even
+    // pixels, (kSyTH / 2) x (kSyE / 2))
+    float* mix = reinterpret_cast<float*>(hsum + kSyEH * kSyHS);
+    float2* mixc = reinterpret_cast<float2*>(mix + kSyTH * kSyE);
+    const int lx = ex - kSyAp, x = X0 + lx;
+    // 2. the mismatch over the region, and the blend inputs of the output pixels
     for (int k = 0; k < kSyK; k++) {
         const int ey = ey0 + (kSyThreads / kSyE) * k;
         const SyCoef cy = rowc[ey];
@@ -343,14 +352,31 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
         warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
         warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
         e[ey * kSyES + ex] = (uint8_t)mismatch<F>(p.f, wa, wc);
+        const int ly = ey - kSyAp;
+        if ((unsigned)ly < (unsigned)kSyTH) {   // warp-uniform
+            if (kYuv) {
+                mix[ly * kSyE + ex] = mixF(wa[0], wc[0], p);
+                if ((((lx | ly) & 1) == 0) && (unsigned)lx < (unsigned)kSyT && x < p.W && Y0 + ly < p.H) {
+                    // the chroma of this 2x2 block, warped from its centre with this pixel's half-vector
+                    const float bx = __fadd_rn(cx.pos, 0.5f), by = __fadd_rn(cy.pos, 0.5f);
+                    const float2 ca = warpChroma<F>(p.ac, p.cpitch, p.W, p.H, rne32(__fsub_rn(bx, __fmul_rn(kA, h.x))),
+                                                    rne32(__fsub_rn(by, __fmul_rn(kA, h.y))));
+                    const float2 cc = warpChroma<F>(p.cc, p.cpitch, p.W, p.H, rne32(__fadd_rn(bx, __fmul_rn(kC, h.x))),
+                                                    rne32(__fadd_rn(by, __fmul_rn(kC, h.y))));
+                    mixc[(ly >> 1) * (kSyE / 2) + (lx >> 1)] = make_float2(mixF(ca.x, cc.x, p), mixF(ca.y, cc.y, p));
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; c++) mix[(c * kSyTH + ly) * kSyE + ex] = mixF(wa[c], wc[c], p);
+            }
+        }
     }
     __syncthreads();
     // 3. horizontal 7-sums (as k_synth)
     syRowSums(e, hsum, tid);
     __syncthreads();
-    // 4. output pixels: vertical 7-sum, trust, the warps again, blend, store
+    // 4. output pixels: vertical 7-sum, trust, blend, store
     unsigned int myCnt = 0;
-    const int lx = ex - kSyAp, x = X0 + lx;
     if ((unsigned)lx < (unsigned)kSyT && x < p.W) {
         const uint8_t* nearF = p.nearC ? p.c : p.a;
 #pragma unroll
@@ -363,18 +389,13 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
             const float u = clampF(__fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan), 0.0f, 1.0f);
             myCnt += u > 0.5f;
             const float iu = __fsub_rn(1.0f, u);
-            const SyCoef cy = rowc[ey];
-            const float2 h = syHalfVec(cy, hrow, ex);
-            float wa[3], wc[3];
-            warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
-            warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
             if (F == kFmtRgb10) {
                 const uint32_t nw = ldw(nearF, p.pitch, x, y);
                 uint32_t ow = nw & 0xC0000000u;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const float nl = __fmul_rn(i2f(rgb10(p.f, nw, c)), p.f.k10);
-                    const float v = clampF(blendF(wa[c], wc[c], nl, u, iu, p), 0.0f, 255.0f);
+                    const float v = clampF(blendM(mix[(c * kSyTH + ly) * kSyE + ex], nl, u, iu), 0.0f, 255.0f);
                     const int code = clampi((int)floorf(__fadd_rn(__fmul_rn(v, p.f.k10i), 0.5f)), 0, 1023);
                     ow |= (uint32_t)code << (p.f.rHigh ? 20 - 10 * c : 10 * c);
                 }
@@ -382,26 +403,22 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
             } else if (F == kFmtF16) {
                 const uint2 nq = __ldg(reinterpret_cast<const uint2*>(nearF + (size_t)y * p.pitch) + x);
                 const float n0 = h2f(nq.x & 0xFFFFu), n1 = h2f(nq.x >> 16), n2 = h2f(nq.y & 0xFFFFu);
-                const uint32_t o0 = __half_as_ushort(__float2half_rn(blendF(wa[0], wc[0], n0, u, iu, p)));
-                const uint32_t o1 = __half_as_ushort(__float2half_rn(blendF(wa[1], wc[1], n1, u, iu, p)));
-                const uint32_t o2 = __half_as_ushort(__float2half_rn(blendF(wa[2], wc[2], n2, u, iu, p)));
+                const uint32_t o0 = __half_as_ushort(__float2half_rn(blendM(mix[(0 * kSyTH + ly) * kSyE + ex], n0, u, iu)));
+                const uint32_t o1 = __half_as_ushort(__float2half_rn(blendM(mix[(1 * kSyTH + ly) * kSyE + ex], n1, u, iu)));
+                const uint32_t o2 = __half_as_ushort(__float2half_rn(blendM(mix[(2 * kSyTH + ly) * kSyE + ex], n2, u, iu)));
                 sink.half4(k, x, y, make_uint2(o0 | (o1 << 16), o2 | (nq.y & 0xFFFF0000u)));
             } else {
                 constexpr float ql = F == kFmtP010 ? 4.0f : 1.0f;   // 1 / YU_QL
                 constexpr int codes = F == kFmtP010 ? 1023 : 255;
                 float ny[3];
                 texel<F>(p.f, nearF, p.pitch, x, y, ny);
-                const float v = blendF(wa[0], wc[0], ny[0], u, iu, p);
+                const float v = blendM(mix[ly * kSyE + ex], ny[0], u, iu);
                 sink.luma(k, x, y, clampi((int)floorf(__fadd_rn(__fmul_rn(v, ql), 0.5f)), 0, codes));
-                if (((x | y) & 1) == 0) {   // the chroma of this 2x2 block, warped from its centre
-                    const float bx = __fadd_rn(cx.pos, 0.5f), by = __fadd_rn(cy.pos, 0.5f);
-                    const float2 ca = warpChroma<F>(p.ac, p.cpitch, p.W, p.H, rne32(__fsub_rn(bx, __fmul_rn(kA, h.x))),
-                                                    rne32(__fsub_rn(by, __fmul_rn(kA, h.y))));
-                    const float2 cc = warpChroma<F>(p.cc, p.cpitch, p.W, p.H, rne32(__fadd_rn(bx, __fmul_rn(kC, h.x))),
-                                                    rne32(__fadd_rn(by, __fmul_rn(kC, h.y))));
+                if (((x | y) & 1) == 0) {   // the chroma of this 2x2 block (warped in stage 2)
+                    const float2 m = mixc[(ly >> 1) * (kSyE / 2) + (lx >> 1)];
                     const float2 nc = ctexel<F>(p.nearC ? p.cc : p.ac, p.cpitch, x >> 1, y >> 1);
-                    const int cb = clampi((int)floorf(__fadd_rn(__fmul_rn(blendF(ca.x, cc.x, nc.x, u, iu, p), ql), 0.5f)), 0, codes);
-                    const int cr = clampi((int)floorf(__fadd_rn(__fmul_rn(blendF(ca.y, cc.y, nc.y, u, iu, p), ql), 0.5f)), 0, codes);
+                    const int cb = clampi((int)floorf(__fadd_rn(__fmul_rn(blendM(m.x, nc.x, u, iu), ql), 0.5f)), 0, codes);
+                    const int cr = clampi((int)floorf(__fadd_rn(__fmul_rn(blendM(m.y, nc.y, u, iu), ql), 0.5f)), 0, codes);
                     sink.chroma(k, x, y, cb, cr);
                 }
             }
@@ -626,8 +643,16 @@ __global__ void __launch_bounds__(256) k_fallback_fmt(const FallbackParams p) {
 }
 
 // ============================================================================================== launchers
+// the dynamic shared memory of a format synthesis: synthSmemBytes + the blend inputs of the output pixels
+static size_t fmtSynthSmem(int format, int fs) {
+    const size_t mix = format == kFmtNv12 || format == kFmtP010
+                           ? (size_t)kSyTH * kSyE * 4 + (size_t)((kSyTH + 1) / 2) * (kSyE / 2) * 8
+                           : (size_t)3 * kSyTH * kSyE * 4;
+    return synthSmemBytes(fs) + mix;
+}
+
 cudaError_t prepareFormatKernels() {
-    const int smem = (int)synthSmemBytes(1);
+    const int smem = (int)fmtSynthSmem(kFmtRgb10, 1);   // the largest
     cudaError_t e = cudaFuncSetAttribute(k_synth_fmt<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -652,7 +677,7 @@ cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s) {
 
 cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
     const dim3 grid(divUp(p.W, kSyT), divUp(p.H, kSyTH));
-    const size_t smem = synthSmemBytes(p.fs);
+    const size_t smem = fmtSynthSmem(p.f.format, p.fs);
     switch (p.f.format) {
         case kFmtRgb10: return launchPdl(k_synth_fmt<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
         case kFmtF16: return launchPdl(k_synth_fmt<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);
@@ -667,7 +692,7 @@ cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s) {
 }
 
 cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s) {
-    const size_t smem = synthSmemBytes(bp.base.fs);
+    const size_t smem = fmtSynthSmem(bp.base.f.format, bp.base.fs);
     const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
     BlurParams p = bp;
     p.fix = fix;
