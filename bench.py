@@ -236,7 +236,8 @@ def batch_arm(a, b3):
                         "P010, 2x / 3x / 4x; one Batch record per step, graph-replayed",
             "generated_frames": len(outs), "generated_megapixels": round(px / 1e6, 1),
             "ms_per_batch_per_synthesis_1_stream": round(base, 3), "ms_per_batch_tuned": round(tuned, 3),
-            "tuned_shape": {"ctas_per_sm": shape[0], "order": shape[1], "streams": shape[2], "index": best},
+            "tuned_shape": {"ctas_per_sm": shape[0], "order": shape[1], "streams": shape[2],
+                            "merge_estimates": shape[3], "index": best},
             "megapixels_per_s_tuned": round(px / 1e6 / (tuned * 1e-3), 1), "reps": a.batch_reps}
 
 

@@ -17,6 +17,21 @@ __device__ __forceinline__ void pdlEnter() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// the item of this CTA in a merged launch and the CTA's coordinates in the item's own grid
+template <class P>
+__device__ __forceinline__ int mergedItem(const Merged<P>& m, int& bx, int& by) {
+    const int b = (int)blockIdx.x;
+    int lo = 0, hi = m.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (m.first[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    const int l = b - m.first[lo], gx = m.gx[lo];
+    bx = l % gx;
+    by = l / gx;
+    return lo;
+}
+
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 // luma texel with clamp-to-edge (== cv2 BORDER_REPLICATE and the replicate pad_to_block, interp.py:68-70)

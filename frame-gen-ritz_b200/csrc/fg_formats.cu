@@ -150,10 +150,9 @@ __device__ __forceinline__ int rneDiv(int num, int n) {
 
 // interp.flow + pyramid for the other formats: one CTA = a 32x32 level-0 tile and its tower (as k_luma_pyr)
 template <int F>
-__global__ void __launch_bounds__(256) k_luma_fmt(const LumaPyrParams p) {
-    pdlEnter();
+__device__ __forceinline__ void lumaFmtCta(const LumaPyrParams& p, int bx, int by) {
     __shared__ float sl[2][kTowerFloats];
-    const int tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 32;
+    const int tx0 = bx * 32, ty0 = by * 32;
     const int fw = p.lw[0], fh = p.lh[0], fs = p.fs;
     for (int i = threadIdx.x; i < 1024; i += 256) {
         const int x = tx0 + (i & 31), y = ty0 + (i >> 5);
@@ -181,6 +180,18 @@ __global__ void __launch_bounds__(256) k_luma_fmt(const LumaPyrParams p) {
     }
     __syncthreads();
     lumaTower<true>(p, sl, tx0, ty0);
+}
+template <int F>
+__global__ void __launch_bounds__(256) k_luma_fmt(const LumaPyrParams p) {
+    pdlEnter();
+    lumaFmtCta<F>(p, blockIdx.x, blockIdx.y);
+}
+template <int F>
+__global__ void __launch_bounds__(256) k_luma_fmt_m(const __grid_constant__ Merged<LumaPyrParams> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    lumaFmtCta<F>(m.item[i], bx, by);
 }
 
 // ============================================================================================== warps
@@ -214,9 +225,56 @@ __device__ __forceinline__ float bil(const Taps& t, float p00, float p01, float 
     return __fadd_rn(r, __fmul_rn(p11, t.w11));
 }
 
+// Integer taps for samples of at most 10 bits (Rgb10 codes, Nv12 bytes). With 1/2^B fractions every product of a
+// sample and a weight and every partial sum of mkTaps / bil is an exact multiple of 2^-2B below 2^(10 + 2B - 2B), so
+// the float bilinear equals S 2^-2B for the integer S = sum p_ij wx_j wy_i (wx, wy in 0..2^B), in any order. The
+// position is clamped to [0, 2^B (n - 1)] and the left tap is min(X >> B, n - 2) with the right weight X - 2^B ix: at
+// the right edge the taps (n - 2, n - 1) with weights (0, 2^B) give mkTaps' clamped (n - 1, n - 1) value, below zero
+// the taps (0, 1) with weights (2^B, 0) its (0, 0) value (frames are at least 16 x 16, so n >= 2).
+struct ITaps {
+    int x, y;                 // the top-left tap
+    uint32_t w0, w1;          // 16-bit lanes: (w00, w01) and (w10, w11)
+};
+template <int B>
+__device__ __forceinline__ ITaps mkITaps(int X, int Y, int w, int h) {
+    constexpr int one = 1 << B;
+    X = clampi(X, 0, one * (w - 1));
+    Y = clampi(Y, 0, one * (h - 1));
+    ITaps t;
+    t.x = min(X >> B, w - 2);
+    t.y = min(Y >> B, h - 2);
+    const uint32_t fx = (uint32_t)(X - one * t.x), fy = (uint32_t)(Y - one * t.y);
+    const uint32_t wx = ((uint32_t)one - fx) | (fx << 16);   // lanes <= 2^B: the products below stay under 2^16
+    t.w0 = wx * ((uint32_t)one - fy);
+    t.w1 = wx * fy;
+    return t;
+}
+
 // the chroma (Cb, Cr) levels warped to the point whose 1/32-px coordinates are (X, Y)
 template <int F>
 __device__ __forceinline__ float2 warpChroma(const uint8_t* cbase, size_t cpitch, int W, int H, int X, int Y) {
+    if (F == kFmtNv12) {   // byte pairs (Cb, Cr): gathered as (Cb00, Cb01, Cr00, Cr01), two dp2a per channel, exact
+        const ITaps t = mkITaps<6>(X - 16, Y - 16, (W + 1) >> 1, (H + 1) >> 1);
+        const unsigned short* q0 = reinterpret_cast<const unsigned short*>(cbase + (size_t)t.y * cpitch) + t.x;
+        const unsigned short* q1 = reinterpret_cast<const unsigned short*>(cbase + (size_t)(t.y + 1) * cpitch) + t.x;
+        const uint32_t c0 = __byte_perm((uint32_t)__ldg(q0), (uint32_t)__ldg(q0 + 1), 0x5140);
+        const uint32_t c1 = __byte_perm((uint32_t)__ldg(q1), (uint32_t)__ldg(q1 + 1), 0x5140);
+        const uint32_t cb = __dp2a_lo(t.w1, c1, __dp2a_lo(t.w0, c0, 0u)), cr = __dp2a_hi(t.w1, c1, __dp2a_hi(t.w0, c0, 0u));
+        return make_float2(__fmul_rn(i2f((int)cb), 0x1p-12f), __fmul_rn(i2f((int)cr), 0x1p-12f));
+    }
+    if (F == kFmtP010) {   // 10-bit codes in the high bits of 16-bit samples: integer taps when the low 6 bits are zero
+        const ITaps t = mkITaps<6>(X - 16, Y - 16, (W + 1) >> 1, (H + 1) >> 1);
+        const uint32_t* q0 = reinterpret_cast<const uint32_t*>(cbase + (size_t)t.y * cpitch) + t.x;
+        const uint32_t* q1 = reinterpret_cast<const uint32_t*>(cbase + (size_t)(t.y + 1) * cpitch) + t.x;
+        const uint32_t p00 = __ldg(q0), p01 = __ldg(q0 + 1), p10 = __ldg(q1), p11 = __ldg(q1 + 1);
+        if (((p00 | p01 | p10 | p11) & 0x003F003Fu) == 0u) {   // codes x 64: every float step exact (ITaps)
+            const uint32_t w00 = t.w0 & 0xFFFFu, w01 = t.w0 >> 16, w10 = t.w1 & 0xFFFFu, w11 = t.w1 >> 16;
+            const uint32_t cb = ((p00 >> 6) & 1023u) * w00 + ((p01 >> 6) & 1023u) * w01 + ((p10 >> 6) & 1023u) * w10 +
+                                ((p11 >> 6) & 1023u) * w11;
+            const uint32_t cr = (p00 >> 22) * w00 + (p01 >> 22) * w01 + (p10 >> 22) * w10 + (p11 >> 22) * w11;
+            return make_float2(__fmul_rn(i2f((int)cb), 0x1p-14f), __fmul_rn(i2f((int)cr), 0x1p-14f));
+        }
+    }
     const Taps t = mkTaps<6>(X - 16, Y - 16, (W + 1) >> 1, (H + 1) >> 1);
     const float2 c00 = ctexel<F>(cbase, cpitch, t.x0, t.y0), c01 = ctexel<F>(cbase, cpitch, t.x1, t.y0);
     const float2 c10 = ctexel<F>(cbase, cpitch, t.x0, t.y1), c11 = ctexel<F>(cbase, cpitch, t.x1, t.y1);
@@ -228,6 +286,48 @@ template <int F>
 __device__ __forceinline__ void warp(const SynthParams& p, const uint8_t* base, const uint8_t* cbase, float px, float py,
                                      float out[3]) {
     const int X = rne32(px), Y = rne32(py);
+    if (F == kFmtRgb10) {   // 10-bit codes: integer taps, exact (ITaps)
+        const ITaps t = mkITaps<5>(X, Y, p.W, p.H);
+        const uint32_t* q0 = reinterpret_cast<const uint32_t*>(base + (size_t)t.y * p.pitch) + t.x;
+        const uint32_t* q1 = reinterpret_cast<const uint32_t*>(base + (size_t)(t.y + 1) * p.pitch) + t.x;
+        const uint32_t p00 = __ldg(q0), p01 = __ldg(q0 + 1), p10 = __ldg(q1), p11 = __ldg(q1 + 1);
+        const uint32_t w00 = t.w0 & 0xFFFFu, w01 = t.w0 >> 16, w10 = t.w1 & 0xFFFFu, w11 = t.w1 >> 16;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int sh = p.f.rHigh ? 20 - 10 * k : 10 * k;
+            const uint32_t S = ((p00 >> sh) & 1023u) * w00 + ((p01 >> sh) & 1023u) * w01 + ((p10 >> sh) & 1023u) * w10 +
+                               ((p11 >> sh) & 1023u) * w11;
+            out[k] = __fmul_rn(__fmul_rn(i2f((int)S), 0x1p-10f), p.f.k10);
+        }
+        return;
+    }
+    if (F == kFmtNv12) {    // 8-bit luma: integer taps, two dp2a (as the 8-bit RGBA sampler), exact
+        const ITaps t = mkITaps<5>(X, Y, p.W, p.H);
+        const uint8_t* q0 = base + (size_t)t.y * p.pitch + t.x;
+        const uint8_t* q1 = q0 + p.pitch;
+        const uint32_t r0 = (uint32_t)__ldg(q0) | ((uint32_t)__ldg(q0 + 1) << 8);
+        const uint32_t r1 = (uint32_t)__ldg(q1) | ((uint32_t)__ldg(q1 + 1) << 8);
+        out[0] = __fmul_rn(i2f((int)__dp2a_lo(t.w1, r1, __dp2a_lo(t.w0, r0, 0u))), 0x1p-10f);
+        const float2 c = warpChroma<F>(cbase, p.cpitch, p.W, p.H, X, Y);
+        out[1] = c.x;
+        out[2] = c.y;
+        return;
+    }
+    if (F == kFmtP010) {    // integer taps when the four samples' low 6 bits are zero (then every float step is exact)
+        const ITaps t = mkITaps<5>(X, Y, p.W, p.H);
+        const unsigned short* q0 = reinterpret_cast<const unsigned short*>(base + (size_t)t.y * p.pitch) + t.x;
+        const unsigned short* q1 = reinterpret_cast<const unsigned short*>(base + (size_t)(t.y + 1) * p.pitch) + t.x;
+        const uint32_t s00 = __ldg(q0), s01 = __ldg(q0 + 1), s10 = __ldg(q1), s11 = __ldg(q1 + 1);
+        if (((s00 | s01 | s10 | s11) & 63u) == 0u) {
+            const uint32_t S = (s00 >> 6) * (t.w0 & 0xFFFFu) + (s01 >> 6) * (t.w0 >> 16) + (s10 >> 6) * (t.w1 & 0xFFFFu) +
+                               (s11 >> 6) * (t.w1 >> 16);
+            out[0] = __fmul_rn(i2f((int)S), 0x1p-12f);   // codes / 4 = the levels
+            const float2 c = warpChroma<F>(cbase, p.cpitch, p.W, p.H, X, Y);
+            out[1] = c.x;
+            out[2] = c.y;
+            return;
+        }
+    }
     const Taps t = mkTaps<5>(X, Y, p.W, p.H);
     float r00[3], r01[3], r10[3], r11[3];
     texel<F>(p.f, base, p.pitch, t.x0, t.y0, r00);
@@ -385,10 +485,19 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
             if ((unsigned)ly >= (unsigned)kSyTH || y >= p.H) continue;
             const unsigned short* q = hsum + ly * kSyHS + lx;
             const int S = q[0] + q[kSyHS] + q[2 * kSyHS] + q[3 * kSyHS] + q[4 * kSyHS] + q[5 * kSyHS] + q[6 * kSyHS];
-            const float eb = (float)((double)S * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
-            const float u = clampF(__fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan), 0.0f, 1.0f);
+            float u, iu;
+            if (S <= p.sZero) {          // the ramp is exactly 0 (host-derived threshold)
+                u = 0.0f;
+                iu = 1.0f;
+            } else if (S >= p.sOne) {    // exactly 1
+                u = 1.0f;
+                iu = 0.0f;
+            } else {
+                const float eb = (float)((double)S * (1.0 / 49.0));   // cv2.blur: double sum * (1/49), to float
+                u = clampF(__fdiv_rn(__fsub_rn(eb, p.trust0), p.trustSpan), 0.0f, 1.0f);
+                iu = __fsub_rn(1.0f, u);
+            }
             myCnt += u > 0.5f;
-            const float iu = __fsub_rn(1.0f, u);
             if (F == kFmtRgb10) {
                 const uint32_t nw = ldw(nearF, p.pitch, x, y);
                 uint32_t ow = nw & 0xC0000000u;
@@ -453,7 +562,7 @@ struct FmtStore {
 };
 
 template <int F>
-__global__ void __launch_bounds__(kSyThreads) k_synth_fmt(const SynthParams p) {
+__global__ void __launch_bounds__(kSyThreads, 3) k_synth_fmt(const SynthParams p) {
     pdlEnter();
     FmtStore<F> store{p};
     synthFmtTile<F, true>(p, blockIdx.x, blockIdx.y, store);
@@ -671,6 +780,24 @@ cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s) {
         case kFmtF16: return launchPdl(k_luma_fmt<kFmtF16>, grid, dim3(256), 0, s, p);
         case kFmtNv12: return launchPdl(k_luma_fmt<kFmtNv12>, grid, dim3(256), 0, s, p);
         case kFmtP010: return launchPdl(k_luma_fmt<kFmtP010>, grid, dim3(256), 0, s, p);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchLumaFmtMerged(Merged<LumaPyrParams>& m, int format, cudaStream_t s) {
+    if (m.n < 1 || m.n > kMergeMax) return cudaErrorInvalidValue;
+    int total = 0;
+    for (int i = 0; i < m.n; i++) {
+        m.first[i] = total;
+        m.gx[i] = (int)divUp(m.item[i].lw[0], 32);
+        total += m.gx[i] * (int)divUp(m.item[i].lh[0], 32);
+    }
+    m.first[m.n] = total;
+    switch (format) {
+        case kFmtRgb10: return launchPdl(k_luma_fmt_m<kFmtRgb10>, dim3(total), dim3(256), 0, s, m);
+        case kFmtF16: return launchPdl(k_luma_fmt_m<kFmtF16>, dim3(total), dim3(256), 0, s, m);
+        case kFmtNv12: return launchPdl(k_luma_fmt_m<kFmtNv12>, dim3(total), dim3(256), 0, s, m);
+        case kFmtP010: return launchPdl(k_luma_fmt_m<kFmtP010>, dim3(total), dim3(256), 0, s, m);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -8,6 +8,7 @@
 //     numpy's operation order with explicit round-to-nearest intrinsics (no contraction);
 //   - reductions whose rounding depends on order (the scene-cut mean) follow numpy's pairwise tree.
 // The whole library is compiled with -fmad=false as a second guard against contraction.
+#include <algorithm>
 #include <atomic>
 #include <cooperative_groups.h>
 
@@ -20,10 +21,9 @@ namespace fgk {
 // the aligned 16x16 .. 1x1 tiles of levels 1..5 above it: a level-(l+1) pixel only averages the 2x2 level-l pixels
 // below it, so the whole tower stays inside the tile. Mean of the valid pixels: sum * 1/n^2 when full, sum / count
 // at the frame's odd edges (cv2's INTER_AREA fast path).
-__global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
-    pdlEnter();
+__device__ __forceinline__ void lumaPyrCta(const LumaPyrParams& p, int bx, int by) {
     __shared__ float sl[2][kTowerFloats];
-    const int tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 32;
+    const int tx0 = bx * 32, ty0 = by * 32;
     const int fw = p.lw[0], fh = p.lh[0], fs = p.fs;
     if (p.vec16 && tx0 + 32 <= fw && ty0 + 32 <= fh) {
         // flowScale 2, 16-byte aligned rows, a full tile: thread = 4 frame pixels (one uint4) x 2 rows = 2 level-0
@@ -88,6 +88,16 @@ __global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
     __syncthreads();
     lumaTower<false>(p, sl, tx0, ty0);
 }
+__global__ void __launch_bounds__(256) k_luma_pyr(const LumaPyrParams p) {
+    pdlEnter();
+    lumaPyrCta(p, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(256) k_luma_pyr_m(const __grid_constant__ Merged<LumaPyrParams> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    lumaPyrCta(m.item[i], bx, by);
+}
 
 // a pyramid level beyond the luma kernel's tower (interp.py:76); round10: the other formats' 2^-10 grid
 __global__ void __launch_bounds__(256) k_down(const DownParams p) {
@@ -121,11 +131,10 @@ __global__ void __launch_bounds__(256) k_down(const DownParams p) {
 template <bool kLat>
 __device__ __forceinline__ void searchSeed(const SearchParams& p, int bx, int by, int lane, int& sx, int& sy);
 
-__global__ void __launch_bounds__(128) k_search(const SearchParams p) {
-    pdlEnter();
+__device__ __forceinline__ void searchCta(const SearchParams& p, int cta) {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * 4 + warp;
+    const int b = cta * 4 + warp;
     if (b >= p.bw * p.bh) return;
     const int R = p.R, T = 8 + 2 * R, D = 2 * R + 1;
     float* sA = smem + warp * 2 * T * T;
@@ -164,6 +173,16 @@ __global__ void __launch_bounds__(128) k_search(const SearchParams p) {
         p.out[b] = make_float2((float)(sx + bci % D - R), (float)(sy + bci / D - R));
         if (p.sadOut) p.sadOut[b] = bsad;
     }
+}
+__global__ void __launch_bounds__(128) k_search(const SearchParams p) {
+    pdlEnter();
+    searchCta(p, blockIdx.x);
+}
+__global__ void __launch_bounds__(128) k_search_m(const __grid_constant__ Merged<SearchParams> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    searchCta(m.item[i], bx);
 }
 
 // The seed of a block (interp.seed_from :131-144 for one fine block), shared by both search kernels. A candidate equal
@@ -266,12 +285,11 @@ constexpr int kSearchLatBlocks = 2048;
 // of a and c are staged in shared memory. Lane = (dy, block row y): it holds a's row y - dy and c's row y + dy in
 // registers and scores every dx from them; the 8 rows of a dy are summed by shuffles (all sums exact).
 template <int R, bool kLat>
-__global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
-    pdlEnter();
+__device__ __forceinline__ void searchRCta(const SearchParams& p, int cta) {
     constexpr int T = 8 + 2 * R, D = 2 * R + 1, NI = 8 * D, ROUNDS = (NI + 31) / 32;
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * 4 + warp;
+    const int b = cta * 4 + warp;
     if (b >= p.bw * p.bh) return;
     float* sA = smem + warp * (2 * T * T + D * D);
     float* sC = sA + T * T;
@@ -336,6 +354,18 @@ __global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
         if (p.sadOut) p.sadOut[b] = bsad;
     }
 }
+template <int R, bool kLat>
+__global__ void __launch_bounds__(128) k_search_r(const SearchParams p) {
+    pdlEnter();
+    searchRCta<R, kLat>(p, blockIdx.x);
+}
+template <int R, bool kLat>
+__global__ void __launch_bounds__(128) k_search_r_m(const __grid_constant__ Merged<SearchParams> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    searchRCta<R, kLat>(m.item[i], bx);
+}
 
 // ============================================================================================== median3 + global median
 __device__ __forceinline__ void cswap(float& a, float& b) {
@@ -360,9 +390,8 @@ __device__ __forceinline__ float med9(float v[9]) {
 // fine blocks' own-parent vectors): every parent vector is added to an exact histogram with the number of fine blocks
 // that take it as their own parent; the last CTA reads off the order statistics k1 = (n-1)/2, k2 = n/2 and writes
 // 2 x the median = v_k1 + v_k2, then clears the histogram for the next estimate.
-__global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
-    pdlEnter();
-    const int b = blockIdx.x * 256 + threadIdx.x;
+__device__ __forceinline__ void median3Cta(const Median3Params& p, int cta, int ctas) {
+    const int b = cta * 256 + threadIdx.x;
     const int n = p.bw * p.bh;
     if (b < n) {
         const int bx = b % p.bw, by = b / p.bw;
@@ -403,7 +432,7 @@ __global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
     __syncthreads();
     if (threadIdx.x == 0) ticket = atomicAdd(p.done, 1u);
     __syncthreads();
-    if (ticket != gridDim.x - 1) return;
+    if (ticket != (unsigned int)ctas - 1u) return;
     __threadfence();
     if (threadIdx.x < 4) found[threadIdx.x] = 0;
     const int nb = 2 * p.B + 1;
@@ -440,6 +469,16 @@ __global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
         *p.done = 0;
     }
     for (int i = threadIdx.x; i < 2 * nb; i += 256) p.hist[i] = 0;
+}
+__global__ void __launch_bounds__(256) k_median3(const Median3Params p) {
+    pdlEnter();
+    median3Cta(p, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_median3_m(const __grid_constant__ Merged<Median3Params> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    median3Cta(m.item[i], bx, m.first[i + 1] - m.first[i]);
 }
 
 // One block of k_median3's work for the shared-memory forms below: the block's 3x3 medians (written to p.out), and
@@ -529,8 +568,7 @@ __device__ __forceinline__ void medianFromHist(const Median3Params& p, const uns
 // the same medians and the same global median, with the histogram in shared memory and the order statistics read
 // off by the same CTA, so no global atomics, no fence and no last-block ticket stand in the estimate's critical path
 // (the coarse levels are latency bound).
-__global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Params p) {
-    pdlEnter();
+__device__ __forceinline__ void median3OneCta(const Median3Params& p) {
     extern __shared__ unsigned int hs1[];   // 2 * nb bins: x then y
     const int nb = 2 * p.B + 1, tid = threadIdx.x;
     for (int i = tid; i < 2 * nb; i += kMed1Threads) hs1[i] = 0;
@@ -541,14 +579,21 @@ __global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Pa
     __syncthreads();
     medianFromHist(p, hs1, nb);
 }
+__global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one(const Median3Params p) {
+    pdlEnter();
+    median3OneCta(p);
+}
+__global__ void __launch_bounds__(kMed1Threads, 1) k_median3_one_m(const __grid_constant__ Merged<Median3Params> m) {
+    pdlEnter();
+    median3OneCta(m.item[blockIdx.x]);   // one CTA per item
+}
 
 // k_median3 for mid-size levels (at most kMedClBlocks blocks): a cluster of kMedCl CTAs, each with its own histogram
 // in shared memory; after the cluster barrier CTA 0 adds the others' histograms through distributed shared memory and
 // reads off the order statistics. No global atomics, no fence, no last-block ticket; the other CTAs stay resident
 // (a second cluster barrier) until CTA 0 has read their shared memory.
 constexpr int kMedCl = 8, kMedClBlocks = kMedCl * kMed1Threads * 2;
-__global__ void __cluster_dims__(kMedCl, 1, 1) __launch_bounds__(kMed1Threads, 1) k_median3_cluster(const Median3Params p) {
-    pdlEnter();
+__device__ __forceinline__ void median3ClusterCta(const Median3Params& p) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ unsigned int hs1[];
@@ -571,6 +616,15 @@ __global__ void __cluster_dims__(kMedCl, 1, 1) __launch_bounds__(kMed1Threads, 1
         medianFromHist(p, hs1, nb);
     }
     cl.sync();
+}
+__global__ void __cluster_dims__(kMedCl, 1, 1) __launch_bounds__(kMed1Threads, 1) k_median3_cluster(const Median3Params p) {
+    pdlEnter();
+    median3ClusterCta(p);
+}
+__global__ void __cluster_dims__(kMedCl, 1, 1) __launch_bounds__(kMed1Threads, 1)
+    k_median3_cluster_m(const __grid_constant__ Merged<Median3Params> m) {
+    pdlEnter();
+    median3ClusterCta(m.item[blockIdx.x / kMedCl]);   // one cluster per item
 }
 
 // ============================================================================================== scene-cut mean
@@ -726,11 +780,10 @@ __device__ __forceinline__ void cutMeanShare(const SubpixParams& p, int b, int n
     }
 }
 
-__global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
-    pdlEnter();
+__device__ __forceinline__ void subpixCta(const SubpixParams& p, int cta) {
     extern __shared__ float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * 4 + warp;
+    const int b = cta * 4 + warp;
     const int nb = p.bw * p.bh;
     if (b < nb) {
         float* tA = smem + warp * kSubWarpFloats;
@@ -844,6 +897,16 @@ __global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
         cutMeanShare(p, b, nb, lane);
     }
 }
+__global__ void __launch_bounds__(128) k_subpix(const SubpixParams p) {
+    pdlEnter();
+    subpixCta(p, blockIdx.x);
+}
+__global__ void __launch_bounds__(128) k_subpix_m(const __grid_constant__ Merged<SubpixParams> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    subpixCta(m.item[i], bx);
+}
 
 // ============================================================================================== per-pixel field
 // interp.pixel_field :167-183 at flow resolution. Candidates per pixel: the bilinear block field (cv2.resize x8,
@@ -940,8 +1003,7 @@ __device__ __forceinline__ void pfBlockCandidate(const PixfieldParams& p, int k,
     }
 }
 
-__global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
-    pdlEnter();
+__device__ __forceinline__ void pixfieldCta(const PixfieldParams& p, int ctaX, int ctaY) {
     // rows padded by one word: the horizontal sums below read down the rows of a column group, one row per lane
     __shared__ int plane[kPfEH][kPfE + 1];
     __shared__ int plane0[kPfEH][kPfE + 1];   // the zero candidate's errors, computed once
@@ -950,7 +1012,7 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
     __shared__ int2 bR[kPfBY][kPfBX];
     __shared__ float4 rowc[kPfEH];   // bilinear candidate, y: (row0, row1 relative to the block region, weights)
     const int tid = threadIdx.x, ex = tid & (kPfE - 1), ey0 = tid >> 6;
-    const int X0 = blockIdx.x * kPfTW, Y0 = blockIdx.y * kPfTH;
+    const int X0 = ctaX * kPfTW, Y0 = ctaY * kPfTH;
     // the block-field region: every block a region pixel's candidates can name
     const int qx0 = clampi(X0 - kPfAp, 0, p.w - 1), qy0 = clampi(Y0 - kPfAp, 0, p.h - 1);
     const int bx0 = max((qx0 >> 3) - 1, 0), by0 = max((qy0 >> 3) - 1, 0);
@@ -1075,6 +1137,16 @@ __global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
         p.pf[(size_t)y * p.w + x] = v;
     }
     (void)bxq;
+}
+__global__ void __launch_bounds__(256) k_pixfield(const PixfieldParams p) {
+    pdlEnter();
+    pixfieldCta(p, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(256) k_pixfield_m(const __grid_constant__ Merged<PixfieldParams> m) {
+    pdlEnter();
+    int bx, by;
+    const int i = mergedItem(m, bx, by);
+    pixfieldCta(m.item[i], bx, by);
 }
 
 // ============================================================================================== synthesis
@@ -1472,6 +1544,105 @@ cudaError_t launchMedian3(const Median3Params& p, cudaStream_t s) {
         return launchPdl(k_median3_cluster, dim3(kMedCl), dim3(kMed1Threads), (size_t)2 * nb * 4, s, p);
     return launchPdl(k_median3, dim3(divUp(p.bw * p.bh, 256)), dim3(256), 0, s, p);
 }
+// ---- merged launches: the items' CTA ranges, then one launch (every item of m takes the same kernel variant)
+template <class P, class F>
+static int layoutMerged(Merged<P>& m, F ctasOf) {   // ctasOf(item, gx&) -> the item's CTA count
+    int total = 0;
+    for (int i = 0; i < m.n; i++) {
+        int gx = 1;
+        const int c = ctasOf(m.item[i], gx);
+        m.first[i] = total;
+        m.gx[i] = gx;
+        total += c;
+    }
+    m.first[m.n] = total;
+    return total;
+}
+cudaError_t launchLumaPyrMerged(Merged<LumaPyrParams>& m, cudaStream_t s) {
+    if (m.n < 1 || m.n > kMergeMax) return cudaErrorInvalidValue;
+    const int total = layoutMerged(m, [](const LumaPyrParams& p, int& gx) {
+        gx = (int)divUp(p.lw[0], 32);
+        return gx * (int)divUp(p.lh[0], 32);
+    });
+    return launchPdl(k_luma_pyr_m, dim3(total), dim3(256), 0, s, m);
+}
+int searchVariant(const SearchParams& p) {
+    if (p.R >= 1 && p.R <= 6) return 2 * p.R + (p.bw * p.bh <= kSearchLatBlocks ? 1 : 0);
+    return 100 + p.R;
+}
+template <int R>
+static cudaError_t launchSearchRMerged(Merged<SearchParams>& m, int total, cudaStream_t s) {
+    constexpr int T = 8 + 2 * R, D = 2 * R + 1;
+    const size_t smem = (size_t)4 * (2 * T * T + D * D) * sizeof(float);
+    if (searchVariant(m.item[0]) & 1) return launchPdl(k_search_r_m<R, true>, dim3(total), dim3(128), smem, s, m);
+    return launchPdl(k_search_r_m<R, false>, dim3(total), dim3(128), smem, s, m);
+}
+cudaError_t launchSearchMerged(Merged<SearchParams>& m, cudaStream_t s) {
+    if (m.n < 1 || m.n > kMergeMax) return cudaErrorInvalidValue;
+    const int v = searchVariant(m.item[0]);
+    for (int i = 1; i < m.n; i++)
+        if (searchVariant(m.item[i]) != v) return cudaErrorInvalidValue;
+    const int total = layoutMerged(m, [](const SearchParams& p, int& gx) {
+        gx = (int)divUp(p.bw * p.bh, 4);
+        return gx;
+    });
+    switch (m.item[0].R) {
+        case 1: return launchSearchRMerged<1>(m, total, s);
+        case 2: return launchSearchRMerged<2>(m, total, s);
+        case 3: return launchSearchRMerged<3>(m, total, s);
+        case 4: return launchSearchRMerged<4>(m, total, s);
+        case 5: return launchSearchRMerged<5>(m, total, s);
+        case 6: return launchSearchRMerged<6>(m, total, s);
+        default: {
+            const int T = 8 + 2 * m.item[0].R;
+            return launchPdl(k_search_m, dim3(total), dim3(128), (size_t)4 * 2 * T * T * sizeof(float), s, m);
+        }
+    }
+}
+int median3Variant(const Median3Params& p) {
+    const int nb = 2 * p.B + 1;
+    if (p.doHist && p.bw * p.bh <= kMed1Blocks && nb <= kMed1MaxBins) return 0;
+    if (p.doHist && p.bw * p.bh <= kMedClBlocks && nb <= kMed1MaxBins) return 1;
+    return 2;
+}
+cudaError_t launchMedian3Merged(Merged<Median3Params>& m, cudaStream_t s) {
+    if (m.n < 1 || m.n > kMergeMax) return cudaErrorInvalidValue;
+    const int v = median3Variant(m.item[0]);
+    size_t smem = 0;
+    for (int i = 0; i < m.n; i++) {
+        if (median3Variant(m.item[i]) != v) return cudaErrorInvalidValue;
+        smem = std::max(smem, (size_t)2 * (2 * m.item[i].B + 1) * 4);
+    }
+    if (v == 0) {
+        layoutMerged(m, [](const Median3Params&, int& gx) { gx = 1; return 1; });
+        return launchPdl(k_median3_one_m, dim3(m.n), dim3(kMed1Threads), smem, s, m);
+    }
+    if (v == 1) {
+        layoutMerged(m, [](const Median3Params&, int& gx) { gx = kMedCl; return kMedCl; });
+        return launchPdl(k_median3_cluster_m, dim3(kMedCl * m.n), dim3(kMed1Threads), smem, s, m);
+    }
+    const int total = layoutMerged(m, [](const Median3Params& p, int& gx) {
+        gx = (int)divUp(p.bw * p.bh, 256);
+        return gx;
+    });
+    return launchPdl(k_median3_m, dim3(total), dim3(256), 0, s, m);
+}
+cudaError_t launchSubpixMerged(Merged<SubpixParams>& m, cudaStream_t s) {
+    if (m.n < 1 || m.n > kMergeMax) return cudaErrorInvalidValue;
+    const int total = layoutMerged(m, [](const SubpixParams& p, int& gx) {
+        gx = (int)divUp(p.bw * p.bh, 4);
+        return gx;
+    });
+    return launchPdl(k_subpix_m, dim3(total), dim3(128), (size_t)4 * kSubWarpFloats * sizeof(float), s, m);
+}
+cudaError_t launchPixfieldMerged(Merged<PixfieldParams>& m, cudaStream_t s) {
+    if (m.n < 1 || m.n > kMergeMax) return cudaErrorInvalidValue;
+    const int total = layoutMerged(m, [](const PixfieldParams& p, int& gx) {
+        gx = (int)divUp(p.w, kPfTW);
+        return gx * (int)divUp(p.h, kPfTH);
+    });
+    return launchPdl(k_pixfield_m, dim3(total), dim3(256), 0, s, m);
+}
 static size_t planBytes(const CutPlan& c) {
     const size_t b = (size_t)(c.nLeaves + c.nInner) * sizeof(float);
     return b <= kPlanSmemMax ? b : 0;   // 0: the node values live in c.gvals
@@ -1483,6 +1654,11 @@ cudaError_t prepareKernels() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_median3_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMed1MaxBins * 4);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_cutmean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_subpix_m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlanSmemMax);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_median3_one_m, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMed1MaxBins * 4);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_median3_cluster_m, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMed1MaxBins * 4);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(synthSmemBytes(1) + kSyWarpBytes));
     if (e == cudaSuccess)

@@ -147,6 +147,19 @@ struct SynthParams {
     const uint32_t* uiA; const uint32_t* uiC;
 };
 
+// One estimate pass of many frame pairs ("items") in one launch: the parameters of every item travel in the launch's
+// own parameter block (a captured graph holds them; nothing is uploaded per record). The grid is one-dimensional:
+// item i owns CTAs [first[i], first[i + 1]), laid out as its own grid of gx[i] CTAs across. At most kMergeMax items
+// per launch (the host splits larger sets).
+constexpr int kMergeMax = 48;
+template <class P>
+struct Merged {
+    P item[kMergeMax];
+    int first[kMergeMax + 1];
+    int gx[kMergeMax];
+    int n;
+};
+
 struct SynthBatchArgs {             // k_synth_batch: a work list of syntheses
     const SynthParams* items;      // per item (device array)
     const int* tileStart;          // nItems + 1: the first tile of each item in the list, then the total
@@ -204,6 +217,16 @@ cudaError_t launchSynth(const SynthParams& p, cudaStream_t s);
 cudaError_t launchFallback(const FallbackParams& p, cudaStream_t s);
 // batches (framegen.cpp Batch): many syntheses in one persistent launch, their fallbacks in one launch
 cudaError_t launchSynthBatch(const SynthBatchArgs& b, int grid, size_t smem, cudaStream_t s);
+// merged estimate passes (every item of a launch takes the same kernel variant; the host groups them by
+// searchVariant / median3Variant); the CTA counts per item (first, gx) are filled in by the launchers
+cudaError_t launchLumaPyrMerged(Merged<LumaPyrParams>& m, cudaStream_t s);
+cudaError_t launchLumaFmtMerged(Merged<LumaPyrParams>& m, int format, cudaStream_t s);
+int searchVariant(const SearchParams& p);     // the kernel a search runs: R (1..6) x 2 + latency form, or 100 + R
+int median3Variant(const Median3Params& p);   // 0: one CTA, 1: cluster, 2: grid with a last-CTA ticket
+cudaError_t launchSearchMerged(Merged<SearchParams>& m, cudaStream_t s);
+cudaError_t launchMedian3Merged(Merged<Median3Params>& m, cudaStream_t s);
+cudaError_t launchSubpixMerged(Merged<SubpixParams>& m, cudaStream_t s);
+cudaError_t launchPixfieldMerged(Merged<PixfieldParams>& m, cudaStream_t s);
 // one pass of a motion blur, 8-bit RGBA frames: the main pass (fix = 0), then the fix-up (fix = 1)
 cudaError_t launchSynthBlur(const BlurParams& bp, int fix, cudaStream_t s);
 int synthBatchCtasPerSm(size_t smem);

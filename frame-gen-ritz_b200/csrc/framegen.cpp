@@ -13,6 +13,7 @@
 #include <cstddef>
 #include <cstring>
 #include <memory>
+#include <numeric>
 #include <vector>
 
 #include "fg_params.h"
@@ -538,17 +539,30 @@ struct Interpolator::Impl {
         return true;
     }
 
-    bool estimate(cudaStream_t s, const Frame& prev, const Frame& curr) {
+    // Every pass of one estimate, its parameters resolved (the luma, the pyramid levels beyond the luma kernel's tower,
+    // per level from the coarsest searched down: search and median3, then the sub-pixel refinement or the scene-cut
+    // mean, then the pixel field). fill: CrosshairV2's estimate fill rebuilds levels >= 1 from the filled level 0.
+    struct EstPlan {
+        fgk::LumaPyrParams luma{};
+        std::vector<fgk::DownParams> down;
+        int top = 0;                                 // the coarsest level searched
+        std::vector<fgk::SearchParams> search;       // by level
+        std::vector<fgk::Median3Params> med;         // by level
+        fgk::SubpixParams sub{};
+        fgk::CutMeanParams cut{};
+        fgk::PixfieldParams pix{};
+    };
+    void planEstimate(const Frame& prev, const Frame& curr, bool fill, EstPlan& e) const {
         const int n = (int)L.lv.size();
         const float lam = set.searchPenalty;
-        if (profiling) { evCount = 0; profileNo++; stamp(s, "start"); }
         // 1-2. luma + pyramid
-        fgk::LumaPyrParams lp{};
+        fgk::LumaPyrParams& lp = e.luma;
+        lp = fgk::LumaPyrParams{};
         lp.a = (const uint8_t*)prev.data; lp.c = (const uint8_t*)curr.data; lp.pitch = prev.pitch;
         lp.W = (int)W; lp.H = (int)H; lp.fs = (int)set.flowScale;
         lp.ri = ri; lp.gi = gi; lp.bi = bi;
-        const int top = snK >= 0 ? snK : n - 1;   // the coarsest level searched
-        lp.nlev = std::min(top + 1, fgk::kPyrInKernel);
+        e.top = snK >= 0 ? snK : n - 1;
+        lp.nlev = std::min(e.top + 1, fgk::kPyrInKernel);
         lp.f = fc;
         lp.vec16 = fmt == Format::Rgba8 && set.flowScale == 2 && prev.pitch % 16 == 0 && ((uintptr_t)prev.data & 15) == 0 && ((uintptr_t)curr.data & 15) == 0 &&
                    W % 4 == 0 && H % 2 == 0;   // complete 2x2 cells in every full tile, 8-byte aligned level-0 rows
@@ -556,41 +570,16 @@ struct Interpolator::Impl {
             lp.lw[l] = L.lv[l].w; lp.lh[l] = L.lv[l].h;
             lp.la[l] = luma + L.lv[l].lumaA; lp.lc[l] = luma + L.lv[l].lumaC;
         }
-        if (prev.pitch != curr.pitch) return false;
-        if (!check(fmt == Format::Rgba8 ? fgk::launchLumaPyr(lp, s) : fgk::launchLumaFmt(lp, s))) return false;
-        stamp(s, "luma");
-        const bool fill = fillMask[0] && fillMask[1];
-        if (fill) {   // CrosshairV2's estimate fill of level 0; the pyramid is then rebuilt from the filled level 0
-            fgk::UiFillParams fp{};
-            fp.a = lp.a; fp.c = lp.c; fp.pitch = lp.pitch;
-            fp.W = (int)W; fp.H = (int)H; fp.ri = ri; fp.gi = gi; fp.bi = bi; fp.fs = (int)set.flowScale;
-            fp.fw = L.lv[0].w; fp.fh = L.lv[0].h;
-            fp.ma = fillMask[0]; fp.mc = fillMask[1];
-            fp.la = luma + L.lv[0].lumaA; fp.lc = luma + L.lv[0].lumaC;
-            fp.cx0 = uiWork[0] / fp.fs; fp.cy0 = uiWork[1] / fp.fs;
-            fp.ncx = (uiWork[0] + uiWork[2] - 1) / fp.fs - fp.cx0 + 1;
-            fp.ncy = (uiWork[1] + uiWork[3] - 1) / fp.fs - fp.cy0 + 1;
-            if (!check(fgk::launchUiFill(fp, s))) return false;
-            stamp(s, "ui fill");
-        }
-        for (int l = fill ? 1 : fgk::kPyrInKernel; l <= top; l++) {
-            fgk::DownParams dp{luma + L.lv[l - 1].lumaA, luma + L.lv[l - 1].lumaC, L.lv[l - 1].w, L.lv[l - 1].h,
-                               luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h, fmt != Format::Rgba8};
-            if (!check(fgk::launchDown(dp, s))) return false;
-        }
-        stamp(s, "pyramid");
-        if (snK >= 0) {   // the seed net on level snK
-            const Level& lk = L.lv[snK];
-            if (!fgk::seedNetForwardLuma(snet, s, luma + lk.lumaA, luma + lk.lumaC, lk.h, lk.w, snOut, &st->err, &lastErr))
-                return false;
-            stamp(s, "seed net");
-        }
+        e.down.clear();
+        for (int l = fill ? 1 : fgk::kPyrInKernel; l <= e.top; l++)
+            e.down.push_back(fgk::DownParams{luma + L.lv[l - 1].lumaA, luma + L.lv[l - 1].lumaC, L.lv[l - 1].w, L.lv[l - 1].h,
+                                             luma + L.lv[l].lumaA, luma + L.lv[l].lumaC, L.lv[l].w, L.lv[l].h, fmt != Format::Rgba8});
         // 3-5. per level, coarse -> fine
-        static const char* names[] = {"level 0 (finest)", "level 1", "level 2", "level 3", "level 4", "level 5",
-                                      "level 6", "level 7"};
-        for (int i = top; i >= 0; i--) {
+        e.search.assign(n, fgk::SearchParams{});
+        e.med.assign(n, fgk::Median3Params{});
+        for (int i = e.top; i >= 0; i--) {
             const Level& l = L.lv[i];
-            fgk::SearchParams sp{};
+            fgk::SearchParams& sp = e.search[i];
             sp.la = luma + l.lumaA; sp.lc = luma + l.lumaC;
             sp.w = l.w; sp.h = l.h; sp.bw = l.bw; sp.bh = l.bh;
             sp.top = i == n - 1 && snK < 0;
@@ -605,8 +594,7 @@ struct Interpolator::Impl {
             for (int k = 0; k <= 2 * sp.R; k++) sp.pen[k] = (float)((double)lam * 1.0 * (double)k);
             sp.out = field + l.fS;
             sp.sadOut = (i == 0 && !set.subpixel) ? sads : nullptr;
-            if (!check(fgk::launchSearch(sp, s))) return false;
-            fgk::Median3Params mp{};
+            fgk::Median3Params& mp = e.med[i];
             mp.in = field + l.fS; mp.out = field + l.fM; mp.bw = l.bw; mp.bh = l.bh;
             mp.doHist = i > 0;
             if (i > 0) {
@@ -614,14 +602,13 @@ struct Interpolator::Impl {
                 mp.hist = hist; mp.done = &st->medDone[i]; mp.medOut = st->med[i - 1];
             }
             mp.err = &st->err;
-            if (!check(fgk::launchMedian3(mp, s))) return false;
-            stamp(s, names[std::min(i, 7)]);
         }
         // 6. sub-pixel refinement + the scene-cut mean
         const Level& l0 = L.lv[0];
         const float2* vfin = field + l0.fM;
         if (set.subpixel) {
-            fgk::SubpixParams sp{};
+            fgk::SubpixParams& sp = e.sub;
+            sp = fgk::SubpixParams{};
             sp.la = luma + l0.lumaA; sp.lc = luma + l0.lumaC;
             sp.w = l0.w; sp.h = l0.h; sp.bw = l0.bw; sp.bh = l0.bh;
             sp.in = field + l0.fM; sp.out = field + L.sub1; sp.out0 = field + L.sub0; sp.sads = sads;
@@ -629,17 +616,56 @@ struct Interpolator::Impl {
             for (int p = 0; p < 2; p++)
                 for (int k = 0; k < 3; k++) sp.pen[p][k] = (float)((double)lam * (double)steps[p] * (double)k);
             sp.plan = plan; sp.cutSad = set.sceneCutSad; sp.st = st;
-            if (!check(fgk::launchSubpix(sp, s))) return false;
             vfin = field + L.sub1;
         } else {
-            fgk::CutMeanParams cp{sads, l0.bw * l0.bh, plan, set.sceneCutSad, st};
-            if (!check(fgk::launchCutMean(cp, s))) return false;
+            e.cut = fgk::CutMeanParams{sads, l0.bw * l0.bh, plan, set.sceneCutSad, st};
         }
-        stamp(s, "subpixel");
         // 8. per-pixel vector choice
-        fgk::PixfieldParams pp{luma + l0.lumaA, luma + l0.lumaC, l0.w, l0.h, vfin, l0.bw, l0.bh, set.smoothBonus,
-                               set.hudBonus, pf};
-        if (!check(fgk::launchPixfield(pp, s))) return false;
+        e.pix = fgk::PixfieldParams{luma + l0.lumaA, luma + l0.lumaC, l0.w, l0.h, vfin, l0.bw, l0.bh, set.smoothBonus,
+                                    set.hudBonus, pf};
+    }
+
+    bool estimate(cudaStream_t s, const Frame& prev, const Frame& curr) {
+        if (prev.pitch != curr.pitch) return false;
+        if (profiling) { evCount = 0; profileNo++; stamp(s, "start"); }
+        const bool fill = fillMask[0] && fillMask[1];
+        EstPlan e;
+        planEstimate(prev, curr, fill, e);
+        const fgk::LumaPyrParams& lp = e.luma;
+        if (!check(fmt == Format::Rgba8 ? fgk::launchLumaPyr(lp, s) : fgk::launchLumaFmt(lp, s))) return false;
+        stamp(s, "luma");
+        if (fill) {   // CrosshairV2's estimate fill of level 0; the pyramid is then rebuilt from the filled level 0
+            fgk::UiFillParams fp{};
+            fp.a = lp.a; fp.c = lp.c; fp.pitch = lp.pitch;
+            fp.W = (int)W; fp.H = (int)H; fp.ri = ri; fp.gi = gi; fp.bi = bi; fp.fs = (int)set.flowScale;
+            fp.fw = L.lv[0].w; fp.fh = L.lv[0].h;
+            fp.ma = fillMask[0]; fp.mc = fillMask[1];
+            fp.la = luma + L.lv[0].lumaA; fp.lc = luma + L.lv[0].lumaC;
+            fp.cx0 = uiWork[0] / fp.fs; fp.cy0 = uiWork[1] / fp.fs;
+            fp.ncx = (uiWork[0] + uiWork[2] - 1) / fp.fs - fp.cx0 + 1;
+            fp.ncy = (uiWork[1] + uiWork[3] - 1) / fp.fs - fp.cy0 + 1;
+            if (!check(fgk::launchUiFill(fp, s))) return false;
+            stamp(s, "ui fill");
+        }
+        for (const fgk::DownParams& dp : e.down)
+            if (!check(fgk::launchDown(dp, s))) return false;
+        stamp(s, "pyramid");
+        if (snK >= 0) {   // the seed net on level snK
+            const Level& lk = L.lv[snK];
+            if (!fgk::seedNetForwardLuma(snet, s, luma + lk.lumaA, luma + lk.lumaC, lk.h, lk.w, snOut, &st->err, &lastErr))
+                return false;
+            stamp(s, "seed net");
+        }
+        static const char* names[] = {"level 0 (finest)", "level 1", "level 2", "level 3", "level 4", "level 5",
+                                      "level 6", "level 7"};
+        for (int i = e.top; i >= 0; i--) {
+            if (!check(fgk::launchSearch(e.search[i], s))) return false;
+            if (!check(fgk::launchMedian3(e.med[i], s))) return false;
+            stamp(s, names[std::min(i, 7)]);
+        }
+        if (!check(set.subpixel ? fgk::launchSubpix(e.sub, s) : fgk::launchCutMean(e.cut, s))) return false;
+        stamp(s, "subpixel");
+        if (!check(fgk::launchPixfield(e.pix, s))) return false;
         stamp(s, "pixel field");
         return true;
     }
@@ -1261,6 +1287,8 @@ struct Batch::Impl {
     int ring = 0;
     // the fork / join pool of the slots' estimates
     static constexpr int kMaxStreams = 8;
+    bool mergeable() const;   // no slot needs a per-slot estimate pass (UI protection, the seed net, profiling)
+    bool mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr);
     cudaStream_t pool[kMaxStreams] = {};
     cudaEvent_t fork = nullptr, join[kMaxStreams] = {};
 
@@ -1320,7 +1348,8 @@ uint32_t Batch::synthsOf(uint32_t i) const { return i < m->mult.size() ? m->mult
 Interpolator* Batch::slot(uint32_t i) { return i < m->slots.size() ? m->slots[i].get() : nullptr; }
 Batch::Shape Batch::shape() const { return m->shape; }
 bool Batch::setShape(const Shape& s) {
-    if (s.ctasPerSm > 4 || s.order > 1 || s.streams < 1 || s.streams > (uint32_t)Impl::kMaxStreams) return false;
+    if (s.ctasPerSm > 4 || s.order > 1 || s.streams < 1 || s.streams > (uint32_t)Impl::kMaxStreams || s.mergeEstimates > 1)
+        return false;
     m->shape = s;
     return true;
 }
@@ -1353,6 +1382,112 @@ int Batch::add(const InitInfo& ii, uint32_t multiplier) {
     return (int)m->slots.size() - 1;
 }
 
+// Items of one estimate pass grouped by key (the kernel variant they take) and launched merged, at most kMergeMax
+// per launch; launch(merged, key)
+template <class P, class Launch>
+static cudaError_t launchMergedGroups(const std::vector<P>& items, const std::vector<int>& keys, Launch launch) {
+    if (items.empty()) return cudaSuccess;
+    std::vector<int> idx(items.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+    std::unique_ptr<fgk::Merged<P>> mg(new fgk::Merged<P>());
+    size_t i = 0;
+    while (i < idx.size()) {
+        const int key = keys[idx[i]];
+        mg->n = 0;
+        while (i < idx.size() && keys[idx[i]] == key && mg->n < fgk::kMergeMax) mg->item[mg->n++] = items[idx[i++]];
+        const cudaError_t e = launch(*mg, key);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Every slot's estimate (streams = 0): one launch per pass for all the slots on the caller's stream, in the order an
+// estimate runs its passes (luma, levels from the coarsest down to level 0 with the finest levels aligned, so level l
+// of every slot that has one is searched in the same launch, sub-pixel, pixel field). The same kernels' work per
+// slot as recordEstimate; only the launches are shared.
+bool Batch::Impl::mergeable() const {
+    for (const auto& I : slots) {
+        const Interpolator::Impl& im = *I->m;
+        if (im.uiOn() || im.snK >= 0 || im.profiling) return false;
+    }
+    return true;
+}
+
+bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr) {
+    const int ns = (int)slots.size();
+    for (int i = 0; i < ns; i++) {
+        slots[i]->beginFrame();
+        const Interpolator::Impl& im = *slots[i]->m;
+        if (!im.W || !im.frameOk(prev[i]) || !im.frameOk(curr[i]) || !im.samePitch(prev[i], curr[i])) {
+            err = "a slot's estimate was refused (frames?)";
+            return false;
+        }
+    }
+    std::vector<Interpolator::Impl::EstPlan> plans(ns);
+    int maxTop = 0;
+    for (int i = 0; i < ns; i++) {
+        Interpolator::Impl& im = *slots[i]->m;
+        im.estSets++;
+        im.haveEst = im.estUi = false;
+        im.planEstimate(prev[i], curr[i], false, plans[i]);
+        maxTop = std::max(maxTop, plans[i].top);
+    }
+    auto fail = [&](cudaError_t e) {
+        if (e == cudaSuccess) return false;
+        cudaGetLastError();
+        err = cudaGetErrorString(e);
+        return true;
+    };
+    std::vector<fgk::LumaPyrParams> luma;
+    std::vector<int> fmts;
+    for (int i = 0; i < ns; i++) {
+        luma.push_back(plans[i].luma);
+        fmts.push_back((int)slots[i]->m->fmt);
+    }
+    if (fail(launchMergedGroups(luma, fmts, [&](fgk::Merged<fgk::LumaPyrParams>& mg, int f) {
+            return f == (int)Format::Rgba8 ? fgk::launchLumaPyrMerged(mg, s) : fgk::launchLumaFmtMerged(mg, mg.item[0].f.format, s);
+        })))
+        return false;
+    for (int i = 0; i < ns; i++)
+        for (const fgk::DownParams& dp : plans[i].down)
+            if (fail(fgk::launchDown(dp, s))) return false;
+    for (int l = maxTop; l >= 0; l--) {
+        std::vector<fgk::SearchParams> se;
+        std::vector<fgk::Median3Params> me;
+        std::vector<int> sk, mk;
+        for (int i = 0; i < ns; i++)
+            if (l <= plans[i].top) {
+                se.push_back(plans[i].search[l]);
+                sk.push_back(fgk::searchVariant(se.back()));
+                me.push_back(plans[i].med[l]);
+                mk.push_back(fgk::median3Variant(me.back()));
+            }
+        if (fail(launchMergedGroups(se, sk, [&](fgk::Merged<fgk::SearchParams>& mg, int) { return fgk::launchSearchMerged(mg, s); })) ||
+            fail(launchMergedGroups(me, mk, [&](fgk::Merged<fgk::Median3Params>& mg, int) { return fgk::launchMedian3Merged(mg, s); })))
+            return false;
+    }
+    std::vector<fgk::SubpixParams> sub;
+    std::vector<fgk::PixfieldParams> pix;
+    for (int i = 0; i < ns; i++) {
+        if (slots[i]->m->set.subpixel) sub.push_back(plans[i].sub);
+        else if (fail(fgk::launchCutMean(plans[i].cut, s))) return false;
+        pix.push_back(plans[i].pix);
+    }
+    if (fail(launchMergedGroups(sub, std::vector<int>(sub.size(), 0),
+                                [&](fgk::Merged<fgk::SubpixParams>& mg, int) { return fgk::launchSubpixMerged(mg, s); })) ||
+        fail(launchMergedGroups(pix, std::vector<int>(pix.size(), 0),
+                                [&](fgk::Merged<fgk::PixfieldParams>& mg, int) { return fgk::launchPixfieldMerged(mg, s); })))
+        return false;
+    for (int i = 0; i < ns; i++) {
+        Interpolator::Impl& im = *slots[i]->m;
+        im.haveEst = true;
+        im.estPrev = prev[i].data;
+        im.estCurr = curr[i].data;
+    }
+    return true;
+}
+
 bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const Frame* outs) {
     m->err = nullptr;
     const int ns = (int)m->slots.size();
@@ -1361,8 +1496,11 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
     std::vector<int> first(ns);   // each slot's first output frame in outs
     for (int i = 0, o = 0; i < ns; i++) { first[i] = o; o += (int)m->mult[i] - 1; }
     const bool batched = m->shape.ctasPerSm > 0;
-    // 1. every slot's estimate (and, for the slots outside the persistent launch, its syntheses), forked over the
-    //    pool: slot i on stream i % streams, joined back into s before the persistent launch
+    // 0. mergeEstimates: every slot's estimate as merged launches on s (when no slot needs a per-slot pass)
+    const bool merged = m->shape.mergeEstimates && m->mergeable();
+    if (merged && !m->mergedEstimates(s, prev, curr)) return false;
+    // 1. every slot's estimate unless merged (and, for the slots outside the persistent launch, its syntheses), forked
+    //    over the pool: slot i on stream i % streams, joined back into s before the persistent launch
     const int nst = (int)std::min<uint32_t>(m->shape.streams, (uint32_t)Impl::kMaxStreams);
     auto streamOf = [&](int i) { return nst > 1 ? m->pool[i % nst] : s; };
     if (nst > 1) {
@@ -1375,8 +1513,10 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
     }
     for (int i = 0; i < ns; i++) {
         Interpolator& I = *m->slots[i];
-        I.beginFrame();
-        if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
+        if (!merged) {
+            I.beginFrame();
+            if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
+        }
         if (batched && I.m->fmt == Format::Rgba8) continue;
         for (uint32_t k = 1; k < m->mult[i]; k++)
             if (!I.recordSynth(streamOf(i), prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
@@ -1447,7 +1587,8 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
 }
 
 int Batch::tune(cudaStream_t s, const Frame* prev, const Frame* curr, const Frame* outs, uint32_t reps) {
-    static const Shape cand[] = {{0, 0, 1}, {3, 1, 1}, {0, 0, 4}, {3, 1, 4}, {0, 0, 8}, {2, 1, 8}, {3, 0, 8}, {3, 1, 8}};
+    static const Shape cand[] = {{0, 0, 1, 0}, {3, 1, 1, 0}, {0, 0, 4, 0}, {3, 1, 4, 0}, {0, 0, 8, 0}, {2, 1, 8, 0},
+                                 {3, 0, 8, 0}, {3, 1, 8, 0}, {0, 0, 1, 1}, {3, 1, 1, 1}, {0, 0, 8, 1}, {3, 1, 8, 1}};
     DeviceGuard g(m->device);
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { cudaGetLastError(); return -1; }
@@ -1719,11 +1860,16 @@ void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* orde
     if (order) *order = s.order;
     if (streams) *streams = s.streams;
 }
+uint32_t fg_batch_merge_estimates(const fg_batch* b) { return b ? b->B.shape().mergeEstimates : 0u; }
 int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order, uint32_t streams) {
+    return fg_batch_set_shape_merged(b, ctas_per_sm, order, streams, 0);
+}
+int fg_batch_set_shape_merged(fg_batch* b, uint32_t ctas_per_sm, uint32_t order, uint32_t streams, uint32_t merge_estimates) {
     Batch::Shape s;
     s.ctasPerSm = ctas_per_sm;
     s.order = order;
     s.streams = streams;
+    s.mergeEstimates = merge_estimates;
     return b && b->B.setShape(s);
 }
 int fg_batch_trace(fg_batch* b, uint32_t slot, void* stream, void* dst) {

@@ -131,6 +131,8 @@ SIGNATURES = {
     "fg_batch_tune": (_I, [_P, _P, _P, _P, _P, _U32]),
     "fg_batch_get_shape": (None, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "fg_batch_set_shape": (_I, [_P, _U32, _U32, _U32]),
+    "fg_batch_set_shape_merged": (_I, [_P, _U32, _U32, _U32, _U32]),
+    "fg_batch_merge_estimates": (_U32, [_P]),
     "fg_batch_trace_layout": (_I, [_P, _U32, ctypes.POINTER(CTraceLayout)]),
     "fg_batch_trace": (_I, [_P, _U32, _P, _P]),
     "fg_set_seed_net": (_I, [_P, _P, _U32]),
@@ -664,12 +666,14 @@ class Batch:
         return int(lib().fg_batch_tune(self._h, _stream(stream), p, c, o, int(reps)))
 
     def shape(self):
+        """(ctasPerSm, order, streams, mergeEstimates)"""
         a, b, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
         lib().fg_batch_get_shape(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
-        return a.value, b.value, c.value
+        return a.value, b.value, c.value, int(lib().fg_batch_merge_estimates(self._h))
 
-    def set_shape(self, ctas_per_sm, order, streams=8):
-        return bool(lib().fg_batch_set_shape(self._h, int(ctas_per_sm), int(order), int(streams)))
+    def set_shape(self, ctas_per_sm, order, streams=8, merge_estimates=0):
+        return bool(lib().fg_batch_set_shape_merged(self._h, int(ctas_per_sm), int(order), int(streams),
+                                                    int(merge_estimates)))
 
 
 def box_rect(settings, W, H):

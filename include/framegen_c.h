@@ -157,6 +157,9 @@ int fg_batch_tune(fg_batch* b, void* stream, const fg_frame* prev, const fg_fram
                   uint32_t reps);
 void fg_batch_get_shape(const fg_batch* b, uint32_t* ctas_per_sm, uint32_t* order, uint32_t* streams);
 int fg_batch_set_shape(fg_batch* b, uint32_t ctas_per_sm, uint32_t order, uint32_t streams);
+/* the same with Batch::Shape::mergeEstimates (fg_batch_set_shape sets it to 0); fg_batch_merge_estimates reads it */
+int fg_batch_set_shape_merged(fg_batch* b, uint32_t ctas_per_sm, uint32_t order, uint32_t streams, uint32_t merge_estimates);
+uint32_t fg_batch_merge_estimates(const fg_batch* b);
 int fg_batch_trace_layout(fg_batch* b, uint32_t slot, fg_trace_layout* l);   /* a slot's Interpolator::traceLayout */
 int fg_batch_trace(fg_batch* b, uint32_t slot, void* stream, void* dst);     /* a slot's Interpolator::recordTrace */
 

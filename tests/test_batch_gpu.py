@@ -1,7 +1,8 @@
 """framegen::Batch (fg_batch_*): many frame pairs of mixed sizes, formats and multipliers recorded together, the
-8-bit RGBA syntheses of all slots in one persistent launch. Every slot's outputs must equal, byte for byte, those of a
-standalone Interpolator on the same pair (whose parity with the oracle the other test files establish), for every
-launch shape the autotuner chooses from, after tune(), and through a CUDA graph.
+8-bit RGBA syntheses of all slots in one persistent launch, the estimates forked over streams or merged into one launch
+per pass for all slots. Every slot's outputs must equal, byte for byte, those of a standalone Interpolator on the same
+pair (whose parity with the oracle the other test files establish), for every launch shape the autotuner chooses from,
+after tune(), and through a CUDA graph.
 """
 import numpy as np
 import pytest
@@ -96,7 +97,8 @@ def case():
     return build_case(c3_slots(scale=8, n=24))
 
 
-@pytest.mark.parametrize("shape", [(0, 0, 1), (3, 1, 1), (0, 0, 4), (2, 0, 8), (2, 1, 8), (3, 0, 8), (3, 1, 8)])
+@pytest.mark.parametrize("shape", [(0, 0, 1), (3, 1, 1), (0, 0, 4), (2, 0, 8), (2, 1, 8), (3, 0, 8), (3, 1, 8),
+                                   (0, 0, 1, 1), (3, 1, 1, 1), (0, 0, 8, 1), (3, 1, 8, 1)])
 def test_batch_matches_standalone(case, shape):
     B, prev, curr, outs, ref = case
     assert B.set_shape(*shape)
@@ -113,15 +115,16 @@ def test_batch_matches_standalone(case, shape):
 def test_tune_then_record(case):
     B, prev, curr, outs, ref = case
     best = B.tune(prev, curr, outs, reps=2)
-    assert 0 <= best < 8
+    assert 0 <= best < 12
     assert B.record(prev, curr, outs)
     torch.cuda.synchronize()
     assert all(same(host(o), r) for o, r in zip(outs, ref))
 
 
-def test_batch_graph_capture(case):
+@pytest.mark.parametrize("shape", [(3, 1, 8), (3, 1, 8, 1)])
+def test_batch_graph_capture(case, shape):
     B, prev, curr, outs, ref = case
-    assert B.set_shape(3, 1, 8)
+    assert B.set_shape(*shape)
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
         assert B.record(prev, curr, outs, stream=s)   # warm (parameter upload ring, lazy module loads)
@@ -136,6 +139,45 @@ def test_batch_graph_capture(case):
     torch.cuda.synchronize()
     assert all(same(host(o), r) for o, r in zip(outs, ref))
     del g
+
+
+def test_merged_estimates_mixed_settings():
+    """merged estimates over slots whose passes take different kernel variants in the same launch step: radii 1 / 3 /
+    6 / 9 (the runtime-radius search), subpixel off (the scene-cut mean instead of the sub-pixel pass), flowScale 1 /
+    4, sizes from 96 x 200 to 1280 x 720 and more slots than one merged launch takes (kMergeMax 48)"""
+    kinds = [dict(searchRadius=1), dict(searchRadius=3, searchRadiusTop=4), dict(searchRadius=6),
+             dict(searchRadius=9, searchRadiusTop=9), dict(subpixel=False), dict(flowScale=1), dict(flowScale=4), {}]
+    sizes = [(128, 96), (160, 90), (320, 180), (640, 360), (1280, 720), (96, 200)]
+    B = fg.Batch()
+    prev, curr, outs, ref = [], [], [], []
+    for i in range(52):
+        w, h = sizes[i % len(sizes)]
+        fmt = ["rgba8", "rgb10", "nv12", "p010"][i % 4]
+        st = fg.Settings(**kinds[i % len(kinds)])
+        assert B.add(w, h, VK[fmt], multiplier=2, settings=st) == i, B.error()
+        p, c, _ = workloads.flow_pair(w, h, seed=500 + i)
+        prev.append(dev(convert(fmt, p)))
+        curr.append(dev(convert(fmt, c)))
+        outs.append(like(prev[-1]))
+        I = fg.Interpolator()
+        assert I.init(w, h, VK[fmt], settings=st), I.init_error()
+        I.begin_frame()
+        assert I.record_estimate(prev[i], curr[i])
+        o = like(prev[i])
+        assert I.record_synth(prev[i], curr[i], o, 0.5)
+        torch.cuda.synchronize()
+        ref.append(host(o))
+        I.close()
+    for shape in [(0, 0, 1, 1), (3, 1, 8, 1)]:
+        assert B.set_shape(*shape)
+        assert B.shape() == shape
+        for o in outs:
+            for x in (o if isinstance(o, tuple) else (o,)):
+                x.fill_(7)
+        assert B.record(prev, curr, outs), B.error()
+        torch.cuda.synchronize()
+        bad = [j for j, (o, r) in enumerate(zip(outs, ref)) if not same(host(o), r)]
+        assert not bad, f"shape {shape}: outputs {bad} differ"
 
 
 def test_rgba8_slot_against_the_oracle():

@@ -191,6 +191,23 @@ def test_hdr_4k_f16_linear():
     check_frames("f16_linear", a, c, [float(np.float32(1 / 3)), T23])
 
 
+@pytest.mark.parametrize("frac", [0.3, 1.0])
+def test_p010_off_grid_low_bits(frac):
+    """P010 samples whose low 6 bits are not zero (off the 10-bit code grid) in a share of the luma and chroma samples:
+    the synthesis filters a tap group of on-grid samples with integer arithmetic and any other group with the float
+    taps, and both must give the oracle's values"""
+    p, c, _ = workloads.flow_pair(200, 120, seed=17)
+    rng = np.random.default_rng(5)
+    frames = []
+    for f in (p, c):
+        y, uv = workloads.to_yuv(f, 10, "bt709", True)
+        for q in (y, uv):
+            hit = rng.random(q.shape) < frac
+            q[hit] |= rng.integers(1, 64, size=int(hit.sum())).astype(q.dtype)
+        frames.append((y, uv))
+    check_frames("p010_709_full", frames[0], frames[1], [0.5, 0.25])
+
+
 def test_format_refusals():
     """YUV frames need their CbCr plane; a bad YUV matrix is refused at init"""
     p, c, _ = workloads.flow_pair(64, 48, seed=1)
