@@ -29,7 +29,8 @@ import workloads_gpu  # noqa: E402
 VK = {"rgba8": fg.VK_R8G8B8A8_UNORM, "rgb10": fg.VK_A2B10G10R10_UNORM, "nv12": fg.VK_R8_UNORM,
       "p010": fg.VK_R16_UNORM}
 SHAPES = [(0, 0, 1, 0), (3, 1, 1, 0), (0, 0, 4, 0), (3, 1, 4, 0), (0, 0, 8, 0), (2, 1, 8, 0), (3, 0, 8, 0), (3, 1, 8, 0),
-          (0, 0, 1, 1), (3, 1, 1, 1), (0, 0, 8, 1), (3, 1, 8, 1)]   # Batch::tune's candidates, in its order
+          (0, 0, 1, 1), (3, 1, 1, 1), (0, 0, 8, 1), (3, 1, 8, 1), (0, 0, 8, 4), (3, 1, 8, 4), (0, 0, 8, 8),
+          (3, 1, 8, 8)]   # Batch::tune's candidates, in its order
 
 
 def slots():
@@ -122,7 +123,7 @@ def main():
         print(json.dumps({"workload": "mixed batch: 64 pairs, 34x720p / 17x1080p / 9x1440p / 4x2160p, Rgba8 / Rgb10 / "
                                       "Nv12 / P010, 2x / 3x / 4x", "ranks": n, "generated_frames": frames,
                           "generated_megapixels": round(px / 1e6, 1), "ms_per_batch": res,
-                          "shape_keys": "ctasPerSm_order_streams_mergeEstimates (ctasPerSm 0: one launch per synthesis; mergeEstimates 1: one launch per estimate pass for all slots)",
+                          "shape_keys": "ctasPerSm_order_streams_mergeEstimates (ctasPerSm 0: one launch per synthesis; mergeEstimates G: the estimates merged into one launch per pass for each of G groups of slots)",
                           "tuned_shape_rank0": "%d_%d_%d_%d" % SHAPES[best] if best >= 0 else None}), flush=True)
 
 

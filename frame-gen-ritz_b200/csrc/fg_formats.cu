@@ -250,6 +250,19 @@ __device__ __forceinline__ ITaps mkITaps(int X, int Y, int w, int h) {
     return t;
 }
 
+// the float taps of warpChroma (formats other than Nv12, and P010 samples off the 10-bit grid)
+template <int F>
+__device__ __forceinline__ float2 warpChromaF(const uint8_t* cbase, size_t cpitch, int W, int H, int X, int Y) {
+    const Taps t = mkTaps<6>(X - 16, Y - 16, (W + 1) >> 1, (H + 1) >> 1);
+    const float2 c00 = ctexel<F>(cbase, cpitch, t.x0, t.y0), c01 = ctexel<F>(cbase, cpitch, t.x1, t.y0);
+    const float2 c10 = ctexel<F>(cbase, cpitch, t.x0, t.y1), c11 = ctexel<F>(cbase, cpitch, t.x1, t.y1);
+    return make_float2(bil(t, c00.x, c01.x, c10.x, c11.x), bil(t, c00.y, c01.y, c10.y, c11.y));
+}
+// out of line: the rare off-grid P010 case keeps its registers out of the synthesis kernels' hot path
+__device__ __noinline__ float2 warpChromaP010Off(const uint8_t* cbase, size_t cpitch, int W, int H, int X, int Y) {
+    return warpChromaF<kFmtP010>(cbase, cpitch, W, H, X, Y);
+}
+
 // the chroma (Cb, Cr) levels warped to the point whose 1/32-px coordinates are (X, Y)
 template <int F>
 __device__ __forceinline__ float2 warpChroma(const uint8_t* cbase, size_t cpitch, int W, int H, int X, int Y) {
@@ -274,11 +287,16 @@ __device__ __forceinline__ float2 warpChroma(const uint8_t* cbase, size_t cpitch
             const uint32_t cr = (p00 >> 22) * w00 + (p01 >> 22) * w01 + (p10 >> 22) * w10 + (p11 >> 22) * w11;
             return make_float2(__fmul_rn(i2f((int)cb), 0x1p-14f), __fmul_rn(i2f((int)cr), 0x1p-14f));
         }
+        return warpChromaP010Off(cbase, cpitch, W, H, X, Y);
     }
-    const Taps t = mkTaps<6>(X - 16, Y - 16, (W + 1) >> 1, (H + 1) >> 1);
-    const float2 c00 = ctexel<F>(cbase, cpitch, t.x0, t.y0), c01 = ctexel<F>(cbase, cpitch, t.x1, t.y0);
-    const float2 c10 = ctexel<F>(cbase, cpitch, t.x0, t.y1), c11 = ctexel<F>(cbase, cpitch, t.x1, t.y1);
-    return make_float2(bil(t, c00.x, c01.x, c10.x, c11.x), bil(t, c00.y, c01.y, c10.y, c11.y));
+    return warpChromaF<F>(cbase, cpitch, W, H, X, Y);
+}
+
+// the float taps of a P010 luma sample off the 10-bit grid (out of line, as warpChromaP010Off)
+__device__ __noinline__ float warpYP010Off(const uint8_t* base, size_t pitch, int W, int H, int X, int Y) {
+    const Taps t = mkTaps<5>(X, Y, W, H);
+    auto v = [&](int x, int y) { return __fmul_rn(i2f((int)ldh(base, pitch, x, y)), 0x1p-8f); };
+    return bil(t, v(t.x0, t.y0), v(t.x1, t.y0), v(t.x0, t.y1), v(t.x1, t.y1));
 }
 
 // the warped sample at (px, py): Rgb10 RGB levels, F16 values, YUV (Y, Cb, Cr) levels
@@ -322,11 +340,13 @@ __device__ __forceinline__ void warp(const SynthParams& p, const uint8_t* base, 
             const uint32_t S = (s00 >> 6) * (t.w0 & 0xFFFFu) + (s01 >> 6) * (t.w0 >> 16) + (s10 >> 6) * (t.w1 & 0xFFFFu) +
                                (s11 >> 6) * (t.w1 >> 16);
             out[0] = __fmul_rn(i2f((int)S), 0x1p-12f);   // codes / 4 = the levels
-            const float2 c = warpChroma<F>(cbase, p.cpitch, p.W, p.H, X, Y);
-            out[1] = c.x;
-            out[2] = c.y;
-            return;
+        } else {
+            out[0] = warpYP010Off(base, p.pitch, p.W, p.H, X, Y);
         }
+        const float2 c = warpChroma<F>(cbase, p.cpitch, p.W, p.H, X, Y);
+        out[1] = c.x;
+        out[2] = c.y;
+        return;
     }
     const Taps t = mkTaps<5>(X, Y, p.W, p.H);
     float r00[3], r01[3], r10[3], r11[3];

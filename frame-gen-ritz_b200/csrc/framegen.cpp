@@ -1288,7 +1288,7 @@ struct Batch::Impl {
     // the fork / join pool of the slots' estimates
     static constexpr int kMaxStreams = 8;
     bool mergeable() const;   // no slot needs a per-slot estimate pass (UI protection, the seed net, profiling)
-    bool mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr);
+    bool mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr, const std::vector<int>& idx);
     cudaStream_t pool[kMaxStreams] = {};
     cudaEvent_t fork = nullptr, join[kMaxStreams] = {};
 
@@ -1348,7 +1348,7 @@ uint32_t Batch::synthsOf(uint32_t i) const { return i < m->mult.size() ? m->mult
 Interpolator* Batch::slot(uint32_t i) { return i < m->slots.size() ? m->slots[i].get() : nullptr; }
 Batch::Shape Batch::shape() const { return m->shape; }
 bool Batch::setShape(const Shape& s) {
-    if (s.ctasPerSm > 4 || s.order > 1 || s.streams < 1 || s.streams > (uint32_t)Impl::kMaxStreams || s.mergeEstimates > 1)
+    if (s.ctasPerSm > 4 || s.order > 1 || s.streams < 1 || s.streams > (uint32_t)Impl::kMaxStreams || s.mergeEstimates > 8)
         return false;
     m->shape = s;
     return true;
@@ -1414,9 +1414,10 @@ bool Batch::Impl::mergeable() const {
     return true;
 }
 
-bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr) {
-    const int ns = (int)slots.size();
-    for (int i = 0; i < ns; i++) {
+bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr, const std::vector<int>& idx) {
+    const int ns = (int)idx.size();
+    for (int j = 0; j < ns; j++) {
+        const int i = idx[j];
         slots[i]->beginFrame();
         const Interpolator::Impl& im = *slots[i]->m;
         if (!im.W || !im.frameOk(prev[i]) || !im.frameOk(curr[i]) || !im.samePitch(prev[i], curr[i])) {
@@ -1426,12 +1427,13 @@ bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame
     }
     std::vector<Interpolator::Impl::EstPlan> plans(ns);
     int maxTop = 0;
-    for (int i = 0; i < ns; i++) {
+    for (int j = 0; j < ns; j++) {
+        const int i = idx[j];
         Interpolator::Impl& im = *slots[i]->m;
         im.estSets++;
         im.haveEst = im.estUi = false;
-        im.planEstimate(prev[i], curr[i], false, plans[i]);
-        maxTop = std::max(maxTop, plans[i].top);
+        im.planEstimate(prev[i], curr[i], false, plans[j]);
+        maxTop = std::max(maxTop, plans[j].top);
     }
     auto fail = [&](cudaError_t e) {
         if (e == cudaSuccess) return false;
@@ -1441,26 +1443,27 @@ bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame
     };
     std::vector<fgk::LumaPyrParams> luma;
     std::vector<int> fmts;
-    for (int i = 0; i < ns; i++) {
-        luma.push_back(plans[i].luma);
+    for (int j = 0; j < ns; j++) {
+        const int i = idx[j];
+        luma.push_back(plans[j].luma);
         fmts.push_back((int)slots[i]->m->fmt);
     }
     if (fail(launchMergedGroups(luma, fmts, [&](fgk::Merged<fgk::LumaPyrParams>& mg, int f) {
             return f == (int)Format::Rgba8 ? fgk::launchLumaPyrMerged(mg, s) : fgk::launchLumaFmtMerged(mg, mg.item[0].f.format, s);
         })))
         return false;
-    for (int i = 0; i < ns; i++)
-        for (const fgk::DownParams& dp : plans[i].down)
+    for (int j = 0; j < ns; j++)
+        for (const fgk::DownParams& dp : plans[j].down)
             if (fail(fgk::launchDown(dp, s))) return false;
     for (int l = maxTop; l >= 0; l--) {
         std::vector<fgk::SearchParams> se;
         std::vector<fgk::Median3Params> me;
         std::vector<int> sk, mk;
-        for (int i = 0; i < ns; i++)
-            if (l <= plans[i].top) {
-                se.push_back(plans[i].search[l]);
+        for (int j = 0; j < ns; j++)
+            if (l <= plans[j].top) {
+                se.push_back(plans[j].search[l]);
                 sk.push_back(fgk::searchVariant(se.back()));
-                me.push_back(plans[i].med[l]);
+                me.push_back(plans[j].med[l]);
                 mk.push_back(fgk::median3Variant(me.back()));
             }
         if (fail(launchMergedGroups(se, sk, [&](fgk::Merged<fgk::SearchParams>& mg, int) { return fgk::launchSearchMerged(mg, s); })) ||
@@ -1469,17 +1472,19 @@ bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame
     }
     std::vector<fgk::SubpixParams> sub;
     std::vector<fgk::PixfieldParams> pix;
-    for (int i = 0; i < ns; i++) {
-        if (slots[i]->m->set.subpixel) sub.push_back(plans[i].sub);
-        else if (fail(fgk::launchCutMean(plans[i].cut, s))) return false;
-        pix.push_back(plans[i].pix);
+    for (int j = 0; j < ns; j++) {
+        const int i = idx[j];
+        if (slots[i]->m->set.subpixel) sub.push_back(plans[j].sub);
+        else if (fail(fgk::launchCutMean(plans[j].cut, s))) return false;
+        pix.push_back(plans[j].pix);
     }
     if (fail(launchMergedGroups(sub, std::vector<int>(sub.size(), 0),
                                 [&](fgk::Merged<fgk::SubpixParams>& mg, int) { return fgk::launchSubpixMerged(mg, s); })) ||
         fail(launchMergedGroups(pix, std::vector<int>(pix.size(), 0),
                                 [&](fgk::Merged<fgk::PixfieldParams>& mg, int) { return fgk::launchPixfieldMerged(mg, s); })))
         return false;
-    for (int i = 0; i < ns; i++) {
+    for (int j = 0; j < ns; j++) {
+        const int i = idx[j];
         Interpolator::Impl& im = *slots[i]->m;
         im.haveEst = true;
         im.estPrev = prev[i].data;
@@ -1496,33 +1501,48 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
     std::vector<int> first(ns);   // each slot's first output frame in outs
     for (int i = 0, o = 0; i < ns; i++) { first[i] = o; o += (int)m->mult[i] - 1; }
     const bool batched = m->shape.ctasPerSm > 0;
-    // 0. mergeEstimates: every slot's estimate as merged launches on s (when no slot needs a per-slot pass)
+    // 0. mergeEstimates = G: the slots' estimates as merged launches on s, in G groups (slots dealt by decreasing pair
+    //    size); each group's syntheses are forked off as soon as its estimates are recorded, so they overlap the next
+    //    group's estimates (merged only when no slot needs a per-slot estimate pass)
     const bool merged = m->shape.mergeEstimates && m->mergeable();
-    if (merged && !m->mergedEstimates(s, prev, curr)) return false;
-    // 1. every slot's estimate unless merged (and, for the slots outside the persistent launch, its syntheses), forked
-    //    over the pool: slot i on stream i % streams, joined back into s before the persistent launch
+    std::vector<std::vector<int>> groups(merged ? std::min<int>((int)m->shape.mergeEstimates, ns) : 1);
+    {
+        std::vector<int> order(ns);
+        std::iota(order.begin(), order.end(), 0);
+        if (merged)
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                return (size_t)m->slots[a]->m->W * m->slots[a]->m->H > (size_t)m->slots[b]->m->W * m->slots[b]->m->H;
+            });
+        for (int j = 0; j < ns; j++) groups[j % groups.size()].push_back(order[j]);
+    }
+    // 1. every slot's estimate (merged, or per slot on its pool stream) and, for the slots outside the persistent launch,
+    //    its syntheses, forked over the pool: slot i on stream i % streams, joined back into s before the persistent
+    //    launch
     const int nst = (int)std::min<uint32_t>(m->shape.streams, (uint32_t)Impl::kMaxStreams);
     auto streamOf = [&](int i) { return nst > 1 ? m->pool[i % nst] : s; };
-    if (nst > 1) {
-        if (cudaEventRecord(m->fork, s) != cudaSuccess) { m->err = cudaGetErrorString(cudaGetLastError()); return false; }
-        for (int k = 0; k < nst; k++)
-            if (cudaStreamWaitEvent(m->pool[k], m->fork, 0) != cudaSuccess) {
-                m->err = cudaGetErrorString(cudaGetLastError());
-                return false;
-            }
-    }
-    for (int i = 0; i < ns; i++) {
-        Interpolator& I = *m->slots[i];
-        if (!merged) {
-            I.beginFrame();
-            if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
+    for (const std::vector<int>& grp : groups) {
+        if (merged && !m->mergedEstimates(s, prev, curr, grp)) return false;
+        if (nst > 1) {
+            if (cudaEventRecord(m->fork, s) != cudaSuccess) { m->err = cudaGetErrorString(cudaGetLastError()); return false; }
+            for (int k = 0; k < nst; k++)
+                if (cudaStreamWaitEvent(m->pool[k], m->fork, 0) != cudaSuccess) {
+                    m->err = cudaGetErrorString(cudaGetLastError());
+                    return false;
+                }
         }
-        if (batched && I.m->fmt == Format::Rgba8) continue;
-        for (uint32_t k = 1; k < m->mult[i]; k++)
-            if (!I.recordSynth(streamOf(i), prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
-                m->err = "a slot's synthesis was refused (frames?)";
-                return false;
+        for (int i : grp) {
+            Interpolator& I = *m->slots[i];
+            if (!merged) {
+                I.beginFrame();
+                if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
             }
+            if (batched && I.m->fmt == Format::Rgba8) continue;
+            for (uint32_t k = 1; k < m->mult[i]; k++)
+                if (!I.recordSynth(streamOf(i), prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
+                    m->err = "a slot's synthesis was refused (frames?)";
+                    return false;
+                }
+        }
     }
     if (nst > 1)
         for (int k = 0; k < nst; k++)
@@ -1588,7 +1608,8 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
 
 int Batch::tune(cudaStream_t s, const Frame* prev, const Frame* curr, const Frame* outs, uint32_t reps) {
     static const Shape cand[] = {{0, 0, 1, 0}, {3, 1, 1, 0}, {0, 0, 4, 0}, {3, 1, 4, 0}, {0, 0, 8, 0}, {2, 1, 8, 0},
-                                 {3, 0, 8, 0}, {3, 1, 8, 0}, {0, 0, 1, 1}, {3, 1, 1, 1}, {0, 0, 8, 1}, {3, 1, 8, 1}};
+                                 {3, 0, 8, 0}, {3, 1, 8, 0}, {0, 0, 1, 1}, {3, 1, 1, 1}, {0, 0, 8, 1}, {3, 1, 8, 1},
+                                 {0, 0, 8, 4}, {3, 1, 8, 4}, {0, 0, 8, 8}, {3, 1, 8, 8}};
     DeviceGuard g(m->device);
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { cudaGetLastError(); return -1; }

@@ -296,9 +296,10 @@ public:
         uint32_t ctasPerSm = 3;   // CTAs per SM of the persistent synthesis launch; 0: one launch per synthesis
         uint32_t order = 1;       // work order: 0 the slots as added, 1 the largest syntheses first
         uint32_t streams = 8;     // the slots' estimates run on this many forked streams (1 = the caller's only)
-        uint32_t mergeEstimates = 0;   // 1: the slots' estimates as merged launches, one per pass and level for all
-                                       // slots, on the caller's stream (slots with UI protection, a seed net or
-                                       // profiling make the batch fall back to per-slot estimates)
+        uint32_t mergeEstimates = 0;   // G = 1..8: the slots' estimates as merged launches (one per pass and level
+                                       // for all slots of a group) on the caller's stream, in G groups whose
+                                       // syntheses start as soon as the group's estimates are recorded; 0: per slot
+                                       // (slots with UI protection, a seed net or profiling fall back to per slot)
     };
     Batch();
     ~Batch();
