@@ -123,11 +123,21 @@ __device__ __forceinline__ float levelOf(const FmtConst& f, float r) {
 
 // ============================================================================================== luma
 // the motion estimate's luma of pixel (x, y) in quarter levels (luma.comp:9-27, format.glsl fgLuma)
+// pq: linear RgbaF16's table of fmtPq255 by half bits (the same function, evaluated once per value), or null
 template <int F>
-__device__ __forceinline__ int lumaQ(const FmtConst& f, const uint8_t* base, size_t pitch, int x, int y) {
+__device__ __forceinline__ int lumaQ(const FmtConst& f, const uint8_t* base, size_t pitch, int x, int y, const float* pq) {
     float r[3];
-    texel<F>(f, base, pitch, x, y, r);
     float yl;
+    if (F == kFmtF16 && pq) {   // the three channels' PQ levels looked up by their bits
+        const uint2 q = __ldg(reinterpret_cast<const uint2*>(base + (size_t)y * pitch) + x);
+        const float lr = __ldg(pq + (q.x & 0xFFFFu)), lg = __ldg(pq + (q.x >> 16)), lb = __ldg(pq + (q.y & 0xFFFFu));
+        float d = __fmul_rn(4899.0f, lr);
+        d = __fadd_rn(d, __fmul_rn(9617.0f, lg));
+        d = __fadd_rn(d, __fmul_rn(1868.0f, lb));
+        yl = __fmul_rn(d, 1.0f / 16384.0f);
+        return __float2int_rn(__fmul_rn(clampF(yl, 0.0f, 255.0f), 4.0f));
+    }
+    texel<F>(f, base, pitch, x, y, r);
     if (F == kFmtNv12 || F == kFmtP010) {
         yl = __fmul_rn(__fsub_rn(r[0], f.black), f.ys);
     } else {
@@ -165,8 +175,8 @@ __device__ __forceinline__ void lumaFmtCta(const LumaPyrParams& p, int bx, int b
                 for (int k = 0; k < fs; k++) {
                     const int xx = x * fs + k;
                     if (xx >= p.W) break;
-                    sa += lumaQ<F>(p.f, p.a, p.pitch, xx, yy);
-                    sc += lumaQ<F>(p.f, p.c, p.pitch, xx, yy);
+                    sa += lumaQ<F>(p.f, p.a, p.pitch, xx, yy, p.pq);
+                    sc += lumaQ<F>(p.f, p.c, p.pitch, xx, yy, p.pq);
                     n++;
                 }
             }
@@ -588,6 +598,37 @@ __global__ void __launch_bounds__(kSyThreads, 3) k_synth_fmt(const SynthParams p
     synthFmtTile<F, true>(p, blockIdx.x, blockIdx.y, store);
 }
 
+// Many syntheses of one format in one persistent launch (as k_synth_batch for 8-bit RGBA): every CTA takes the next
+// tile of the work list from an atomic counter until the list is exhausted; an item's parameters are staged in shared
+// memory per tile.
+template <int F>
+__global__ void __launch_bounds__(kSyThreads, 3) k_synth_fmt_batch(const SynthBatchArgs b) {
+    pdlEnter();
+    __shared__ int work, item;
+    __shared__ __align__(16) SynthParams sp;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            work = (int)atomicAdd(b.counter, 1u);
+            int lo = 0, hi = b.nItems - 1;   // the item whose tile range holds `work`
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (b.tileStart[mid] <= work) lo = mid; else hi = mid - 1;
+            }
+            item = lo;
+        }
+        __syncthreads();
+        const int w = work, it = item;
+        if (w >= b.total) break;
+        for (int i = threadIdx.x; i < (int)(sizeof(SynthParams) / 4); i += kSyThreads)
+            reinterpret_cast<uint32_t*>(&sp)[i] = __ldg(reinterpret_cast<const uint32_t*>(b.items + it) + i);
+        __syncthreads();
+        const int t = w - b.tileStart[it], tx = b.tilesX[it];
+        FmtStore<F> store{sp};
+        synthFmtTile<F, true>(sp, t % tx, t / tx, store);
+        __syncthreads();   // the tile's shared memory is free again
+    }
+}
+
 // ============================================================================================== motion blur
 // recordSynthBlur in the other formats (gpu/framegen.h:553-573): the weighted average of n sub-frames, each the
 // values recordSynth(t_k) stores, rounded once. Integer formats (Rgb10 codes, Nv12 / P010 luma and chroma codes):
@@ -749,10 +790,8 @@ __global__ void __launch_bounds__(kSyThreads, 1) k_synth_blur_fmt(const BlurPara
 
 // interp.py:238-239 for the other formats: more than globalFallback of the pixels untrusted -> the nearer real frame
 // (both planes of YUV) over the output. Every CTA exits at once in the normal case; clears the next synth's counter.
-__global__ void __launch_bounds__(256) k_fallback_fmt(const FallbackParams p) {
-    pdlEnter();
+__device__ __forceinline__ void fallbackFmtCta(const FallbackParams& p) {
     const unsigned int cnt = *p.untrusted;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *p.untrustedNext = 0;
     if (!((double)cnt / ((double)p.W * (double)p.H) > p.frac)) return;
     const uint8_t* n = p.nearC ? p.c : p.a;
     const size_t stride = (size_t)gridDim.x * 256;
@@ -771,6 +810,18 @@ __global__ void __launch_bounds__(256) k_fallback_fmt(const FallbackParams p) {
     }
 }
 
+__global__ void __launch_bounds__(256) k_fallback_fmt(const FallbackParams p) {
+    pdlEnter();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *p.untrustedNext = 0;
+    fallbackFmtCta(p);
+}
+// the untrusted-share decision of many syntheses of the other formats (grid.y = item; the item counters are zeroed by
+// the host before the batch's synthesis launch)
+__global__ void __launch_bounds__(256) k_fallback_fmt_batch(const FallbackParams* __restrict__ items) {
+    pdlEnter();
+    fallbackFmtCta(items[blockIdx.y]);
+}
+
 // ============================================================================================== launchers
 // the dynamic shared memory of a format synthesis: synthSmemBytes + the blend inputs of the output pixels
 static size_t fmtSynthSmem(int format, int fs) {
@@ -786,6 +837,10 @@ cudaError_t prepareFormatKernels() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -822,6 +877,15 @@ cudaError_t launchLumaFmtMerged(Merged<LumaPyrParams>& m, int format, cudaStream
     }
 }
 
+__global__ void __launch_bounds__(256) k_pq_table(float* tab, float kWhite) {
+    const int i = blockIdx.x * 256 + threadIdx.x;   // the half's bits
+    tab[i] = fmtPq255(h2f((uint32_t)i), kWhite);
+}
+cudaError_t launchPqTable(float* tab, float kWhite, cudaStream_t s) {
+    k_pq_table<<<65536 / 256, 256, 0, s>>>(tab, kWhite);
+    return cudaGetLastError();
+}
+
 cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
     const dim3 grid(divUp(p.W, kSyT), divUp(p.H, kSyTH));
     const size_t smem = fmtSynthSmem(p.f.format, p.fs);
@@ -832,6 +896,38 @@ cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
         case kFmtP010: return launchPdl(k_synth_fmt<kFmtP010>, grid, dim3(kSyThreads), smem, s, p);
         default: return cudaErrorInvalidValue;
     }
+}
+
+size_t synthFmtKernelSmem(int format, int fs) { return fmtSynthSmem(format, fs); }
+template <int F>
+static int fmtBatchOcc(size_t smem) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_synth_fmt_batch<F>, kSyThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ;
+}
+int synthFmtBatchCtasPerSm(int format, size_t smem) {
+    switch (format) {
+        case kFmtRgb10: return fmtBatchOcc<kFmtRgb10>(smem);
+        case kFmtF16: return fmtBatchOcc<kFmtF16>(smem);
+        case kFmtNv12: return fmtBatchOcc<kFmtNv12>(smem);
+        case kFmtP010: return fmtBatchOcc<kFmtP010>(smem);
+        default: return 0;
+    }
+}
+cudaError_t launchSynthFmtBatch(const SynthBatchArgs& b, int format, int grid, size_t smem, cudaStream_t s) {
+    switch (format) {
+        case kFmtRgb10: return launchPdl(k_synth_fmt_batch<kFmtRgb10>, dim3(grid), dim3(kSyThreads), smem, s, b);
+        case kFmtF16: return launchPdl(k_synth_fmt_batch<kFmtF16>, dim3(grid), dim3(kSyThreads), smem, s, b);
+        case kFmtNv12: return launchPdl(k_synth_fmt_batch<kFmtNv12>, dim3(grid), dim3(kSyThreads), smem, s, b);
+        case kFmtP010: return launchPdl(k_synth_fmt_batch<kFmtP010>, dim3(grid), dim3(kSyThreads), smem, s, b);
+        default: return cudaErrorInvalidValue;
+    }
+}
+cudaError_t launchFallbackFmtBatch(const FallbackParams* items, int nItems, cudaStream_t s) {
+    return launchPdl(k_fallback_fmt_batch, dim3(smCount(), nItems), dim3(256), 0, s, items);
 }
 
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s) {

@@ -1479,6 +1479,7 @@ __global__ void __launch_bounds__(kSyThreads, 3) k_synth_batch(const SynthBatchA
 // the untrusted-share decision of many syntheses (grid.y = item), the batched k_fallback (the item counters are
 // zeroed by the host before the batch's synth launch)
 __global__ void __launch_bounds__(256) k_fallback_batch(const FallbackParams* __restrict__ items) {
+    pdlEnter();   // the counters are complete only when the synthesis launch is
     const FallbackParams& p = items[blockIdx.y];
     const unsigned int cnt = *p.untrusted;
     if (!((double)cnt / ((double)p.W * (double)p.H) > p.frac)) return;

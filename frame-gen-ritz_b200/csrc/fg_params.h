@@ -48,6 +48,7 @@ struct LumaPyrParams {
     int ri, gi, bi;        // byte offsets of R, G, B in a 4-byte pixel
     int nlev;              // levels written here (<= kPyrInKernel)
     int vec16;             // flowScale 2 with 16-byte aligned frames and rows: the uint4 path
+    const float* pq;       // RgbaF16 linear: the PQ level (fmtPq255) of every half value, indexed by its bits, or null
     int lw[kPyrInKernel], lh[kPyrInKernel];
     float* la[kPyrInKernel];
     float* lc[kPyrInKernel];
@@ -237,7 +238,14 @@ int synthTilesY(int H);
 // the other formats (fg_formats.cu)
 cudaError_t prepareFormatKernels();
 cudaError_t launchLumaFmt(const LumaPyrParams& p, cudaStream_t s);
+// the PQ level of every half value (65536 floats) for a linear RgbaF16 luma at this white level
+cudaError_t launchPqTable(float* tab, float kWhite, cudaStream_t s);
 cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s);
+// many syntheses of one of the other formats in one persistent launch (as launchSynthBatch), and their fallbacks
+cudaError_t launchSynthFmtBatch(const SynthBatchArgs& b, int format, int grid, size_t smem, cudaStream_t s);
+int synthFmtBatchCtasPerSm(int format, size_t smem);
+size_t synthFmtKernelSmem(int format, int fs);   // k_synth_fmt's / k_synth_fmt_batch's dynamic shared memory
+cudaError_t launchFallbackFmtBatch(const FallbackParams* items, int nItems, cudaStream_t s);
 // one pass of a motion blur in the other formats (bp.base.f.format): the main pass (fix = 0), then the fix-up
 cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s);
 cudaError_t launchFallbackFmt(const FallbackParams& p, cudaStream_t s);

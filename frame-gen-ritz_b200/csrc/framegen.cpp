@@ -218,6 +218,7 @@ struct Interpolator::Impl {
     char* arena = nullptr;
     size_t arenaBytes = 0;
     float* luma = nullptr;
+    float* pqTab = nullptr;   // linear RgbaF16: the PQ level of every half value (the luma pass looks them up)
     float2* field = nullptr;
     float* sads = nullptr;
     float2* pf = nullptr;
@@ -430,6 +431,7 @@ struct Interpolator::Impl {
         freeSeedNet();
         if (arena) cudaFree(arena);
         arena = nullptr;
+        pqTab = nullptr;
         arenaBytes = 0;
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         events.clear();
@@ -466,6 +468,8 @@ struct Interpolator::Impl {
         const size_t oDepth = take(P.depthStart.size() * 4 + 4);
         const size_t oVals = take((P.leaves.size() + P.inner.size()) * 4);
         const size_t oLeafOf = take((size_t)nb0 * 4), oLeafCnt = take(P.leaves.size() * 4), oLeafS = take(P.leaves.size() * 4);
+        const bool pqLuma = fmt == Format::RgbaF16 && fc.linear;
+        const size_t oPq = take(pqLuma ? (size_t)65536 * 4 : 0);
         if (cudaMalloc(&arena, off) != cudaSuccess) { arena = nullptr; cudaGetLastError(); return kErrAlloc; }
         arenaBytes = off;
         cudaMemset(arena, 0, off);
@@ -477,6 +481,8 @@ struct Interpolator::Impl {
         st = (fgk::DevState*)(arena + oSt);
         blurCnt = (unsigned int*)(arena + oBlur);
         emap = (uint8_t*)(arena + oEmap);
+        pqTab = pqLuma ? (float*)(arena + oPq) : nullptr;
+        if (pqTab) fgk::launchPqTable(pqTab, fc.kWhite, 0);
         cudaMemcpy(arena + oLeaves, P.leaves.data(), P.leaves.size() * 8, cudaMemcpyHostToDevice);
         if (!P.inner.empty()) cudaMemcpy(arena + oInner, P.inner.data(), P.inner.size() * 8, cudaMemcpyHostToDevice);
         cudaMemcpy(arena + oDepth, P.depthStart.data(), P.depthStart.size() * 4, cudaMemcpyHostToDevice);
@@ -564,6 +570,7 @@ struct Interpolator::Impl {
         e.top = snK >= 0 ? snK : n - 1;
         lp.nlev = std::min(e.top + 1, fgk::kPyrInKernel);
         lp.f = fc;
+        lp.pq = pqTab;
         lp.vec16 = fmt == Format::Rgba8 && set.flowScale == 2 && prev.pitch % 16 == 0 && ((uintptr_t)prev.data & 15) == 0 && ((uintptr_t)curr.data & 15) == 0 &&
                    W % 4 == 0 && H % 2 == 0;   // complete 2x2 cells in every full tile, 8-byte aligned level-0 rows
         for (int l = 0; l < lp.nlev; l++) {
@@ -1273,6 +1280,7 @@ bool Interpolator::recordTrace(cudaStream_t stream, void* dst) {
 // ================================================================================================== batches
 struct Batch::Impl {
     static constexpr int kRing = 8;   // pinned upload buffers: at most this many records in flight
+    static constexpr int kFormats = 5;   // persistent synthesis launches: at most one per frame format
     std::vector<std::unique_ptr<Interpolator>> slots;
     std::vector<uint32_t> mult;
     Shape shape;
@@ -1281,7 +1289,7 @@ struct Batch::Impl {
     int maxItems = 0;
     // the work list on the device, one blob: items, fallbacks, tile starts, tiles across; then the counters
     char* dev = nullptr;
-    unsigned int* counters = nullptr;   // maxItems per-item untrusted counters + the work counter
+    unsigned int* counters = nullptr;   // maxItems per-item untrusted counters + a work counter per format
     size_t oFall = 0, oStart = 0, oTx = 0, blobBytes = 0;
     char* host = nullptr;               // kRing x blobBytes, pinned
     int ring = 0;
@@ -1329,7 +1337,7 @@ struct Batch::Impl {
         oStart = alignUp(oFall + n * sizeof(fgk::FallbackParams), 256);
         oTx = alignUp(oStart + (n + 1) * 4, 256);
         blobBytes = alignUp(oTx + n * 4, 256);
-        if (cudaMalloc(&dev, blobBytes + (n + 1) * 4) != cudaSuccess ||
+        if (cudaMalloc(&dev, blobBytes + (n + kFormats) * 4) != cudaSuccess ||
             cudaMallocHost(&host, blobBytes * kRing) != cudaSuccess) {
             cudaGetLastError();
             release();
@@ -1536,7 +1544,7 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
                 I.beginFrame();
                 if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
             }
-            if (batched && I.m->fmt == Format::Rgba8) continue;
+            if (batched) continue;   // in the persistent launches
             for (uint32_t k = 1; k < m->mult[i]; k++)
                 if (!I.recordSynth(streamOf(i), prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
                     m->err = "a slot's synthesis was refused (frames?)";
@@ -1550,58 +1558,74 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
                 m->err = cudaGetErrorString(cudaGetLastError());
                 return false;
             }
-    // 2. the work list of the 8-bit RGBA syntheses
-    struct Item { int slot, k, tiles; };
+    // 2. the work lists of the syntheses: one persistent launch per frame format (its items contiguous in the blob,
+    //    each format's tile starts counted from 0, its own work counter after the items' untrusted counters), then
+    //    the fallbacks of each format in one launch
+    struct Item { int slot, k, tiles, fmt; };
     std::vector<Item> items;
     for (int i = 0; i < ns && batched; i++) {
         const Interpolator::Impl* im = m->slots[i]->m;
-        if (im->fmt != Format::Rgba8) continue;
         const int tiles = fgk::synthTilesX((int)im->W) * fgk::synthTilesY((int)im->H);
-        for (uint32_t k = 1; k < m->mult[i]; k++) items.push_back({i, (int)k, tiles});
+        for (uint32_t k = 1; k < m->mult[i]; k++) items.push_back({i, (int)k, tiles, (int)im->fmt});
     }
-    if (m->shape.order == 1)
-        std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.tiles > y.tiles; });
+    std::stable_sort(items.begin(), items.end(), [&](const Item& x, const Item& y) {
+        return x.fmt != y.fmt ? x.fmt < y.fmt : (m->shape.order == 1 && x.tiles > y.tiles);
+    });
     const int n = (int)items.size();
-    if (n) {
-        char* blob = m->host + (size_t)m->ring * m->blobBytes;
-        m->ring = (m->ring + 1) % Impl::kRing;
-        fgk::SynthParams* sp = (fgk::SynthParams*)blob;
-        fgk::FallbackParams* fp = (fgk::FallbackParams*)(blob + m->oFall);
-        int* start = (int*)(blob + m->oStart);
-        int* tx = (int*)(blob + m->oTx);
-        size_t smem = 0;
-        int total = 0;
-        for (int j = 0; j < n; j++) {
-            const Item& it = items[j];
-            const Interpolator::Impl* im = m->slots[it.slot]->m;
-            const Frame& out = outs[first[it.slot] + it.k - 1];
-            if (!im->frameOk(out)) { m->err = "an output frame does not fit its slot"; return false; }
-            const float t = (float)it.k / (float)m->mult[it.slot];
-            sp[j] = im->synthParams(prev[it.slot], curr[it.slot], out, t, m->counters + j);
-            sp[j].emap = nullptr;
-            fp[j] = im->fallbackParams(sp[j], nullptr);
-            start[j] = total;
-            tx[j] = fgk::synthTilesX((int)im->W);
-            total += it.tiles;
-            smem = std::max(smem, fgk::synthKernelSmem((int)im->set.flowScale));
-        }
-        start[n] = total;
+    if (!n) return true;
+    char* blob = m->host + (size_t)m->ring * m->blobBytes;
+    m->ring = (m->ring + 1) % Impl::kRing;
+    fgk::SynthParams* sp = (fgk::SynthParams*)blob;
+    fgk::FallbackParams* fp = (fgk::FallbackParams*)(blob + m->oFall);
+    int* start = (int*)(blob + m->oStart);
+    int* tx = (int*)(blob + m->oTx);
+    struct Segment { int first, count, total, fmt; size_t smem; };
+    std::vector<Segment> segs;
+    for (int j = 0; j < n; j++) {
+        const Item& it = items[j];
+        const Interpolator::Impl* im = m->slots[it.slot]->m;
+        const Frame& out = outs[first[it.slot] + it.k - 1];
+        if (!im->frameOk(out)) { m->err = "an output frame does not fit its slot"; return false; }
+        if (segs.empty() || segs.back().fmt != it.fmt) segs.push_back({j, 0, 0, it.fmt, 0});
+        Segment& g = segs.back();
+        const float t = (float)it.k / (float)m->mult[it.slot];
+        sp[j] = im->synthParams(prev[it.slot], curr[it.slot], out, t, m->counters + j);
+        sp[j].emap = nullptr;
+        fp[j] = im->fallbackParams(sp[j], nullptr);
+        start[j] = g.total;
+        tx[j] = fgk::synthTilesX((int)im->W);
+        g.total += it.tiles;
+        g.count++;
+        g.smem = std::max(g.smem, it.fmt == (int)Format::Rgba8 ? fgk::synthKernelSmem((int)im->set.flowScale)
+                                                               : fgk::synthFmtKernelSmem(sp[j].f.format, (int)im->set.flowScale));
+    }
+    if (cudaMemcpyAsync(m->dev, blob, m->blobBytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemsetAsync(m->counters, 0, (size_t)(n + Impl::kFormats) * 4, s) != cudaSuccess) {
+        m->err = cudaGetErrorString(cudaGetLastError());
+        return false;
+    }
+    const fgk::SynthParams* dItems = (const fgk::SynthParams*)m->dev;
+    const fgk::FallbackParams* dFall = (const fgk::FallbackParams*)(m->dev + m->oFall);
+    for (size_t g = 0; g < segs.size(); g++) {
+        const Segment& sg = segs[g];
         fgk::SynthBatchArgs a{};
-        a.items = (const fgk::SynthParams*)m->dev;
-        a.tileStart = (const int*)(m->dev + m->oStart);
-        a.tilesX = (const int*)(m->dev + m->oTx);
-        a.nItems = n;
-        a.total = total;
-        a.counter = m->counters + n;
-        const int occ = fgk::synthBatchCtasPerSm(smem);
-        const int grid = m->sms * std::max(1, std::min((int)m->shape.ctasPerSm, occ));
-        if (cudaMemcpyAsync(m->dev, blob, m->blobBytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-            cudaMemsetAsync(m->counters, 0, (size_t)(n + 1) * 4, s) != cudaSuccess ||
-            fgk::launchSynthBatch(a, std::min(grid, total), smem, s) != cudaSuccess ||
-            fgk::launchFallbackBatch((const fgk::FallbackParams*)(m->dev + m->oFall), n, s) != cudaSuccess) {
-            m->err = cudaGetErrorString(cudaGetLastError());
-            return false;
-        }
+        a.items = dItems + sg.first;
+        a.tileStart = (const int*)(m->dev + m->oStart) + sg.first;
+        a.tilesX = (const int*)(m->dev + m->oTx) + sg.first;
+        a.nItems = sg.count;
+        a.total = sg.total;
+        a.counter = m->counters + n + g;
+        const bool rgba = sg.fmt == (int)Format::Rgba8;
+        const int fmtK = rgba ? 0 : sp[sg.first].f.format;
+        const int occ = rgba ? fgk::synthBatchCtasPerSm(sg.smem) : fgk::synthFmtBatchCtasPerSm(fmtK, sg.smem);
+        const int grid = std::min(m->sms * std::max(1, std::min((int)m->shape.ctasPerSm, occ)), sg.total);
+        const cudaError_t e = rgba ? fgk::launchSynthBatch(a, grid, sg.smem, s) : fgk::launchSynthFmtBatch(a, fmtK, grid, sg.smem, s);
+        if (e != cudaSuccess) { cudaGetLastError(); m->err = cudaGetErrorString(e); return false; }
+    }
+    for (const Segment& sg : segs) {
+        const cudaError_t e = sg.fmt == (int)Format::Rgba8 ? fgk::launchFallbackBatch(dFall + sg.first, sg.count, s)
+                                                           : fgk::launchFallbackFmtBatch(dFall + sg.first, sg.count, s);
+        if (e != cudaSuccess) { cudaGetLastError(); m->err = cudaGetErrorString(e); return false; }
     }
     return true;
 }

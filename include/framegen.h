@@ -282,10 +282,11 @@ private:
 
 // B200-build extension (no counterpart in the reference): many frame pairs of any sizes and formats recorded
 // together, one Interpolator per pair ("slot"). record() records every slot's estimate as recordEstimate does; the
-// syntheses of all 8-bit RGBA slots and times then run in ONE persistent launch whose CTAs take output tiles from a
-// shared work counter (mixed sizes balance across the SMs) and their whole-frame fallbacks in one more launch; slots
-// of the other formats record their syntheses one by one. The slots' estimate chains (small, launch-latency bound
-// passes) are forked onto a pool of streams (events join them back), so independent slots overlap on the GPU. A slot of multiplier m gets the generated frames at
+// syntheses of all slots and times then run in one persistent launch per frame format whose CTAs take output tiles
+// from a shared work counter (mixed sizes balance across the SMs) and their whole-frame fallbacks in one more launch
+// per format (or one launch per synthesis: Shape::ctasPerSm = 0). The slots' estimate chains (small,
+// launch-latency bound passes) are forked onto a pool of streams (events join them back), so independent slots
+// overlap on the GPU, or merged into one launch per pass (Shape::mergeEstimates). A slot of multiplier m gets the generated frames at
 // t = k/m, k = 1 .. m-1 (outs: each slot's m - 1 output frames, slots in order). Records allocate nothing and can be
 // captured in a CUDA graph; their small parameter upload goes through a ring of 8 pinned buffers, so at most 8 records
 // may be in flight. tune() times the candidate launch shapes on the device (synchronising the stream) and keeps the
@@ -293,7 +294,7 @@ private:
 class Batch {
 public:
     struct Shape {
-        uint32_t ctasPerSm = 3;   // CTAs per SM of the persistent synthesis launch; 0: one launch per synthesis
+        uint32_t ctasPerSm = 3;   // CTAs per SM of the persistent synthesis launches; 0: one launch per synthesis
         uint32_t order = 1;       // work order: 0 the slots as added, 1 the largest syntheses first
         uint32_t streams = 8;     // the slots' estimates run on this many forked streams (1 = the caller's only)
         uint32_t mergeEstimates = 0;   // G = 1..8: the slots' estimates as merged launches (one per pass and level

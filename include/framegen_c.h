@@ -141,8 +141,8 @@ int fg_record_trace(fg_interpolator* fg, void* stream, void* dst);              
 const char* fg_last_error(const fg_interpolator* fg);   /* the last CUDA error a record met (null if none) */
 
 /* Batches -- no counterpart in the reference (B200-build extension; framegen::Batch in include/framegen.h): many
- * frame pairs of any sizes and formats recorded together, one interpolator per slot; the 8-bit RGBA syntheses of all
- * slots run in one persistent launch. fg_batch_add: the slot's init info and multiplier m (t = k/m, k = 1 .. m-1);
+ * frame pairs of any sizes and formats recorded together, one interpolator per slot; the syntheses of all slots run
+ * in one persistent launch per frame format. fg_batch_add: the slot's init info and multiplier m (t = k/m, k = 1 .. m-1);
  * returns its index or -1. fg_batch_record: prev[i], curr[i] per slot and outs = every slot's m - 1 output frames,
  * slots in order. fg_batch_tune: times the launch shapes on these frames (synchronises the stream), keeps the
  * fastest, returns its index (-1 on failure). */

@@ -180,6 +180,44 @@ def test_merged_estimates_mixed_settings():
         assert not bad, f"shape {shape}: outputs {bad} differ"
 
 
+@pytest.mark.parametrize("shape", [(3, 1, 8), (0, 0, 1), (3, 1, 1, 1), (0, 0, 8, 2)])
+def test_batch_whole_frame_fallbacks(shape):
+    """every synthesis flicks (a tiny globalFallback with a steep trust ramp): the batch's fallback launches must see
+    the complete untrusted counts of their syntheses and copy the nearer frame, as standalone Interpolators do"""
+    st = fg.Settings(globalFallback=1e-6, trustLow=0.0, trustHigh=0.5)
+    slots = [(160, 96, "rgba8", 3), (320, 180, "rgb10", 2), (200, 120, "nv12", 4), (128, 96, "p010", 2),
+             (320, 180, "rgba8", 4), (96, 64, "rgba8", 2)]
+    B = fg.Batch()
+    prev, curr, outs, ref, near = [], [], [], [], []
+    for i, (w, h, fmt, m) in enumerate(slots):
+        assert B.add(w, h, VK[fmt], multiplier=m, settings=st) == i, B.error()
+        p, c, _ = workloads.flow_pair(w, h, seed=900 + i)
+        prev.append(dev(convert(fmt, p)))
+        curr.append(dev(convert(fmt, c)))
+        I = fg.Interpolator()
+        assert I.init(w, h, VK[fmt], settings=st), I.init_error()
+        I.begin_frame()
+        assert I.record_estimate(prev[i], curr[i])
+        for t in fg.Batch.times(m):
+            outs.append(like(prev[i]))
+            o = like(prev[i])
+            assert I.record_synth(prev[i], curr[i], o, t)
+            torch.cuda.synchronize()
+            ref.append(host(o))
+            near.append(host(curr[i] if t > 0.5 else prev[i]))
+        I.close()
+    assert sum(same(r, n) for r, n in zip(ref, near)) >= len(ref) // 2, "the settings should make the syntheses flick"
+    assert B.set_shape(*shape)
+    for _ in range(2):
+        for o in outs:
+            for x in (o if isinstance(o, tuple) else (o,)):
+                x.fill_(7)
+        assert B.record(prev, curr, outs), B.error()
+        torch.cuda.synchronize()
+        bad = [j for j, (o, r) in enumerate(zip(outs, ref)) if not same(host(o), r)]
+        assert not bad, f"shape {shape}: outputs {bad} differ"
+
+
 def test_rgba8_slot_against_the_oracle():
     """one batched 8-bit RGBA slot straight against the oracle (interp.py's restatement)"""
     p, c, _ = workloads.flow_pair(320, 180, seed=99)
