@@ -184,7 +184,8 @@ def test_merged_estimates_mixed_settings():
 def test_batch_whole_frame_fallbacks(shape):
     """every synthesis flicks (a tiny globalFallback with a steep trust ramp): the batch's fallback launches must see
     the complete untrusted counts of their syntheses and copy the nearer frame, as standalone Interpolators do"""
-    st = fg.Settings(globalFallback=1e-6, trustLow=0.0, trustHigh=0.5)
+    st = fg.Settings(globalFallback=1e-6, trustLow=0.0, trustHigh=1.0)
+    assert fg.validate(st)
     slots = [(160, 96, "rgba8", 3), (320, 180, "rgb10", 2), (200, 120, "nv12", 4), (128, 96, "p010", 2),
              (320, 180, "rgba8", 4), (96, 64, "rgba8", 2)]
     B = fg.Batch()
