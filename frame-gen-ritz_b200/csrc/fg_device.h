@@ -109,6 +109,15 @@ __device__ __forceinline__ bool uiHitMask(const uint32_t* __restrict__ m, int X,
     return false;
 }
 
+// is the frame pixel (x, y) a UI pixel of the mask (header + bytes)?
+__device__ __forceinline__ bool uiPx(const uint32_t* __restrict__ m, int x, int y) {
+    const uint32_t o = __ldg(m + 1), wh = __ldg(m + 2);
+    x -= (int)(o & 0xFFFFu);
+    y -= (int)(o >> 16);
+    if (x < 0 || y < 0 || x >= (int)(wh & 0xFFFFu) || y >= (int)(wh >> 16)) return false;
+    return ((__ldg(m + kUiMaskHeader + y * (int)__ldg(m + 3) + (x >> 2)) >> (8 * (x & 3))) & 255u) != 0u;
+}
+
 __device__ __forceinline__ float2 rne32bits(float2 v) {
     return __ffma2_rn(v, make_float2(32.0f, 32.0f), make_float2(12582912.0f, 12582912.0f));
 }

@@ -445,7 +445,9 @@ __device__ __forceinline__ void copyNear(const SynthParams& p, int x, int y) {
 // YUV (codes; chroma for even-even pixels only); k is the thread's region-row slot. kCut: under a scene cut the tile is
 // a copy of the nearer frame (and the core returns); without kCut the caller has taken the cut into account. The
 // untrusted count goes to *p.untrusted unless that is null.
-template <int F, bool kCut, class Sink>
+// kUi (Rgb10 / RgbaF16): CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl): a tap whose bilinear
+// footprint touches its own frame's UI mask (p.uiA / p.uiC) takes the other frame's tap (both or neither: kept)
+template <int F, bool kCut, bool kUi = false, class Sink>
 __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int by, Sink& sink) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ SyCoef rowc[kSyEH];
@@ -479,8 +481,22 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
         const SyCoef cy = rowc[ey];
         const float2 h = syHalfVec(cy, hrow, ex);
         float wa[3], wc[3];
-        warp<F>(p, p.a, p.ac, __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), __fsub_rn(cy.pos, __fmul_rn(kA, h.y)), wa);
-        warp<F>(p, p.c, p.cc, __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), __fadd_rn(cy.pos, __fmul_rn(kC, h.y)), wc);
+        const float pax = __fsub_rn(cx.pos, __fmul_rn(kA, h.x)), pay = __fsub_rn(cy.pos, __fmul_rn(kA, h.y));
+        const float pcx = __fadd_rn(cx.pos, __fmul_rn(kC, h.x)), pcy = __fadd_rn(cy.pos, __fmul_rn(kC, h.y));
+        warp<F>(p, p.a, p.ac, pax, pay, wa);
+        warp<F>(p, p.c, p.cc, pcx, pcy, wc);
+        if (kUi) {
+            static_assert(!kUi || F == kFmtRgb10 || F == kFmtF16, "the tap rejection is built for the RGB formats");
+            const bool ha = p.uiA && uiHitMask(p.uiA, rne32(pax), rne32(pay));
+            const bool hc = p.uiC && uiHitMask(p.uiC, rne32(pcx), rne32(pcy));
+            if (ha != hc) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    if (ha) wa[c] = wc[c];
+                    else wc[c] = wa[c];
+                }
+            }
+        }
         e[ey * kSyES + ex] = (uint8_t)mismatch<F>(p.f, wa, wc);
         const int ly = ey - kSyAp;
         if ((unsigned)ly < (unsigned)kSyTH) {   // warp-uniform
@@ -597,6 +613,13 @@ __global__ void __launch_bounds__(kSyThreads, 3) k_synth_fmt(const SynthParams p
     FmtStore<F> store{p};
     synthFmtTile<F, true>(p, blockIdx.x, blockIdx.y, store);
 }
+// the same with CrosshairV2's tap rejection (Rgb10 / RgbaF16); a separate kernel so the plain one is unchanged
+template <int F>
+__global__ void __launch_bounds__(kSyThreads, 3) k_synth_fmt_ui(const SynthParams p) {
+    pdlEnter();
+    FmtStore<F> store{p};
+    synthFmtTile<F, true, true>(p, blockIdx.x, blockIdx.y, store);
+}
 
 // Many syntheses of one format in one persistent launch (as k_synth_batch for 8-bit RGBA): every CTA takes the next
 // tile of the work list from an atomic counter until the list is exhausted; an item's parameters are staged in shared
@@ -682,7 +705,7 @@ __device__ __forceinline__ void frameValues(const SynthParams& p, const uint8_t*
     }
 }
 
-template <int F>
+template <int F, bool kUi = false>
 __global__ void __launch_bounds__(kSyThreads, 1) k_synth_blur_fmt(const BlurParams bp) {
     pdlEnter();
     __shared__ __align__(16) SynthParams sp;
@@ -749,7 +772,7 @@ __global__ void __launch_bounds__(kSyThreads, 1) k_synth_blur_fmt(const BlurPara
             sp.emap = nullptr;
         }
         __syncthreads();
-        synthFmtTile<F, false>(sp, blockIdx.x, blockIdx.y, acc);
+        synthFmtTile<F, false, kUi>(sp, blockIdx.x, blockIdx.y, acc);
         __syncthreads();   // the tile's shared memory and sp are free again
     }
     if (!colOk) return;
@@ -841,6 +864,12 @@ cudaError_t prepareFormatKernels() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_ui<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_ui<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtRgb10, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtF16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -877,6 +906,50 @@ cudaError_t launchLumaFmtMerged(Merged<LumaPyrParams>& m, int format, cudaStream
     }
 }
 
+// CrosshairV2's estimate fill (gpu/shaders/ui_v2_lumafill.comp) for Rgb10 / RgbaF16 frames, as k_ui_v2_fill for 8-bit
+// RGBA with the format's luma: a level-0 cell holding a UI pixel takes the luma of its not-UI pixels, the window
+// widened by fs px per step up to 8 px while it has none, formed as the luma pass forms a cell (quarter levels summed,
+// rneDiv(4 sum, n) / 16, so the estimate's sums stay exact)
+template <int F>
+__global__ void __launch_bounds__(64) k_ui_fill_fmt(const UiFillParams p) {
+    pdlEnter();
+    const int cx = p.cx0 + (int)(blockIdx.x * 8 + (threadIdx.x & 7)), cy = p.cy0 + (int)(blockIdx.y * 8 + (threadIdx.x >> 3));
+    if (cx >= p.cx0 + p.ncx || cy >= p.cy0 + p.ncy || cx >= p.fw || cy >= p.fh) return;
+    const bool isC = blockIdx.z != 0;
+    const uint32_t* __restrict__ m = isC ? p.mc : p.ma;
+    const uint8_t* f = isC ? p.c : p.a;
+    const int fs = p.fs, px = cx * fs, py = cy * fs;
+    bool has = false;
+    for (int j = 0; j < fs && !has; j++)
+        for (int i = 0; i < fs; i++)
+            if (px + i < p.W && py + j < p.H && uiPx(m, px + i, py + j)) {
+                has = true;
+                break;
+            }
+    if (!has) return;
+    for (int k = 0; k <= 8; k += fs) {
+        int sum = 0, n = 0;
+        for (int y = py - k; y < py + fs + k; y++)
+            for (int x = px - k; x < px + fs + k; x++) {
+                if (x < 0 || y < 0 || x >= p.W || y >= p.H || uiPx(m, x, y)) continue;
+                sum += lumaQ<F>(p.f, f, p.pitch, x, y, p.pq);
+                n++;
+            }
+        if (n > 0) {
+            (isC ? p.lc : p.la)[(size_t)cy * p.fw + cx] = __fmul_rn(i2f(rneDiv(4 * sum, n)), 1.0f / 16.0f);
+            return;
+        }
+    }
+}
+cudaError_t launchUiFillFmt(const UiFillParams& p, cudaStream_t s) {
+    const dim3 grid(divUp(p.ncx, 8), divUp(p.ncy, 8), 2);
+    switch (p.f.format) {
+        case kFmtRgb10: return launchPdl(k_ui_fill_fmt<kFmtRgb10>, grid, dim3(64), 0, s, p);
+        case kFmtF16: return launchPdl(k_ui_fill_fmt<kFmtF16>, grid, dim3(64), 0, s, p);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_pq_table(float* tab, float kWhite) {
     const int i = blockIdx.x * 256 + threadIdx.x;   // the half's bits
     tab[i] = fmtPq255(h2f((uint32_t)i), kWhite);
@@ -889,6 +962,13 @@ cudaError_t launchPqTable(float* tab, float kWhite, cudaStream_t s) {
 cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
     const dim3 grid(divUp(p.W, kSyT), divUp(p.H, kSyTH));
     const size_t smem = fmtSynthSmem(p.f.format, p.fs);
+    if (p.uiA || p.uiC) {   // CrosshairV2: the RGB formats only
+        switch (p.f.format) {
+            case kFmtRgb10: return launchPdl(k_synth_fmt_ui<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
+            case kFmtF16: return launchPdl(k_synth_fmt_ui<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (p.f.format) {
         case kFmtRgb10: return launchPdl(k_synth_fmt<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
         case kFmtF16: return launchPdl(k_synth_fmt<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);
@@ -939,6 +1019,13 @@ cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s) {
     const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
     BlurParams p = bp;
     p.fix = fix;
+    if (bp.base.uiA || bp.base.uiC) {   // CrosshairV2: the RGB formats only
+        switch (bp.base.f.format) {
+            case kFmtRgb10: return launchPdl(k_synth_blur_fmt<kFmtRgb10, true>, grid, dim3(kSyThreads), smem, s, p);
+            case kFmtF16: return launchPdl(k_synth_blur_fmt<kFmtF16, true>, grid, dim3(kSyThreads), smem, s, p);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (bp.base.f.format) {
         case kFmtRgb10: return launchPdl(k_synth_blur_fmt<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
         case kFmtF16: return launchPdl(k_synth_blur_fmt<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);

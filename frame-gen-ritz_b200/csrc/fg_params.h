@@ -261,6 +261,8 @@ constexpr int kUiMaskHeader = 4;
 struct UiV2Params {
     const uint8_t* frame; size_t pitch;
     int W, H, ri, gi, bi;
+    FmtConst f;                    // the frame format (8-bit RGBA / BGRA, Rgb10 or RgbaF16)
+    const float* pq;               // linear RgbaF16: the PQ level of every half value (LumaPyrParams::pq)
     int bx, by, bw, bh;            // the box (detection)
     int wx, wy, ww, wh;            // the work rectangle (state and mask)
     uint32_t* st;
@@ -274,6 +276,7 @@ struct UiPatchParams {
     const uint8_t* curr; size_t pitch;
     uint8_t* out; size_t outPitch;
     const uint32_t* mask;
+    int format;                    // kFmt*: 8-bit RGBA / BGRA, Rgb10 or RgbaF16
 };
 // the estimate fill (Settings::uiEstimateFill): level-0 luma cells holding UI pixels re-averaged over their not-UI
 // pixels, prev's (mask ma, luma la) and curr's (mc, lc); cells of the rectangle (cx0, cy0) .. + (ncx, ncy)
@@ -283,8 +286,11 @@ struct UiFillParams {
     const uint32_t* ma; const uint32_t* mc;
     float* la; float* lc;
     int cx0, cy0, ncx, ncy;
+    FmtConst f;                    // Rgb10 / RgbaF16 (launchUiFillFmt): the format's luma
+    const float* pq;
 };
 cudaError_t launchUiFill(const UiFillParams& p, cudaStream_t s);
+cudaError_t launchUiFillFmt(const UiFillParams& p, cudaStream_t s);   // the estimate fill of Rgb10 / RgbaF16 frames
 cudaError_t launchUiV2Update(const UiV2Params& p, cudaStream_t s);
 cudaError_t launchUiV2Mask(const UiV2Params& p, cudaStream_t s);
 cudaError_t launchUiPatch(const UiPatchParams& p, int wx, int wy, int ww, int wh, cudaStream_t s);

@@ -1,5 +1,7 @@
-// Static-UI protection, CrosshairV2 mode, for 8-bit RGBA / BGRA frames: the passes of recordObserve / recordTrack and
-// the paste-back after a synthesis. The warp-tap rejection between them lives in the synthesis kernels (uiHitMask in
+// Static-UI protection, CrosshairV2 mode, for 8-bit RGBA / BGRA, Rgb10 and RgbaF16 frames: the passes of recordObserve
+// / recordTrack and the paste-back after a synthesis. Pixels enter the state machine as the shaders' 8-bit-equivalent
+// levels (format.glsl FG_STILL): the bytes of 8-bit RGBA, floor(code x fl32(255 / 1023) + 0.5) for Rgb10,
+// clamp(floor(level + 0.5), 0, 255) for RgbaF16 (level: the PQ code x 255 of a linear value, the value x 255 encoded). The warp-tap rejection between them lives in the synthesis kernels (uiHitMask in
 // fg_device.h). Restates the reference's Vulkan shaders gpu/shaders/ui_v2_update.comp, ui_v2_mask.comp and
 // ui_patch.comp (binary paste); layouts in fg_params.h (UiV2Params).
 //
@@ -15,6 +17,8 @@
 // The work rectangle of a 4K frame's default box is 56 x 56 pixels: these passes are latency-sized, not bandwidth-sized.
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #include "fg_device.h"
 #include "fg_params.h"
 
@@ -23,10 +27,32 @@ namespace {
 
 constexpr int kUiTX = 16, kUiTY = 8;   // threads per CTA of the update and patch passes
 
+// an RgbaF16 half's 8-bit-equivalent level
+__device__ __forceinline__ uint32_t uiLevelF16(const UiV2Params& p, uint32_t bits) {
+    const float lv = p.f.linear ? __ldg(p.pq + bits)
+                                : __fmul_rn(__half2float(__ushort_as_half((unsigned short)bits)), 255.0f);
+    return (uint32_t)fminf(fmaxf(floorf(__fadd_rn(lv, 0.5f)), 0.0f), 255.0f);   // NaN -> 0
+}
+
 __device__ __forceinline__ uint32_t uiPixel(const UiV2Params& p, int x, int y) {   // r | g << 8 | b << 16, clamped
     x = min(max(x, 0), p.W - 1);
     y = min(max(y, 0), p.H - 1);
-    const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(p.frame + (size_t)y * p.pitch) + x);
+    const uint8_t* row = p.frame + (size_t)y * p.pitch;
+    if (p.f.format == kFmtRgb10) {
+        const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(row) + x);
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const uint32_t code = (w >> (p.f.rHigh ? 20 - 10 * k : 10 * k)) & 1023u;
+            o |= (uint32_t)floorf(__fadd_rn(__fmul_rn((float)code, p.f.k10), 0.5f)) << (8 * k);
+        }
+        return o;
+    }
+    if (p.f.format == kFmtF16) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2*>(row) + x);
+        return uiLevelF16(p, q.x & 0xFFFFu) | (uiLevelF16(p, q.x >> 16) << 8) | (uiLevelF16(p, q.y & 0xFFFFu) << 16);
+    }
+    const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(row) + x);
     return ((v >> (8 * p.ri)) & 255u) | (((v >> (8 * p.gi)) & 255u) << 8) | (((v >> (8 * p.bi)) & 255u) << 16);
 }
 
@@ -153,18 +179,17 @@ __global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_patch(const UiPatchParams 
     const int stride = (int)p.mask[3];
     const uint32_t a = (p.mask[kUiMaskHeader + y * stride + (x >> 2)] >> (8 * (x & 3))) & 255u;
     if (a != 255u) return;
+    if (p.format == kFmtF16) {   // R, G, B halves from the real frame, alpha kept
+        uint2* o = reinterpret_cast<uint2*>(p.out + (size_t)(wy + y) * p.outPitch) + wx + x;
+        const uint2 real = __ldg(reinterpret_cast<const uint2*>(p.curr + (size_t)(wy + y) * p.pitch) + wx + x);
+        *o = make_uint2(real.x, (real.y & 0xFFFFu) | (o->y & 0xFFFF0000u));
+        return;
+    }
+    // colour channels from the real frame, alpha kept (8-bit RGBA: byte 3; Rgb10: the top 2 bits)
+    const uint32_t keep = p.format == kFmtRgb10 ? 0xC0000000u : 0xFF000000u;
     uint32_t* o = reinterpret_cast<uint32_t*>(p.out + (size_t)(wy + y) * p.outPitch) + wx + x;
     const uint32_t real = __ldg(reinterpret_cast<const uint32_t*>(p.curr + (size_t)(wy + y) * p.pitch) + wx + x);
-    *o = (real & 0x00FFFFFFu) | (*o & 0xFF000000u);   // colour channels from the real frame, alpha kept
-}
-
-// is the frame pixel (x, y) a UI pixel of the mask (header + bytes)?
-__device__ __forceinline__ bool uiPx(const uint32_t* __restrict__ m, int x, int y) {
-    const uint32_t o = __ldg(m + 1), wh = __ldg(m + 2);
-    x -= (int)(o & 0xFFFFu);
-    y -= (int)(o >> 16);
-    if (x < 0 || y < 0 || x >= (int)(wh & 0xFFFFu) || y >= (int)(wh >> 16)) return false;
-    return ((__ldg(m + kUiMaskHeader + y * (int)__ldg(m + 3) + (x >> 2)) >> (8 * (x & 3))) & 255u) != 0u;
+    *o = (real & ~keep) | (*o & keep);
 }
 
 // The estimate fill (gpu/shaders/ui_v2_lumafill.comp), one thread per level-0 cell of the mask rectangle, z = 0 prev,

@@ -139,7 +139,7 @@ size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 const char* kErrSettings = "invalid settings: a field is out of range or not finite (see Interpolator::validate)";
 const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
 const char* kErrUi = "static-UI protection: only CrosshairV2 is built into this library (Crosshair and WholeScreen are not)";
-const char* kErrUiFormat = "static-UI protection (CrosshairV2) is built for the 8-bit RGBA / BGRA formats only";
+const char* kErrUiFormat = "static-UI protection (CrosshairV2) is built for the 8-bit RGBA / BGRA, Rgb10 and RgbaF16 formats only";
 const char* kErrNoFormat = "unsupported viewFormat (see framegen::Format)";
 const char* kErrYuvMatrix = "yuvMatrix must be Bt601, Bt709 or Bt2020";
 const char* kErrNits = "linearWhiteNits must be in (0, 10000]";
@@ -377,6 +377,8 @@ struct Interpolator::Impl {
         fgk::UiV2Params p{};
         p.frame = (const uint8_t*)f.data; p.pitch = f.pitch;
         p.W = (int)W; p.H = (int)H; p.ri = ri; p.gi = gi; p.bi = bi;
+        p.f = fc;
+        p.pq = pqTab;
         p.bx = uiBox[0]; p.by = uiBox[1]; p.bw = uiBox[2]; p.bh = uiBox[3];
         p.wx = uiWork[0]; p.wy = uiWork[1]; p.ww = uiWork[2]; p.wh = uiWork[3];
         p.st = uiState;
@@ -419,7 +421,7 @@ struct Interpolator::Impl {
     }
 
     bool uiPatch(cudaStream_t s, const Frame& curr, const Frame& out, const uint32_t* mc) {
-        fgk::UiPatchParams pp{(const uint8_t*)curr.data, curr.pitch, (uint8_t*)out.data, out.pitch, mc};
+        fgk::UiPatchParams pp{(const uint8_t*)curr.data, curr.pitch, (uint8_t*)out.data, out.pitch, mc, fc.format};
         if (!check(fgk::launchUiPatch(pp, uiWork[0], uiWork[1], uiWork[2], uiWork[3], s))) return false;
         stamp(s, "ui patch");
         return true;
@@ -651,7 +653,9 @@ struct Interpolator::Impl {
             fp.cx0 = uiWork[0] / fp.fs; fp.cy0 = uiWork[1] / fp.fs;
             fp.ncx = (uiWork[0] + uiWork[2] - 1) / fp.fs - fp.cx0 + 1;
             fp.ncy = (uiWork[1] + uiWork[3] - 1) / fp.fs - fp.cy0 + 1;
-            if (!check(fgk::launchUiFill(fp, s))) return false;
+            fp.f = fc;
+            fp.pq = pqTab;
+            if (!check(fmt == Format::Rgba8 ? fgk::launchUiFill(fp, s) : fgk::launchUiFillFmt(fp, s))) return false;
             stamp(s, "ui fill");
         }
         for (const fgk::DownParams& dp : e.down)
@@ -807,7 +811,8 @@ const char* Interpolator::settingsError(const Settings& s, Format f) {
     if (!validate(s)) return kErrSettings;
     if (s.motionVersion != MotionVersion::V1) return kErrVersion;
     if (s.uiProtection != UiProtection::Off && s.uiProtection != UiProtection::CrosshairV2) return kErrUi;
-    if (s.uiProtection == UiProtection::CrosshairV2 && f != Format::Rgba8) return kErrUiFormat;
+    if (s.uiProtection == UiProtection::CrosshairV2 && f != Format::Rgba8 && f != Format::Rgb10 && f != Format::RgbaF16)
+        return kErrUiFormat;
     return nullptr;
 }
 
@@ -1544,7 +1549,7 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
                 I.beginFrame();
                 if (!I.recordEstimate(streamOf(i), prev[i], curr[i])) { m->err = "a slot's estimate was refused (frames?)"; return false; }
             }
-            if (batched) continue;   // in the persistent launches
+            if (batched && !I.m->uiOn()) continue;   // in the persistent launches
             for (uint32_t k = 1; k < m->mult[i]; k++)
                 if (!I.recordSynth(streamOf(i), prev[i], curr[i], outs[first[i] + k - 1], (float)k / (float)m->mult[i])) {
                     m->err = "a slot's synthesis was refused (frames?)";
@@ -1565,6 +1570,7 @@ bool Batch::record(cudaStream_t s, const Frame* prev, const Frame* curr, const F
     std::vector<Item> items;
     for (int i = 0; i < ns && batched; i++) {
         const Interpolator::Impl* im = m->slots[i]->m;
+        if (im->uiOn()) continue;   // CrosshairV2 slots synthesize through recordSynth (tap rejection, paste-back)
         const int tiles = fgk::synthTilesX((int)im->W) * fgk::synthTilesY((int)im->H);
         for (uint32_t k = 1; k < m->mult[i]; k++) items.push_back({i, (int)k, tiles, (int)im->fmt});
     }

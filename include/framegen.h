@@ -80,9 +80,9 @@ struct Settings {
     uint32_t searchRadius = 2;      // [1, 12]
     uint32_t searchRadiusTop = 6;   // [1, 12]
     bool subpixel = true;
-    // Static-UI protection (gpu/framegen.h:196-305): Off, or CrosshairV2 for the 8-bit RGBA / BGRA formats (the box
-    // fields, uiHistory, uiStillFrames, uiStillThreshold, uiContrastThreshold, uiLeaveFrames, uiReentryFrames and
-    // uiEstimateFill apply). Crosshair, WholeScreen and the other formats are refused by settingsError with a reason;
+    // Static-UI protection (gpu/framegen.h:196-305): Off, or CrosshairV2 for the 8-bit RGBA / BGRA, Rgb10 and RgbaF16
+    // formats (the box fields, uiHistory, uiStillFrames, uiStillThreshold, uiContrastThreshold, uiLeaveFrames,
+    // uiReentryFrames and uiEstimateFill apply). Crosshair, WholeScreen and the YUV formats are refused by settingsError with a reason;
     // uiInpaintReach and uiMaxStillFraction (Crosshair / WholeScreen fields) are validated with the reference's ranges.
     UiProtection uiProtection = UiProtection::Off;
     uint32_t uiHistory = 3;                          // [3, 65]

@@ -438,37 +438,11 @@ static void pixel_field(const float* v, int bw, int bh, const float* ya, const f
 
 /* ---------------------------------------------------------------------------------------------- estimate */
 
-/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl; gpu/shaders/motion_v1.glsl:117-129): the UI mask of a
- * frame over its rectangle (bytes, 0 = not UI). A tap at p reads the pixels lo..hi with X = roundEven(32 p),
- * lo = X >> 5, hi = lo + (X & 31 != 0) per axis; does any of them lie on the mask? */
-typedef struct { const uint8_t* m; int x, y, w, h, stride; } fgo_uimask;
-
-static int ui_hit(const fgo_uimask* u, float px, float py) {
-    if (!u || !u->m || u->w <= 0 || u->h <= 0) return 0;
-    int X = (int)nearbyintf(px * 32.0f), Y = (int)nearbyintf(py * 32.0f);
-    int lx = X >> 5, ly = Y >> 5, hx = lx + ((X & 31) != 0), hy = ly + ((Y & 31) != 0);
-    int x0 = lx - u->x, y0 = ly - u->y, x1 = hx - u->x, y1 = hy - u->y;
-    if (x0 < 0) x0 = 0;
-    if (y0 < 0) y0 = 0;
-    if (x1 > u->w - 1) x1 = u->w - 1;
-    if (y1 > u->h - 1) y1 = u->h - 1;
-    for (int y = y0; y <= y1; y++)
-        for (int x = x0; x <= x1; x++)
-            if (u->m[(size_t)y * u->stride + x]) return 1;
-    return 0;
-}
-
 /* CrosshairV2's estimate fill (Settings::uiEstimateFill; gpu/shaders/ui_v2_lumafill.comp), restated for this
  * library's level-0 luma: every flow cell of the mask rectangle's cells that holds a UI pixel (mask byte != 0) takes
  * the mean gray level of its not-UI pixels, the window widened by S px on every side per step, up to 8 px, while it has
  * none (no such pixel within 8 px: the cell keeps its luma). The mean is rounded half up to the level-0 grid (a
  * multiple of 1 / S^2), where the reference keeps it unrounded, so the estimate's sums stay exact in any order. */
-static int ui_px(const fgo_uimask* u, int x, int y) {
-    x -= u->x;
-    y -= u->y;
-    return x >= 0 && y >= 0 && x < u->w && y < u->h && u->m[(size_t)y * u->stride + x] != 0;
-}
-
 static void ui_fill(const img8* m, const fgo_uimask* u, int fs, float* L0, int fw, int fh) {
     if (!u || !u->m || u->w <= 0 || u->h <= 0) return;
     const int cx0 = u->x / fs, cx1 = (u->x + u->w - 1) / fs, cy0 = u->y / fs, cy1 = (u->y + u->h - 1) / fs;

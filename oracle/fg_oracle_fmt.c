@@ -254,9 +254,50 @@ static int lumaQ(const fgo_fmt* f, const fgo_frame* F, int x, int y) {
 
 /* ---------------------------------------------------------------------------------------------- estimate */
 
+/* CrosshairV2's estimate fill (gpu/shaders/ui_v2_lumafill.comp) for these formats: every level-0 cell of the mask
+ * rectangle that holds a UI pixel takes the luma of its not-UI pixels, the window widened by fs px per step up to 8 px
+ * while it has none, formed as the luma pass forms a cell (quarter levels summed, rne_div(4 sum, n) / 16). */
+static void ui_fill_fmt(const fgo_fmt* f, const fgo_frame* F, int W, int H, const fgo_uimask* u, int fs, float* L0, int fw,
+                        int fh) {
+    if (!u || !u->m || u->w <= 0 || u->h <= 0) return;
+    const int cx0 = u->x / fs, cx1 = (u->x + u->w - 1) / fs, cy0 = u->y / fs, cy1 = (u->y + u->h - 1) / fs;
+    for (int cy = cy0; cy <= cy1 && cy < fh; cy++)
+        for (int cx = cx0; cx <= cx1 && cx < fw; cx++) {
+            const int px = cx * fs, py = cy * fs;
+            int has = 0;
+            for (int j = 0; j < fs && !has; j++)
+                for (int i = 0; i < fs; i++)
+                    if (px + i < W && py + j < H && ui_px(u, px + i, py + j)) { has = 1; break; }
+            if (!has) continue;
+            for (int k = 0; k <= 8; k += fs) {
+                int sum = 0, n = 0;
+                for (int y = py - k; y < py + fs + k; y++)
+                    for (int x = px - k; x < px + fs + k; x++) {
+                        if (x < 0 || y < 0 || x >= W || y >= H || ui_px(u, x, y)) continue;
+                        sum += lumaQ(f, F, x, y);
+                        n++;
+                    }
+                if (n > 0) {
+                    L0[(size_t)cy * fw + cx] = (float)rne_div(4 * sum, n) * (1.0f / 16.0f);
+                    break;
+                }
+            }
+        }
+}
+
+int fgo_estimate_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const fgo_fmt* f, const fgo_settings* s,
+                        float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean,
+                        int* cut, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc);
 int fgo_estimate_fmt(const fgo_frame* A, const fgo_frame* C, int W, int H, const fgo_fmt* f, const fgo_settings* s,
                      float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean,
                      int* cut, int nthreads) {
+    return fgo_estimate_fmt_ui(A, C, W, H, f, s, luma, fields, seeds, meds, sads, pf, sad_mean, cut, nthreads, NULL, NULL);
+}
+
+/* the same with CrosshairV2's estimate fill of both frames' level 0 (ua, uc: their UI masks; none when either is NULL) */
+int fgo_estimate_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const fgo_fmt* f, const fgo_settings* s,
+                        float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf, float* sad_mean,
+                        int* cut, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #else
@@ -283,6 +324,10 @@ int fgo_estimate_fmt(const fgo_frame* A, const fgo_frame* C, int W, int H, const
                     }
                 out[(size_t)y * fw + x] = (float)rne_div(4 * sum, cnt) * (1.0f / 16.0f);
             }
+    }
+    if (ua && uc) {
+        ui_fill_fmt(f, A, W, H, ua, fs, L[0][0], fw, fh);
+        ui_fill_fmt(f, C, W, H, uc, fs, L[0][1], fw, fh);
     }
     for (int l = 1; l < n; l++)
         for (int k = 0; k < 2; k++) fgo_i_area_half(L[l - 1][k], lw[l - 1], lh[l - 1], L[l][k], lw[l], lh[l], 1);
@@ -389,9 +434,33 @@ static void copy_near(const fgo_fmt* f, const fgo_frame* N, const fgo_frame* O, 
 }
 
 /* interp.synth for the other formats; arguments as fgo_synth, frames as fgo_frame (O: the output planes) */
+/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl) for the RGB formats: a tap whose bilinear footprint
+ * touches its own frame's UI mask takes the other frame's tap (both or neither: unchanged) */
+static inline void ui_reject(const fgo_uimask* ua, const fgo_uimask* uc, float pax, float pay, float pcx, float pcy,
+                             float wa[3], float wc[3]) {
+    if (!ua && !uc) return;
+    const int ha = ui_hit(ua, pax, pay), hc = ui_hit(uc, pcx, pcy);
+    if (ha == hc) return;
+    for (int k = 0; k < 3; k++) {
+        if (ha) wa[k] = wc[k];
+        else wc[k] = wa[k];
+    }
+}
+
+int fgo_synth_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const fgo_fmt* f, const fgo_settings* s,
+                     const float* pf, int cut, float t, const fgo_frame* O, float* field_t, uint8_t* emap,
+                     long long* untrusted, int* reason, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc);
 int fgo_synth_fmt(const fgo_frame* A, const fgo_frame* C, int W, int H, const fgo_fmt* f, const fgo_settings* s,
                   const float* pf, int cut, float t, const fgo_frame* O, float* field_t, uint8_t* emap,
                   long long* untrusted, int* reason, int nthreads) {
+    return fgo_synth_fmt_ui(A, C, W, H, f, s, pf, cut, t, O, field_t, emap, untrusted, reason, nthreads, NULL, NULL);
+}
+
+/* the same with CrosshairV2's warp-tap rejection (ua, uc: prev's and curr's UI masks, either may be NULL; RGB formats
+ * only) */
+int fgo_synth_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const fgo_fmt* f, const fgo_settings* s,
+                     const float* pf, int cut, float t, const fgo_frame* O, float* field_t, uint8_t* emap,
+                     long long* untrusted, int* reason, int nthreads, const fgo_uimask* ua, const fgo_uimask* uc) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #else
@@ -430,6 +499,7 @@ int fgo_synth_fmt(const fgo_frame* A, const fgo_frame* C, int W, int H, const fg
             float wa[3], wc[3];
             warp(f, A, W, H, (float)x - ka * hx, (float)y - ka * hy, wa);
             warp(f, C, W, H, (float)x + kc * hx, (float)y + kc * hy, wc);
+            ui_reject(ua, uc, (float)x - ka * hx, (float)y - ka * hy, (float)x + kc * hx, (float)y + kc * hy, wa, wc);
             const int m = mismatch(f, wa, wc);
             e[(size_t)y * W + x] = (uint8_t)m;
             ef[(size_t)y * W + x] = (float)m;
@@ -460,6 +530,7 @@ int fgo_synth_fmt(const fgo_frame* A, const fgo_frame* C, int W, int H, const fg
                 float wa[3], wc[3];
                 warp(f, A, W, H, (float)x - ka * hx, (float)y - ka * hy, wa);
                 warp(f, C, W, H, (float)x + kc * hx, (float)y + kc * hy, wc);
+                ui_reject(ua, uc, (float)x - ka * hx, (float)y - ka * hy, (float)x + kc * hx, (float)y + kc * hy, wa, wc);
                 const float u = eb[q], iu = 1.0f - u;
                 uint8_t* o = (uint8_t*)O->p + (size_t)y * O->pitch;
                 if (f->format == FMT_RGB10) {

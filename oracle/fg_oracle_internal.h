@@ -4,6 +4,8 @@
  */
 #ifndef FG_ORACLE_INTERNAL_H
 #define FG_ORACLE_INTERNAL_H
+#include <math.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #define BLOCK 8
@@ -32,4 +34,32 @@ void fgo_i_field_at(const float* pf, int w, int h, float sf, float* out);
 int fgo_i_estimate_levels(float* L[][2], int n, const int* lw, const int* lh, const fgo_settings* s, int cnnLevel,
                           const float* cnn, float* luma, float* fields, float* seeds, float* meds, float* sads, float* pf,
                           float* sad_mean, int* cut);
+
+/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl; gpu/shaders/motion_v1.glsl:117-129): the UI mask of a
+ * frame over its rectangle (bytes, 0 = not UI). A tap at p reads the pixels lo..hi with X = roundEven(32 p),
+ * lo = X >> 5, hi = lo + (X & 31 != 0) per axis; does any of them lie on the mask? */
+typedef struct { const uint8_t* m; int x, y, w, h, stride; } fgo_uimask;
+
+static inline int ui_hit(const fgo_uimask* u, float px, float py) {
+    if (!u || !u->m || u->w <= 0 || u->h <= 0) return 0;
+    int X = (int)nearbyintf(px * 32.0f), Y = (int)nearbyintf(py * 32.0f);
+    int lx = X >> 5, ly = Y >> 5, hx = lx + ((X & 31) != 0), hy = ly + ((Y & 31) != 0);
+    int x0 = lx - u->x, y0 = ly - u->y, x1 = hx - u->x, y1 = hy - u->y;
+    if (x0 < 0) x0 = 0;
+    if (y0 < 0) y0 = 0;
+    if (x1 > u->w - 1) x1 = u->w - 1;
+    if (y1 > u->h - 1) y1 = u->h - 1;
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++)
+            if (u->m[(size_t)y * u->stride + x]) return 1;
+    return 0;
+}
+
+static inline int ui_px(const fgo_uimask* u, int x, int y) {
+    x -= u->x;
+    y -= u->y;
+    return x >= 0 && y >= 0 && x < u->w && y < u->h && u->m[(size_t)y * u->stride + x] != 0;
+}
+
+
 #endif

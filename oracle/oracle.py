@@ -337,6 +337,10 @@ def _fmt_lib():
                                     ctypes.POINTER(_CFmt), ctypes.POINTER(_CSettings), P, ctypes.c_int, ctypes.c_float,
                                     ctypes.POINTER(_CFrame), P, P, P, P, ctypes.c_int]
         L.fgo_synth_fmt.restype = ctypes.c_int
+        L.fgo_estimate_fmt_ui.argtypes = L.fgo_estimate_fmt.argtypes + [ctypes.POINTER(_CUiMask), ctypes.POINTER(_CUiMask)]
+        L.fgo_estimate_fmt_ui.restype = ctypes.c_int
+        L.fgo_synth_fmt_ui.argtypes = L.fgo_synth_fmt.argtypes + [ctypes.POINTER(_CUiMask), ctypes.POINTER(_CUiMask)]
+        L.fgo_synth_fmt_ui.restype = ctypes.c_int
         for n in ("fgo_log2", "fgo_exp2"):
             getattr(L, n).argtypes = [ctypes.c_float]
             getattr(L, n).restype = ctypes.c_float
@@ -375,8 +379,9 @@ def empty_like_frame(frame, spec):
     return np.zeros_like(frame)
 
 
-def estimate_fmt(a, c, spec, settings=None, trace=True, threads=0):
-    """estimate() for the other formats (same dict)."""
+def estimate_fmt(a, c, spec, settings=None, trace=True, threads=0, ui_fill=None):
+    """estimate() for the other formats (same dict). ui_fill = (prev's mask, curr's mask), each (bytes, rect):
+    CrosshairV2's estimate fill of both frames' level 0 (Rgb10 / RgbaF16)."""
     s = settings or Settings()
     W, H = frame_size(a, spec)
     L = layout(W, H, s.flowScale, s.pyramidMinSide)
@@ -392,9 +397,12 @@ def estimate_fmt(a, c, spec, settings=None, trace=True, threads=0):
     pf = np.zeros((L.fh, L.fw, 2), np.float32)
     mean, cut = ctypes.c_float(), ctypes.c_int()
     fa, fc = _cframe(a, spec), _cframe(c, spec)
-    n = _fmt_lib().fgo_estimate_fmt(ctypes.byref(fa), ctypes.byref(fc), W, H, ctypes.byref(fmt_struct(spec)),
-                                    ctypes.byref(_cs(s)), _p(luma), _p(fields), _p(seeds), _p(meds), _p(sads), _p(pf),
-                                    ctypes.byref(mean), ctypes.byref(cut), threads)
+    (ma, ka), (mc, kc) = (_uimask(ui_fill[0]), _uimask(ui_fill[1])) if ui_fill else ((None, None), (None, None))
+    n = _fmt_lib().fgo_estimate_fmt_ui(ctypes.byref(fa), ctypes.byref(fc), W, H, ctypes.byref(fmt_struct(spec)),
+                                       ctypes.byref(_cs(s)), _p(luma), _p(fields), _p(seeds), _p(meds), _p(sads), _p(pf),
+                                       ctypes.byref(mean), ctypes.byref(cut), threads,
+                                       ctypes.byref(ma) if ma is not None else None,
+                                       ctypes.byref(mc) if mc is not None else None)
     if n != len(L.levels):
         raise RuntimeError("fgo_estimate_fmt failed")
     est = {"sad": float(mean.value), "cut": bool(cut.value), "pf": pf, "layout": L,
@@ -415,9 +423,10 @@ def estimate_fmt(a, c, spec, settings=None, trace=True, threads=0):
     return est
 
 
-def synth_fmt(a, c, est, t, spec, settings=None, trace=False, threads=0):
+def synth_fmt(a, c, est, t, spec, settings=None, trace=False, threads=0, ui=None):
     """synth() for the other formats: returns (frame, reason) or, with trace, a dict with out, reason, field_t, e,
-    untrusted. The frame has the input's layout (a tuple of planes for YUV)."""
+    untrusted. The frame has the input's layout (a tuple of planes for YUV). ui = (prev's mask, curr's mask), each
+    (bytes, rect) or None: CrosshairV2's warp-tap rejection (Rgb10 / RgbaF16; no paste-back here: ui_v2.patch_fmt)."""
     s = settings or Settings()
     W, H = frame_size(a, spec)
     out = empty_like_frame(a, spec)
@@ -427,9 +436,12 @@ def synth_fmt(a, c, est, t, spec, settings=None, trace=False, threads=0):
     e = np.zeros((H, W), np.uint8) if trace else None
     unt, reason = ctypes.c_longlong(), ctypes.c_int()
     fa, fc, fo = _cframe(a, spec), _cframe(c, spec), _cframe(out, spec)
-    r = _fmt_lib().fgo_synth_fmt(ctypes.byref(fa), ctypes.byref(fc), W, H, ctypes.byref(fmt_struct(spec)),
-                                 ctypes.byref(_cs(s)), _p(pf), int(est["cut"]), float(t), ctypes.byref(fo), _p(ft), _p(e),
-                                 ctypes.byref(unt), ctypes.byref(reason), threads)
+    (ma, ka), (mc, kc) = (_uimask(ui[0]), _uimask(ui[1])) if ui else ((None, None), (None, None))
+    r = _fmt_lib().fgo_synth_fmt_ui(ctypes.byref(fa), ctypes.byref(fc), W, H, ctypes.byref(fmt_struct(spec)),
+                                    ctypes.byref(_cs(s)), _p(pf), int(est["cut"]), float(t), ctypes.byref(fo), _p(ft),
+                                    _p(e), ctypes.byref(unt), ctypes.byref(reason), threads,
+                                    ctypes.byref(ma) if ma is not None else None,
+                                    ctypes.byref(mc) if mc is not None else None)
     if r != 0:
         raise ValueError("fgo_synth_fmt failed (t outside (0, 1)?)")
     if trace:
@@ -437,18 +449,19 @@ def synth_fmt(a, c, est, t, spec, settings=None, trace=False, threads=0):
     return out, REASONS[reason.value]
 
 
-def synth_blur_fmt(a, c, est, t0, t1, samples, gaussian, spec, settings=None):
+def synth_blur_fmt(a, c, est, t0, t1, samples, gaussian, spec, settings=None, ui=None):
     """recordSynthBlur's frame in the other formats (None if refused), from synth_fmt's sub-frames: Rgb10 codes (by bit
     position, alpha's 2 bits included) and Nv12 / P010 luma and chroma codes averaged as (sum q_k v_k + 2^15) >> 16;
     RgbaF16 summed in sample order as float32 sums of fl32(q_k 2^-16 h_k) per channel (alpha included), then rounded
-    to half. With blur off (N < 2) or t0 == t1 and t1 inside (0, 1): synth_fmt(t1)."""
+    to half. With blur off (N < 2) or t0 == t1 and t1 inside (0, 1): synth_fmt(t1). ui: as synth_fmt's, for every
+    synthesized sub-frame."""
     t0f, t1f = np.float32(t0), np.float32(t1)
     if not (t0f >= 0 and t1f <= 1 and t0f <= t1f):
         return None
     if not (samples >= 2 and t0f < t1f) and 0 < t1f < 1:
-        return synth_fmt(a, c, est, float(t1f), spec, settings)[0]
+        return synth_fmt(a, c, est, float(t1f), spec, settings, ui=ui)[0]
     times, q = blur_plan(samples, gaussian, t0, t1)
-    subs = [a if tk <= 0 else c if tk >= 1 else synth_fmt(a, c, est, float(tk), spec, settings)[0]
+    subs = [a if tk <= 0 else c if tk >= 1 else synth_fmt(a, c, est, float(tk), spec, settings, ui=ui)[0]
             for tk in times.tolist()]
 
     def avg_codes(planes, shift):   # integer codes (after >> shift), then back

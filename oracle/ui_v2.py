@@ -1,15 +1,18 @@
 """Test infrastructure (the oracle): a CPU restatement of frame-gen-ritz's static-UI protection in its CrosshairV2 mode
-for 8-bit RGBA frames. Only the tests use it, as the checker of the library's kernels; the library never runs it.
+for 8-bit RGBA frames and the Rgb10 / RgbaF16 formats. Only the tests use it, as the checker of the library's kernels;
+the library never runs it.
 
 The reference implements this mode only as Vulkan compute shaders (no CPU version exists), so this file restates the
-shader math step by step; each function cites the shader it follows. Levels are the 8-bit values themselves (the
-shaders' FG_STILL of an 8-bit UNORM texel, gpu/shaders/format.glsl:35).
+shader math step by step; each function cites the shader it follows. Levels are the shaders' 8-bit-equivalent FG_STILL
+levels (gpu/shaders/format.glsl:35-53): the 8-bit values themselves, floor(code x 255 / 1023 + 0.5) for Rgb10,
+clamp(floor(level + 0.5), 0, 255) for RgbaF16 (level: the PQ code x 255 of a linear value, value x 255 encoded).
 
   box_size / box_rect / work_rect    gpu/framegen.cpp:1041-1075 (Interpolator::boxSize, boxRect, boxMargin, workRect)
   State.update                       gpu/shaders/ui_v2_update.comp (observe and recordTrack: the per-pixel state machine)
   State.mask                         gpu/shaders/ui_v2_mask.comp (the mask bytes 255 / 64 / 0 with the 1 px grow)
   footprint / hit                    gpu/shaders/ui_reject.glsl:22-58 (which pixels a warp tap reads; is one of them UI)
-  patch                              gpu/shaders/ui_patch.comp with binary = 1 (paste the real curr pixel where 255)
+  patch / patch_fmt                  gpu/shaders/ui_patch.comp with binary = 1 (paste the real curr pixel where 255)
+  levels_fmt                         gpu/shaders/ui_v2_update.comp pixAt with format.glsl FG_STILL (Rgb10, RgbaF16)
 The warp-tap rejection itself sits inside the oracle's synthesis (fg_oracle.c, fgo_synth_ui).
 """
 import math
@@ -54,6 +57,40 @@ def _levels(frame, order):
     return frame[..., idx].astype(np.int32)
 
 
+_PQ_TABLES = {}
+
+
+def _pq_table(white):
+    """the oracle's PQ level (x 255) of every half value, by its bits"""
+    if white not in _PQ_TABLES:
+        import oracle
+        L = oracle._fmt_lib()
+        kw = float(np.float32(white) / np.float32(10000.0))
+        _PQ_TABLES[white] = np.array([L.fgo_pq255(L.fgo_h2f(i), kw) for i in range(65536)], np.float32)
+    return _PQ_TABLES[white]
+
+
+def levels_fmt(frame, spec):
+    """(H, W, 3) int32 8-bit-equivalent levels in R, G, B order of an Rgb10 frame ((H, W) uint32 words) or an
+    RgbaF16 frame ((H, W, 4) halves): FG_STILL of gpu/shaders/format.glsl, in float32 steps"""
+    if spec.format == "rgb10":
+        w = frame.view(np.uint32)
+        shifts = (20, 10, 0) if spec.r_high else (0, 10, 20)
+        codes = np.stack([(w >> sh) & 1023 for sh in shifts], axis=-1).astype(np.float32)
+        k10 = np.float32(255.0 / 1023.0)
+        return np.floor((codes * k10).astype(np.float32) + np.float32(0.5)).astype(np.int32)
+    if spec.format == "f16":
+        bits = frame.view(np.uint16)[..., :3]
+        if spec.linear:
+            lv = _pq_table(spec.white)[bits]
+        else:
+            lv = (bits.view(np.float16).astype(np.float32) * np.float32(255.0)).astype(np.float32)
+        v = np.floor((lv + np.float32(0.5)).astype(np.float32))
+        v = np.nan_to_num(v, nan=0.0, posinf=255.0, neginf=0.0)
+        return np.clip(v, 0, 255).astype(np.int32)
+    raise ValueError("CrosshairV2 levels: Rgb10 and RgbaF16 only")
+
+
 def _median7(lv, y, x):
     """per channel, the median of the 7x7 window around (y, x), taps clamped to the frame (the 25th of 49 values)"""
     H, W = lv.shape[:2]
@@ -81,10 +118,11 @@ class State:
         self.match = np.zeros((wh, ww), np.int32)
         self.reset = True
 
-    def update(self, frame, order="rgba"):
-        """one observed (or tracked) frame: gpu/shaders/ui_v2_update.comp"""
+    def update(self, frame, order="rgba", spec=None):
+        """one observed (or tracked) frame: gpu/shaders/ui_v2_update.comp; spec: the frame's format (oracle.FormatSpec)
+        when it is not 8-bit RGBA / BGRA"""
         s = self.s
-        lv = _levels(frame, order)
+        lv = _levels(frame, order) if spec is None else levels_fmt(frame, spec)
         wx, wy, ww, wh = self.work
         bx, by, bw, bh = self.box
         thr = float(np.float32(s.uiStillThreshold))
@@ -175,6 +213,23 @@ def patch(out, curr, mask, rect):
     sel = mask == 255
     reg = out[oy:oy + h, ox:ox + w]
     src = curr[oy:oy + h, ox:ox + w]
+    for c in range(3):
+        reg[..., c][sel] = src[..., c][sel]
+    return out
+
+
+def patch_fmt(out, curr, mask, rect, spec):
+    """patch() for Rgb10 (the colour codes from curr, the 2 alpha bits kept) and RgbaF16 (R, G, B halves from curr,
+    alpha kept)"""
+    ox, oy, w, h = rect
+    sel = mask == 255
+    if spec.format == "rgb10":
+        reg = out.view(np.uint32)[oy:oy + h, ox:ox + w]
+        src = curr.view(np.uint32)[oy:oy + h, ox:ox + w]
+        reg[sel] = (src[sel] & np.uint32(0x3FFFFFFF)) | (reg[sel] & np.uint32(0xC0000000))
+        return out
+    reg = out.view(np.uint16)[oy:oy + h, ox:ox + w]
+    src = curr.view(np.uint16)[oy:oy + h, ox:ox + w]
     for c in range(3):
         reg[..., c][sel] = src[..., c][sel]
     return out
