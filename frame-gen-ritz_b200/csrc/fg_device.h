@@ -118,6 +118,24 @@ __device__ __forceinline__ bool uiPx(const uint32_t* __restrict__ m, int x, int 
     return ((__ldg(m + kUiMaskHeader + y * (int)__ldg(m + 3) + (x >> 2)) >> (8 * (x & 3))) & 255u) != 0u;
 }
 
+// the same for a YUV sample (gpu/shaders/ui_reject.glsl uiFootprint, FG_YUV): the 2x2 texels of the half-resolution
+// chroma plane around it, c = X - 16 in 1/64 chroma texels, i = c >> 6, the second texel only if the fraction is not
+// 0: the pixels 2 i .. 2 (i + n) + 1 per axis, which contain the luma taps too
+__device__ __forceinline__ bool uiHitMaskYuv(const uint32_t* __restrict__ m, int X, int Y) {
+    const uint32_t wh = __ldg(m + 2);
+    if (wh == 0u) return false;
+    const uint32_t o = __ldg(m + 1);
+    const int ox = (int)(o & 0xFFFFu), oy = (int)(o >> 16), w = (int)(wh & 0xFFFFu), h = (int)(wh >> 16);
+    const int stride = (int)__ldg(m + 3);
+    const int cx = X - 16, cy = Y - 16, ix = cx >> 6, iy = cy >> 6;
+    const int x0 = max(2 * ix - ox, 0), y0 = max(2 * iy - oy, 0);
+    const int x1 = min(2 * (ix + ((cx & 63) != 0)) + 1 - ox, w - 1), y1 = min(2 * (iy + ((cy & 63) != 0)) + 1 - oy, h - 1);
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++)
+            if ((__ldg(m + 4 + y * stride + (x >> 2)) >> (8 * (x & 3))) & 255u) return true;
+    return false;
+}
+
 __device__ __forceinline__ float2 rne32bits(float2 v) {
     return __ffma2_rn(v, make_float2(32.0f, 32.0f), make_float2(12582912.0f, 12582912.0f));
 }

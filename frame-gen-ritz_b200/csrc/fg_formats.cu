@@ -445,8 +445,9 @@ __device__ __forceinline__ void copyNear(const SynthParams& p, int x, int y) {
 // YUV (codes; chroma for even-even pixels only); k is the thread's region-row slot. kCut: under a scene cut the tile is
 // a copy of the nearer frame (and the core returns); without kCut the caller has taken the cut into account. The
 // untrusted count goes to *p.untrusted unless that is null.
-// kUi (Rgb10 / RgbaF16): CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl): a tap whose bilinear
-// footprint touches its own frame's UI mask (p.uiA / p.uiC) takes the other frame's tap (both or neither: kept)
+// kUi: CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl): a tap whose footprint (YUV: the 2x2 chroma
+// texels around it) touches its own frame's UI mask (p.uiA / p.uiC) takes the other frame's tap (both or neither:
+// kept); the block-centre chroma of the even-even pixels is rejected on its own positions (uiRejectC)
 template <int F, bool kCut, bool kUi = false, class Sink>
 __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int by, Sink& sink) {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -486,9 +487,8 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
         warp<F>(p, p.a, p.ac, pax, pay, wa);
         warp<F>(p, p.c, p.cc, pcx, pcy, wc);
         if (kUi) {
-            static_assert(!kUi || F == kFmtRgb10 || F == kFmtF16, "the tap rejection is built for the RGB formats");
-            const bool ha = p.uiA && uiHitMask(p.uiA, rne32(pax), rne32(pay));
-            const bool hc = p.uiC && uiHitMask(p.uiC, rne32(pcx), rne32(pcy));
+            const bool ha = p.uiA && (kYuv ? uiHitMaskYuv(p.uiA, rne32(pax), rne32(pay)) : uiHitMask(p.uiA, rne32(pax), rne32(pay)));
+            const bool hc = p.uiC && (kYuv ? uiHitMaskYuv(p.uiC, rne32(pcx), rne32(pcy)) : uiHitMask(p.uiC, rne32(pcx), rne32(pcy)));
             if (ha != hc) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
@@ -505,10 +505,18 @@ __device__ __forceinline__ void synthFmtTile(const SynthParams& p, int bx, int b
                 if ((((lx | ly) & 1) == 0) && (unsigned)lx < (unsigned)kSyT && x < p.W && Y0 + ly < p.H) {
                     // the chroma of this 2x2 block, warped from its centre with this pixel's half-vector
                     const float bx = __fadd_rn(cx.pos, 0.5f), by = __fadd_rn(cy.pos, 0.5f);
-                    const float2 ca = warpChroma<F>(p.ac, p.cpitch, p.W, p.H, rne32(__fsub_rn(bx, __fmul_rn(kA, h.x))),
-                                                    rne32(__fsub_rn(by, __fmul_rn(kA, h.y))));
-                    const float2 cc = warpChroma<F>(p.cc, p.cpitch, p.W, p.H, rne32(__fadd_rn(bx, __fmul_rn(kC, h.x))),
-                                                    rne32(__fadd_rn(by, __fmul_rn(kC, h.y))));
+                    const float qax = __fsub_rn(bx, __fmul_rn(kA, h.x)), qay = __fsub_rn(by, __fmul_rn(kA, h.y));
+                    const float qcx = __fadd_rn(bx, __fmul_rn(kC, h.x)), qcy = __fadd_rn(by, __fmul_rn(kC, h.y));
+                    float2 ca = warpChroma<F>(p.ac, p.cpitch, p.W, p.H, rne32(qax), rne32(qay));
+                    float2 cc = warpChroma<F>(p.cc, p.cpitch, p.W, p.H, rne32(qcx), rne32(qcy));
+                    if (kUi) {   // uiRejectC: the block-centre taps, with their own footprints
+                        const bool ha = p.uiA && uiHitMaskYuv(p.uiA, rne32(qax), rne32(qay));
+                        const bool hc = p.uiC && uiHitMaskYuv(p.uiC, rne32(qcx), rne32(qcy));
+                        if (ha != hc) {
+                            if (ha) ca = cc;
+                            else cc = ca;
+                        }
+                    }
                     mixc[(ly >> 1) * (kSyE / 2) + (lx >> 1)] = make_float2(mixF(ca.x, cc.x, p), mixF(ca.y, cc.y, p));
                 }
             } else {
@@ -866,6 +874,12 @@ cudaError_t prepareFormatKernels() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_batch<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_ui<kFmtRgb10>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_ui<kFmtF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_ui<kFmtNv12>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_fmt_ui<kFmtP010>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtNv12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtP010, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_synth_blur_fmt<kFmtRgb10, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
@@ -946,6 +960,8 @@ cudaError_t launchUiFillFmt(const UiFillParams& p, cudaStream_t s) {
     switch (p.f.format) {
         case kFmtRgb10: return launchPdl(k_ui_fill_fmt<kFmtRgb10>, grid, dim3(64), 0, s, p);
         case kFmtF16: return launchPdl(k_ui_fill_fmt<kFmtF16>, grid, dim3(64), 0, s, p);
+        case kFmtNv12: return launchPdl(k_ui_fill_fmt<kFmtNv12>, grid, dim3(64), 0, s, p);
+        case kFmtP010: return launchPdl(k_ui_fill_fmt<kFmtP010>, grid, dim3(64), 0, s, p);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -962,10 +978,12 @@ cudaError_t launchPqTable(float* tab, float kWhite, cudaStream_t s) {
 cudaError_t launchSynthFmt(const SynthParams& p, cudaStream_t s) {
     const dim3 grid(divUp(p.W, kSyT), divUp(p.H, kSyTH));
     const size_t smem = fmtSynthSmem(p.f.format, p.fs);
-    if (p.uiA || p.uiC) {   // CrosshairV2: the RGB formats only
+    if (p.uiA || p.uiC) {   // CrosshairV2: the tap rejection compiled in
         switch (p.f.format) {
             case kFmtRgb10: return launchPdl(k_synth_fmt_ui<kFmtRgb10>, grid, dim3(kSyThreads), smem, s, p);
             case kFmtF16: return launchPdl(k_synth_fmt_ui<kFmtF16>, grid, dim3(kSyThreads), smem, s, p);
+            case kFmtNv12: return launchPdl(k_synth_fmt_ui<kFmtNv12>, grid, dim3(kSyThreads), smem, s, p);
+            case kFmtP010: return launchPdl(k_synth_fmt_ui<kFmtP010>, grid, dim3(kSyThreads), smem, s, p);
             default: return cudaErrorInvalidValue;
         }
     }
@@ -1019,10 +1037,12 @@ cudaError_t launchSynthBlurFmt(const BlurParams& bp, int fix, cudaStream_t s) {
     const dim3 grid(divUp(bp.base.W, kSyT), divUp(bp.base.H, kSyTH));
     BlurParams p = bp;
     p.fix = fix;
-    if (bp.base.uiA || bp.base.uiC) {   // CrosshairV2: the RGB formats only
+    if (bp.base.uiA || bp.base.uiC) {   // CrosshairV2: the tap rejection compiled in
         switch (bp.base.f.format) {
             case kFmtRgb10: return launchPdl(k_synth_blur_fmt<kFmtRgb10, true>, grid, dim3(kSyThreads), smem, s, p);
             case kFmtF16: return launchPdl(k_synth_blur_fmt<kFmtF16, true>, grid, dim3(kSyThreads), smem, s, p);
+            case kFmtNv12: return launchPdl(k_synth_blur_fmt<kFmtNv12, true>, grid, dim3(kSyThreads), smem, s, p);
+            case kFmtP010: return launchPdl(k_synth_blur_fmt<kFmtP010, true>, grid, dim3(kSyThreads), smem, s, p);
             default: return cudaErrorInvalidValue;
         }
     }

@@ -261,8 +261,9 @@ constexpr int kUiMaskHeader = 4;
 struct UiV2Params {
     const uint8_t* frame; size_t pitch;
     int W, H, ri, gi, bi;
-    FmtConst f;                    // the frame format (8-bit RGBA / BGRA, Rgb10 or RgbaF16)
+    FmtConst f;                    // the frame format
     const float* pq;               // linear RgbaF16: the PQ level of every half value (LumaPyrParams::pq)
+    const uint8_t* frameC; size_t cpitch;   // YUV: the frame's CbCr plane
     int bx, by, bw, bh;            // the box (detection)
     int wx, wy, ww, wh;            // the work rectangle (state and mask)
     uint32_t* st;
@@ -276,7 +277,9 @@ struct UiPatchParams {
     const uint8_t* curr; size_t pitch;
     uint8_t* out; size_t outPitch;
     const uint32_t* mask;
-    int format;                    // kFmt*: 8-bit RGBA / BGRA, Rgb10 or RgbaF16
+    int format;                    // kFmt*
+    const uint8_t* currC; size_t cpitch;     // YUV: the CbCr planes of curr and of the output
+    uint8_t* outC; size_t outCPitch;
 };
 // the estimate fill (Settings::uiEstimateFill): level-0 luma cells holding UI pixels re-averaged over their not-UI
 // pixels, prev's (mask ma, luma la) and curr's (mc, lc); cells of the rectangle (cx0, cy0) .. + (ncx, ncy)

@@ -52,6 +52,14 @@ __device__ __forceinline__ uint32_t uiPixel(const UiV2Params& p, int x, int y) {
         const uint2 q = __ldg(reinterpret_cast<const uint2*>(row) + x);
         return uiLevelF16(p, q.x & 0xFFFFu) | (uiLevelF16(p, q.x >> 16) << 8) | (uiLevelF16(p, q.y & 0xFFFFu) << 16);
     }
+    const uint8_t* crow = p.frameC + (size_t)(y >> 1) * p.cpitch;
+    if (p.f.format == kFmtNv12)   // (Y, Cb, Cr): the bytes themselves
+        return (uint32_t)__ldg(row + x) | ((uint32_t)__ldg(reinterpret_cast<const unsigned short*>(crow) + (x >> 1)) << 8);
+    if (p.f.format == kFmtP010) {   // floor(s 2^-8 + 0.5) of each 16-bit sample, at most 255
+        auto lv = [](uint32_t s16) { return min((s16 + 128u) >> 8, 255u); };
+        const uint32_t c = __ldg(reinterpret_cast<const uint32_t*>(crow) + (x >> 1));
+        return lv(__ldg(reinterpret_cast<const unsigned short*>(row) + x)) | (lv(c & 0xFFFFu) << 8) | (lv(c >> 16) << 16);
+    }
     const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(row) + x);
     return ((v >> (8 * p.ri)) & 255u) | (((v >> (8 * p.gi)) & 255u) << 8) | (((v >> (8 * p.bi)) & 255u) << 16);
 }
@@ -63,14 +71,15 @@ __device__ __forceinline__ int maxAbsDiff(uint32_t a, uint32_t b) {
     return m;
 }
 
-// max channel |v - median7x7| at (x, y)
-__device__ int contrastAt(const UiV2Params& p, int x, int y, uint32_t v) {
+// max channel |v - median7x7| at (x, y); YUV: of the R'G'B' difference the (Y, Cb, Cr) difference stands for
+// (format.glsl fgYuvDiff, in the order of the synthesis' mismatch)
+__device__ float contrastAt(const UiV2Params& p, int x, int y, uint32_t v) {
     uint32_t w[49];
 #pragma unroll
     for (int j = 0; j < 7; j++)
 #pragma unroll
         for (int i = 0; i < 7; i++) w[j * 7 + i] = uiPixel(p, x + i - 3, y + j - 3);
-    int d = 0;
+    int d = 0, dc[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         int lo = 0, hi = 255;
@@ -82,9 +91,18 @@ __device__ int contrastAt(const UiV2Params& p, int x, int y, uint32_t v) {
             if (cnt >= 25) hi = mid;
             else lo = mid + 1;
         }
-        d = max(d, abs((int)((v >> (8 * c)) & 255u) - lo));
+        dc[c] = (int)((v >> (8 * c)) & 255u) - lo;
+        d = max(d, abs(dc[c]));
     }
-    return d;
+    if (p.f.format == kFmtNv12 || p.f.format == kFmtP010) {
+        const float dy = (float)dc[0], db = (float)dc[1], dr = (float)dc[2];
+        const float yv = __fmul_rn(p.f.ys, dy);
+        const float r = __fadd_rn(yv, __fmul_rn(p.f.rcr, dr));
+        const float g = __fadd_rn(__fadd_rn(yv, __fmul_rn(p.f.gcb, db)), __fmul_rn(p.f.gcr, dr));
+        const float b = __fadd_rn(yv, __fmul_rn(p.f.bcb, db));
+        return fmaxf(fabsf(r), fmaxf(fabsf(g), fabsf(b)));
+    }
+    return (float)d;
 }
 
 __global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_v2_update(const UiV2Params p) {
@@ -114,7 +132,7 @@ __global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_v2_update(const UiV2Params
         bool inMask = (flags & 1u) != 0u, hasStored = (flags & 2u) != 0u;
         const bool matchS = !inMask && hasStored && p.reentry > 0 && (float)maxAbsDiff(now, stored) <= p.thr;
         bool contrasty = p.cthr <= 0.0f;
-        if (!inMask && !contrasty && (still || matchS)) contrasty = (float)contrastAt(p, sx, sy, now) >= p.cthr;
+        if (!inMask && !contrasty && (still || matchS)) contrasty = contrastAt(p, sx, sy, now) >= p.cthr;
         if (inMask) {
             leave = still ? 0u : min(leave + 1u, 255u);
             if (still) stored = now;
@@ -179,6 +197,13 @@ __global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_patch(const UiPatchParams 
     const int stride = (int)p.mask[3];
     const uint32_t a = (p.mask[kUiMaskHeader + y * stride + (x >> 2)] >> (8 * (x & 3))) & 255u;
     if (a != 255u) return;
+    if (p.format == kFmtNv12 || p.format == kFmtP010) {   // the luma sample (the chroma: k_ui_patch_chroma)
+        const size_t o = (size_t)(wy + y), i = (size_t)(wx + x);
+        if (p.format == kFmtNv12) p.out[o * p.outPitch + i] = __ldg(p.curr + o * p.pitch + i);
+        else reinterpret_cast<unsigned short*>(p.out + o * p.outPitch)[i] =
+                 __ldg(reinterpret_cast<const unsigned short*>(p.curr + o * p.pitch) + i);
+        return;
+    }
     if (p.format == kFmtF16) {   // R, G, B halves from the real frame, alpha kept
         uint2* o = reinterpret_cast<uint2*>(p.out + (size_t)(wy + y) * p.outPitch) + wx + x;
         const uint2 real = __ldg(reinterpret_cast<const uint2*>(p.curr + (size_t)(wy + y) * p.pitch) + wx + x);
@@ -190,6 +215,29 @@ __global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_patch(const UiPatchParams 
     uint32_t* o = reinterpret_cast<uint32_t*>(p.out + (size_t)(wy + y) * p.outPitch) + wx + x;
     const uint32_t real = __ldg(reinterpret_cast<const uint32_t*>(p.curr + (size_t)(wy + y) * p.pitch) + wx + x);
     *o = (real & ~keep) | (*o & keep);
+}
+
+// YUV: gpu/shaders/ui_patch_chroma.comp (binary): one thread per CbCr texel of the work rectangle; a texel takes the
+// strongest mask byte of its 2x2 pixels inside the rectangle and is copied from the real frame where that is 255
+__global__ void __launch_bounds__(kUiTX * kUiTY) k_ui_patch_chroma(const UiPatchParams p, int wx, int wy, int ww, int wh) {
+    pdlEnter();
+    const int tx = (wx >> 1) + (int)(blockIdx.x * kUiTX + threadIdx.x), ty = (wy >> 1) + (int)(blockIdx.y * kUiTY + threadIdx.y);
+    if (tx > (wx + ww - 1) >> 1 || ty > (wy + wh - 1) >> 1) return;
+    const int stride = (int)p.mask[3];
+    uint32_t a = 0;
+    for (int j = 0; j < 2; j++)
+        for (int i = 0; i < 2; i++) {
+            const int rx = 2 * tx + i - wx, ry = 2 * ty + j - wy;
+            if (rx < 0 || ry < 0 || rx >= ww || ry >= wh) continue;
+            a = max(a, (p.mask[kUiMaskHeader + ry * stride + (rx >> 2)] >> (8 * (rx & 3))) & 255u);
+        }
+    if (a != 255u) return;
+    if (p.format == kFmtNv12)
+        reinterpret_cast<unsigned short*>(p.outC + (size_t)ty * p.outCPitch)[tx] =
+            __ldg(reinterpret_cast<const unsigned short*>(p.currC + (size_t)ty * p.cpitch) + tx);
+    else
+        reinterpret_cast<uint32_t*>(p.outC + (size_t)ty * p.outCPitch)[tx] =
+            __ldg(reinterpret_cast<const uint32_t*>(p.currC + (size_t)ty * p.cpitch) + tx);
 }
 
 // The estimate fill (gpu/shaders/ui_v2_lumafill.comp), one thread per level-0 cell of the mask rectangle, z = 0 prev,
@@ -241,7 +289,13 @@ cudaError_t launchUiV2Mask(const UiV2Params& p, cudaStream_t s) {
     return launchPdl(k_ui_v2_mask, dim3(divUp(p.maskStride * p.wh, 128)), dim3(128), 0, s, p);
 }
 cudaError_t launchUiPatch(const UiPatchParams& p, int wx, int wy, int ww, int wh, cudaStream_t s) {
-    return launchPdl(k_ui_patch, dim3(divUp(ww, kUiTX), divUp(wh, kUiTY)), dim3(kUiTX, kUiTY), 0, s, p, wx, wy, ww, wh);
+    cudaError_t e = launchPdl(k_ui_patch, dim3(divUp(ww, kUiTX), divUp(wh, kUiTY)), dim3(kUiTX, kUiTY), 0, s, p, wx, wy, ww, wh);
+    if (e == cudaSuccess && (p.format == kFmtNv12 || p.format == kFmtP010)) {
+        const int tw = ((wx + ww - 1) >> 1) - (wx >> 1) + 1, th = ((wy + wh - 1) >> 1) - (wy >> 1) + 1;
+        e = launchPdl(k_ui_patch_chroma, dim3(divUp(tw, kUiTX), divUp(th, kUiTY)), dim3(kUiTX, kUiTY), 0, s, p, wx, wy,
+                      ww, wh);
+    }
+    return e;
 }
 
 }  // namespace fgk

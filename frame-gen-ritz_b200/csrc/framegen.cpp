@@ -139,7 +139,7 @@ size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 const char* kErrSettings = "invalid settings: a field is out of range or not finite (see Interpolator::validate)";
 const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
 const char* kErrUi = "static-UI protection: only CrosshairV2 is built into this library (Crosshair and WholeScreen are not)";
-const char* kErrUiFormat = "static-UI protection (CrosshairV2) is built for the 8-bit RGBA / BGRA, Rgb10 and RgbaF16 formats only";
+const char* kErrUiFormat = "static-UI protection (CrosshairV2): unknown frame format";
 const char* kErrNoFormat = "unsupported viewFormat (see framegen::Format)";
 const char* kErrYuvMatrix = "yuvMatrix must be Bt601, Bt709 or Bt2020";
 const char* kErrNits = "linearWhiteNits must be in (0, 10000]";
@@ -379,6 +379,7 @@ struct Interpolator::Impl {
         p.W = (int)W; p.H = (int)H; p.ri = ri; p.gi = gi; p.bi = bi;
         p.f = fc;
         p.pq = pqTab;
+        p.frameC = (const uint8_t*)f.chroma; p.cpitch = f.chromaPitch;
         p.bx = uiBox[0]; p.by = uiBox[1]; p.bw = uiBox[2]; p.bh = uiBox[3];
         p.wx = uiWork[0]; p.wy = uiWork[1]; p.ww = uiWork[2]; p.wh = uiWork[3];
         p.st = uiState;
@@ -421,7 +422,8 @@ struct Interpolator::Impl {
     }
 
     bool uiPatch(cudaStream_t s, const Frame& curr, const Frame& out, const uint32_t* mc) {
-        fgk::UiPatchParams pp{(const uint8_t*)curr.data, curr.pitch, (uint8_t*)out.data, out.pitch, mc, fc.format};
+        fgk::UiPatchParams pp{(const uint8_t*)curr.data, curr.pitch, (uint8_t*)out.data, out.pitch, mc, fc.format,
+                              (const uint8_t*)curr.chroma, curr.chromaPitch, (uint8_t*)out.chroma, out.chromaPitch};
         if (!check(fgk::launchUiPatch(pp, uiWork[0], uiWork[1], uiWork[2], uiWork[3], s))) return false;
         stamp(s, "ui patch");
         return true;
@@ -811,8 +813,7 @@ const char* Interpolator::settingsError(const Settings& s, Format f) {
     if (!validate(s)) return kErrSettings;
     if (s.motionVersion != MotionVersion::V1) return kErrVersion;
     if (s.uiProtection != UiProtection::Off && s.uiProtection != UiProtection::CrosshairV2) return kErrUi;
-    if (s.uiProtection == UiProtection::CrosshairV2 && f != Format::Rgba8 && f != Format::Rgb10 && f != Format::RgbaF16)
-        return kErrUiFormat;
+    if (s.uiProtection == UiProtection::CrosshairV2 && (uint32_t)f > (uint32_t)Format::P010) return kErrUiFormat;
     return nullptr;
 }
 

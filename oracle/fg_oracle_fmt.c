@@ -434,14 +434,35 @@ static void copy_near(const fgo_fmt* f, const fgo_frame* N, const fgo_frame* O, 
 }
 
 /* interp.synth for the other formats; arguments as fgo_synth, frames as fgo_frame (O: the output planes) */
-/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl) for the RGB formats: a tap whose bilinear footprint
- * touches its own frame's UI mask takes the other frame's tap (both or neither: unchanged) */
-static inline void ui_reject(const fgo_uimask* ua, const fgo_uimask* uc, float pax, float pay, float pcx, float pcy,
-                             float wa[3], float wc[3]) {
+/* The pixels a YUV sample at p reads with a non-zero weight (gpu/shaders/ui_reject.glsl uiFootprint, FG_YUV): the 2x2
+ * texels of the half-resolution chroma plane around it, c = roundEven(32 p) - 16 in 1/64 chroma texels, i = c >> 6,
+ * the second texel only if the fraction is not 0: pixels 2 i .. 2 (i + n) + 1 per axis (they contain the luma taps) */
+static int ui_hit_yuv(const fgo_uimask* u, float px, float py) {
+    if (!u || !u->m || u->w <= 0 || u->h <= 0) return 0;
+    const int cx = (int)nearbyintf(px * 32.0f) - 16, cy = (int)nearbyintf(py * 32.0f) - 16;
+    const int ix = cx >> 6, iy = cy >> 6;
+    int x0 = 2 * ix - u->x, y0 = 2 * iy - u->y;
+    int x1 = 2 * (ix + ((cx & 63) != 0)) + 1 - u->x, y1 = 2 * (iy + ((cy & 63) != 0)) + 1 - u->y;
+    if (x0 < 0) x0 = 0;
+    if (y0 < 0) y0 = 0;
+    if (x1 > u->w - 1) x1 = u->w - 1;
+    if (y1 > u->h - 1) y1 = u->h - 1;
+    for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++)
+            if (u->m[(size_t)y * u->stride + x]) return 1;
+    return 0;
+}
+
+/* CrosshairV2's warp-tap rejection (gpu/shaders/ui_reject.glsl uiReject / uiRejectC): a tap whose footprint touches
+ * its own frame's UI mask takes the other frame's tap (both or neither: unchanged); n values (3, or YUV chroma: 2) */
+static inline void ui_reject(const fgo_fmt* f, const fgo_uimask* ua, const fgo_uimask* uc, float pax, float pay,
+                             float pcx, float pcy, float* wa, float* wc, int n) {
     if (!ua && !uc) return;
-    const int ha = ui_hit(ua, pax, pay), hc = ui_hit(uc, pcx, pcy);
+    const int yuv = f->format == FMT_NV12 || f->format == FMT_P010;
+    const int ha = yuv ? ui_hit_yuv(ua, pax, pay) : ui_hit(ua, pax, pay);
+    const int hc = yuv ? ui_hit_yuv(uc, pcx, pcy) : ui_hit(uc, pcx, pcy);
     if (ha == hc) return;
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < n; k++) {
         if (ha) wa[k] = wc[k];
         else wc[k] = wa[k];
     }
@@ -499,7 +520,7 @@ int fgo_synth_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const
             float wa[3], wc[3];
             warp(f, A, W, H, (float)x - ka * hx, (float)y - ka * hy, wa);
             warp(f, C, W, H, (float)x + kc * hx, (float)y + kc * hy, wc);
-            ui_reject(ua, uc, (float)x - ka * hx, (float)y - ka * hy, (float)x + kc * hx, (float)y + kc * hy, wa, wc);
+            ui_reject(f, ua, uc, (float)x - ka * hx, (float)y - ka * hy, (float)x + kc * hx, (float)y + kc * hy, wa, wc, 3);
             const int m = mismatch(f, wa, wc);
             e[(size_t)y * W + x] = (uint8_t)m;
             ef[(size_t)y * W + x] = (float)m;
@@ -530,7 +551,7 @@ int fgo_synth_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const
                 float wa[3], wc[3];
                 warp(f, A, W, H, (float)x - ka * hx, (float)y - ka * hy, wa);
                 warp(f, C, W, H, (float)x + kc * hx, (float)y + kc * hy, wc);
-                ui_reject(ua, uc, (float)x - ka * hx, (float)y - ka * hy, (float)x + kc * hx, (float)y + kc * hy, wa, wc);
+                ui_reject(f, ua, uc, (float)x - ka * hx, (float)y - ka * hy, (float)x + kc * hx, (float)y + kc * hy, wa, wc, 3);
                 const float u = eb[q], iu = 1.0f - u;
                 uint8_t* o = (uint8_t*)O->p + (size_t)y * O->pitch;
                 if (f->format == FMT_RGB10) {
@@ -566,6 +587,7 @@ int fgo_synth_fmt_ui(const fgo_frame* A, const fgo_frame* C, int W, int H, const
                         const float bx = (float)x + 0.5f, by = (float)y + 0.5f;
                         warpC(f, A, W, H, bx - ka * hx, by - ka * hy, ca);
                         warpC(f, C, W, H, bx + kc * hx, by + kc * hy, cc);
+                        ui_reject(f, ua, uc, bx - ka * hx, by - ka * hy, bx + kc * hx, by + kc * hy, ca, cc, 2);
                         uint8_t* oc = (uint8_t*)O->c + (size_t)(y / 2) * O->cpitch;
                         for (int k = 0; k < 2; k++) {
                             const float nc = raw(f, N, x / 2, y / 2, 1 + k);

@@ -88,7 +88,31 @@ def levels_fmt(frame, spec):
         v = np.floor((lv + np.float32(0.5)).astype(np.float32))
         v = np.nan_to_num(v, nan=0.0, posinf=255.0, neginf=0.0)
         return np.clip(v, 0, 255).astype(np.int32)
-    raise ValueError("CrosshairV2 levels: Rgb10 and RgbaF16 only")
+    if spec.format in ("nv12", "p010"):   # fgStillYuv: (Y, Cb, Cr) levels of the pixel and its chroma texel
+        y, uv = frame
+        yc = y.view(np.uint16 if spec.format == "p010" else np.uint8).astype(np.float32)
+        cc = uv.view(np.uint16 if spec.format == "p010" else np.uint8).astype(np.float32)
+        if spec.format == "p010":
+            yc, cc = yc * np.float32(2 ** -8), cc * np.float32(2 ** -8)
+        H, W = yc.shape
+        c = cc[np.arange(H)[:, None] // 2, np.arange(W)[None, :] // 2]   # (H, W, 2)
+        lv = np.concatenate([yc[..., None], c], axis=-1).astype(np.float32)
+        return np.clip(np.floor((lv + np.float32(0.5)).astype(np.float32)), 0, 255).astype(np.int32)
+    raise ValueError("CrosshairV2 levels: not this format")
+
+
+def yuv_diff_max(d, spec):
+    """format.glsl fgYuvDiff + max |.|: the R'G'B' difference a (Y, Cb, Cr) level difference stands for, in the
+    library's float32 order (y = ys dY; r = y + rcr dCr; g = (y + gcb dCb) + gcr dCr; b = y + bcb dCb)"""
+    import oracle
+    f = oracle.fmt_struct(spec)
+    f32 = np.float32
+    dy, db, dr = (f32(v) for v in d)
+    y = f32(f32(f.ys) * dy)
+    r = f32(y + f32(f32(f.rcr) * dr))
+    g = f32(f32(y + f32(f32(f.gcb) * db)) + f32(f32(f.gcr) * dr))
+    b = f32(y + f32(f32(f.bcb) * db))
+    return max(abs(r), abs(g), abs(b))
 
 
 def _median7(lv, y, x):
@@ -123,6 +147,7 @@ class State:
         when it is not 8-bit RGBA / BGRA"""
         s = self.s
         lv = _levels(frame, order) if spec is None else levels_fmt(frame, spec)
+        yuv = spec is not None and spec.format in ("nv12", "p010")
         wx, wy, ww, wh = self.work
         bx, by, bw, bh = self.box
         thr = float(np.float32(s.uiStillThreshold))
@@ -150,7 +175,8 @@ class State:
                     match_s = (not in_mask) and has_stored and s.uiReentryFrames > 0 and np.abs(now - stored).max() <= thr
                     contrasty = cthr <= 0.0
                     if not in_mask and not contrasty and (still or match_s):
-                        contrasty = np.abs(now - _median7(lv, sy, sx)).max() >= cthr
+                        d = now - _median7(lv, sy, sx)
+                        contrasty = (yuv_diff_max(d, spec) if yuv else np.abs(d).max()) >= cthr
                     if in_mask:
                         leave = 0 if still else min(leave + 1, 255)
                         if still:
@@ -219,10 +245,26 @@ def patch(out, curr, mask, rect):
 
 
 def patch_fmt(out, curr, mask, rect, spec):
-    """patch() for Rgb10 (the colour codes from curr, the 2 alpha bits kept) and RgbaF16 (R, G, B halves from curr,
-    alpha kept)"""
+    """patch() for Rgb10 (the colour codes from curr, the 2 alpha bits kept), RgbaF16 (R, G, B halves from curr,
+    alpha kept) and YUV (the luma plane where 255; a chroma texel takes the strongest mask byte of its 2x2 pixels
+    inside the rectangle and is copied where that is 255: gpu/shaders/ui_patch_chroma.comp, binary)"""
     ox, oy, w, h = rect
     sel = mask == 255
+    if spec.format in ("nv12", "p010"):
+        oy_, ouv = out
+        cy_, cuv = curr
+        oy_[oy:oy + h, ox:ox + w][sel] = cy_[oy:oy + h, ox:ox + w][sel]
+        for ty in range(oy >> 1, ((oy + h - 1) >> 1) + 1):
+            for tx in range(ox >> 1, ((ox + w - 1) >> 1) + 1):
+                a = 0
+                for j in range(2):
+                    for i in range(2):
+                        ry, rx = 2 * ty + j - oy, 2 * tx + i - ox
+                        if 0 <= ry < h and 0 <= rx < w:
+                            a = max(a, int(mask[ry, rx]))
+                if a == 255:
+                    ouv[ty, tx] = cuv[ty, tx]
+        return out
     if spec.format == "rgb10":
         reg = out.view(np.uint32)[oy:oy + h, ox:ox + w]
         src = curr.view(np.uint32)[oy:oy + h, ox:ox + w]

@@ -86,13 +86,11 @@ def test_settings_error_names_unbuilt_parts():
     for mode in (1, 2):   # Crosshair, WholeScreen
         s = fg.Settings(uiProtection=mode)
         assert fg.validate(s) and "only CrosshairV2" in fg.settings_error(s)
-    s = fg.Settings(uiProtection=3)   # CrosshairV2: built for 8-bit RGBA, Rgb10 and RgbaF16, with or without the fill
+    s = fg.Settings(uiProtection=3)   # CrosshairV2: built for every frame format, with or without the fill
     assert fg.validate(s) and fg.settings_error(s) is None
-    for fmt in ("Rgba8", "Rgb10", "RgbaF16"):
+    for fmt in ("Rgba8", "Rgb10", "RgbaF16", "Nv12", "P010"):
         assert fg.settings_error(s, fmt=fmt) is None
         assert fg.settings_error(fg.Settings(uiProtection=3, uiEstimateFill=True), fmt=fmt) is None
-    for fmt in ("Nv12", "P010"):
-        assert "Rgb10 and RgbaF16" in fg.settings_error(s, fmt=fmt)
 
 
 def test_box_geometry():

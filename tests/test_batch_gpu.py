@@ -219,6 +219,35 @@ def test_batch_whole_frame_fallbacks(shape):
         assert not bad, f"shape {shape}: outputs {bad} differ"
 
 
+@pytest.mark.parametrize("shape", [(3, 1, 8), (0, 0, 1), (3, 1, 1, 1)])
+def test_batch_with_a_crosshair_slot(shape):
+    """a CrosshairV2 slot in a batch synthesizes through recordSynth (tap rejection, paste-back) whatever the launch
+    shape, next to plain slots: over a sequence of records (the implicit observe of each pair), its outputs equal a
+    standalone Interpolator's on the same sequence"""
+    from test_ui_v2_gpu import grain_scene, v2_settings
+    W, H = 320, 192
+    frames, _ = grain_scene(W, H, 10)
+    st = v2_settings()
+    dframes = [torch.from_numpy(f).cuda() for f in frames]
+    B = fg.Batch()
+    assert B.add(W, H, fg.VK_R8G8B8A8_UNORM, multiplier=2, settings=st) == 0, B.error()
+    assert B.add(W, H, fg.VK_R8G8B8A8_UNORM, multiplier=2) == 1, B.error()
+    assert B.set_shape(*shape)
+    I = fg.Interpolator()
+    assert I.init(W, H, fg.VK_R8G8B8A8_UNORM, settings=st), I.init_error()
+    outs = [torch.zeros_like(dframes[0]) for _ in range(2)]
+    ref = torch.zeros_like(dframes[0])
+    for k in range(1, len(frames)):
+        assert B.record([dframes[k - 1], dframes[k - 1]], [dframes[k], dframes[k]], outs), B.error()
+        I.begin_frame()
+        assert I.record_estimate(dframes[k - 1], dframes[k])
+        assert I.record_synth(dframes[k - 1], dframes[k], ref, 0.5)
+        torch.cuda.synchronize()
+        assert np.array_equal(outs[0].cpu().numpy(), ref.cpu().numpy()), f"record {k}: the CrosshairV2 slot differs"
+    assert fg.read_ui(I, dframes[-1], st, W, H)["mask"].max() == 255, "the plus should be protected by the end"
+    I.close()
+
+
 def test_rgba8_slot_against_the_oracle():
     """one batched 8-bit RGBA slot straight against the oracle (interp.py's restatement)"""
     p, c, _ = workloads.flow_pair(320, 180, seed=99)
