@@ -294,8 +294,9 @@ private:
 class Batch {
 public:
     struct Shape {
-        uint32_t ctasPerSm = 3;   // CTAs per SM of the persistent synthesis launches; 0: one launch per synthesis
-        uint32_t order = 1;       // work order: 0 the slots as added, 1 the largest syntheses first
+        // the default is the shape tune() picks on the 64-pair mixed batch (one launch per synthesis, 8 streams)
+        uint32_t ctasPerSm = 0;   // CTAs per SM of the persistent synthesis launches; 0: one launch per synthesis
+        uint32_t order = 0;       // work order: 0 the slots as added, 1 the largest syntheses first
         uint32_t streams = 8;     // the slots' estimates run on this many forked streams (1 = the caller's only)
         uint32_t mergeEstimates = 0;   // G = 1..8: the slots' estimates as merged launches (one per pass and level
                                        // for all slots of a group) on the caller's stream, in G groups whose
