@@ -1416,10 +1416,7 @@ static cudaError_t launchMergedGroups(const std::vector<P>& items, const std::ve
     return cudaSuccess;
 }
 
-// Every slot's estimate (streams = 0): one launch per pass for all the slots on the caller's stream, in the order an
-// estimate runs its passes (luma, levels from the coarsest down to level 0 with the finest levels aligned, so level l
-// of every slot that has one is searched in the same launch, sub-pixel, pixel field). The same kernels' work per
-// slot as recordEstimate; only the launches are shared.
+// Merged estimates need every slot's estimate to be the plain pass sequence
 bool Batch::Impl::mergeable() const {
     for (const auto& I : slots) {
         const Interpolator::Impl& im = *I->m;
@@ -1428,6 +1425,10 @@ bool Batch::Impl::mergeable() const {
     return true;
 }
 
+// The estimates of the slots idx (Shape::mergeEstimates): one launch per pass for all of them on the caller's stream,
+// in the order an estimate runs its passes (luma, levels from the coarsest down to level 0 with the finest levels
+// aligned, so level l of every slot that has one is searched in the same launch, sub-pixel, pixel field). The same
+// kernels' work per slot as recordEstimate; only the launches are shared.
 bool Batch::Impl::mergedEstimates(cudaStream_t s, const Frame* prev, const Frame* curr, const std::vector<int>& idx) {
     const int ns = (int)idx.size();
     for (int j = 0; j < ns; j++) {
