@@ -182,3 +182,17 @@ def test_noalloc_frame_span_limit():
     # the field is read as float pairs: a 4-byte aligned stand-in pointer is refused before CUDA is used
     ok, msg = call(at, field=(1 << 20) + 4)
     assert not ok and "8-byte aligned" in msg, msg
+
+
+def test_batch_shape_round_trip():
+    """Batch::Shape through the C ABI (no slots, no device needed): the default is the forked per-synthesis shape,
+    fg_batch_set_shape_merged keeps mergeEstimates (1..8 groups), fg_batch_set_shape resets it, and shapes outside the
+    ranges are refused without changing the current one"""
+    B = fg.Batch()
+    assert B.shape() == (0, 0, 8, 0)
+    assert B.set_shape(0, 0, 8, 4) and B.shape() == (0, 0, 8, 4)
+    assert B.set_shape(3, 1, 8) and B.shape() == (3, 1, 8, 0)
+    for bad in ((0, 0, 0), (5, 0, 8), (0, 2, 8), (0, 0, 9), (0, 0, 8, 9)):
+        assert not B.set_shape(*bad), bad
+    assert B.shape() == (3, 1, 8, 0)
+    B.close()
