@@ -10,7 +10,9 @@ pool slot's step is a CUDA graph of the library's own launches; `value` = max-ov
 pinned memory, records the estimate and 3 synths, and copies the 3 frames back.
 `roofline` is the dominant kernel (the fused synth) against the measured HBM copy bandwidth, its duration from the
 library's own per-pass CUDA events. `cpu_baseline` is the oracle (a plain-C restatement of proto/interp.py) on this
-host's cores. --impl reference times that CPU implementation itself (rank 0 only).
+host's cores. --impl reference times that CPU implementation itself (rank 0 only); where FGR_REF names a checkout
+of the reference, it times the reference's own proto/interp.py (NumPy + OpenCV) on the same pairs instead and keeps
+the port as a second row.
 Multi-GPU: every rank runs its own pairs (weak scaling, no collective on the data path). `--gpus N` without a
 launcher starts the N ranks itself (one process per GPU, the launcher's environment variables, rendezvous on
 127.0.0.1); under torchrun the launcher's ranks are used and must number N. `value` is then the whole job's time per
@@ -47,6 +49,8 @@ def args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--pool", type=int, default=8, help="distinct 4K pairs cycled through (8 x 66 MB > L2)")
     ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--interp-pairs", type=int, default=5,
+                    help="--impl reference with FGR_REF set: 4K pairs of proto/interp.py timed (median)")
     ap.add_argument("--copy-streams", type=int, default=1,
                     help="e2e: streams per copy direction, each frame split into that many row bands (on a B200 one "
                          "stream already fills the PCIe link: 1.96 ms per pair with 1, 2.00-2.02 with 2-4)")
@@ -502,15 +506,69 @@ def run_reference(a):
             step_ms.append((time.perf_counter() - t0) * 1e3)
     v = statistics.median(step_ms)
     sample = f"full 3840x2160 pairs (4 distinct, cycled), estimate + 3 synths per step; oracle, {cores} threads"
-    print(json.dumps({"metric": METRIC, "value": round(v, 3), "unit": "ms", "impl": "reference", "n_gpus": a.gpus,
-                      "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
-                      "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-                      "config": {"workload": "V1 plain, 3840x2160 Rgba8, 4x (estimate + 3 synths), flowScale 2",
-                                 "cpu_impl": "oracle port (plain C, OpenMP) of proto/interp.py"},
-                      "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "port", "sample": sample,
-                                       "cpu_model": cpu_model()},
-                      "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
-          flush=True)
+    port = {"value": round(v, 3), "unit": "ms", "cores": cores, "kind": "port", "sample": sample,
+            "cpu_model": cpu_model()}
+    cpu_impl = "oracle port (plain C, OpenMP) of proto/interp.py"
+    numpy_ref = reference_interp_leg(a, p, c)
+    if numpy_ref is not None:   # the reference's own NumPy + OpenCV code is the arm; the port stays as a second row
+        v, cpu_impl = numpy_ref["value"], "proto/interp.py (NumPy + OpenCV), imported from FGR_REF"
+        base = dict(numpy_ref, kind="reference")
+    else:
+        base = port
+    line = {"metric": METRIC, "value": round(v, 3), "unit": "ms", "impl": "reference", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "V1 plain, 3840x2160 Rgba8, 4x (estimate + 3 synths), flowScale 2",
+                       "cpu_impl": cpu_impl},
+            "cpu_baseline": base,
+            "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if numpy_ref is not None:
+        line["port"] = port
+    print(json.dumps(line), flush=True)
+
+
+INTERP_SHA256 = "b5f5c7000221002e31a1f4c2b2883878eeab4ffd83760c4080facad527904315"
+
+
+def reference_interp_leg(a, p, c):
+    """The reference's own CPU implementation, proto/interp.py (NumPy + OpenCV), timed on the same full 3840x2160
+    pairs as the port: estimate + 3 synths per pair, median over --interp-pairs pairs after one untimed pair, each
+    pair's 3 frames compared byte for byte with the port's. Runs only where FGR_REF names a checkout of the reference
+    (the directory that holds proto/interp.py, sha256-pinned) and cv2 imports; None otherwise."""
+    ref = os.environ.get("FGR_REF")
+    if not ref or a.interp_pairs <= 0:
+        return None
+    path = os.path.join(ref, "proto", "interp.py")
+    if not os.path.isfile(path):
+        return None
+    try:
+        import cv2
+    except ImportError:
+        return None
+    import hashlib
+    with open(path, "rb") as f:
+        digest = hashlib.sha256(f.read()).hexdigest()
+    if digest != INTERP_SHA256:
+        raise SystemExit(f"{path}: sha256 {digest} is not the pinned {INTERP_SHA256}")
+    sys.path.insert(0, os.path.dirname(path))
+    import interp
+    import oracle
+    ms, equal = [], True
+    for i in range(1 + a.interp_pairs):
+        k = i % 4
+        pa, pc = np.roll(p, (53 * k, 97 * k), axis=(0, 1)), np.roll(c, (53 * k, 97 * k), axis=(0, 1))
+        ba, bc = pa[..., [2, 1, 0]].copy(), pc[..., [2, 1, 0]].copy()   # interp.py takes 8-bit BGR
+        t0 = time.perf_counter()
+        est = interp.estimate(ba, bc)
+        got = [interp.synth(ba, bc, est, t) for t in TS]
+        if i >= 1:
+            ms.append((time.perf_counter() - t0) * 1e3)
+        eo = oracle.estimate(pa, pc, trace=False)
+        equal &= all(np.array_equal(g, oracle.synth(pa, pc, eo, t)[0][..., [2, 1, 0]]) for g, t in zip(got, TS))
+    return {"value": round(statistics.median(ms), 3), "unit": "ms", "pairs": len(ms),
+            "cores": cv2.getNumThreads(), "cv2_threads": cv2.getNumThreads(), "cv2": cv2.__version__,
+            "numpy": np.__version__, "cpu_model": cpu_model(), "bytes_equal_to_port": bool(equal),
+            "sample": f"{len(ms)} full 3840x2160 pairs (4 distinct, cycled), estimate + 3 synths each, after 1 untimed"}
 
 
 def seed_net_arm(a, fg, pool, outs, stream, world, plain):
