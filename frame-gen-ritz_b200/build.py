@@ -10,8 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libframegen_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("fg_kernels.cu", "fg_formats.cu", "fg_seednet.cu", "fg_seednet_tc.cu", "fg_seednet_bwd.cu", "fg_seednet_host.cpp",
-                                                    "framegen.cpp", "fg_noalloc.cu", "fg_ui.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fg_params.h", "fg_device.h", "fg_seednet.h", "fg_tc.h")] + \
+                                                    "framegen.cpp", "fg_noalloc.cu", "fg_ui.cu", "fg_blur.cu")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fg_params.h", "fg_device.h", "fg_seednet.h", "fg_tc.h", "fg_blur.h")] + \
           [os.path.join(REPO, "include", "framegen.h"), os.path.join(REPO, "include", "framegen_c.h")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

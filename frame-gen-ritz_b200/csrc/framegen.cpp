@@ -16,6 +16,7 @@
 #include <numeric>
 #include <vector>
 
+#include "fg_blur.h"
 #include "fg_params.h"
 #include "fg_seednet.h"
 #include "framegen.h"
@@ -136,6 +137,10 @@ CutPlanHost buildCutPlan(int N) {
 
 size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// the most device memory recordSynthBlur's stored sub-frames may take (16 samples of a 3840x2160 frame are 531 MB);
+// past it the blur runs as the fused kernel, which stores none
+constexpr size_t kBlurSubMaxBytes = (size_t)1 << 30;
+
 const char* kErrSettings = "invalid settings: a field is out of range or not finite (see Interpolator::validate)";
 const char* kErrVersion = "this library runs MotionVersion::V1 only (V2, Learned and V3 are not built into it)";
 const char* kErrUi = "static-UI protection: only CrosshairV2 is built into this library (Crosshair and WholeScreen are not)";
@@ -226,6 +231,10 @@ struct Interpolator::Impl {
     int histB = 0;
     fgk::DevState* st = nullptr;
     unsigned int* blurCnt = nullptr;   // recordSynthBlur: per sample, its untrusted pixels (kBlurMax)
+    // recordSynthBlur's sub-frames (8-bit RGBA): blurSubCap frames of blurSubPitch x H bytes, or none
+    uint8_t* blurSub = nullptr;
+    size_t blurSubPitch = 0;
+    uint32_t blurSubCap = 0;
     uint8_t* emap = nullptr;
     fgk::CutPlan plan{};
     // trust-ramp shortcuts of the current settings
@@ -429,9 +438,38 @@ struct Interpolator::Impl {
         return true;
     }
 
+    void blurFree() {
+        DeviceGuard g(device);
+        if (blurSub) cudaFree(blurSub);
+        blurSub = nullptr;
+        blurSubPitch = 0;
+        blurSubCap = 0;
+    }
+
+    // the sub-frames of the current size and settings (after allocSize and on a settings change; outside any capture).
+    // 8-bit RGBA with blur on keeps one frame per sample while they fit kBlurSubMaxBytes; otherwise, or when the
+    // allocation fails, recordSynthBlur runs the fused kernel, which stores none (not an error)
+    void blurSetup() {
+        const uint32_t need = fmt == Format::Rgba8 && W && set.blurSamples >= 2
+                                  ? std::min<uint32_t>(set.blurSamples, Interpolator::kBlurMaxSamples) : 0u;
+        const size_t pitch = alignUp((size_t)W * 4, 256);
+        if (!need || (size_t)need * pitch * H > kBlurSubMaxBytes) { blurFree(); return; }
+        if (blurSubCap >= need && blurSubPitch == pitch) return;
+        blurFree();
+        DeviceGuard g(device);
+        if (cudaMalloc((void**)&blurSub, (size_t)need * pitch * H) != cudaSuccess) {
+            cudaGetLastError();
+            blurSub = nullptr;
+            return;
+        }
+        blurSubPitch = pitch;
+        blurSubCap = need;
+    }
+
     void freeAll() {
         DeviceGuard g(device);
         uiFree();
+        blurFree();
         freeSeedNet();
         if (arena) cudaFree(arena);
         arena = nullptr;
@@ -512,6 +550,7 @@ struct Interpolator::Impl {
         H = h;
         haveEst = false;
         if (const char* e = setupSeedNet()) return e;
+        blurSetup();
         return uiSetup(true);
     }
 
@@ -758,6 +797,40 @@ struct Interpolator::Impl {
         bp.cnt = blurCnt;
         if (!check(cudaMemsetAsync(blurCnt, 0, (size_t)fgk::kBlurMax * 4, s))) return false;
         const bool rgba8 = fmt == Format::Rgba8;
+        int nSynth = 0;
+        for (int k = 0; k < n; k++) nSynth += bp.smp[k].mode == 0;
+        if (rgba8 && blurSub && (uint32_t)nSynth <= blurSubCap) {
+            // each synthesized sample to its own sub-frame by the synthesis kernel, counting into blurCnt[k]; then
+            // one blend of the sub-frames and the real frames (the flick test from the counters)
+            fgk::BlurBlendParams bb{};
+            bb.a = bp.base.a; bb.c = bp.base.c; bb.pitch = bp.base.pitch;
+            bb.sub = blurSub; bb.subPitch = blurSubPitch; bb.subStride = blurSubPitch * H;
+            bb.out = (uint8_t*)out.data; bb.outPitch = out.pitch;
+            bb.W = (int)W; bb.H = (int)H; bb.n = n;
+            bb.frac = bp.frac;
+            bb.cnt = blurCnt;
+            int slot = 0;
+            for (int k = 0; k < n; k++) {
+                const fgk::BlurSample& m = bp.smp[k];
+                bb.mode[k] = m.mode;
+                bb.nearC[k] = m.nearC;
+                bb.q[k] = m.q;
+                if (m.mode != 0) continue;
+                bb.slot[k] = slot;
+                fgk::SynthParams sp = synthParams(prev, curr, out, tk[k], blurCnt + k);
+                sp.out = blurSub + (size_t)slot * bb.subStride;
+                sp.outPitch = blurSubPitch;
+                sp.emap = nullptr;
+                sp.uiA = ma;
+                sp.uiC = mc;
+                if (!check(fgk::launchSynth(sp, s))) return false;
+                slot++;
+            }
+            stamp(s, "blur samples");
+            if (!check(fgk::launchBlurBlend(bb, s))) return false;
+            stamp(s, "blur blend");
+            return !mc || uiPatch(s, curr, out, mc);
+        }
         if (!check(rgba8 ? fgk::launchSynthBlur(bp, 0, s) : fgk::launchSynthBlurFmt(bp, 0, s))) return false;
         stamp(s, "blur resolve");
         if (!check(rgba8 ? fgk::launchSynthBlur(bp, 1, s) : fgk::launchSynthBlurFmt(bp, 1, s))) return false;
@@ -915,6 +988,7 @@ bool Interpolator::setSettings(const Settings& s) {
     }
     if (restart) m->haveEst = m->estUi = false;
     m->updateTrust();
+    m->blurSetup();
     return true;
 }
 
@@ -930,6 +1004,7 @@ bool Interpolator::reconfigure(const Settings& s) {
         const bool restart = uiGeometryChanged(old, s);
         if (m->uiSetup(restart)) { m->set = old; m->updateTrust(); return false; }
         if (restart) m->haveEst = m->estUi = false;
+        m->blurSetup();
     }
     return true;
 }
@@ -1178,20 +1253,21 @@ bool Interpolator::readCosts(CostTimings& c) {
     std::vector<uint64_t> ns;
     if (!readTimings(names, ns)) return false;
     static const char* const kEstimate[] = {"luma", "pyramid", "seed net", "subpixel", "pixel field"};
-    static const char* const kSynth[] = {"synth", "fallback", "blur resolve", "blur fixup"};
-    auto in = [](const char* n, const char* const* set, size_t k) {
-        for (size_t i = 0; i < k; i++)
-            if (std::strcmp(n, set[i]) == 0) return true;
+    static const char* const kSynth[] = {"synth", "fallback", "blur resolve", "blur fixup", "blur samples", "blur blend"};
+    auto in = [](const char* n, const auto& set) {
+        for (const char* s : set)
+            if (std::strcmp(n, s) == 0) return true;
         return false;
     };
     uint64_t est = 0, syn = 0;
     bool haveEst = false;
     for (size_t i = 0; i < names.size(); i++) {
         const char* n = names[i];
-        if (in(n, kEstimate, 5) || std::strncmp(n, "level ", 6) == 0) { est += ns[i]; haveEst = true; }
-        else if (in(n, kSynth, 4)) {
+        if (in(n, kEstimate) || std::strncmp(n, "level ", 6) == 0) { est += ns[i]; haveEst = true; }
+        else if (in(n, kSynth)) {
             syn += ns[i];
-            if (std::strcmp(n, "synth") == 0 || std::strcmp(n, "blur resolve") == 0) c.synths++;
+            if (std::strcmp(n, "synth") == 0 || std::strcmp(n, "blur resolve") == 0 || std::strcmp(n, "blur samples") == 0)
+                c.synths++;
         }
     }
     if (haveEst) c.estimateMs = (float)((double)est * 1e-6);

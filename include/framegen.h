@@ -206,8 +206,11 @@ public:
     // of 2^-16 (largest-remainder rounding, blurPlan). N < 2 or t0 == t1: the single instant t1 (recordSynth(t1); a copy
     // of prev / curr at t1 = 0 / 1). false (nothing recorded) unless 0 <= t0 <= t1 <= 1, and in recordSynth's cases.
     // Other formats: the stored values are averaged the same way (Rgb10 / Nv12 / P010 codes, exact integer sums);
-    // RgbaF16 sums fl32(q_k 2^-16 h_k) in sample order in float32 and rounds to half once. Takes one synth of the ring;
-    // two launches whatever N is.
+    // RgbaF16 sums fl32(q_k 2^-16 h_k) in sample order in float32 and rounds to half once. Takes one synth of the ring.
+    // 8-bit RGBA with blur on keeps one stored sub-frame per sample (allocated by init / setSettings / reconfigure
+    // while they fit 1 GiB): each synthesized sample is one synthesis launch into its sub-frame, then one blend launch
+    // (profile groups "blur samples", "blur blend"). Otherwise (other formats, or past the cap) two launches whatever
+    // N is, the samples accumulated in registers ("blur resolve", "blur fixup"). The bytes are the same either way.
     bool recordSynthBlur(cudaStream_t stream, Frame prev, Frame curr, Frame out, float t0, float t1);
     // the samples of a blur: their times and weights (units of 2^-16, summing to 2^16); returns their count (0 if
     // refused: t0, t1 out of order or range)
@@ -219,8 +222,9 @@ public:
     bool readTimings(std::vector<const char*>& names, std::vector<uint64_t>& ticks);
     // B200-build extension: the cost-guard inputs of gpu/pacing.h:869-871 (Pacer::Inputs::estimateMs / synthMs /
     // costSeq) from the last profile: estimateMs = the estimate's pass groups (luma .. pixel field), synthMs = the
-    // synth-side groups (synth, fallback; blur resolve, blur fixup) per recorded synthesis; -1 where the profile has
-    // none; seq changes with every new profile read. false if profiling is off or nothing was recorded.
+    // synth-side groups (synth, fallback; blur samples, blur blend or blur resolve, blur fixup) per recorded synthesis;
+    // -1 where the profile has none; seq changes with every new profile read. false if profiling is off or nothing was
+    // recorded.
     struct CostTimings {
         float estimateMs = -1.0f, synthMs = -1.0f;
         uint32_t seq = 0, synths = 0;

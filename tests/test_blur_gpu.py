@@ -222,7 +222,7 @@ def test_blur_graph_capture_and_profiling():
     assert ctx.I.set_profiling(True)
     ctx.blur(0.2, 0.9, 6, True)
     names = [name for name, _ in ctx.I.read_timings()]
-    assert names[-2:] == ["blur resolve", "blur fixup"], names
+    assert names[-2:] == ["blur samples", "blur blend"], names   # 8-bit RGBA: the stored sub-frames and their blend
     c = ctx.I.read_costs()
     assert c["synths"] == 1 and c["synth_ms"] > 0, c
     ctx.close()
@@ -251,5 +251,43 @@ def test_blur_4k_is_the_rounded_mean_of_the_syntheses():
         I.begin_frame()
         assert I.record_synth_blur(a, cc, o, t0, t1)
         torch.cuda.synchronize()
+        assert torch.equal(o, want), f"N={n} [{t0},{t1}]: {int((o != want).sum())} bytes differ"
+    I.close()
+
+
+def test_blur_fused_and_stored_sub_frames_agree_8k():
+    """7680x4320 (a 4K pair tiled 2 x 2): 16 samples would take 2.1 GB of sub-frames, past the library's 1 GiB cap,
+    so the fused kernel (k_synth_blur_t, main and fix-up passes) runs; 4 samples fit and run as stored sub-frames and
+    their blend. Both equal the rounded mean of recordSynth at the sample times (even weights, N a power of two), and
+    the profile names show which path ran."""
+    p, c, _ = workloads.flow_pair(3840, 2160, seed=3)
+    p, c = np.tile(p, (2, 2, 1)), np.tile(c, (2, 2, 1))
+    W, H = 7680, 4320
+    I = fg.Interpolator()
+    assert I.init(W, H, fg.VK_R8G8B8A8_UNORM), I.init_error()
+    a, cc = to_dev(p), to_dev(c)
+    I.begin_frame()
+    assert I.record_estimate(a, cc)
+    o = torch.empty_like(a)
+    for n, (t0, t1), names in [(16, (0.0, 1.0), ["blur resolve", "blur fixup"]),
+                               (4, (0.125, 0.875), ["blur samples", "blur blend"])]:
+        times, _ = oracle.blur_plan(n, False, t0, t1)
+        acc = torch.zeros((H, W, 4), dtype=torch.int32, device="cuda")
+        for t in times.tolist():
+            I.begin_frame()
+            assert I.record_synth(a, cc, o, t)
+            acc += o.int()
+        want = ((acc + n // 2) // n).to(torch.uint8)
+        del acc
+        fs = fg.Settings()
+        fs.blurSamples, fs.blurWeights = n, 0
+        assert I.set_settings(fs)
+        assert I.set_profiling(True)
+        I.begin_frame()
+        assert I.record_synth_blur(a, cc, o, t0, t1)
+        torch.cuda.synchronize()
+        got = [name for name, _ in I.read_timings()]
+        assert I.set_profiling(False)
+        assert got[-2:] == names, (n, got)
         assert torch.equal(o, want), f"N={n} [{t0},{t1}]: {int((o != want).sum())} bytes differ"
     I.close()
